@@ -1,0 +1,119 @@
+// capi.cu -- extern "C" entry points of the FMM path and library utilities.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "dust_common.cuh"
+#include "fmm_internal.h"
+
+static std::mutex g_err_mu;
+static std::string g_err;
+
+void dust_set_last_error(const char *msg, const char *file, int line) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%s:%d)", msg ? msg : "?", file, line);
+  g_err = buf;
+}
+
+extern "C" const char *dust_last_error(void) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  return g_err.c_str();
+}
+
+extern "C" const char *dust_status_string(int s) {
+  switch (s) {
+    case DUST_OK: return "ok";
+    case DUST_ERR_CUDA: return "CUDA error";
+    case DUST_ERR_OUT_OF_BOX: return "particle outside the octree box";
+    case DUST_ERR_SINGULAR: return "singular matrix (zero pivot)";
+    case DUST_ERR_NOT_CONVERGED: return "iterative solve did not converge";
+    case DUST_ERR_TIMEOUT: return "bounded device wait timed out";
+    case DUST_ERR_BAD_ARG: return "invalid argument";
+    case DUST_ERR_NO_DEVICE: return "no usable CUDA device";
+    case DUST_ERR_CAPACITY: return "size above the supported maximum";
+    default: return "unknown status";
+  }
+}
+
+extern "C" int dust_device_ok(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return DUST_ERR_NO_DEVICE;
+  cudaDeviceProp p;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DUST_ERR_NO_DEVICE;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return DUST_ERR_NO_DEVICE;
+  if (p.major != 10) return DUST_ERR_NO_DEVICE;
+  return DUST_OK;
+}
+
+// Sizes of the ABI structs, for binding checks.
+extern "C" int dust_abi_sizes(int64_t *out, int n) {
+  int64_t s[] = {(int64_t)sizeof(dust_fmm_params), (int64_t)sizeof(dust_panels),
+                 (int64_t)sizeof(dust_lines),      (int64_t)sizeof(dust_elements),
+                 (int64_t)sizeof(dust_fmm_stats),  (int64_t)sizeof(dust_solve_report),
+                 (int64_t)sizeof(dust_wake_rows)};
+  int m = (int)(sizeof(s) / sizeof(s[0]));
+  for (int i = 0; i < n && i < m; ++i) out[i] = s[i];
+  return m;
+}
+
+static int64_t n_elem_of(const dust_elements *e) {
+  if (!e) return 0;
+  return (int64_t)e->body.n + e->wake.n + e->end_vort.n;
+}
+
+extern "C" int dust_fmm_apply(dust_octree *o, int n, const double *cen, const double *dir,
+                              const double *mag, const double *r_vortex,
+                              const dust_elements *elems, double *vel, double *stretch,
+                              double *rotu) {
+  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex || !vel)))
+    return DUST_ERR_BAD_ARG;
+  cudaStream_t st = o->stream;
+  size_t N = (size_t)(n > 0 ? n : 1);
+  DUST_TRY(devbuf_grow(o->h_in, N * 8 * 8));
+  DUST_TRY(devbuf_grow(o->h_out, N * 9 * 8));
+  double *dc = (double *)o->h_in.p, *dd = dc + 3 * N, *dm = dd + 3 * N, *dr = dm + N;
+  double *ov = (double *)o->h_out.p, *os = ov + 3 * N, *orr = os + 3 * N;
+  if (n > 0) {
+    DUST_CUDA(cudaMemcpyAsync(dc, cen, (size_t)n * 24, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dd, dir, (size_t)n * 24, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dm, mag, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dr, r_vortex, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  }
+  ElemDev e;
+  DUST_TRY(elem_build_device(elems ? &elems->body : nullptr, elems ? &elems->wake : nullptr,
+                             elems ? &elems->end_vort : nullptr, o->prm.u_inf,
+                             reg_params(&o->prm), true, o->el_raw, o->el_geo, e, st));
+  DUST_TRY(fmm_run_device(o, n, dc, dd, dm, dr, st));
+  DUST_TRY(fmm_finish_device(o, n, e, ov, stretch ? os : nullptr, rotu ? orr : nullptr, st));
+  if (n > 0) {
+    DUST_CUDA(cudaMemcpyAsync(vel, ov, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+    if (stretch)
+      DUST_CUDA(cudaMemcpyAsync(stretch, os, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+    if (rotu) DUST_CUDA(cudaMemcpyAsync(rotu, orr, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+  }
+  DUST_CUDA(cudaStreamSynchronize(st));
+  fmm_collect_stats(o, n, n_elem_of(elems));
+  return DUST_OK;
+}
+
+extern "C" int dust_fmm_apply_device(dust_octree *o, int n, const double *cen,
+                                     const double *dir, const double *mag,
+                                     const double *r_vortex, const dust_elements *elems,
+                                     double *vel, double *stretch, double *rotu, void *stream,
+                                     int sync) {
+  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex || !vel)))
+    return DUST_ERR_BAD_ARG;
+  cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
+  ElemDev e;
+  DUST_TRY(elem_build_device(elems ? &elems->body : nullptr, elems ? &elems->wake : nullptr,
+                             elems ? &elems->end_vort : nullptr, o->prm.u_inf,
+                             reg_params(&o->prm), false, o->el_raw, o->el_geo, e, st));
+  DUST_TRY(fmm_run_device(o, n, cen, dir, mag, r_vortex, st));
+  DUST_TRY(fmm_finish_device(o, n, e, vel, stretch, rotu, st));
+  if (sync) DUST_CUDA(cudaStreamSynchronize(st));
+  if (o->timing || sync) fmm_collect_stats(o, n, n_elem_of(elems));
+  return DUST_OK;
+}

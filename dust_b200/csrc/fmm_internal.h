@@ -1,0 +1,81 @@
+// fmm_internal.h -- handle layout and internal entry points of the FMM.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dust_common.cuh"
+#include "elements.cuh"
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+void devbuf_free(DevBuf &b);
+int devbuf_grow(DevBuf &b, size_t bytes);
+
+// Everything a kernel needs, passed by value.
+struct FmmDev {
+  TreeGeom G;
+  uint32_t n;
+  int p, nm, nm1, nD;
+  int use_vs, use_df, use_vd;
+  double nu_inf;
+  double u_inf[3];
+  const double *dtab[DUST_MAXLEV + 1];
+  int kdlen[DUST_MAXLEV + 1][3];
+  const uint16_t *idxsum;
+  const uint32_t *cstart, *perm;
+  const double *P;  // sorted SoA: x y z ax ay az sigma
+  const uint8_t *flags;
+  const uint32_t *cidx;
+  const uint32_t *act_key;
+  const uint8_t *act_lev;
+  const uint32_t *leaf_ci;
+  double *A, *B, *Gx;  // multipole a, local b (deg p), local g (deg p+1)
+  double *out;         // sorted-order vel(3), stretch(3), rotu(3), SoA
+  double inv_fact[224];
+};
+
+struct ElemDev {
+  const PanelGeo *body, *wake;
+  const LineGeo *lines;
+  int nbody, nwake, nline;
+  RegParams rp;
+};
+
+struct dust_octree {
+  dust_fmm_params prm;
+  TreeGeom G;
+  int p, nm, nm1, nD;
+  uint64_t ncell_tot = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8];
+  bool timing = false;
+  DevBuf dtab[DUST_MAXLEV + 1];
+  int kdlen[DUST_MAXLEV + 1][3];
+  DevBuf idxsum;
+  // per-call buffers (grown on demand, kept across calls)
+  DevBuf keys, keys_s, vals, perm, cnt, cstart, part, flags, ind, cidx, lidx;
+  DevBuf act_key, act_lev, leaf_ci, mp, outs, cub_tmp, small;
+  DevBuf h_in, h_out, el_geo, el_raw;  // staging of host-API calls
+  int64_t n_active = 0, n_leaves = 0;
+  int64_t act_off[DUST_MAXLEV + 3];
+  int bad_particle = -1;
+  FmmDev dev;
+  dust_fmm_stats stats;
+};
+
+int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
+                   const double *mag, const double *rv, cudaStream_t st);
+int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
+                      double *rot, cudaStream_t st);
+void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem);
+
+// elements.cu
+int elem_build_device(const dust_panels *body, const dust_panels *wake,
+                      const dust_lines *lines, const double *u_inf, const RegParams &rp,
+                      bool host_arrays, DevBuf &raw, DevBuf &geo, ElemDev &out,
+                      cudaStream_t st);
+RegParams reg_params(const dust_fmm_params *prm);

@@ -1,0 +1,266 @@
+/*
+ * dust_b200.h -- C ABI of the B200 (sm_100a) implementation of DUST's
+ * per-timestep aerodynamic hot path.
+ *
+ * The reference (DUST, Fortran 2008 + OpenMP) reaches this path through
+ * module procedures of mod_octree and mod_linsys.  Every entry point below
+ * replaces one of them and is meant to be bound from Fortran with
+ * ISO_C_BINDING (see INTEGRATION.md for the interface module).  Arrays are
+ * plain host (or, for the *_device variants, device) pointers in the
+ * Fortran layout: a particle/panel coordinate array `x(3,n)` is passed as a
+ * double* of length 3*n with the three components of one item contiguous.
+ *
+ * All calls return an int status (DUST_OK == 0).  A non-zero status maps to
+ * the reference's `call error(...)` (src/general/mod_handling.f90:181).
+ * Handles are not re-entrant: one handle is driven by one host thread and
+ * owns one CUDA stream.
+ */
+#ifndef DUST_B200_H
+#define DUST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DUST_API __attribute__((visibility("default")))
+#else
+#define DUST_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define DUST_OK                0
+#define DUST_ERR_CUDA          1  /* CUDA runtime / launch failure            */
+#define DUST_ERR_OUT_OF_BOX    2  /* particle outside the octree box
+                                     (mod_octree.f90:758-762)                 */
+#define DUST_ERR_SINGULAR      3  /* zero pivot in an LU factorisation
+                                     (LAPACK info>0, mod_linsys.f90:241-245)  */
+#define DUST_ERR_NOT_CONVERGED 4  /* iterative solve did not reach tolerance  */
+#define DUST_ERR_TIMEOUT       5  /* a bounded device wait gave up            */
+#define DUST_ERR_BAD_ARG       6  /* invalid argument                         */
+#define DUST_ERR_NO_DEVICE     7  /* no CUDA device / library not usable      */
+#define DUST_ERR_CAPACITY      8  /* size above a documented maximum          */
+
+/* ------------------------------------------------------- element kinds */
+#define DUST_ELEM_SURFPAN  1   /* 'p': source+doublet panel, Dirichlet row
+                                  (src/aeroel/mod_surfpan.f90)                */
+#define DUST_ELEM_VORTLATT 2   /* 'v': vortex ring, Neumann row
+                                  (src/aeroel/mod_vortlatt.f90)               */
+
+/* ------------------------------------------------------ precision modes */
+#define DUST_PREC_FP64   0     /* plain: FP64 everywhere                      */
+#define DUST_PREC_FP32C  1     /* FP32 arithmetic with compensated (two-sum)
+                                  accumulation; FP64 root-level translations */
+
+/* Octree / FMM parameters.  One field per DUST input key
+ * (src/general/mod_sim_param.f90:376-452, read at :772-804). */
+typedef struct dust_fmm_params {
+  double box_length;          /* box_length                                  */
+  int    n_box[3];            /* n_box                                       */
+  double origin[3];           /* octree_origin                               */
+  int    n_octree_levels;     /* n_octree_levels                             */
+  int    min_octree_part;     /* min_octree_part                             */
+  int    multipole_degree;    /* multipole_degree (p)                        */
+  double rankine_rad;         /* rankine_rad: M2L kernel regularisation
+                                 (octree%delta, dust.f90:377) and the Rankine
+                                 core of panel/line induction                 */
+  double cutoff_rad;          /* cutoff_rad                                  */
+  double far_field_ratio_doublet; /* far_field_ratio_doublet (10)            */
+  int    vortstretch;         /* vortstretch                                 */
+  int    divergence_filtering;/* divergence_filtering                        */
+  int    diffusion;           /* diffusion                                   */
+  int    turbulent_viscosity; /* turbulent_viscosity                         */
+  double nu_inf;              /* mu_inf/rho_inf                              */
+  double u_inf[3];            /* u_inf (uniform wind, mod_wind.f90:66-77)    */
+  int    precision;           /* DUST_PREC_*                                 */
+} dust_fmm_params;
+
+/* A set of flat panels (quads or triangles).  Geometry is given by the
+ * vertices; the derived quantities of calc_geo_data_surfpan
+ * (mod_surfpan.f90:888-951) / calc_geo_data_vortlatt (mod_vortlatt.f90:
+ * 601-669) are computed by the library. */
+typedef struct dust_panels {
+  int           n;      /* number of panels                                  */
+  const int    *n_ver;  /* [n] 3 or 4                                        */
+  const int    *kind;   /* [n] DUST_ELEM_*; NULL = all DUST_ELEM_VORTLATT    */
+  const double *ver;    /* [12*n] ver(3,4) per panel (4th unused for tris)   */
+  const double *mag;    /* [n] doublet intensity; NULL = 0                   */
+  const double *ub;     /* [3*n] body velocity at the centre; NULL = 0       */
+  const double *uvort;  /* [3*n] vortex-induced velocity at the centre
+                           (surface-panel source strength); NULL = 0         */
+} dust_panels;
+
+/* Vortex line segments (end vortices of panel wakes, mod_vortline.f90). */
+typedef struct dust_lines {
+  int           n;
+  const double *ver;    /* [6*n] ver(3,2) per line                           */
+  const double *mag;    /* [n]                                               */
+} dust_lines;
+
+/* The non-particle vortical elements that act on particles in
+ * apply_multipole (mod_octree.f90:1350-1373). */
+typedef struct dust_elements {
+  dust_panels body;     /* elem: implicit body elements                      */
+  dust_panels wake;     /* wpan: wake panels (vortex rings)                  */
+  dust_lines  end_vort; /* wvort: end vortices                               */
+} dust_elements;
+
+/* Counters of the last FMM evaluation (for logs and roofline figures). */
+typedef struct dust_fmm_stats {
+  int64_t n_particles;
+  int64_t n_leaves;
+  int64_t n_active_cells;
+  int64_t n_m2l_pairs;       /* (target, active source) pairs over levels    */
+  int64_t n_p2p_pairs;       /* particle pairs of the reference's near field */
+  int64_t n_elem_pairs;      /* particle x element evaluations               */
+  int     n_levels;
+  float   ms_tree, ms_upward, ms_m2l, ms_p2p, ms_elems, ms_total;
+} dust_fmm_stats;
+
+typedef struct dust_octree dust_octree;
+
+/* ------------------------------------------------------------- octree */
+
+/* Replaces initialize_octree (src/fmm/mod_octree.f90:251-518): builds the
+ * level geometry and the per-level kernel-derivative tables
+ * (compute_der_ker, src/fmm/mod_multipole.f90:388-450) on the device. */
+DUST_API int dust_octree_create(const dust_fmm_params *prm, dust_octree **out);
+
+/* Replaces destroy_octree (mod_octree.f90:691-695). */
+DUST_API int dust_octree_destroy(dust_octree *oct);
+
+/* Replaces sort_particles + calculate_multipole + apply_multipole
+ * (mod_octree.f90:703-996, 1002-1133, 1139-1429) for n live particles.
+ * Host arrays.  Outputs (caller order): vel(3,n) = induced velocity + wind;
+ * stretch(3,n) (vortex stretching + diffusion, when either is on) and
+ * rotu(3,n) (divergence-filter curl, when on); either may be NULL. */
+DUST_API int dust_fmm_apply(dust_octree *oct, int n,
+                   const double *cen, const double *dir, const double *mag,
+                   const double *r_vortex, const dust_elements *elems,
+                   double *vel, double *stretch, double *rotu);
+
+/* Same as dust_fmm_apply with every array (including those inside *elems)
+ * already resident in device memory; runs on `stream` (cudaStream_t, NULL =
+ * the handle's stream) and returns without a host synchronisation when
+ * `sync` == 0 (errors are then reported by the next call). */
+DUST_API int dust_fmm_apply_device(dust_octree *oct, int n,
+                          const double *cen, const double *dir,
+                          const double *mag, const double *r_vortex,
+                          const dust_elements *elems,
+                          double *vel, double *stretch, double *rotu,
+                          void *stream, int sync);
+
+/* Counters of the last dust_fmm_apply*.  Timings are filled only when
+ * `timing` was enabled with dust_octree_set_timing. */
+DUST_API int dust_octree_get_stats(const dust_octree *oct, dust_fmm_stats *st);
+DUST_API int dust_octree_set_timing(dust_octree *oct, int on);
+
+/* Direct O(N^2) evaluation of the same particle kernels over all pairs
+ * (the reference's P2P formulas of src/aeroel/mod_vortpart.f90:139-336
+ * applied to every particle pair); used as the FMM truth.  Targets are the
+ * first n_tgt particles.  Host arrays. */
+DUST_API int dust_direct_particles(const dust_fmm_params *prm, int n,
+                          const double *cen, const double *dir,
+                          const double *mag, const double *r_vortex,
+                          int n_tgt, double *vel, double *stretch,
+                          double *rotu);
+
+/* Replaces get_vort_vel_surfpan / get_vort_vel_vortlatt over all vortical
+ * elements (mod_surfpan.f90:962-977, mod_vortlatt.f90:676-693, called from
+ * mod_linsys.f90:295-299): uvort(3,n_pts) at the given points (panel
+ * centres) induced by the n particles plus the end vortices.  Host arrays. */
+DUST_API int dust_points_uvort(const dust_fmm_params *prm, int n_pts,
+                      const double *pts, int n, const double *cen,
+                      const double *dir, const double *mag,
+                      const double *r_vortex, const dust_lines *end_vort,
+                      double *uvort);
+
+/* Velocity induced at n_pts points by a set of panels and lines
+ * (compute_vel of surfpan/vortlatt/vortline, divided by 4*pi) plus u_inf.
+ * Host arrays. */
+DUST_API int dust_elements_vel(const dust_fmm_params *prm, int n_pts,
+                      const double *pts, const dust_elements *elems,
+                      double *vel);
+
+/* Panel centres / unit normals as computed by calc_geo_data (for callers
+ * that need the collocation points).  Host arrays. */
+DUST_API int dust_panels_geometry(const dust_panels *pan, double *cen, double *nor,
+                         double *area);
+
+/* --------------------------------------------------------- linear system */
+
+typedef struct dust_linsys dust_linsys;
+
+/* Solve modes. */
+#define DUST_SOLVE_LU64      0  /* plain FP64 block LU (static LU reused +
+                                   Schur update of the moving block), the
+                                   reference's solve_linsys sequence          */
+#define DUST_SOLVE_MIXED     1  /* FP32 LU (tensor-core trailing updates) +
+                                   FP64 iterative refinement                  */
+#define DUST_SOLVE_GMRES_NN  2  /* learned-preconditioned FP64 GMRES, plain LU
+                                   fallback                                   */
+
+typedef struct dust_solve_report {
+  int    mode_used;       /* DUST_SOLVE_* that produced the solution         */
+  int    iterations;      /* refinement / GMRES iterations                   */
+  int    fell_back;       /* 1 if GMRES stalled and LU was used              */
+  double residual;        /* final ||b - A x||_inf / (||A||_inf ||x||_inf)   */
+  float  ms_factor, ms_solve;
+} dust_solve_report;
+
+/* Implicit wake panels (first n_impl wake panels) couple into A through
+ * their generating elements (wake%pan_gen_elems_id, mod_wake.f90:150):
+ * impl_ind[2*j], impl_ind[2*j+1] = 1-based element indices (0 = none). */
+typedef struct dust_wake_rows {
+  dust_panels  pan;       /* all wake panels, implicit ones first            */
+  int          n_impl;
+  const int   *impl_ind;  /* [2*n_impl]                                      */
+} dust_wake_rows;
+
+/* Replaces initialize_linsys (mod_linsys.f90:109-267) for `rank` implicit
+ * elements of which the first `nstatic` do not move: builds the static rows,
+ * adds the static wake, and LU-factors the static block once. */
+DUST_API int dust_linsys_create(int rank, int nstatic, const dust_fmm_params *prm,
+                       const dust_panels *elems, const dust_wake_rows *wake,
+                       dust_linsys **out);
+DUST_API int dust_linsys_destroy(dust_linsys *ls);
+
+/* Replaces assemble_linsys (mod_linsys.f90:279-344) minus the uvort step
+ * (pass elems->uvort, computed by dust_points_uvort): rebuilds the moving
+ * columns of static rows, all columns of moving rows, the RHS and the wake
+ * terms. */
+DUST_API int dust_linsys_assemble(dust_linsys *ls, const dust_panels *elems,
+                         const dust_wake_rows *wake);
+
+/* Replaces solve_linsys (mod_linsys.f90:352-482).  res[rank] receives the
+ * doublet intensities. */
+DUST_API int dust_linsys_solve(dust_linsys *ls, int mode, double *res,
+                      dust_solve_report *rep);
+
+/* Copies of the assembled matrix (column-major, rank x rank, BEFORE
+ * factorisation of the moving part) and right-hand side, as dump_linsys
+ * (mod_linsys.f90:503-524) writes them.  Either pointer may be NULL. */
+DUST_API int dust_linsys_get_system(dust_linsys *ls, double *A, double *b);
+
+/* Standalone dense solve A X = B (column-major; n x n, nrhs columns) with
+ * partial-pivoting LU as LAPACK dgetrf+dgetrs (mod_linsys.f90:470-474).
+ * mode: DUST_SOLVE_LU64 or DUST_SOLVE_MIXED (refined to `tol`). */
+DUST_API int dust_dense_solve(int n, int nrhs, const double *A, const double *B,
+                     double *X, int mode, double tol, dust_solve_report *rep);
+
+/* ---------------------------------------------------------------- misc */
+DUST_API const char *dust_status_string(int status);
+DUST_API const char *dust_last_error(void); /* text of the last CUDA error seen      */
+DUST_API int dust_device_ok(void);   /* DUST_OK if a usable sm_100 device is present */
+/* sizeof() of the ABI structs in declaration order (dust_fmm_params,
+ * dust_panels, dust_lines, dust_elements, dust_fmm_stats, dust_solve_report,
+ * dust_wake_rows), for binding checks; returns the number of sizes. */
+DUST_API int dust_abi_sizes(int64_t *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DUST_B200_H */

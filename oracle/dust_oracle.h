@@ -1,0 +1,106 @@
+/*
+ * dust_oracle.h -- CPU oracle (test infrastructure only).
+ *
+ * A plain-C, FP64, OpenMP restatement of the reference's hot path, used
+ * only by the tests, by __graft_entry__.smoke() and by bench.py's CPU
+ * baseline as the checker.  The product never links or calls it.
+ *
+ * Reference files restated (paths inside the DUST project):
+ *   src/fmm/mod_multipole.f90    polynomial tools, P2M, M2M, M2L, L2L,
+ *                                kernel-derivative recurrence
+ *   src/fmm/mod_octree.f90       octree geometry, leaf rule, leaf_neigh,
+ *                                interaction lists, calculate/apply_multipole
+ *   src/aeroel/mod_vortpart.f90  particle kernels (vel, stretch, rotu, PSE)
+ *   src/aeroel/mod_doublet.f90   doublet potential / velocity
+ *   src/aeroel/mod_surfpan.f90   source potential / velocity, rows
+ *   src/aeroel/mod_vortlatt.f90  vortex-lattice rows
+ *   src/aeroel/mod_vortline.f90  vortex line velocity
+ *   src/linsys/mod_linsys.f90    static/moving block LU sequence
+ *
+ * Parity pins: the reference is Fortran and cannot be compiled here (no
+ * Fortran compiler, LAPACK or HDF5), and it has no unit-level golden vectors
+ * for this path.  The LU sequence is pinned against LAPACK itself (the
+ * reference's third-party solver) through scipy; the FMM and the influence
+ * kernels are pinned only by analytic known answers (solid-angle sums,
+ * FMM -> direct-sum convergence).  Parity of those parts is "unpinned".
+ */
+#ifndef DUST_ORACLE_H
+#define DUST_ORACLE_H
+
+#include "../include/dust_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* 1 = reproduce the reference's default-integer (32-bit, wrapping)
+ * factorials in the M2L weights (mod_multipole.f90:489-497, 524-537);
+ * 0 (default) = exact factorials. */
+void or_set_factorial_wrap(int on);
+
+/* Full FMM evaluation: initialize_octree + sort_particles +
+ * calculate_multipole + apply_multipole.  Returns DUST_* status. */
+int or_fmm_apply(const dust_fmm_params *prm, int n, const double *cen,
+                 const double *dir, const double *mag, const double *r_vortex,
+                 const dust_elements *elems, double *vel, double *stretch,
+                 double *rotu, int64_t *counters /* [4]: leaves, active,
+                 m2l pairs, p2p pairs; may be NULL */);
+
+/* Tree of the last or_fmm_apply (for structure checks):
+ * per level l (1..ll) the dense flag array in Morton-key order
+ * (bit0 leaf, bit1 branch, bit2 active).  flags must hold
+ * sum_l prod(nbox)*8^(l-1) bytes. */
+int or_last_tree_flags(unsigned char *flags, int64_t cap);
+
+/* Direct sum of the particle kernels over all pairs (targets = first n_tgt). */
+int or_direct_particles(const dust_fmm_params *prm, int n, const double *cen,
+                        const double *dir, const double *mag,
+                        const double *r_vortex, int n_tgt, double *vel,
+                        double *stretch, double *rotu);
+
+/* Element influence at points (compute_vel / 4pi summed + u_inf). */
+int or_elements_vel(const dust_fmm_params *prm, int n_pts, const double *pts,
+                    const dust_elements *elems, double *vel);
+
+/* uvort at points from particles + end vortices (get_vort_vel_*). */
+int or_points_uvort(const dust_fmm_params *prm, int n_pts, const double *pts,
+                    int n, const double *cen, const double *dir,
+                    const double *mag, const double *r_vortex,
+                    const dust_lines *end_vort, double *uvort);
+
+/* Single-element kernels (for unit tests).  kind = DUST_ELEM_*. */
+int or_panel_geometry(const dust_panels *pan, double *cen, double *nor,
+                      double *area);
+double or_potential_doublet(const dust_fmm_params *prm, const dust_panels *pan,
+                            int j, const double *pos);
+void or_velocity_doublet(const dust_fmm_params *prm, const dust_panels *pan,
+                         int j, const double *pos, double *v);
+double or_potential_source(const dust_fmm_params *prm, const dust_panels *pan,
+                           int j, double dou, const double *pos);
+void or_velocity_source(const dust_fmm_params *prm, const dust_panels *pan,
+                        int j, const double *pos, double *v);
+
+/* Linear system: assemble (initialize_linsys + assemble_linsys without the
+ * uvort step) and solve with the reference's block LU sequence.
+ * A_out (rank x rank, column-major) / b_out receive the assembled system
+ * before the moving-block factorisation; res the solution. */
+int or_linsys_run(const dust_fmm_params *prm, int rank, int nstatic,
+                  const dust_panels *elems_init, const dust_panels *elems_step,
+                  const dust_wake_rows *wake_init,
+                  const dust_wake_rows *wake_step,
+                  double *A_out, double *b_out, double *res);
+
+/* LAPACK-equivalent dense kernels (column-major). */
+int  or_dgetrf(int m, int n, double *A, int lda, int *ipiv);
+void or_dgetrs(int n, int nrhs, const double *A, int lda, const int *ipiv,
+               double *B, int ldb);
+void or_dlaswp(int n, double *A, int lda, int k1, int k2, const int *ipiv);
+void or_dtrsm_llnu(int m, int n, const double *A, int lda, double *B, int ldb);
+void or_dtrsm_runn(int m, int n, const double *A, int lda, double *B, int ldb);
+void or_dgemm_nn_minus(int m, int n, int k, const double *A, int lda,
+                       const double *B, int ldb, double *C, int ldc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
