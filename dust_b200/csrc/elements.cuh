@@ -22,6 +22,7 @@ struct PanelGeo {
   double edge_vec[4][3], edge_uni[4][3], edge_len[4];
   double verp[4][3], cosTi[4], sinTi[4];
   double area, max_edge, mag, sig;  // sig = nor.(ub - wind - uvort)
+  double sig0;                       // nor.(-wind - uvort) (static RHS columns)
   int nv, kind;
 };
 
@@ -101,10 +102,13 @@ __host__ __device__ inline void panel_build(const double *ver12, int nv, int kin
     }
   }
   p.mag = mag;
-  double rel[3];
-  for (int d = 0; d < 3; ++d)
+  double rel[3], rel0[3];
+  for (int d = 0; d < 3; ++d) {
+    rel0[d] = -(u_inf ? u_inf[d] : 0.0) - (uvort ? uvort[d] : 0.0);
     rel[d] = (ub ? ub[d] : 0.0) - (u_inf ? u_inf[d] : 0.0) - (uvort ? uvort[d] : 0.0);
+  }
   p.sig = d3dot(p.nor, rel);
+  p.sig0 = d3dot(p.nor, rel0);
 }
 
 __host__ __device__ inline void line_build(const double *ver6, double mag, LineGeo &l) {

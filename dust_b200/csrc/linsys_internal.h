@@ -1,0 +1,35 @@
+// linsys_internal.h -- linear-system handle and internal entry points.
+#pragma once
+
+#include <cublas_v2.h>
+
+#include "dust_common.cuh"
+#include "elements.cuh"
+#include "fmm_internal.h"
+#include "lu.cuh"
+
+struct dust_linsys {
+  int n = 0, nst = 0, nmv = 0;
+  dust_fmm_params prm;
+  RegParams rp;
+  cudaStream_t st = nullptr;
+  cublasHandle_t cb = nullptr;
+  DevBuf A;     // column-major rank x rank, FP64; static block holds its LU
+  DevBuf As;    // unfactored static block (nst x nst) for residuals
+  DevBuf b, bst, piv, info, geo, raw, impl, work, A32, gm;
+  LuWork lu;
+  const PanelGeo *el = nullptr, *wk = nullptr;
+  int nwake = 0, n_impl = 0;
+  bool assembled = false, factored = false, keep_static_copy = true;
+};
+
+int linsys_solve_lu64(dust_linsys *L, double *res_dev);
+int linsys_solve_iterative(dust_linsys *L, int mode, double *x_dev, dust_solve_report *rep);
+void linsys_shift_pivots(cudaStream_t st, int *P, int n, int off);
+
+// Mixed-precision dense solve on device arrays: FP32 LU (tensor-core
+// trailing updates when use_tc) of A64, FP64 iterative refinement to `tol`.
+int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w32,
+                       DevBuf &wrk, int n, int nrhs, const double *A64, const double *B,
+                       double *X, double tol, int max_iter, int use_tc,
+                       dust_solve_report *rep);

@@ -1,0 +1,368 @@
+// lu.cu -- blocked LU with partial pivoting (FP64 and FP32) on sm_100a.
+//
+// LAPACK dgetrf semantics (used by src/linsys/mod_linsys.f90:230-246 and
+// :428-438): pivot = first row of maximum |a(i,j)|, ipiv 1-based, rows
+// swapped across the whole matrix, L unit lower, U upper, info = first
+// zero pivot.
+//
+// Panel factorisation: one cooperative launch of G CTAs; CTA g keeps rows
+// [g*R, (g+1)*R) of the panel in shared memory.  Per column there is a
+// single grid-wide barrier: before it every CTA publishes its local maximum
+// and that row, and the owner of the diagonal row publishes it; after it
+// every CTA selects the same pivot, performs its part of the swap from the
+// published rows and updates its rows.  Published buffers alternate between
+// two copies so a CTA one column ahead never overwrites data still read.
+// The barrier spins with an iteration limit and raises an error flag
+// instead of hanging.
+#include <climits>
+
+#include "lu.cuh"
+
+#define PAN_T 256
+#define PAN_MIN_ROWS 32
+#define BAR_SPIN_LIMIT (1ll << 25)
+
+template <typename T>
+struct PanelArgs {
+  T *A;
+  int lda, k, jb, m, G, R;
+  int *ipiv, *info;
+  unsigned *bar;  // [0] arrivals, [1] generation
+  int *err;
+  T *cval;        // [2][G]
+  int *crow;      // [2][G]
+  T *crowv;       // [2][G][jb]
+  T *srow;        // [2][jb]
+};
+
+__device__ __forceinline__ void grid_barrier(unsigned *bar, int G, int *err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *vgen = bar + 1;
+    unsigned g0 = *vgen;
+    __threadfence();
+    unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == (unsigned)G - 1u) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*vgen == g0) {
+        if (++it > BAR_SPIN_LIMIT) {
+          atomicExch(err, 1);
+          break;
+        }
+        if (it > 64) __nanosleep(20);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ T ldcg(const T *p) {
+  return __ldcg(p);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PAN_T) k_panel(PanelArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *sp = (T *)smraw;  // R rows x LD, row-major
+  __shared__ T s_prow[128];
+  __shared__ T s_wv[PAN_T / 32];
+  __shared__ int s_wr[PAN_T / 32];
+  __shared__ int s_p, s_gw;
+  __shared__ T s_pv;
+  const int g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int NW = PAN_T / 32;
+  const int jb = a.jb, LD = jb + 1;
+  const int r0 = g * a.R, r1 = min(a.m, r0 + a.R), nr = max(0, r1 - r0);
+  T *Ap = a.A + (size_t)a.k + (size_t)a.k * a.lda;
+  for (int idx = tid; idx < nr * jb; idx += PAN_T) {
+    int c = idx / nr, r = idx % nr;
+    sp[r * LD + c] = Ap[(size_t)(r0 + r) + (size_t)c * a.lda];
+  }
+  __syncthreads();
+  for (int j = 0; j < jb; ++j) {
+    const int buf = j & 1;
+    // local maximum of |a(r, j)| over own rows r >= j (first index on ties)
+    T best = (T)-1;
+    int brow = INT_MAX;
+    for (int r = tid; r < nr; r += PAN_T) {
+      int gr = r0 + r;
+      if (gr < j) continue;
+      T v = fabs(sp[r * LD + j]);
+      if (v != v) v = (T)-0.5;  // NaN: still a candidate, below every number
+      if (v > best || (v == best && gr < brow)) {
+        best = v;
+        brow = gr;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      T ov = __shfl_down_sync(0xffffffffu, best, o);
+      int orr = __shfl_down_sync(0xffffffffu, brow, o);
+      if (ov > best || (ov == best && orr < brow)) {
+        best = ov;
+        brow = orr;
+      }
+    }
+    if (lane == 0) {
+      s_wv[warp] = best;
+      s_wr[warp] = brow;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      T b = s_wv[0];
+      int br = s_wr[0];
+      for (int w = 1; w < NW; ++w)
+        if (s_wv[w] > b || (s_wv[w] == b && s_wr[w] < br)) {
+          b = s_wv[w];
+          br = s_wr[w];
+        }
+      s_p = br;
+      a.crow[buf * a.G + g] = br;
+      a.cval[buf * a.G + g] = (br == INT_MAX) ? (T)-1 : b;
+    }
+    __syncthreads();
+    const int mybest = s_p;
+    if (mybest != INT_MAX)
+      for (int c = tid; c < jb; c += PAN_T)
+        a.crowv[((size_t)buf * a.G + g) * jb + c] = sp[(mybest - r0) * LD + c];
+    if (j >= r0 && j < r1)
+      for (int c = tid; c < jb; c += PAN_T) a.srow[buf * jb + c] = sp[(j - r0) * LD + c];
+    grid_barrier(a.bar, a.G, a.err);
+    // global pivot: maximum over the published candidates
+    {
+      T bv = (T)-1;
+      int br = INT_MAX, bg = -1;
+      for (int q = tid; q < a.G; q += PAN_T) {
+        int rr = ldcg(a.crow + buf * a.G + q);
+        T vv = ldcg(a.cval + buf * a.G + q);
+        if (rr != INT_MAX && (vv > bv || (vv == bv && rr < br))) {
+          bv = vv;
+          br = rr;
+          bg = q;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        T ov = __shfl_down_sync(0xffffffffu, bv, o);
+        int orr = __shfl_down_sync(0xffffffffu, br, o);
+        int og = __shfl_down_sync(0xffffffffu, bg, o);
+        if (ov > bv || (ov == bv && orr < br)) {
+          bv = ov;
+          br = orr;
+          bg = og;
+        }
+      }
+      __syncthreads();
+      if (lane == 0) {
+        s_wv[warp] = bv;
+        s_wr[warp] = br;
+      }
+      __shared__ int s_wg[PAN_T / 32];
+      if (lane == 0) s_wg[warp] = bg;
+      __syncthreads();
+      if (tid == 0) {
+        T b = s_wv[0];
+        int rr = s_wr[0], gg = s_wg[0];
+        for (int w = 1; w < NW; ++w)
+          if (s_wv[w] > b || (s_wv[w] == b && s_wr[w] < rr)) {
+            b = s_wv[w];
+            rr = s_wr[w];
+            gg = s_wg[w];
+          }
+        s_p = rr;
+        s_gw = gg;
+      }
+      __syncthreads();
+    }
+    int p = s_p, gw = s_gw;
+    if (gw < 0 || gw >= a.G || p < j || p >= a.m) {
+      // cannot happen while some CTA owns a row >= j; keep the indices in
+      // bounds and report instead of reading outside the published buffers
+      if (tid == 0) atomicExch(a.err, 2);
+      gw = (j >= r0 && j < r1) ? g : 0;
+      p = j;
+    }
+    for (int c = tid; c < jb; c += PAN_T) s_prow[c] = ldcg(a.crowv + ((size_t)buf * a.G + gw) * jb + c);
+    __syncthreads();
+    if (tid == 0) s_pv = s_prow[j];
+    if (g == 0 && tid == 0) {
+      a.ipiv[a.k + j] = a.k + p + 1;
+      if (s_prow[j] == (T)0 && *a.info == 0) *a.info = a.k + j + 1;
+    }
+    if (p != j) {
+      if (j >= r0 && j < r1)
+        for (int c = tid; c < jb; c += PAN_T) sp[(j - r0) * LD + c] = s_prow[c];
+      if (p >= r0 && p < r1)
+        for (int c = tid; c < jb; c += PAN_T) sp[(p - r0) * LD + c] = ldcg(a.srow + buf * jb + c);
+    }
+    __syncthreads();
+    const T pv = s_pv;
+    if (pv != (T)0) {
+      const T rinv = (T)1 / pv;
+      for (int r = warp; r < nr; r += NW) {
+        if (r0 + r <= j) continue;
+        T l = sp[r * LD + j] * rinv;
+        for (int c = j + 1 + lane; c < jb; c += 32) sp[r * LD + c] -= l * s_prow[c];
+        __syncwarp();
+        if (lane == 0) sp[r * LD + j] = l;
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < nr * jb; idx += PAN_T) {
+    int c = idx / nr, r = idx % nr;
+    Ap[(size_t)(r0 + r) + (size_t)c * a.lda] = sp[r * LD + c];
+  }
+}
+
+template <typename T>
+__global__ void k_laswp(T *A, int lda, int c0, int c1, int k1, int k2, const int *ipiv) {
+  int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
+  T *col = A + (size_t)c * lda;
+  for (int i = k1; i < k2; ++i) {
+    int p = ipiv[i] - 1;
+    if (p != i && p >= 0 && p < lda) {
+      T t = col[i];
+      col[i] = col[p];
+      col[p] = t;
+    }
+  }
+}
+
+template <typename T>
+void lu_laswp(cudaStream_t st, T *A, int lda, int c0, int c1, int k1, int k2,
+              const int *ipiv) {
+  if (c1 <= c0 || k2 <= k1) return;
+  int nc = c1 - c0;
+  k_laswp<T><<<(nc + 127) / 128, 128, 0, st>>>(A, lda, c0, c1, k1, k2, ipiv);
+}
+
+static cublasStatus_t trsm_(cublasHandle_t h, cublasSideMode_t s, cublasFillMode_t u,
+                            cublasDiagType_t d, int m, int n, const double *A, int lda,
+                            double *B, int ldb) {
+  const double one = 1.0;
+  return cublasDtrsm(h, s, u, CUBLAS_OP_N, d, m, n, &one, A, lda, B, ldb);
+}
+static cublasStatus_t trsm_(cublasHandle_t h, cublasSideMode_t s, cublasFillMode_t u,
+                            cublasDiagType_t d, int m, int n, const float *A, int lda,
+                            float *B, int ldb) {
+  const float one = 1.0f;
+  return cublasStrsm(h, s, u, CUBLAS_OP_N, d, m, n, &one, A, lda, B, ldb);
+}
+static cublasStatus_t gemm_minus_(cublasHandle_t h, int m, int n, int k, const double *A,
+                                  int lda, const double *B, int ldb, double *C, int ldc) {
+  const double mone = -1.0, one = 1.0;
+  return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, lda, B, ldb, &one, C, ldc);
+}
+static cublasStatus_t gemm_minus_(cublasHandle_t h, int m, int n, int k, const float *A,
+                                  int lda, const float *B, int ldb, float *C, int ldc) {
+  const float mone = -1.0f, one = 1.0f;
+  return cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, lda, B, ldb, &one, C, ldc);
+}
+
+// tcgen05 TF32 trailing update (gemm_tc.cu); C -= A B, FP32 column-major.
+int gemm_tf32_minus(cudaStream_t st, int m, int n, int k, const float *A, int lda,
+                    const float *B, int ldb, float *C, int ldc);
+
+#define CUBLAS_OK(x)                                                      \
+  do {                                                                    \
+    if ((x) != CUBLAS_STATUS_SUCCESS) {                                   \
+      dust_set_last_error("cuBLAS call failed", __FILE__, __LINE__);      \
+      return DUST_ERR_CUDA;                                               \
+    }                                                                     \
+  } while (0)
+
+template <typename T>
+int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
+             int *ipiv, int *info_dev, int gemm_update) {
+  if (n <= 0) return DUST_OK;
+  const int nb = 64;
+  if (w.nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&w.nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (w.nsm <= 0) w.nsm = 1;
+  }
+  const int Gmax = w.nsm;
+  size_t bytes = 64 + 2 * Gmax * (sizeof(T) + sizeof(int)) + 2 * (size_t)Gmax * nb * sizeof(T) +
+                 2 * nb * sizeof(T) + 256;
+  DUST_TRY(devbuf_grow(w.sync, bytes));
+  char *base = (char *)w.sync.p;
+  unsigned *bar = (unsigned *)base;
+  int *err = (int *)(base + 16);
+  T *cval = (T *)(base + 64);
+  int *crow = (int *)(cval + 2 * Gmax);
+  T *crowv = (T *)(((uintptr_t)(crow + 2 * Gmax) + 15) & ~(uintptr_t)15);
+  T *srow = crowv + 2 * (size_t)Gmax * nb;
+  DUST_CUDA(cudaMemsetAsync(base, 0, 64, st));
+  DUST_CUDA(cudaMemsetAsync(info_dev, 0, sizeof(int), st));
+  CUBLAS_OK(cublasSetStream(cb, st));
+  for (int k = 0; k < n; k += nb) {
+    const int jb = std::min(nb, n - k), m = n - k;
+    int G = std::min(Gmax, std::max(1, (m + PAN_MIN_ROWS - 1) / PAN_MIN_ROWS));
+    int R = (m + G - 1) / G;
+    G = (m + R - 1) / R;
+    size_t sm = (size_t)R * (jb + 1) * sizeof(T);
+    if (sm > 48 * 1024)
+      DUST_CUDA(cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sm));
+    PanelArgs<T> pa{A, lda, k, jb, m, G, R, ipiv, info_dev, bar, err, cval, crow, crowv, srow};
+    void *args[] = {&pa};
+    DUST_CUDA(cudaMemsetAsync(bar, 0, 8, st));
+    DUST_CUDA(cudaLaunchCooperativeKernel((void *)k_panel<T>, dim3(G), dim3(PAN_T), args, sm, st));
+    lu_laswp<T>(st, A, lda, 0, k, k, k + jb, ipiv);
+    lu_laswp<T>(st, A, lda, k + jb, n, k, k + jb, ipiv);
+    if (k + jb < n) {
+      CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_UNIT, jb,
+                      n - k - jb, A + k + (size_t)k * lda, lda, A + k + (size_t)(k + jb) * lda,
+                      lda));
+      int m2 = n - k - jb;
+      if (gemm_update == 1 && sizeof(T) == 4) {
+        DUST_TRY(gemm_tf32_minus(st, m2, m2, jb, (const float *)(A + (k + jb) + (size_t)k * lda),
+                                 lda, (const float *)(A + k + (size_t)(k + jb) * lda), lda,
+                                 (float *)(A + (k + jb) + (size_t)(k + jb) * lda), lda));
+      } else {
+        CUBLAS_OK(gemm_minus_(cb, m2, m2, jb, A + (k + jb) + (size_t)k * lda, lda,
+                              A + k + (size_t)(k + jb) * lda, lda,
+                              A + (k + jb) + (size_t)(k + jb) * lda, lda));
+      }
+    }
+  }
+  DUST_CUDA(cudaGetLastError());
+  int herr = 0;
+  DUST_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  if (herr == 1) return DUST_ERR_TIMEOUT;
+  if (herr) return DUST_ERR_CUDA;
+  return DUST_OK;
+}
+
+template <typename T>
+int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, int lda,
+             const int *ipiv, T *B, int ldb) {
+  if (n <= 0 || nrhs <= 0) return DUST_OK;
+  CUBLAS_OK(cublasSetStream(cb, st));
+  lu_laswp<T>(st, B, ldb, 0, nrhs, 0, n, ipiv);
+  CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_UNIT, n, nrhs, A,
+                  lda, B, ldb));
+  CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, nrhs,
+                  A, lda, B, ldb));
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+template int lu_getrf<double>(cublasHandle_t, cudaStream_t, LuWork &, int, double *, int, int *,
+                              int *, int);
+template int lu_getrf<float>(cublasHandle_t, cudaStream_t, LuWork &, int, float *, int, int *,
+                             int *, int);
+template void lu_laswp<double>(cudaStream_t, double *, int, int, int, int, int, const int *);
+template void lu_laswp<float>(cudaStream_t, float *, int, int, int, int, int, const int *);
+template int lu_getrs<double>(cublasHandle_t, cudaStream_t, int, int, const double *, int,
+                              const int *, double *, int);
+template int lu_getrs<float>(cublasHandle_t, cudaStream_t, int, int, const float *, int,
+                             const int *, float *, int);

@@ -1,0 +1,38 @@
+// lu.cuh -- dense LU with partial pivoting on the device (column-major).
+//
+// Blocked right-looking LU as LAPACK dgetrf (partial pivoting, first
+// maximum wins like idamax), used by solve_linsys's sequence
+// (src/linsys/mod_linsys.f90:352-482).  The panel is factored by one
+// cooperative kernel that keeps its rows in shared memory, one grid-wide
+// barrier per column; trailing updates are GEMMs.
+#pragma once
+
+#include <cublas_v2.h>
+
+#include "dust_common.cuh"
+#include "fmm_internal.h"
+
+struct LuWork {
+  DevBuf sync;   // barrier counters, error flag, partials, candidate rows
+  int nsm = 0;
+};
+
+// Factors the m x n column-major matrix A (lda) in place: ipiv (1-based,
+// relative to A's first row) as LAPACK.  *info_dev receives the first zero
+// pivot (1-based) or stays 0; the returned status reports launch errors and
+// barrier timeouts.  `gemm_update` selects the trailing update:
+// 0 = cuBLAS DGEMM/SGEMM (plain), 1 = tcgen05 TF32 (FP32 only).
+template <typename T>
+int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
+             int *ipiv, int *info_dev, int gemm_update);
+
+// Row interchanges of rows [k1, k2) (0-based) given ipiv (1-based, absolute
+// row numbers relative to A), applied to columns [c0, c1) of A.
+template <typename T>
+void lu_laswp(cudaStream_t st, T *A, int lda, int c0, int c1, int k1, int k2,
+              const int *ipiv);
+
+// Solves A X = B with the factors (nrhs columns, ldb).
+template <typename T>
+int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, int lda,
+             const int *ipiv, T *B, int ldb);

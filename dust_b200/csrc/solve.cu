@@ -1,0 +1,267 @@
+// solve.cu -- dense solves: the plain FP64 LU path and the mixed-precision
+// path (FP32 LU, tensor-core trailing updates, FP64 iterative refinement).
+//
+// The plain path is LAPACK's dgetrf + dgetrs as the reference calls them
+// (src/linsys/mod_linsys.f90:470-474).  The mixed path factors an FP32 copy
+// of A and recovers FP64 accuracy by refinement: r = B - A X in FP64 (A kept
+// in FP64), d = U^-1 L^-1 P r in FP32, X += d, until
+// ||r||_inf <= tol * ||A||_inf ||X||_inf.
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dust_common.cuh"
+#include "linsys_internal.h"
+#include "lu.cuh"
+
+static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__global__ void k_to_f32(size_t n, const double *a, float *b) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+__global__ void k_add_f32(size_t n, const float *d, double *x) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] += (double)d[i];
+}
+// row sums |A| (for ||A||_inf), one thread per row, column-major
+__global__ void k_rowabs(int n, const double *A, double *rs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < n; ++j) s += fabs(A[(size_t)i + (size_t)j * n]);
+  rs[i] = s;
+}
+// per column: max |r| and max |x|
+__global__ void k_colmax(int n, int nrhs, const double *R, const double *X, double *out) {
+  int c = blockIdx.x;
+  double mr = 0.0, mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    mr = fmax(mr, fabs(R[(size_t)c * n + i]));
+    mx = fmax(mx, fabs(X[(size_t)c * n + i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, o));
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  __shared__ double sr[32], sx[32];
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sr[w] = mr;
+    sx[w] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      mr = fmax(mr, sr[q]);
+      mx = fmax(mx, sx[q]);
+    }
+    out[2 * c] = fmax(mr, sr[0]);
+    out[2 * c + 1] = fmax(mx, sx[0]);
+  }
+}
+
+int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w32,
+                       DevBuf &wrk, int n, int nrhs, const double *A64, const double *B,
+                       double *X, double tol, int max_iter, int use_tc,
+                       dust_solve_report *rep) {
+  size_t nn = (size_t)n * n, nr = (size_t)n * nrhs;
+  DUST_TRY(devbuf_grow(w32, nn * 4 + nr * 4 + (size_t)n * 4 + 256));
+  DUST_TRY(devbuf_grow(wrk, nr * 8 + (size_t)n * 8 + (size_t)nrhs * 16 + 64 + 256));
+  float *A32 = (float *)w32.p;
+  float *D32 = A32 + nn;
+  int *ipiv = (int *)(D32 + nr);
+  double *R = (double *)wrk.p;
+  double *rs = R + nr;
+  double *cm = rs + n;
+  int *info = (int *)(cm + 2 * nrhs);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  k_to_f32<<<1184, 256, 0, st>>>(nn, A64, A32);
+  int s = lu_getrf<float>(cb, st, lu, n, A32, n, ipiv, info, use_tc);
+  cudaEventRecord(e1, st);
+  if (s != DUST_OK) return s;
+  int hinfo = 0;
+  DUST_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  if (rep) cudaEventElapsedTime(&rep->ms_factor, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (hinfo) return DUST_ERR_SINGULAR;
+  k_rowabs<<<nblk(n, 128), 128, 0, st>>>(n, A64, rs);
+  int imax = 0;
+  double anorm = 0.0;
+  cublasSetStream(cb, st);
+  cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST);
+  if (cublasIdamax(cb, n, rs, 1, &imax) != CUBLAS_STATUS_SUCCESS) return DUST_ERR_CUDA;
+  DUST_CUDA(cudaMemcpyAsync(&anorm, rs + imax - 1, 8, cudaMemcpyDeviceToHost, st));
+  // X0 = LU \ B (in FP32)
+  DUST_CUDA(cudaMemsetAsync(X, 0, nr * 8, st));
+  DUST_CUDA(cudaMemcpyAsync(R, B, nr * 8, cudaMemcpyDeviceToDevice, st));
+  std::vector<double> hcm(2 * (size_t)nrhs);
+  const double one = 1.0, mone = -1.0;
+  int it = 0;
+  double worst = 0.0;
+  for (it = 0; it <= max_iter; ++it) {
+    if (it > 0) {
+      // R = B - A X (FP64)
+      DUST_CUDA(cudaMemcpyAsync(R, B, nr * 8, cudaMemcpyDeviceToDevice, st));
+      if (cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, n, nrhs, n, &mone, A64, n, X, n, &one, R,
+                      n) != CUBLAS_STATUS_SUCCESS)
+        return DUST_ERR_CUDA;
+      k_colmax<<<nrhs, 256, 0, st>>>(n, nrhs, R, X, cm);
+      DUST_CUDA(cudaMemcpyAsync(hcm.data(), cm, 16 * (size_t)nrhs, cudaMemcpyDeviceToHost, st));
+      DUST_CUDA(cudaStreamSynchronize(st));
+      worst = 0.0;
+      for (int c = 0; c < nrhs; ++c) {
+        double den = anorm * hcm[2 * c + 1];
+        double rel = den > 0 ? hcm[2 * c] / den : hcm[2 * c];
+        worst = std::max(worst, rel);
+      }
+      if (worst <= tol) break;
+      if (it == max_iter) break;
+    }
+    k_to_f32<<<256, 256, 0, st>>>(nr, R, D32);
+    DUST_TRY(lu_getrs<float>(cb, st, n, nrhs, A32, n, ipiv, D32, n));
+    k_add_f32<<<256, 256, 0, st>>>(nr, D32, X);
+  }
+  DUST_CUDA(cudaGetLastError());
+  if (rep) {
+    rep->iterations = it;
+    rep->residual = worst;
+    rep->mode_used = DUST_SOLVE_MIXED;
+  }
+  return worst <= tol ? DUST_OK : DUST_ERR_NOT_CONVERGED;
+}
+
+extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *B, double *X,
+                                int mode, double tol, dust_solve_report *rep) {
+  if (n <= 0 || nrhs <= 0 || !A || !B || !X) return DUST_ERR_BAD_ARG;
+  if (mode != DUST_SOLVE_LU64 && mode != DUST_SOLVE_MIXED) return DUST_ERR_BAD_ARG;
+  cudaStream_t st;
+  cublasHandle_t cb;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return DUST_ERR_CUDA;
+  if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) {
+    cudaStreamDestroy(st);
+    return DUST_ERR_CUDA;
+  }
+  cublasSetStream(cb, st);
+  DevBuf dA, dB, dX, w32, wrk;
+  LuWork lu;
+  dust_solve_report r;
+  memset(&r, 0, sizeof(r));
+  size_t nn = (size_t)n * n, nr = (size_t)n * nrhs;
+  int s = DUST_OK;
+  if ((s = devbuf_grow(dA, nn * 8)) == DUST_OK && (s = devbuf_grow(dB, nr * 8)) == DUST_OK &&
+      (s = devbuf_grow(dX, nr * 8 + 64)) == DUST_OK) {
+    cudaMemcpyAsync(dA.p, A, nn * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dB.p, B, nr * 8, cudaMemcpyHostToDevice, st);
+    if (mode == DUST_SOLVE_LU64) {
+      cudaEvent_t e0, e1, e2;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventCreate(&e2);
+      int *ipiv = nullptr, *info = nullptr;
+      DevBuf piv;
+      s = devbuf_grow(piv, (size_t)n * 4 + 64);
+      if (s == DUST_OK) {
+        ipiv = (int *)piv.p;
+        info = ipiv + n;
+        cudaEventRecord(e0, st);
+        s = lu_getrf<double>(cb, st, lu, n, (double *)dA.p, n, ipiv, info, 0);
+        cudaEventRecord(e1, st);
+        int hinfo = 0;
+        if (s == DUST_OK) {
+          cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st);
+          cudaStreamSynchronize(st);
+          if (hinfo) s = DUST_ERR_SINGULAR;
+        }
+        if (s == DUST_OK) {
+          cudaMemcpyAsync(dX.p, dB.p, nr * 8, cudaMemcpyDeviceToDevice, st);
+          s = lu_getrs<double>(cb, st, n, nrhs, (const double *)dA.p, n, ipiv, (double *)dX.p, n);
+          cudaEventRecord(e2, st);
+        }
+        if (s == DUST_OK && cudaStreamSynchronize(st) == cudaSuccess) {
+          cudaEventElapsedTime(&r.ms_factor, e0, e1);
+          cudaEventElapsedTime(&r.ms_solve, e1, e2);
+        }
+      }
+      devbuf_free(piv);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaEventDestroy(e2);
+      r.mode_used = DUST_SOLVE_LU64;
+    } else {
+      s = mixed_solve_device(cb, st, lu, w32, wrk, n, nrhs, (const double *)dA.p,
+                             (const double *)dB.p, (double *)dX.p, tol > 0 ? tol : 1e-12, 30,
+                             1, &r);
+    }
+    if (s == DUST_OK || s == DUST_ERR_NOT_CONVERGED) {
+      if (cudaMemcpyAsync(X, dX.p, nr * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        s = DUST_ERR_CUDA;
+    }
+  }
+  devbuf_free(dA);
+  devbuf_free(dB);
+  devbuf_free(dX);
+  devbuf_free(w32);
+  devbuf_free(wrk);
+  devbuf_free(lu.sync);
+  cublasDestroy(cb);
+  cudaStreamDestroy(st);
+  if (rep) *rep = r;
+  return s;
+}
+
+// Mixed / learned solves of the linsys handle (full unfactored FP64 matrix).
+__global__ void k_put_static(int n, int nst, const double *As, double *Af) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t tot = (size_t)nst * nst;
+  if (idx >= tot) return;
+  int j = (int)(idx / nst), i = (int)(idx % nst);
+  Af[(size_t)i + (size_t)j * n] = As[idx];
+}
+
+int linsys_full_matrix(dust_linsys *L, double *Af) {
+  size_t n = L->n;
+  DUST_CUDA(cudaMemcpyAsync(Af, L->A.p, n * n * 8, cudaMemcpyDeviceToDevice, L->st));
+  if (L->nst > 0) {
+    size_t tot = (size_t)L->nst * L->nst;
+    k_put_static<<<nblk(tot, 256), 256, 0, L->st>>>(L->n, L->nst, (const double *)L->As.p, Af);
+  }
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+int linsys_gmres_nn(dust_linsys *L, const double *Af, double *x, dust_solve_report *rep);
+
+int linsys_solve_iterative(dust_linsys *L, int mode, double *x_dev, dust_solve_report *rep) {
+  size_t n = L->n;
+  DUST_TRY(devbuf_grow(L->gm, n * n * 8 + 256));
+  double *Af = (double *)L->gm.p;
+  DUST_TRY(linsys_full_matrix(L, Af));
+  if (mode == DUST_SOLVE_GMRES_NN) {
+    int s = linsys_gmres_nn(L, Af, x_dev, rep);
+    if (s == DUST_OK) {
+      L->factored = true;
+      return DUST_OK;
+    }
+    if (rep) rep->fell_back = 1;
+    // plain LU remains the fallback (the step's result is then exact LU)
+    DUST_TRY(linsys_solve_lu64(L, x_dev));
+    if (rep) rep->mode_used = DUST_SOLVE_LU64;
+    return DUST_OK;
+  }
+  DevBuf wrk;
+  int s = mixed_solve_device(L->cb, L->st, L->lu, L->A32, wrk, L->n, 1, Af,
+                             (const double *)L->b.p, x_dev, 1e-14, 30, 1, rep);
+  devbuf_free(wrk);
+  L->factored = true;
+  return s;
+}

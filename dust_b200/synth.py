@@ -84,7 +84,10 @@ def ellipsoid(n_target=16384, axes=(4.0, 1.0, 0.5), seed=0):
     poles and the two polar caps are closed by triangle fans."""
     rng = np.random.default_rng(seed)
     n_v = int(round(np.sqrt(n_target / 2.0)))
-    n_u = n_target // n_v
+    # even azimuthal count: with an odd one, a cap triangle's centroid lies on
+    # the extension of the opposite fan edge, where the solid-angle formula of
+    # potential_calc_doublet divides by zero
+    n_u = (n_target // n_v) // 2 * 2
     # quads: n_u (azimuth) x (n_v - 2) latitude bands; caps: 2 * n_u triangles
     n_lat = n_v
     th = np.linspace(0.0, np.pi, n_lat + 1)  # polar angle
@@ -175,6 +178,7 @@ def rotor_blades(n_blades=3, radius=1.0, root=0.2, chord=0.1, n_span=40, n_chord
 def cylinder(n_target=6000, length=4.0, radius=0.3, center=(0.0, 0.0, -0.6)):
     """Closed cylinder along x of surface panels with triangle-fan end caps."""
     n_th = max(8, int(round(np.sqrt(n_target * 2 * np.pi * radius / length))))
+    n_th += n_th % 2  # even: see ellipsoid()
     n_x = max(2, (n_target - 2 * n_th) // n_th)
     x = np.linspace(-length / 2, length / 2, n_x + 1)
     th = np.linspace(0.0, 2 * np.pi, n_th + 1)
@@ -190,3 +194,32 @@ def cylinder(n_target=6000, length=4.0, radius=0.3, center=(0.0, 0.0, -0.6)):
     nver = np.concatenate([np.full(len(quads), 4), np.full(len(tris), 3)])
     ps = abi.PanelSet(ver, n_ver=nver, kind=np.full(ver.shape[0], abi.DUST_ELEM_SURFPAN))
     return _orient_outward(ps)
+
+
+def te_wake(panels, te_idx, offset, second=None, mag=None):
+    """One row of wake panels behind trailing-edge panels: the trailing edge
+    of panel i is the edge ver[1] -> ver[2] (chordwise-last vertices of the
+    structured grids above), extended by ``offset``.  Returns the wake
+    PanelSet and the 1-based generating-element pairs (second element 0 when
+    ``second`` is None, as for vortex-lattice trailing edges)."""
+    te_idx = np.asarray(te_idx)
+    v = panels.ver[te_idx]
+    off = np.asarray(offset, dtype=np.float64)
+    w = np.stack([v[:, 1], v[:, 1] + off, v[:, 2] + off, v[:, 2]], axis=1)
+    n = len(te_idx)
+    ps = abi.PanelSet(w, kind=np.full(n, abi.DUST_ELEM_VORTLATT),
+                      mag=np.zeros(n) if mag is None else mag)
+    ind = np.zeros((n, 2), dtype=np.int32)
+    ind[:, 0] = te_idx + 1
+    if second is not None:
+        ind[:, 1] = np.asarray(second) + 1
+    return ps, ind
+
+
+def concat_panels(*sets):
+    g = lambda name: None if all(getattr(s, name) is None for s in sets) else np.concatenate(
+        [getattr(s, name) if getattr(s, name) is not None else
+         np.zeros((s.n, 3) if name in ("ub", "uvort") else s.n) for s in sets])
+    return abi.PanelSet(np.concatenate([s.ver for s in sets]),
+                        np.concatenate([s.n_ver for s in sets]),
+                        np.concatenate([s.kind for s in sets]), g("mag"), g("ub"), g("uvort"))

@@ -1,0 +1,119 @@
+"""CPU checks of the oracle against known answers and LAPACK (no GPU).
+
+The reference has no unit-level golden vectors for this path; these tests
+pin the oracle by (a) LAPACK itself (the reference's third-party solver,
+reached here through scipy), (b) analytic identities of the influence
+kernels, (c) FMM -> direct-sum convergence.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+from scipy.linalg import lapack
+
+import oracle as O
+from dust_b200 import abi, synth
+from dust_b200.params import FmmParams
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_oracle_getrf_matches_lapack():
+    rng = np.random.default_rng(0)
+    for n in (1, 7, 64, 150):
+        A = rng.standard_normal((n, n))
+        A[0, :] *= 1e-3  # force pivoting
+        LU, piv, info = O.dgetrf(A)
+        lu_l, piv_l, info_l = lapack.dgetrf(A)
+        assert info == info_l == 0
+        assert np.array_equal(piv, piv_l + 1)  # scipy returns 0-based
+        assert np.max(np.abs(LU - lu_l)) < 1e-12 * max(1.0, np.max(np.abs(lu_l)))
+
+
+def test_oracle_getrf_singular_info():
+    A = np.array([[1.0, 2.0], [2.0, 4.0]])
+    _, _, info = O.dgetrf(A)
+    _, _, info_l = lapack.dgetrf(A)
+    assert info == info_l == 2
+
+
+def _wing_case(n_span=8, n_chord=4):
+    wing, te = synth.flat_wing(span=4.0, chord=1.0, n_span=n_span, n_chord=n_chord,
+                               alpha_deg=5.0)
+    wake, ind = synth.te_wake(wing, te, (0.3, 0.0, 0.02))
+    far, _ = synth.te_wake(wing, te, (1.0, 0.0, 0.05))
+    far.ver = far.ver + np.array([0.3, 0.0, 0.02])
+    far.mag = np.linspace(-0.1, 0.1, far.n)
+    wk = synth.concat_panels(wake, far)
+    return wing, wk, wake.n, ind
+
+
+def test_linsys_schur_sequence_equals_full_lu():
+    """solve_linsys' static/moving block LU (dlaswp, dtrsm x2, dgemm, dgetrf,
+    dgetrs) gives the solution of the full system."""
+    prm = FmmParams(u_inf=(1.0, 0.0, 0.0), rankine_rad=0.1)
+    wing, wk, n_impl, ind = _wing_case()
+    rng = np.random.default_rng(1)
+    wing.uvort = rng.standard_normal((wing.n, 3)) * 0.05
+    n = wing.n
+    nst = n // 2
+    _, _, res_blk = O.linsys_run(prm, n, nst, wing, wing, (wk, n_impl, ind), (wk, n_impl, ind))
+    A0, b0, res0 = O.linsys_run(prm, n, 0, wing, wing, (wk, n_impl, ind), (wk, n_impl, ind))
+    assert rel(res0, np.linalg.solve(A0, b0)) < 1e-12
+    assert rel(res_blk, res0) < 1e-10
+
+
+def test_closed_body_row_sums_are_4pi():
+    """Dirichlet rows of a closed surface: sum_j A(i,j) = 4 pi (solid angle
+    of the whole body seen from its surface, self term 2 pi)."""
+    body = synth.ellipsoid(n_target=400, axes=(2.0, 1.0, 0.7), seed=3)
+    prm = FmmParams(u_inf=(1.0, 0.0, 0.0))
+    n = body.n
+    A, b, res = O.linsys_run(prm, n, 0, body, body, (abi.empty_panels(), 0, None),
+                             (abi.empty_panels(), 0, None))
+    rs = A.sum(axis=1)
+    assert np.max(np.abs(rs - 4 * np.pi)) < 0.05 * 4 * np.pi
+    assert abs(np.mean(rs) - 4 * np.pi) < 0.01 * 4 * np.pi
+
+
+def test_source_potential_far_near_consistency():
+    """The near-field source formula approaches the far-field A/r as the
+    point leaves the 10*edge threshold."""
+    pan = abi.PanelSet(np.array([[[0, 0, 0], [0.1, 0, 0], [0.1, 0.1, 0], [0, 0.1, 0]]]),
+                       kind=np.array([abi.DUST_ELEM_SURFPAN]))
+    prm = FmmParams()
+    pos = np.array([0.05, 0.05, 0.99])  # just inside 10 * edge
+    dou = O.potential_doublet(prm, pan, 0, pos)
+    near = O.potential_source(prm, pan, 0, dou, pos)
+    far = 0.01 / np.linalg.norm(pos - np.array([0.05, 0.05, 0.0]))
+    assert abs(near - far) / far < 1e-3
+
+
+def test_fmm_oracle_converges_and_factorial_wrap():
+    cen, dir_, mag = synth.ring_particles(1800, 200, seed=1)
+    rv = np.full(len(mag), 0.02)
+    base = dict(box_length=4.0, origin=(-2, -2, -2), n_octree_levels=4, min_octree_part=5,
+                rankine_rad=0.02)
+    dv, _, _ = O.direct_particles(FmmParams(**base), cen, dir_, mag, rv)
+    errs = {}
+    for p in (2, 4, 8):
+        v, _, _, _ = O.fmm_apply(FmmParams(multipole_degree=p, **base), cen, dir_, mag, rv)
+        errs[p] = rel(v, dv)
+    assert errs[2] > errs[4] > errs[8]
+    # the reference's 32-bit factorials wrap for degree >= 13 (p >= 7)
+    O.set_factorial_wrap(1)
+    try:
+        vw, _, _, _ = O.fmm_apply(FmmParams(multipole_degree=8, **base), cen, dir_, mag, rv)
+        v4w, _, _, _ = O.fmm_apply(FmmParams(multipole_degree=4, **base), cen, dir_, mag, rv)
+    finally:
+        O.set_factorial_wrap(0)
+    v4, _, _, _ = O.fmm_apply(FmmParams(multipole_degree=4, **base), cen, dir_, mag, rv)
+    assert np.array_equal(v4w, v4)  # no wrap below degree 13
+    assert rel(vw, dv) > 3 * errs[8]
+
+
+def test_oracle_fmm_out_of_box():
+    with pytest.raises(RuntimeError):
+        O.fmm_apply(FmmParams(box_length=1.0), np.array([[2.0, 0.5, 0.5]]),
+                    np.array([[0, 0, 1.0]]), np.array([1.0]), np.array([0.1]))
