@@ -429,3 +429,38 @@ extern "C" int dust_panels_geometry(const dust_panels *pan, double *cen, double 
   DUST_CUDA(cudaStreamSynchronize(st));
   return DUST_OK;
 }
+
+extern "C" int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts, const double *pts,
+                                        int n, const double *cen, const double *dir,
+                                        const double *mag, const double *r_vortex,
+                                        const dust_lines *end_vort, double *uvort, void *stream) {
+  if (!prm || n_pts < 0 || n < 0) return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  static thread_local Scratch s;
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), false,
+                             s.raw, s.geo, e, st));
+  DUST_TRY(points_uvort_device(prm, n_pts, pts, n, cen, dir, mag, r_vortex, e, uvort, st));
+  return DUST_OK;
+}
+
+__global__ void k_centres(PanRaw r, double *cen) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= r.n) return;
+  int nv = r.n_ver ? r.n_ver[j] : 4;
+  for (int d = 0; d < 3; ++d) {
+    double s = 0.0;
+    for (int v = 0; v < nv; ++v) s += r.ver[12 * (size_t)j + 3 * v + d];
+    cen[3 * (size_t)j + d] = s / (double)nv;
+  }
+}
+
+extern "C" int dust_panels_centres_device(const dust_panels *pan, double *cen, void *stream) {
+  if (!pan || pan->n < 0 || (pan->n > 0 && (!pan->ver || !cen))) return DUST_ERR_BAD_ARG;
+  if (pan->n == 0) return DUST_OK;
+  PanRaw r{pan->n, pan->n_ver, pan->kind, pan->ver, pan->mag, pan->ub, pan->uvort};
+  k_centres<<<nblk(pan->n, 128), 128, 0, (cudaStream_t)stream>>>(r, cen);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}

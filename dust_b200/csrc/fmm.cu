@@ -370,6 +370,7 @@ __global__ void k_p2m(FmmDev d) {
   double c[3];
   cell_center(d.G, l, ci_, cj, ck, c);
   uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
+  if (hi == lo) return;  // empty leaf: a = 0 (block zeroed before the pass)
   int m = threadIdx.x;
   int mi = 0, mj = 0, mk = 0;
   if (m < d.nm) mono_exp(m, mi, mj, mk);
@@ -462,6 +463,9 @@ __global__ void k_m2l(FmmDev d, int l, uint32_t act_lo) {
   double *s_a = sh;  // 3*nm
   uint32_t ci = act_lo + blockIdx.x;
   uint32_t key = d.act_key[ci];
+  // an empty target cell is a leaf without particles: its local expansion
+  // is never evaluated (and it has no children to pass it to)
+  if (cell_hi(d.G, d.cstart, l, key) == cell_lo(d.G, d.cstart, l, key)) return;
   int i, j, k;
   cart_of_key(d.G, l, key, i, j, k);
   const int nm = d.nm;
@@ -484,6 +488,8 @@ __global__ void k_m2l(FmmDev d, int l, uint32_t act_lo) {
       if (abs(si - i) <= 1 && abs(sj - j) <= 1 && abs(sk - k) <= 1) continue;
       uint32_t skey = key_of(d.G, l, si, sj, sk);
       if (!(d.flags[lo_l + skey] & FL_ACTIVE)) continue;
+      // an empty source has a = 0: adding it changes nothing
+      if (cell_hi(d.G, d.cstart, l, skey) == cell_lo(d.G, d.cstart, l, skey)) continue;
       int q = atomicAdd(&s_n, 1);
       s_src[q] = (int)d.cidx[lo_l + skey];
       s_tab[q] = (si - i + Lx) + (2 * Lx + 1) * ((sj - j + Ly) + (2 * Ly + 1) * (sk - k + Lz));
@@ -492,6 +498,7 @@ __global__ void k_m2l(FmmDev d, int l, uint32_t act_lo) {
   __syncthreads();
   int nsrc = s_n;
   int nlev1 = (l == 1) ? (int)d.G.ncell[1] : 0;
+  if (threadIdx.x == 0 && d.counters) atomicAdd((unsigned long long *)d.counters, (unsigned long long)nsrc);
   int mo = threadIdx.x;  // output monomial
   int oi = 0, oj = 0, ok = 0;
   if (mo < nout) mono_exp(mo, oi, oj, ok);
@@ -509,6 +516,7 @@ __global__ void k_m2l(FmmDev d, int l, uint32_t act_lo) {
       cart_of_key(d.G, 1, sk1, si, sj, sk);
       if (abs(si - i) <= 1 && abs(sj - j) <= 1 && abs(sk - k) <= 1) continue;
       if (!(d.flags[lo_l + sk1] & FL_ACTIVE)) continue;
+      if (cell_hi(d.G, d.cstart, 1, sk1) == cell_lo(d.G, d.cstart, 1, sk1)) continue;
       src = (int)d.cidx[lo_l + sk1];
       tab = (si - i + Lx) + (2 * Lx + 1) * ((sj - j + Ly) + (2 * Ly + 1) * (sk - k + Lz));
     }
@@ -670,10 +678,23 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
   double cc[3];
   cell_center(d.G, l, ci_, cj, ck, cc);
   const uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
+  if (hi == lo) return;
   const int nm = d.nm, nm1 = d.nm1;
   for (int t = tid; t < 3 * nm; t += P2P_T) s_loc[t] = d.B[(size_t)ci * 3 * nm + t];
   if (VS)
     for (int t = tid; t < 3 * nm1; t += P2P_T) s_loc[3 * nm + t] = d.Gx[(size_t)ci * 3 * nm1 + t];
+  // monomial tables: exponents (packed) and, for the gradient, the indices
+  // of m + e_r in the degree-(p+1) ordering
+  int *s_mexp = (int *)(s_loc + 3 * (nm + nm1));
+  int *s_mgr = s_mexp + nm;
+  for (int m = tid; m < nm; m += P2P_T) {
+    int mi, mj, mk;
+    mono_exp(m, mi, mj, mk);
+    s_mexp[m] = mi | (mj << 8) | (mk << 16);
+    s_mgr[3 * m + 0] = mono_idx(mi + 1, mj, mk);
+    s_mgr[3 * m + 1] = mono_idx(mi, mj + 1, mk);
+    s_mgr[3 * m + 2] = mono_idx(mi, mj, mk + 1);
+  }
   // near-field source ranges: 26 same-level neighbours (active), the leaf
   // neighbours (leaves among the neighbours of every ancestor), own leaf.
   if (warp == 0) {
@@ -723,6 +744,8 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
   const uint32_t S = s_rcum[nr];
   const size_t n = d.n;
   const int nt = (int)(hi - lo);
+  if (tid == 0 && d.counters)
+    atomicAdd((unsigned long long *)d.counters + 1, (unsigned long long)nt * (S - 1));
   const double k4pi = 1.0 / (4.0 * DUST_PI);
 
   double ave_ros = 0.0;
@@ -768,21 +791,34 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
     for (int e = 0; e < 3; ++e) A.v[e] = A.s[e] = A.r[e] = A.f[e] = 0.0;
     double lv[3] = {0, 0, 0}, ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
     if (act && grp == 0) {
-      // L2P (mod_octree.f90:1171-1212)
+      // L2P (mod_octree.f90:1171-1212): vel from b (degree p), grad(r,:)
+      // = sum_m (m_r+1) g(m+e_r) (x-c)^m
       double x = tp[0] - cc[0], y = tp[1] - cc[1], z = tp[2] - cc[2];
+      double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
+      px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+      for (int e = 1; e <= DUST_MAXP; ++e) {
+        px[e] = px[e - 1] * x;
+        py[e] = py[e - 1] * y;
+        pz[e] = pz[e - 1] * z;
+      }
       double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int m = 0; m < nm; ++m) {
-        int mi, mj, mk;
-        mono_exp(m, mi, mj, mk);
-        double pr = ipow_d(x, mi) * ipow_d(y, mj) * ipow_d(z, mk);
+        int ex = s_mexp[m];
+        int mi = ex & 255, mj = (ex >> 8) & 255, mk = ex >> 16;
+        double pr = px[mi] * py[mj] * pz[mk];
         for (int e = 0; e < 3; ++e) lv[e] += s_loc[3 * m + e] * pr;
         if (VS) {
-          int mr[3] = {mono_idx(mi + 1, mj, mk), mono_idx(mi, mj + 1, mk),
-                       mono_idx(mi, mj, mk + 1)};
-          double fr[3] = {(double)(mi + 1), (double)(mj + 1), (double)(mk + 1)};
-          for (int r = 0; r < 3; ++r)
-            for (int e = 0; e < 3; ++e)
-              g[r + 3 * e] += fr[r] * s_loc[3 * nm + 3 * mr[r] + e] * pr;
+          const double *gl = s_loc + 3 * nm;
+          double f0 = (double)(mi + 1) * pr, f1 = (double)(mj + 1) * pr,
+                 f2 = (double)(mk + 1) * pr;
+          const double *g0 = gl + 3 * s_mgr[3 * m], *g1 = gl + 3 * s_mgr[3 * m + 1],
+                       *g2 = gl + 3 * s_mgr[3 * m + 2];
+          for (int e = 0; e < 3; ++e) {
+            g[0 + 3 * e] += f0 * g0[e];
+            g[1 + 3 * e] += f1 * g1[e];
+            g[2 + 3 * e] += f2 * g2[e];
+          }
         }
       }
       if (VS) {
@@ -1034,7 +1070,10 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   o->dev = d;
   if (o->timing) cudaEventRecord(o->ev[1], st);
   // upward pass
-  DUST_CUDA(cudaMemsetAsync(d.B, 0, (size_t)nact * 3 * (o->nm + o->nm1) * 8, st));
+  DUST_CUDA(cudaMemsetAsync(d.A, 0, (size_t)nact * 3 * (2 * o->nm + o->nm1) * 8, st));
+  d.counters = (int64_t *)(small + 48);
+  DUST_CUDA(cudaMemsetAsync(d.counters, 0, 4 * sizeof(int64_t), st));
+  o->dev = d;
   if (o->n_leaves > 0) {
     int thr = std::max(64, (o->nm + 31) / 32 * 32);
     k_p2m<<<(unsigned)o->n_leaves, thr, 6 * 64 * 8, st>>>(d);
@@ -1059,7 +1098,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   if (o->timing) cudaEventRecord(o->ev[3], st);
   // leaves: L2P + P2P
   if (o->n_leaves > 0) {
-    size_t shl = (size_t)3 * (o->nm + o->nm1) * 8;
+    size_t shl = (size_t)3 * (o->nm + o->nm1) * 8 + (size_t)4 * o->nm * 4;
     bool vs = d.use_vs, df = d.use_df, vd = d.use_vd, tv = o->prm.turbulent_viscosity != 0;
 #define LAUNCH_P2P(A, B, C, D) \
   k_p2p<A, B, C, D><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d)
@@ -1091,6 +1130,12 @@ int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, doub
 void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
   dust_fmm_stats &s = o->stats;
   memset(&s, 0, sizeof(s));
+  if (o->dev.counters) {
+    int64_t c[4] = {0, 0, 0, 0};
+    cudaMemcpy(c, o->dev.counters, sizeof(c), cudaMemcpyDeviceToHost);
+    s.n_m2l_pairs = c[0];
+    s.n_p2p_pairs = c[1];
+  }
   s.n_particles = n;
   s.n_leaves = o->n_leaves;
   s.n_active_cells = o->n_active;

@@ -35,6 +35,7 @@ struct FmmDev {
   const uint32_t *leaf_ci;
   double *A, *B, *Gx;  // multipole a, local b (deg p), local g (deg p+1)
   double *out;         // sorted-order vel(3), stretch(3), rotu(3), SoA
+  int64_t *counters;   // [0] M2L pairs, [1] P2P pairs
   double inv_fact[224];
 };
 

@@ -152,11 +152,12 @@ __global__ void k_add_wake(const PanelGeo *el, const PanelGeo *wk, int nwake, in
 }
 
 // ------------------------------------------------------------------- host
-static int load_geometry(dust_linsys *L, const dust_panels *elems, const dust_wake_rows *wake) {
+static int load_geometry(dust_linsys *L, const dust_panels *elems, const dust_wake_rows *wake,
+                         bool host = true) {
   if (!elems || elems->n != L->n) return DUST_ERR_BAD_ARG;
   ElemDev e;
   DUST_TRY(elem_build_device(elems, wake ? &wake->pan : nullptr, nullptr, L->prm.u_inf, L->rp,
-                             true, L->raw, L->geo, e, L->st));
+                             host, L->raw, L->geo, e, L->st));
   L->el = e.body;
   L->wk = e.wake;
   L->nwake = e.nwake;
@@ -165,7 +166,8 @@ static int load_geometry(dust_linsys *L, const dust_panels *elems, const dust_wa
   if (L->n_impl > 0) {
     DUST_TRY(devbuf_grow(L->impl, (size_t)L->n_impl * 2 * sizeof(int)));
     DUST_CUDA(cudaMemcpyAsync(L->impl.p, wake->impl_ind, (size_t)L->n_impl * 2 * sizeof(int),
-                              cudaMemcpyHostToDevice, L->st));
+                              host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                              L->st));
   }
   return DUST_OK;
 }
@@ -259,10 +261,10 @@ extern "C" int dust_linsys_destroy(dust_linsys *L) {
   return DUST_OK;
 }
 
-extern "C" int dust_linsys_assemble(dust_linsys *L, const dust_panels *elems,
-                                    const dust_wake_rows *wake) {
+static int assemble(dust_linsys *L, const dust_panels *elems, const dust_wake_rows *wake,
+                    bool host) {
   if (!L) return DUST_ERR_BAD_ARG;
-  DUST_TRY(load_geometry(L, elems, wake));
+  DUST_TRY(load_geometry(L, elems, wake, host));
   const int n = L->n, nst = L->nst;
   DUST_CUDA(cudaMemsetAsync(L->b.p, 0, (size_t)n * 8, L->st));
   // build_row: static rows get the moving columns, moving rows all columns
@@ -279,6 +281,15 @@ extern "C" int dust_linsys_assemble(dust_linsys *L, const dust_panels *elems,
   L->factored = false;
   L->assembled = true;
   return DUST_OK;
+}
+
+extern "C" int dust_linsys_assemble(dust_linsys *L, const dust_panels *elems,
+                                    const dust_wake_rows *wake) {
+  return assemble(L, elems, wake, true);
+}
+extern "C" int dust_linsys_assemble_device(dust_linsys *L, const dust_panels *elems,
+                                           const dust_wake_rows *wake) {
+  return assemble(L, elems, wake, false);
 }
 
 extern "C" int dust_linsys_get_system(dust_linsys *L, double *A, double *b) {
@@ -340,8 +351,7 @@ void linsys_shift_pivots(cudaStream_t st, int *P, int n, int off) {
   if (n > 0) k_shift<<<nblk(n, 128), 128, 0, st>>>(P, n, off);
 }
 
-extern "C" int dust_linsys_solve(dust_linsys *L, int mode, double *res,
-                                 dust_solve_report *rep) {
+static int solve(dust_linsys *L, int mode, double *res, dust_solve_report *rep, bool host) {
   if (!L || !res || !L->assembled) return DUST_ERR_BAD_ARG;
   if (L->factored) return DUST_ERR_BAD_ARG;  // assemble before every solve
   DUST_TRY(devbuf_grow(L->work, (size_t)L->n * 8 * 8));
@@ -363,7 +373,9 @@ extern "C" int dust_linsys_solve(dust_linsys *L, int mode, double *res,
   }
   cudaEventRecord(e1, L->st);
   if (st == DUST_OK) {
-    if (cudaMemcpyAsync(res, x, (size_t)L->n * 8, cudaMemcpyDeviceToHost, L->st) != cudaSuccess)
+    if (cudaMemcpyAsync(res, x, (size_t)L->n * 8,
+                        host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                        L->st) != cudaSuccess)
       st = DUST_ERR_CUDA;
     if (cudaStreamSynchronize(L->st) != cudaSuccess) st = DUST_ERR_CUDA;
     cudaEventElapsedTime(&r.ms_solve, e0, e1);
@@ -372,4 +384,13 @@ extern "C" int dust_linsys_solve(dust_linsys *L, int mode, double *res,
   cudaEventDestroy(e1);
   if (rep) *rep = r;
   return st;
+}
+
+extern "C" int dust_linsys_solve(dust_linsys *L, int mode, double *res,
+                                 dust_solve_report *rep) {
+  return solve(L, mode, res, rep, true);
+}
+extern "C" int dust_linsys_solve_device(dust_linsys *L, int mode, double *res,
+                                        dust_solve_report *rep) {
+  return solve(L, mode, res, rep, false);
 }

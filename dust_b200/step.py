@@ -1,0 +1,155 @@
+"""One aerodynamic timestep of the hot path, in the reference's order.
+
+The reference's time loop (src/dust.f90:510-1160) runs, per step:
+prepare_wake (sort_particles + calculate_multipole, mod_wake.f90:797-801),
+assemble_linsys (uvort by direct sum over particles + end vortices, rows,
+wake terms; dust.f90:620), solve_linsys (dust.f90:647-649) and
+update_wake -> apply_multipole (mod_wake.f90:1115-1118).  ``Stepper`` runs
+the same sequence on the GPU through the C ABI:
+
+  1. uvort at every implicit element centre  (dust_points_uvort[_device])
+  2. dust_linsys_assemble[_device]
+  3. dust_linsys_solve[_device]              (doublet intensities)
+  4. wake bookkeeping: implicit wake panel mag = mag(ind1) - mag(ind2)
+     (update_wake, mod_wake.f90:881-889)
+  5. dust_fmm_apply[_device]                 (particle velocity, stretching,
+                                              div-filter curl: tree build,
+                                              multipoles, L2P, P2P, elements)
+
+Two drivers: ``HostStepper`` takes host (pinned) arrays and lets the library
+copy them every step (end-to-end); ``DeviceStepper`` keeps everything in HBM
+(torch tensors as plumbing) and calls the *_device entry points.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import check, lib
+from .linsys import Linsys
+from .octree import Octree
+
+
+class HostStepper:
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64):
+        self.case = case
+        self.params = params
+        self.mode = mode
+        c = case
+        self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
+        self.oc = Octree(params)
+        self.ind = c.impl_ind.astype(np.int64) - 1
+
+    def step(self):
+        """Returns (res, vel, stretch, rotu) as host arrays."""
+        c, p = self.case, self.params
+        cen_el = c.elems.ver.mean(axis=1)  # overwritten below for triangles
+        nv = c.elems.n_ver
+        tri = nv == 3
+        if tri.any():
+            cen_el[tri] = c.elems.ver[tri, :3].mean(axis=1)
+        ps = p.struct()
+        evs = c.end_vort.struct()
+        uv = np.empty((c.rank, 3))
+        cen_el = np.ascontiguousarray(cen_el)
+        check(lib().dust_points_uvort(C.byref(ps), c.rank, abi.dptr(cen_el), c.mag.shape[0],
+                                      abi.dptr(c.cen), abi.dptr(c.dir), abi.dptr(c.mag),
+                                      abi.dptr(c.r_vortex), C.byref(evs), abi.dptr(uv)),
+              "dust_points_uvort")
+        c.elems.uvort = uv
+        self.ls.assemble_linsys(c.elems, c.wake, c.n_impl, c.impl_ind)
+        res, rep = self.ls.solve_linsys(self.mode)
+        self.last_report = rep
+        c.elems.mag = res
+        m2 = np.where(self.ind[:, 1] >= 0, res[np.maximum(self.ind[:, 1], 0)], 0.0)
+        c.wake.mag = res[self.ind[:, 0]] - m2
+        els = abi.elements_struct(c.elems, c.wake, c.end_vort)
+        vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els)
+        return res, vel, st, ro
+
+
+class DeviceStepper:
+    """All per-step inputs resident in HBM; library calls on device pointers."""
+
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda"):
+        import torch
+        self.torch = torch
+        self.case = case
+        self.params = params
+        self.mode = mode
+        c = case
+        dev = torch.device(device)
+        T = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt,
+                                                        device=dev)
+        self.cen = T(c.cen)
+        self.dir = T(c.dir)
+        self.mag = T(c.mag)
+        self.rv = T(c.r_vortex)
+        self.n = c.mag.shape[0]
+        self.ever = T(c.elems.ver)
+        self.env = T(c.elems.n_ver, torch.int32)
+        self.ekind = T(c.elems.kind, torch.int32)
+        self.eub = T(c.elems.ub)
+        self.euv = torch.zeros((c.rank, 3), dtype=torch.float64, device=dev)
+        self.emag = torch.zeros(c.rank, dtype=torch.float64, device=dev)
+        self.ecen = torch.zeros((c.rank, 3), dtype=torch.float64, device=dev)
+        self.wver = T(c.wake.ver)
+        self.wnv = T(c.wake.n_ver, torch.int32)
+        self.wkind = T(c.wake.kind, torch.int32)
+        self.wmag = torch.zeros(c.wake.n, dtype=torch.float64, device=dev)
+        self.impl = T(c.impl_ind, torch.int32)
+        ind = c.impl_ind.astype(np.int64) - 1
+        self.i1 = T(ind[:, 0], torch.int64)
+        self.i2 = T(np.maximum(ind[:, 1], 0), torch.int64)
+        self.has2 = T((ind[:, 1] >= 0).astype(np.float64))
+        self.lver = T(c.end_vort.ver)
+        self.lmag = T(c.end_vort.mag)
+        self.vel = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
+        self.str = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
+        self.rot = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
+        self.res = torch.empty(c.rank, dtype=torch.float64, device=dev)
+        self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
+        self.oc = Octree(params)
+        self._ps = params.struct()
+
+    @staticmethod
+    def _p(t, ctype=C.c_double):
+        return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))
+
+    def step(self):
+        torch = self.torch
+        c = self.case
+        P = self._p
+        stream = torch.cuda.current_stream().cuda_stream
+        el = abi.Panels(c.rank, P(self.env, C.c_int), P(self.ekind, C.c_int), P(self.ever),
+                        P(self.emag), P(self.eub), P(self.euv))
+        check(lib().dust_panels_centres_device(C.byref(el), P(self.ecen), C.c_void_p(stream)),
+              "dust_panels_centres_device")
+        lines = abi.Lines(c.end_vort.n, P(self.lver), P(self.lmag))
+        check(lib().dust_points_uvort_device(C.byref(self._ps), c.rank, P(self.ecen), self.n,
+                                             P(self.cen), P(self.dir), P(self.mag), P(self.rv),
+                                             C.byref(lines), P(self.euv), C.c_void_p(stream)),
+              "dust_points_uvort_device")
+        torch.cuda.current_stream().synchronize()
+        wk = abi.WakeRows(abi.Panels(c.wake.n, P(self.wnv, C.c_int), P(self.wkind, C.c_int),
+                                     P(self.wver), P(self.wmag), abi._dp(), abi._dp()),
+                          c.n_impl, P(self.impl, C.c_int))
+        check(lib().dust_linsys_assemble_device(self.ls._h, C.byref(el), C.byref(wk)),
+              "dust_linsys_assemble_device")
+        rep = abi.SolveReport()
+        check(lib().dust_linsys_solve_device(self.ls._h, int(self.mode), P(self.res),
+                                             C.byref(rep)), "dust_linsys_solve_device")
+        self.last_report = {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+        # element strengths and implicit wake panels (update_wake :881-889)
+        self.emag.copy_(self.res)
+        self.wmag.copy_(self.res[self.i1] - self.res[self.i2] * self.has2)
+        body = abi.Panels(c.rank, P(self.env, C.c_int), P(self.ekind, C.c_int), P(self.ever),
+                          P(self.emag), P(self.eub), P(self.euv))
+        wake = abi.Panels(c.wake.n, P(self.wnv, C.c_int), P(self.wkind, C.c_int),
+                          P(self.wver), P(self.wmag), abi._dp(), abi._dp())
+        els = abi.Elements(body, wake, lines)
+        check(lib().dust_fmm_apply_device(self.oc._h, self.n, P(self.cen), P(self.dir),
+                                          P(self.mag), P(self.rv), C.byref(els), P(self.vel),
+                                          P(self.str), P(self.rot), C.c_void_p(stream), 0),
+              "dust_fmm_apply_device")
+        return self.res

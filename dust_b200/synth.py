@@ -223,3 +223,204 @@ def concat_panels(*sets):
     return abi.PanelSet(np.concatenate([s.ver for s in sets]),
                         np.concatenate([s.n_ver for s in sets]),
                         np.concatenate([s.kind for s in sets]), g("mag"), g("ub"), g("uvort"))
+
+
+def naca_wing(span=6.0, chord=1.0, n_span=98, n_around=120, thick=0.12, alpha_deg=5.0,
+              center=(0.0, 0.0, 0.0)):
+    """Closed NACA 00xx wing of surface panels: n_span x n_around quads
+    (cosine chordwise spacing, sharp trailing edge) plus triangle-fan tip caps
+    (2 * n_around triangles).  Returns (PanelSet, te_upper, te_lower, dy):
+    the upper/lower trailing-edge panel indices and stripe widths."""
+    nh = n_around // 2
+    beta = np.linspace(0.0, np.pi, nh + 1)
+    xc = 0.5 * (1.0 - np.cos(beta))  # 0 (LE) .. 1 (TE)
+    yt = 5 * thick * (0.2969 * np.sqrt(xc) - 0.1260 * xc - 0.3516 * xc ** 2 +
+                      0.2843 * xc ** 3 - 0.1036 * xc ** 4)
+    # closed loop TE -> upper -> LE -> lower -> TE (n_around + 1 points)
+    xs = np.concatenate([xc[::-1], xc[1:]]) * chord
+    zs = np.concatenate([yt[::-1], -yt[1:]]) * chord
+    y = np.linspace(-span / 2, span / 2, n_span + 1)
+    X = np.broadcast_to(xs[:, None], (len(xs), len(y)))
+    Z = np.broadcast_to(zs[:, None], (len(xs), len(y)))
+    Y = np.broadcast_to(y[None, :], (len(xs), len(y)))
+    P = np.stack([X, Y, Z], axis=2)
+    a = np.deg2rad(alpha_deg)
+    R = np.array([[np.cos(a), 0, np.sin(a)], [0, 1, 0], [-np.sin(a), 0, np.cos(a)]])
+    P = P @ R.T + np.asarray(center)
+    # quads (i around, j span); around runs TE->upper->LE->lower so with
+    # vertex order (i,j),(i,j+1),(i+1,j+1),(i+1,j) the normals point outward
+    q = np.stack([P[:-1, :-1], P[:-1, 1:], P[1:, 1:], P[1:, :-1]], axis=2)
+    quads = q.reshape(-1, 4, 3)
+    # tip caps: fans around the section centroid at each tip
+    tris = []
+    for jj, sgn in ((0, -1), (len(y) - 1, 1)):
+        c = P[:-1, jj].mean(axis=0)
+        for i in range(n_around):
+            a0, a1 = P[i, jj], P[i + 1, jj]
+            t = [c, a1, a0] if sgn < 0 else [c, a0, a1]
+            tris.append(t + [np.zeros(3)])
+    tris = np.asarray(tris)
+    ver = np.concatenate([quads, tris], axis=0)
+    nver = np.concatenate([np.full(len(quads), 4), np.full(len(tris), 3)])
+    ps = abi.PanelSet(ver, n_ver=nver, kind=np.full(len(ver), abi.DUST_ELEM_SURFPAN))
+    # panel (i, j) index = i * n_span + j; TE upper: i = 0, TE lower: i = n_around-1
+    te_up = np.arange(0, n_span)
+    te_lo = (n_around - 1) * n_span + np.arange(0, n_span)
+    dy = np.diff(y)
+    return ps, te_up, te_lo, dy
+
+
+def _rotz(v, ang):
+    c, s = np.cos(ang), np.sin(ang)
+    out = v.copy()
+    out[..., 0] = c * v[..., 0] - s * v[..., 1]
+    out[..., 1] = s * v[..., 0] + c * v[..., 1]
+    return out
+
+
+class FullStepCase:
+    """Two counter-rotating 3-blade vortex-lattice rotors (radius 1, 40 x 8
+    panels per blade) above the tips of a 12,000-panel surface-panel wing,
+    with a particle wake (rotor helices + wing sheet) of ``n_particles``.
+    Element order: wing (static) first, then the rotors (moving)."""
+
+    def __init__(self, n_particles=2_000_000, seed=0, n_span_blade=40, n_chord_blade=8,
+                 wing_span=98, wing_around=120, omega=60.0, u_inf=(5.0, 0.0, 0.0)):
+        rng = np.random.default_rng(seed)
+        self.u_inf = np.asarray(u_inf, dtype=np.float64)
+        self.omega = omega
+        self.dt = 2 * np.pi / omega / 72.0
+        wing, te_up, te_lo, dy = naca_wing(n_span=wing_span, n_around=wing_around)
+        self.wing = wing
+        self.centers = [np.array([0.3, -3.2, 1.0]), np.array([0.3, 3.2, 1.0])]
+        self.spins = [1, -1]
+        rotors, rtes = [], []
+        base = wing.n
+        for c, sp in zip(self.centers, self.spins):
+            r, te = rotor_blades(n_blades=3, radius=1.0, root=0.15, chord=0.08,
+                                 n_span=n_span_blade, n_chord=n_chord_blade, center=c,
+                                 spin=sp)
+            rotors.append(r)
+            rtes.append(te + base)
+            base += r.n
+        self.nstatic = wing.n
+        self.rotor_ver0 = np.concatenate([r.ver for r in rotors])
+        self.elems = concat_panels(wing, *rotors)
+        self.rank = self.elems.n
+        self.rotor_slices = [slice(wing.n, wing.n + rotors[0].n),
+                             slice(wing.n + rotors[0].n, self.rank)]
+        # implicit wake row: wing TE (upper, lower pair) and blade TEs
+        off_w = self.u_inf * self.dt * 0.3 / max(np.linalg.norm(self.u_inf), 1e-9) * 5.0
+        ww, wind = te_wake(wing, te_up, off_w, second=te_lo)
+        self.wing_te = (te_up, te_lo, dy)
+        self.rotor_te = rtes
+        wr = []
+        winds = [wind]
+        for k, te in enumerate(rtes):
+            v = self.elems.ver[te]
+            r = v.mean(axis=1) - self.centers[k]
+            tang = np.cross([0, 0, self.spins[k] * self.omega], r)
+            offs = -tang * self.dt * 0.3
+            w = np.stack([v[:, 1], v[:, 1] + offs, v[:, 2] + offs, v[:, 2]], axis=1)
+            wr.append(abi.PanelSet(w, kind=np.full(len(te), abi.DUST_ELEM_VORTLATT)))
+            ind = np.zeros((len(te), 2), dtype=np.int32)
+            ind[:, 0] = te + 1
+            winds.append(ind)
+        self.wake = concat_panels(ww, *wr)
+        self.wake.mag = np.zeros(self.wake.n)
+        self.n_impl = self.wake.n
+        self.impl_ind = np.ascontiguousarray(np.concatenate(winds).astype(np.int32))
+        # end vortices: downstream edges of the implicit wake panels
+        self.end_vort = abi.LineSet(np.stack([self.wake.ver[:, 1], self.wake.ver[:, 2]], axis=1),
+                                    rng.standard_normal(self.wake.n) * 0.05)
+        self._particles(n_particles, rng)
+        self.set_angle(0.0)
+
+    def _particles(self, n, rng):
+        n_w = n // 5
+        n_r = (n - n_w) // 2
+        cen, dirs = [], []
+        for k, (c, sp) in enumerate(zip(self.centers, self.spins)):
+            m = n_r if k == 0 else n - n_w - n_r
+            age = rng.uniform(0.0, 1.5, m)
+            r = np.where(rng.random(m) < 0.5, 0.92 + 0.03 * rng.standard_normal(m),
+                         rng.uniform(0.2, 0.95, m))
+            blade = rng.integers(0, 3, m)
+            psi = sp * (2 * np.pi * blade / 3 - self.omega * age)
+            contr = 1.0 - 0.25 * np.minimum(age, 1.0)
+            x = c[0] + r * contr * np.cos(psi) + self.u_inf[0] * age
+            y = c[1] + r * contr * np.sin(psi)
+            z = c[2] - 2.5 * age + 0.01 * rng.standard_normal(m)
+            cen.append(np.stack([x, y, z], axis=1))
+            d = np.stack([-np.sin(psi) * sp, np.cos(psi) * sp, np.zeros(m)], axis=1)
+            dirs.append(d)
+        age = rng.uniform(0.0, 1.5, n_w)
+        yy = rng.uniform(-3.0, 3.0, n_w)
+        xw = 1.0 + self.u_inf[0] * age
+        zw = 0.02 * rng.standard_normal(n_w) - 0.1 * age
+        cen.append(np.stack([xw, yy, zw], axis=1))
+        dirs.append(np.tile([0.0, 1.0, 0.0], (n_w, 1)) * np.sign(yy)[:, None])
+        self.cen = np.ascontiguousarray(np.concatenate(cen))
+        d = np.concatenate(dirs)
+        self.dir = np.ascontiguousarray(d / np.linalg.norm(d, axis=1)[:, None])
+        self.mag = np.abs(1e-3 + 2e-4 * rng.standard_normal(n))
+        self.r_vortex = np.full(n, 0.04)
+        lo = self.cen.min(axis=0) - 0.5
+        hi = self.cen.max(axis=0) + 0.5
+        lo = np.minimum(lo, self.elems.ver.reshape(-1, 3).min(axis=0) - 0.5)
+        hi = np.maximum(hi, self.elems.ver.reshape(-1, 3).max(axis=0) + 0.5)
+        self.box_length = 2.0
+        self.n_box = tuple(int(np.ceil((hi[d] - lo[d]) / self.box_length)) for d in range(3))
+        self.origin = tuple(lo)
+
+    def set_angle(self, ang):
+        """Rotate the rotors to azimuth ``ang`` and refresh the body velocity."""
+        v = self.rotor_ver0.copy().reshape(-1, 4, 3)
+        ub = np.zeros((self.rank, 3))
+        base = self.nstatic
+        for k, (c, sp) in enumerate(zip(self.centers, self.spins)):
+            sl = self.rotor_slices[k]
+            nk = sl.stop - sl.start
+            vk = v[sl.start - base:sl.stop - base] - c
+            vk = _rotz(vk, sp * ang) + c
+            v[sl.start - base:sl.stop - base] = vk
+            cen = vk.mean(axis=1)
+            ub[sl] = np.cross([0, 0, sp * self.omega], cen - c)
+        ver = self.elems.ver.copy()
+        ver[base:] = v
+        self.elems.ver = np.ascontiguousarray(ver)
+        self.elems.ub = ub
+        if self.elems.uvort is None:
+            self.elems.uvort = np.zeros((self.rank, 3))
+
+    def fmm_params(self, degree=4, min_part=8, max_leaf=64):
+        from .params import FmmParams
+        ll = choose_levels(self.cen, self.box_length, self.n_box, self.origin, max_leaf)
+        return FmmParams(box_length=self.box_length, n_box=self.n_box, origin=self.origin,
+                         n_octree_levels=ll, min_octree_part=min_part,
+                         multipole_degree=degree, rankine_rad=0.1, cutoff_rad=0.001,
+                         u_inf=tuple(self.u_inf))
+
+    def loads(self, res, rho=1.225):
+        """Integrated loads from the doublet strengths: wing lift from the
+        trailing-edge doublet jump (rho |U| sum (mu_up - mu_lo) dy) and rotor
+        thrust by Kutta-Joukowski on the bound vortices with the panel-centre
+        relative velocity (restating compute_dforce_jukowski_vortlatt,
+        src/aeroel/mod_vortlatt.f90:502-545, without the unsteady term)."""
+        te_up, te_lo, dy = self.wing_te
+        lift = rho * np.linalg.norm(self.u_inf) * np.sum((res[te_up] - res[te_lo]) * dy)
+        out = [lift]
+        ver = self.elems.ver
+        for k, sl in enumerate(self.rotor_slices):
+            idx = np.arange(sl.start, sl.stop)
+            nch = 8
+            g = res[idx]
+            # upstream element of each chordwise stripe (previous chord row)
+            nsb = (sl.stop - sl.start) // 3 // nch
+            gb = g.reshape(3, nch, nsb)
+            gup = np.concatenate([np.zeros((3, 1, nsb)), gb[:, :-1, :]], axis=1).reshape(-1)
+            e1 = (ver[idx, 3] - ver[idx, 0])  # spanwise (bound-vortex) edge
+            urel = self.u_inf - self.elems.ub[idx] + self.elems.uvort[idx]
+            f = rho * np.cross(urel, e1) * (g - gup)[:, None]
+            out.append(f.sum(axis=0)[2])
+        return np.asarray(out)

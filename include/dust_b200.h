@@ -178,6 +178,20 @@ DUST_API int dust_points_uvort(const dust_fmm_params *prm, int n_pts,
                       const double *r_vortex, const dust_lines *end_vort,
                       double *uvort);
 
+/* Device-resident variant of dust_points_uvort (all arrays, including
+ * end_vort's, in device memory; stream = cudaStream_t or NULL). */
+DUST_API int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts,
+                                      const double *pts, int n,
+                                      const double *cen, const double *dir,
+                                      const double *mag, const double *r_vortex,
+                                      const dust_lines *end_vort, double *uvort,
+                                      void *stream);
+
+/* Panel centres (calc_geo_data) of a device-resident panel set into
+ * cen(3,n) in device memory. */
+DUST_API int dust_panels_centres_device(const dust_panels *pan, double *cen,
+                                        void *stream);
+
 /* Velocity induced at n_pts points by a set of panels and lines
  * (compute_vel of surfpan/vortlatt/vortline, divided by 4*pi) plus u_inf.
  * Host arrays. */
@@ -235,10 +249,19 @@ DUST_API int dust_linsys_destroy(dust_linsys *ls);
 DUST_API int dust_linsys_assemble(dust_linsys *ls, const dust_panels *elems,
                          const dust_wake_rows *wake);
 
+/* dust_linsys_assemble with the panel arrays (and impl_ind) in device
+ * memory. */
+DUST_API int dust_linsys_assemble_device(dust_linsys *ls, const dust_panels *elems,
+                                         const dust_wake_rows *wake);
+
 /* Replaces solve_linsys (mod_linsys.f90:352-482).  res[rank] receives the
  * doublet intensities. */
 DUST_API int dust_linsys_solve(dust_linsys *ls, int mode, double *res,
                       dust_solve_report *rep);
+
+/* dust_linsys_solve writing res[rank] to device memory. */
+DUST_API int dust_linsys_solve_device(dust_linsys *ls, int mode, double *res,
+                                      dust_solve_report *rep);
 
 /* Copies of the assembled matrix (column-major, rank x rank, BEFORE
  * factorisation of the moving part) and right-hand side, as dump_linsys
