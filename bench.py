@@ -247,6 +247,10 @@ def main():
         return
     import torch
     from dust_b200 import abi, step
+    # all work on one explicit stream: the library treats a NULL stream as
+    # "the handle's own stream", so torch's legacy default stream (handle 0)
+    # must not be used for timing
+    torch.cuda.set_stream(torch.cuda.Stream())
     case = make_case(args)
     params = case.fmm_params(degree=args.degree)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -254,7 +258,8 @@ def main():
     results = {}
     steppers = {}
     for name, mode in modes:
-        st = step.DeviceStepper(case, params, mode)
+        prm = params if name == "plain" else params.replace(precision=abi.DUST_PREC_FP32C)
+        st = step.DeviceStepper(case, prm, mode)
         steppers[name] = st
         for _ in range(max(args.warmup, 1 if args.profile_step else 3)):
             st.step()
@@ -272,7 +277,7 @@ def main():
     if args.profile_step:
         return
     # phase breakdown (plain and mixed share the FMM): one timed step with events
-    ph = phase_breakdown(steppers["plain"], case, params)
+    ph = {k: phase_breakdown(steppers[k], case, params) for k in steppers}
     best = min(results, key=lambda k: results[k]["ms"])
     lp = results["plain"]["loads"]
     load_err = {k: float(np.max(np.abs(results[k]["loads"] - lp) / np.maximum(np.abs(lp), 1e-30)))
@@ -320,25 +325,27 @@ def main():
 
 
 def phase_breakdown(st, case, params):
-    """Per-phase device times of one plain step (CUDA events on the phase
-    boundaries; the library records its own FMM phase events)."""
+    """Per-phase device times of one step (CUDA events at the phase
+    boundaries of DeviceStepper.step; the library records its own FMM phase
+    events on the same stream)."""
     import torch
     st.oc.set_timing(True)
+    st.phase_events = True
     torch.cuda.synchronize()
-    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    e[0].record()
     st.step()
-    e[1].record()
     torch.cuda.synchronize()
     s = st.oc.stats()
+    ev = st.events
     st.oc.set_timing(False)
-    total = e[0].elapsed_time(e[1])
-    fmm = s["ms_total"]
-    return {"total": round(total, 3), "fmm_tree": round(s["ms_tree"], 3),
+    st.phase_events = False
+    t = lambda a, b: round(ev[a].elapsed_time(ev[b]), 3)
+    return {"total": t(0, 4), "uvort": t(0, 1), "assemble": t(1, 2), "solve": t(2, 3),
+            "fmm_total": t(3, 4), "fmm_tree": round(s["ms_tree"], 3),
             "fmm_upward": round(s["ms_upward"], 3), "fmm_m2l": round(s["ms_m2l"], 3),
             "fmm_p2p": round(s["ms_p2p"], 3), "fmm_elements": round(s["ms_elems"], 3),
-            "uvort+assemble+solve": round(total - fmm, 3), "n_leaves": s["n_leaves"],
-            "n_active_cells": s["n_active_cells"]}
+            "n_leaves": s["n_leaves"], "n_active_cells": s["n_active_cells"],
+            "n_m2l_pairs": s["n_m2l_pairs"], "n_p2p_pairs": s["n_p2p_pairs"],
+            "n_elem_pairs": s["n_elem_pairs"]}
 
 
 def roofline(ph, case, params):

@@ -1,0 +1,305 @@
+// direct.cu -- the O(N*M) direct sums of the step:
+//   * elements -> particles (apply_multipole's element loop,
+//     src/fmm/mod_octree.f90:1350-1373) fused with the wind and the scatter
+//     of all FMM outputs to the caller's particle order;
+//   * particles (+ end vortices) -> collocation points (get_vort_vel,
+//     src/aeroel/mod_surfpan.f90:962-977, mod_vortlatt.f90:676-693).
+//
+// Far field.  When a point lies beyond the far-field radius of both the
+// doublet (far_field_ratio_doublet * max edge) and the source (10 * max
+// edge), the reference evaluates velocity_calc_doublet's dipole and
+// velocity_calc_sou_surfpan's point-source formulas in the panel's tangent
+// frame (mod_doublet.f90:199-212, mod_surfpan.f90:285-291).  Summed as
+// compute_vel_surfpan does (vdou*mag - vsou*sigma) they are exactly
+//   v = (A / r^3) [ r (3 mu (r.n) / r^2 + sigma) - mu n ],   mu = mag,
+// which is evaluated here with one reciprocal square root (the frame
+// vectors cancel algebraically; only rounding differs).  Nearer pairs use
+// the reference's full formulas (elements.cuh) in FP64.
+//
+// Precision.  FP64 everywhere in the plain mode.  In the FP32C mode the far
+// field runs in FP32 on coordinates taken relative to a reference point of
+// the CTA's particle tile (so no large-coordinate cancellation), partial
+// sums over a tile of sources are compensated (Knuth TwoSum) and then added
+// into FP64 accumulators; near pairs stay FP64.
+#include <algorithm>
+#include <cstring>
+
+#include "dust_common.cuh"
+#include "elements.cuh"
+#include "fmm_internal.h"
+
+static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+struct FFRec {  // far-field record of a panel (double)
+  double c[3], n[3];
+  double amu, asig;  // area*mag, area*sig
+  double ff2;        // squared radius beyond which both far fields apply
+  double pad;
+};
+
+__global__ void k_ffrec(const PanelGeo *pg, int n, double ff_dou, FFRec *out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const PanelGeo &p = pg[j];
+  FFRec r;
+  for (int d = 0; d < 3; ++d) {
+    r.c[d] = p.cen[d];
+    r.n[d] = p.nor[d];
+  }
+  r.amu = p.area * p.mag;
+  bool sp = p.kind == DUST_ELEM_SURFPAN;
+  // compute_vel_surfpan adds -vsou*sig and the far-field vsou is -A r/r^3
+  r.asig = sp ? p.area * p.sig : 0.0;
+  double f = sp ? fmax(ff_dou, 10.0) : ff_dou;
+  r.ff2 = (f * p.max_edge) * (f * p.max_edge);
+  r.pad = 0.0;
+  out[j] = r;
+}
+
+// exact reference evaluation of one panel (x 4 pi)
+__device__ inline void near_pan(const RegParams &rp, const PanelGeo *pg, int j,
+                                const double *pos, double *v) {
+  vel_pan(rp, pg[j], pos, v);
+}
+
+#define EF_T 128
+#define EF_TILE 64
+
+template <bool F32>
+__global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FFRec *ff,
+                                                   double *vel, double *str, double *rot) {
+  __shared__ double s_c[EF_TILE][3], s_n[EF_TILE][3];
+  __shared__ double s_amu[EF_TILE], s_asig[EF_TILE], s_ff2[EF_TILE];
+  __shared__ float f_c[EF_TILE][3], f_n[EF_TILE][3], f_amu[EF_TILE], f_asig[EF_TILE],
+      f_ff2[EF_TILE];
+  const uint32_t t = blockIdx.x * EF_T + threadIdx.x;
+  const size_t n = d.n;
+  const bool act = t < n;
+  const uint32_t t0 = blockIdx.x * EF_T;
+  // reference point of the tile (first particle of the CTA)
+  const double ref[3] = {d.P[t0], d.P[n + t0], d.P[2 * n + t0]};
+  double pos[3] = {ref[0], ref[1], ref[2]};
+  if (act)
+    for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
+  const float px = (float)(pos[0] - ref[0]), py = (float)(pos[1] - ref[1]),
+              pz = (float)(pos[2] - ref[2]);
+  double v[3] = {0, 0, 0};
+  const int ntot = e.nbody + e.nwake;
+  for (int p0 = 0; p0 < ntot; p0 += EF_TILE) {
+    __syncthreads();
+    const int m = min(EF_TILE, ntot - p0);
+    for (int q = threadIdx.x; q < m; q += EF_T) {
+      const FFRec &r = ff[p0 + q];
+      if (F32) {
+        for (int c = 0; c < 3; ++c) {
+          f_c[q][c] = (float)(r.c[c] - ref[c]);
+          f_n[q][c] = (float)r.n[c];
+        }
+        f_amu[q] = (float)r.amu;
+        f_asig[q] = (float)r.asig;
+        // squared far-field radius, rounded up so a far pair in FP32 is far
+        // in FP64 too; pairs within rounding of the threshold go near
+        f_ff2[q] = (float)r.ff2 * 1.000001f;
+      } else {
+        for (int c = 0; c < 3; ++c) {
+          s_c[q][c] = r.c[c];
+          s_n[q][c] = r.n[c];
+        }
+        s_amu[q] = r.amu;
+        s_asig[q] = r.asig;
+        s_ff2[q] = r.ff2;
+      }
+    }
+    __syncthreads();
+    if (!act) continue;
+    if (F32) {
+      f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
+      for (int q = 0; q < m; ++q) {
+        float rx = px - f_c[q][0], ry = py - f_c[q][1], rz = pz - f_c[q][2];
+        float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        if (r2 > f_ff2[q]) {
+          float ir = rsqrtf(r2);
+          float ir2 = ir * ir;
+          float rn = fmaf(rx, f_n[q][0], fmaf(ry, f_n[q][1], rz * f_n[q][2]));
+          float k3 = ir2 * ir;
+          float coef = fmaf(3.0f * f_amu[q] * rn, ir2, f_asig[q]);
+          two_sum_acc(ax, k3 * fmaf(coef, rx, -f_amu[q] * f_n[q][0]));
+          two_sum_acc(ay, k3 * fmaf(coef, ry, -f_amu[q] * f_n[q][1]));
+          two_sum_acc(az, k3 * fmaf(coef, rz, -f_amu[q] * f_n[q][2]));
+        } else {
+          int j = p0 + q;
+          const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
+          int jj = j < e.nbody ? j : j - e.nbody;
+          double u[3];
+          near_pan(e.rp, pg, jj, pos, u);
+          for (int c = 0; c < 3; ++c) v[c] += u[c];
+        }
+      }
+      v[0] += (double)ax.s + (double)ax.c;
+      v[1] += (double)ay.s + (double)ay.c;
+      v[2] += (double)az.s + (double)az.c;
+    } else {
+      for (int q = 0; q < m; ++q) {
+        double rx = pos[0] - s_c[q][0], ry = pos[1] - s_c[q][1], rz = pos[2] - s_c[q][2];
+        double r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 > s_ff2[q]) {
+          double ir = rsqrt(r2);
+          double ir2 = ir * ir;
+          double rn = rx * s_n[q][0] + ry * s_n[q][1] + rz * s_n[q][2];
+          double k3 = ir2 * ir;
+          double coef = 3.0 * s_amu[q] * rn * ir2 + s_asig[q];
+          v[0] += k3 * (coef * rx - s_amu[q] * s_n[q][0]);
+          v[1] += k3 * (coef * ry - s_amu[q] * s_n[q][1]);
+          v[2] += k3 * (coef * rz - s_amu[q] * s_n[q][2]);
+        } else {
+          int j = p0 + q;
+          const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
+          int jj = j < e.nbody ? j : j - e.nbody;
+          double u[3];
+          near_pan(e.rp, pg, jj, pos, u);
+          for (int c = 0; c < 3; ++c) v[c] += u[c];
+        }
+      }
+    }
+  }
+  if (!act) return;
+  for (int q = 0; q < e.nline; ++q) {
+    double u[3];
+    vel_line(e.rp, e.lines[q], pos, u);
+    for (int c = 0; c < 3; ++c) v[c] += u[c];
+  }
+  const uint32_t ip = d.perm[t];
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  for (int c = 0; c < 3; ++c) {
+    vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + v[c] * k4pi + d.u_inf[c];
+    if (str) str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
+    if (rot) rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
+  }
+}
+
+int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
+                       double *str, double *rot, cudaStream_t st) {
+  int ntot = e.nbody + e.nwake;
+  DUST_TRY(devbuf_grow(ffbuf, sizeof(FFRec) * (size_t)std::max(ntot, 1)));
+  FFRec *ff = (FFRec *)ffbuf.p;
+  if (e.nbody) k_ffrec<<<nblk(e.nbody, 128), 128, 0, st>>>(e.body, e.nbody, e.rp.ff_dou, ff);
+  if (e.nwake)
+    k_ffrec<<<nblk(e.nwake, 128), 128, 0, st>>>(e.wake, e.nwake, e.rp.ff_dou, ff + e.nbody);
+  if (d.n > 0) {
+    if (precision == DUST_PREC_FP32C)
+      k_elem_out<true><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
+    else
+      k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
+  }
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+// ---------------------------------------------------------------- uvort
+// Grid: (point blocks) x (particle chunks); each CTA sums one chunk of
+// particles for 128 points and adds its partial sums atomically.
+#define UV2_T 128
+#define UV2_TILE 128
+
+template <bool F32>
+__global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, int n,
+                                                 const double *cen, const double *dir,
+                                                 const double *mag, const double *rv,
+                                                 int chunk, double *uv) {
+  // particles arrive in the caller's order, so a tile is not spatially
+  // compact: the FP32 path takes the point-particle difference in FP64 and
+  // rounds only the difference
+  __shared__ double s_x[UV2_TILE][3], s_a[UV2_TILE][3], s_s[UV2_TILE];
+  __shared__ float f_a[UV2_TILE][3], f_s2[UV2_TILE];
+  const int t = blockIdx.x * UV2_T + threadIdx.x;
+  const bool act = t < npts;
+  const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
+  double pos[3] = {0, 0, 0};
+  if (act)
+    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
+  double v[3] = {0, 0, 0};
+  for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
+    __syncthreads();
+    const int q = q0 + threadIdx.x;
+    const int m = min(UV2_TILE, q_hi - q0);
+    if (threadIdx.x < m) {
+      double mg = mag[q];
+      for (int c = 0; c < 3; ++c) s_x[threadIdx.x][c] = cen[3 * (size_t)q + c];
+      if (F32) {
+        for (int c = 0; c < 3; ++c) f_a[threadIdx.x][c] = (float)(mg * dir[3 * (size_t)q + c]);
+        f_s2[threadIdx.x] = (float)(rv[q] * rv[q]);
+      } else {
+        for (int c = 0; c < 3; ++c) s_a[threadIdx.x][c] = mg * dir[3 * (size_t)q + c];
+        s_s[threadIdx.x] = rv[q];
+      }
+    }
+    __syncthreads();
+    if (!act) continue;
+    if (F32) {
+      f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
+      for (int u = 0; u < m; ++u) {
+        float dx = (float)(pos[0] - s_x[u][0]), dy = (float)(pos[1] - s_x[u][1]),
+              dz = (float)(pos[2] - s_x[u][2]);
+        float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, f_s2[u])));
+        float ir = rsqrtf(r2);
+        float c = -ir * ir * ir;
+        two_sum_acc(ax, c * (dy * f_a[u][2] - dz * f_a[u][1]));
+        two_sum_acc(ay, c * (dz * f_a[u][0] - dx * f_a[u][2]));
+        two_sum_acc(az, c * (dx * f_a[u][1] - dy * f_a[u][0]));
+      }
+      v[0] += (double)ax.s + (double)ax.c;
+      v[1] += (double)ay.s + (double)ay.c;
+      v[2] += (double)az.s + (double)az.c;
+    } else {
+      for (int u = 0; u < m; ++u) {
+        double dx = pos[0] - s_x[u][0], dy = pos[1] - s_x[u][1], dz = pos[2] - s_x[u][2];
+        double r2 = dx * dx + dy * dy + dz * dz + s_s[u] * s_s[u];
+        double ir = rsqrt(r2);
+        double c = -ir * ir * ir;
+        v[0] += c * (dy * s_a[u][2] - dz * s_a[u][1]);
+        v[1] += c * (dz * s_a[u][0] - dx * s_a[u][2]);
+        v[2] += c * (dx * s_a[u][1] - dy * s_a[u][0]);
+      }
+    }
+  }
+  if (!act) return;
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
+}
+
+__global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  double pos[3] = {pts[3 * (size_t)t], pts[3 * (size_t)t + 1], pts[3 * (size_t)t + 2]};
+  double v[3] = {0, 0, 0};
+  for (int q = 0; q < e.nline; ++q) {
+    double u[3];
+    vel_line(e.rp, e.lines[q], pos, u);
+    for (int c = 0; c < 3; ++c) v[c] += u[c];
+  }
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
+}
+
+int points_uvort_run(int precision, int n_pts, const double *pts, int n, const double *cen,
+                     const double *dir, const double *mag, const double *rv,
+                     const ElemDev &lines, double *uv, cudaStream_t st) {
+  if (n_pts <= 0) return DUST_OK;
+  DUST_CUDA(cudaMemsetAsync(uv, 0, (size_t)n_pts * 24, st));
+  if (n > 0) {
+    int pb = (int)nblk(n_pts, UV2_T);
+    // enough CTAs for every SM several times over; chunks of whole tiles
+    int want = std::max(1, (148 * 8 + pb - 1) / pb);
+    int chunk = (n + want - 1) / want;
+    chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);
+    int nch = (n + chunk - 1) / chunk;
+    dim3 grd(pb, nch);
+    if (precision == DUST_PREC_FP32C)
+      k_uvort<true><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
+    else
+      k_uvort<false><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
+  }
+  if (lines.nline > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, lines, uv);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}

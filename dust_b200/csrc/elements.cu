@@ -173,54 +173,7 @@ __global__ void __launch_bounds__(EP_T) k_elements_vel(int n, const double *pts,
   vel[3 * (size_t)t + 2] = v[2] * k4pi + u2;
 }
 
-// uvort at points: particles (compute_vel_vortpart) + end vortices.
-// Particles are streamed through shared memory in tiles; one thread per point.
 #define UV_T 128
-__global__ void __launch_bounds__(UV_T) k_points_uvort(int npts, const double *pts, int n,
-                                                       const double *cen, const double *dir,
-                                                       const double *mag, const double *rv,
-                                                       ElemDev e, double *uv) {
-  __shared__ double s[7][UV_T];
-  int t = blockIdx.x * UV_T + threadIdx.x;
-  bool act = t < npts;
-  double pos[3] = {0, 0, 0};
-  if (act)
-    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
-  double v[3] = {0, 0, 0};
-  for (int q0 = 0; q0 < n; q0 += UV_T) {
-    __syncthreads();
-    int q = q0 + threadIdx.x;
-    if (q < n) {
-      double m = mag[q];
-      for (int c = 0; c < 3; ++c) {
-        s[c][threadIdx.x] = cen[3 * (size_t)q + c];
-        s[3 + c][threadIdx.x] = m * dir[3 * (size_t)q + c];
-      }
-      s[6][threadIdx.x] = rv[q];
-    }
-    __syncthreads();
-    int m = min(UV_T, n - q0);
-    if (act)
-      for (int u = 0; u < m; ++u) {
-        double dx = pos[0] - s[0][u], dy = pos[1] - s[1][u], dz = pos[2] - s[2][u];
-        double r2 = dx * dx + dy * dy + dz * dz + s[6][u] * s[6][u];
-        double inv = rsqrt(r2);
-        double c = -inv * inv * inv;
-        v[0] += c * (dy * s[5][u] - dz * s[4][u]);
-        v[1] += c * (dz * s[3][u] - dx * s[5][u]);
-        v[2] += c * (dx * s[4][u] - dy * s[3][u]);
-      }
-  }
-  if (!act) return;
-  for (int q = 0; q < e.nline; ++q) {
-    double u[3];
-    vel_line(e.rp, e.lines[q], pos, u);
-    for (int c = 0; c < 3; ++c) v[c] += u[c];
-  }
-  const double k4pi = 1.0 / (4.0 * DUST_PI);
-  for (int c = 0; c < 3; ++c) uv[3 * (size_t)t + c] = v[c] * k4pi;
-}
-
 // All-pairs particle kernels (direct-sum truth).
 __global__ void __launch_bounds__(UV_T) k_direct(int n, int ntgt, const double *cen,
                                                  const double *dir, const double *mag,
@@ -333,12 +286,7 @@ extern "C" int dust_elements_vel(const dust_fmm_params *prm, int n_pts, const do
 int points_uvort_device(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                         const double *cen, const double *dir, const double *mag,
                         const double *rv, const ElemDev &lines, double *uv, cudaStream_t st) {
-  (void)prm;
-  if (n_pts <= 0) return DUST_OK;
-  k_points_uvort<<<nblk(n_pts, UV_T), UV_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, lines,
-                                                     uv);
-  DUST_CUDA(cudaGetLastError());
-  return DUST_OK;
+  return points_uvort_run(prm->precision, n_pts, pts, n, cen, dir, mag, rv, lines, uv, st);
 }
 
 extern "C" int dust_points_uvort(const dust_fmm_params *prm, int n_pts, const double *pts,

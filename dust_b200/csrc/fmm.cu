@@ -189,6 +189,7 @@ extern "C" int dust_octree_create(const dust_fmm_params *prm, dust_octree **out)
   }
   for (int e = 0; e < 8; ++e) cudaEventCreate(&o->ev[e]);
   st = build_tables(o);
+  if (st == DUST_OK) st = m2l_batch_tables(o);
   if (st != DUST_OK) {
     dust_octree_destroy(o);
     return st;
@@ -200,7 +201,15 @@ extern "C" int dust_octree_create(const dust_fmm_params *prm, dust_octree **out)
 extern "C" int dust_octree_destroy(dust_octree *o) {
   if (!o) return DUST_OK;
   cudaStreamSynchronize(o->stream);
-  for (int l = 0; l <= DUST_MAXLEV; ++l) devbuf_free(o->dtab[l]);
+  for (int l = 0; l <= DUST_MAXLEV; ++l) {
+    devbuf_free(o->dtab[l]);
+    devbuf_free(o->dtab32[l]);
+    devbuf_free(o->dtabs[l]);
+  }
+  devbuf_free(o->m2l_buf);
+  devbuf_free(o->ahat);
+  devbuf_free(o->m2l_bat);
+  devbuf_free(o->ffbuf);
   DevBuf *bufs[] = {&o->idxsum, &o->keys,   &o->keys_s, &o->vals,   &o->perm,
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
                     &o->cidx,   &o->lidx,   &o->act_key, &o->act_lev, &o->leaf_ci,
@@ -581,7 +590,7 @@ __global__ void k_l2l(FmmDev d, int l, uint32_t act_lo) {
           acc[2] += w * bp[3 * s + 2];
         }
     double *b = d.B + (size_t)ci * 3 * d.nm;
-    for (int e = 0; e < 3; ++e) b[3 * m + e] = acc[e];
+    for (int e = 0; e < 3; ++e) b[3 * m + e] += acc[e];
   }
   if (d.use_vs && m < d.nm1) {
     int mi, mj, mk;
@@ -600,7 +609,7 @@ __global__ void k_l2l(FmmDev d, int l, uint32_t act_lo) {
           acc[2] += w * gp[3 * s + 2];
         }
     double *g = d.Gx + (size_t)ci * 3 * d.nm1;
-    for (int e = 0; e < 3; ++e) g[3 * m + e] = acc[e];
+    for (int e = 0; e < 3; ++e) g[3 * m + e] += acc[e];
   }
 }
 
@@ -659,7 +668,53 @@ __device__ __forceinline__ void p2p_pair(const double *tp, const double *ta, dou
   }
 }
 
-template <bool VS, bool DF, bool VD, bool TV>
+struct P2PAccF {
+  float v[3], s[3], r[3], f[3];
+};
+
+// FP32 form of p2p_pair on coordinates relative to the leaf centre
+template <bool VS, bool DF, bool VD>
+__device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, float qx, float qy,
+                                           float qz, float qax, float qay, float qaz, float sq,
+                                           P2PAccF &A) {
+  float dx = tp[0] - qx, dy = tp[1] - qy, dz = tp[2] - qz;
+  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float s2 = sq * sq;
+  float inv = rsqrtf(r2 + s2);
+  float inv2 = inv * inv;
+  float c = -inv2 * inv;
+  float dd = -3.0f * c * inv2;
+  float cx = dy * qaz - dz * qay, cy = dz * qax - dx * qaz, cz = dx * qay - dy * qax;
+  A.v[0] = fmaf(c, cx, A.v[0]);
+  A.v[1] = fmaf(c, cy, A.v[1]);
+  A.v[2] = fmaf(c, cz, A.v[2]);
+  if (VS) {
+    float vx = ta[1] * qaz - ta[2] * qay, vy = ta[2] * qax - ta[0] * qaz,
+          vz = ta[0] * qay - ta[1] * qax;
+    float dv = dx * vx + dy * vy + dz * vz;
+    A.s[0] -= c * vx + dd * dx * dv;
+    A.s[1] -= c * vy + dd * dy * dv;
+    A.s[2] -= c * vz + dd * dz * dv;
+    if (DF) {
+      float da = dx * qax + dy * qay + dz * qaz;
+      A.r[0] += -2.0f * c * qax + dd * (dx * da - qax * r2);
+      A.r[1] += -2.0f * c * qay + dd * (dy * da - qay * r2);
+      A.r[2] += -2.0f * c * qaz + dd * (dz * da - qaz * r2);
+    }
+  }
+  if (VD) {
+    float is2 = 1.0f / s2;
+    float t = fmaf(r2, is2, 1.0f);
+    float rt = rsqrtf(t);
+    float rt2 = rt * rt, rt4 = rt2 * rt2;
+    float w = 17.5f * is2 * (rt4 * rt4 * rt);
+    A.f[0] += w * (qax - ta[0]);
+    A.f[1] += w * (qay - ta[1]);
+    A.f[2] += w * (qaz - ta[2]);
+  }
+}
+
+template <bool VS, bool DF, bool VD, bool TV, bool F32 = false>
 __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
   __shared__ double s_src[7][P2P_TILE];
   __shared__ uint32_t s_sid[P2P_TILE];
@@ -841,16 +896,44 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
         }
         uint32_t sidx = s_rlo[a] + (v - s_rcum[a]);
         s_sid[tid] = sidx;
-        for (int q = 0; q < 7; ++q) s_src[q][tid] = d.P[(size_t)q * n + sidx];
+        if (F32) {
+          float *fs = (float *)&s_src[0][0];  // 7 x TILE floats in the double tile
+          for (int q = 0; q < 3; ++q) fs[q * P2P_TILE + tid] = (float)(d.P[(size_t)q * n + sidx] - cc[q]);
+          for (int q = 3; q < 7; ++q) fs[q * P2P_TILE + tid] = (float)d.P[(size_t)q * n + sidx];
+        } else {
+          for (int q = 0; q < 7; ++q) s_src[q][tid] = d.P[(size_t)q * n + sidx];
+        }
       }
       __syncthreads();
       const int m = (int)min((uint32_t)P2P_TILE, S - s0);
-      if (act)
-        for (int u = grp; u < m; u += G) {
-          if (s_sid[u] == ti) continue;
-          p2p_pair<VS, DF, VD>(tp, ta, s_src[0][u], s_src[1][u], s_src[2][u], s_src[3][u],
-                               s_src[4][u], s_src[5][u], s_src[6][u], A);
+      if (act) {
+        if (F32) {
+          const float *fs = (const float *)&s_src[0][0];
+          float ftp[3] = {(float)(tp[0] - cc[0]), (float)(tp[1] - cc[1]), (float)(tp[2] - cc[2])};
+          float fta[3] = {(float)ta[0], (float)ta[1], (float)ta[2]};
+          P2PAccF B;
+          for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+          for (int u = grp; u < m; u += G) {
+            if (s_sid[u] == ti) continue;
+            p2p_pair_f<VS, DF, VD>(ftp, fta, fs[u], fs[P2P_TILE + u], fs[2 * P2P_TILE + u],
+                                   fs[3 * P2P_TILE + u], fs[4 * P2P_TILE + u],
+                                   fs[5 * P2P_TILE + u], fs[6 * P2P_TILE + u], B);
+          }
+          // FP32 partial sums of one tile (at most 128/G terms) folded into FP64
+          for (int e = 0; e < 3; ++e) {
+            A.v[e] += (double)B.v[e];
+            A.s[e] += (double)B.s[e];
+            A.r[e] += (double)B.r[e];
+            A.f[e] += (double)B.f[e];
+          }
+        } else {
+          for (int u = grp; u < m; u += G) {
+            if (s_sid[u] == ti) continue;
+            p2p_pair<VS, DF, VD>(tp, ta, s_src[0][u], s_src[1][u], s_src[2][u], s_src[3][u],
+                                 s_src[4][u], s_src[5][u], s_src[6][u], A);
+          }
         }
+      }
     }
     // reduce the groups
     __syncthreads();
@@ -885,54 +968,6 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
         d.out[(size_t)(6 + e) * n + ti] = lr[e] + A.r[e] * k4pi;
       }
     }
-  }
-}
-
-// Elements -> particles (mod_octree.f90:1350-1373), wind, and scatter of
-// all outputs to the caller's particle order.
-#define EL_T 128
-#define EL_TILE 16
-__global__ void __launch_bounds__(EL_T) k_elem_final(FmmDev d, ElemDev e, double *vel,
-                                                     double *str, double *rot) {
-  __shared__ PanelGeo s_p[EL_TILE];
-  uint32_t t = blockIdx.x * EL_T + threadIdx.x;
-  const size_t n = d.n;
-  bool act = t < n;
-  double pos[3] = {0, 0, 0};
-  if (act)
-    for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
-  double v[3] = {0, 0, 0};
-  int ntot = e.nbody + e.nwake;
-  for (int p0 = 0; p0 < ntot; p0 += EL_TILE) {
-    __syncthreads();
-    int m = min(EL_TILE, ntot - p0);
-    const int words = sizeof(PanelGeo) / 8;
-    for (int w = threadIdx.x; w < m * words; w += EL_T) {
-      int pp = w / words, ww = w % words;
-      int gidx = p0 + pp;
-      const PanelGeo *src = gidx < e.nbody ? e.body + gidx : e.wake + (gidx - e.nbody);
-      ((double *)&s_p[pp])[ww] = ((const double *)src)[ww];
-    }
-    __syncthreads();
-    if (act)
-      for (int q = 0; q < m; ++q) {
-        double u[3];
-        vel_pan(e.rp, s_p[q], pos, u);
-        for (int c = 0; c < 3; ++c) v[c] += u[c];
-      }
-  }
-  if (!act) return;
-  for (int q = 0; q < e.nline; ++q) {
-    double u[3];
-    vel_line(e.rp, e.lines[q], pos, u);
-    for (int c = 0; c < 3; ++c) v[c] += u[c];
-  }
-  uint32_t ip = d.perm[t];
-  const double k4pi = 1.0 / (4.0 * DUST_PI);
-  for (int c = 0; c < 3; ++c) {
-    vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + v[c] * k4pi + d.u_inf[c];
-    if (str) str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
-    if (rot) rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
   }
 }
 
@@ -974,6 +1009,7 @@ static void fill_dev(dust_octree *o, FmmDev &d, int n) {
 int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
                    const double *mag, const double *rv, cudaStream_t st) {
   TreeGeom &G = o->G;
+  o->last_stream = st;
   const int ll = G.ll;
   const uint32_t nfine = G.ncell[ll];
   const uint32_t ntot = (uint32_t)o->ncell_tot;
@@ -1074,6 +1110,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   d.counters = (int64_t *)(small + 48);
   DUST_CUDA(cudaMemsetAsync(d.counters, 0, 4 * sizeof(int64_t), st));
   o->dev = d;
+  DUST_TRY(m2l_prepare(o, d, st));
   if (o->n_leaves > 0) {
     int thr = std::max(64, (o->nm + 31) / 32 * 32);
     k_p2m<<<(unsigned)o->n_leaves, thr, 6 * 64 * 8, st>>>(d);
@@ -1083,25 +1120,38 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
     if (na > 0)
       k_m2m<<<(unsigned)na, (o->nm + 31) / 32 * 32, 0, st>>>(d, l, (uint32_t)o->act_off[l]);
   }
+  DUST_TRY(m2l_scale_sources(o, d, st));
   if (o->timing) cudaEventRecord(o->ev[2], st);
-  // downward pass
+  // downward pass: M2L of every level (level 1 per target, levels >= 2 in
+  // one batched launch), then L2L level by level adds the parents' final
+  // local expansions (mod_octree.f90:1074-1125 in another, equivalent order:
+  // both are sums of the same terms)
   int thr_m2l = (std::max(o->nm, d.use_vs ? o->nm1 : o->nm) + 31) / 32 * 32;
-  for (int l = 1; l <= ll; ++l) {
+  {
+    int64_t na1 = o->act_off[2 <= ll ? 2 : ll + 1] - o->act_off[1];
+    if (na1 > 0)
+      k_m2l<<<(unsigned)na1, thr_m2l, 3 * o->nm * 8, st>>>(d, 1, (uint32_t)o->act_off[1]);
+  }
+  DUST_TRY(m2l_all_levels(o, d, st));
+  for (int l = 2; l <= ll; ++l) {
     int64_t na = o->act_off[l + 1] - o->act_off[l];
     if (na <= 0) continue;
-    if (l >= 2) {
-      int thr = ((d.use_vs ? o->nm1 : o->nm) + 31) / 32 * 32;
-      k_l2l<<<(unsigned)na, thr, 0, st>>>(d, l, (uint32_t)o->act_off[l]);
-    }
-    k_m2l<<<(unsigned)na, thr_m2l, 3 * o->nm * 8, st>>>(d, l, (uint32_t)o->act_off[l]);
+    int thr = ((d.use_vs ? o->nm1 : o->nm) + 31) / 32 * 32;
+    k_l2l<<<(unsigned)na, thr, 0, st>>>(d, l, (uint32_t)o->act_off[l]);
   }
   if (o->timing) cudaEventRecord(o->ev[3], st);
   // leaves: L2P + P2P
   if (o->n_leaves > 0) {
     size_t shl = (size_t)3 * (o->nm + o->nm1) * 8 + (size_t)4 * o->nm * 4;
     bool vs = d.use_vs, df = d.use_df, vd = d.use_vd, tv = o->prm.turbulent_viscosity != 0;
-#define LAUNCH_P2P(A, B, C, D) \
-  k_p2p<A, B, C, D><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d)
+    const bool f32 = o->prm.precision == DUST_PREC_FP32C;
+#define LAUNCH_P2P(A, B, C, D)                                                   \
+  do {                                                                         \
+    if (f32)                                                                   \
+      k_p2p<A, B, C, D, true><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);    \
+    else                                                                       \
+      k_p2p<A, B, C, D, false><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);   \
+  } while (0)
     if (vs && df && vd && !tv) LAUNCH_P2P(true, true, true, false);
     else if (vs && df && vd && tv) LAUNCH_P2P(true, true, true, true);
     else if (vs && df && !vd) LAUNCH_P2P(true, true, false, false);
@@ -1120,8 +1170,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
 
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st) {
-  if (n > 0)
-    k_elem_final<<<nblk(n, EL_T), EL_T, 0, st>>>(o->dev, e, vel, str, rot);
+  if (n > 0) DUST_TRY(elem_output_device(o->dev, e, o->ffbuf, o->prm.precision, vel, str, rot, st));
   if (o->timing) cudaEventRecord(o->ev[5], st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
@@ -1130,6 +1179,7 @@ int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, doub
 void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
   dust_fmm_stats &s = o->stats;
   memset(&s, 0, sizeof(s));
+  cudaStreamSynchronize(o->last_stream);
   if (o->dev.counters) {
     int64_t c[4] = {0, 0, 0, 0};
     cudaMemcpy(c, o->dev.counters, sizeof(c), cudaMemcpyDeviceToHost);

@@ -52,6 +52,7 @@ struct dust_octree {
   int p, nm, nm1, nD;
   uint64_t ncell_tot = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t last_stream = nullptr;  // stream of the last evaluation
   cudaEvent_t ev[8];
   bool timing = false;
   DevBuf dtab[DUST_MAXLEV + 1];
@@ -61,6 +62,15 @@ struct dust_octree {
   DevBuf keys, keys_s, vals, perm, cnt, cstart, part, flags, ind, cidx, lidx;
   DevBuf act_key, act_lev, leaf_ci, mp, outs, cub_tmp, small;
   DevBuf h_in, h_out, el_geo, el_raw;  // staging of host-API calls
+  DevBuf ffbuf;                        // far-field panel records
+  DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless M2L tables (FP64)
+  DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless M2L tables (FP32)
+  DevBuf m2l_buf;                      // class-sorted M2L target lists
+  DevBuf m2l_bat;                      // M2L batch descriptors
+  uint32_t *m2l_list = nullptr;
+  DevBuf ahat;                         // pre-scaled M2L source coefficients
+  uint32_t ahat_c0 = 0;
+  int m2l_cnt[8 * (DUST_MAXLEV + 1)];
   int64_t n_active = 0, n_leaves = 0;
   int64_t act_off[DUST_MAXLEV + 3];
   int bad_particle = -1;
@@ -80,3 +90,16 @@ int elem_build_device(const dust_panels *body, const dust_panels *wake,
                       bool host_arrays, DevBuf &raw, DevBuf &geo, ElemDev &out,
                       cudaStream_t st);
 RegParams reg_params(const dust_fmm_params *prm);
+
+// m2l.cu
+int m2l_batch_tables(dust_octree *o);
+int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st);
+int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st);
+int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
+
+// direct.cu
+int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
+                       double *str, double *rot, cudaStream_t st);
+int points_uvort_run(int precision, int n_pts, const double *pts, int n, const double *cen,
+                     const double *dir, const double *mag, const double *rv,
+                     const ElemDev &lines, double *uv, cudaStream_t st);

@@ -1,0 +1,355 @@
+// m2l.cu -- batched multipole-to-local translation (levels >= 2).
+//
+// M2L_multipole (src/fmm/mod_multipole.f90:282-356) in the form
+//   g(m') = (-1)^|m'| / m'!  sum_n  Dhat(m'+n) x ahat(n),  |m'| <= p+1,
+// Dhat = k! D(k) of compute_der_ker (:388-450), ahat(n) = a(n)/n!.
+//
+// Work decomposition.  The targets of a level are the non-empty active
+// cells, grouped by their position in the parent (octant class q = key & 7):
+// all targets of one class share the same 189 interaction offsets
+// (children of the parent's 26 neighbours that are not adjacent,
+// mod_octree.f90:440-476).  A CTA takes NB targets of one class and loops
+// over the 189 offsets; per offset it stages the offset's Dhat table once
+// (shared by all NB targets) and the NB source multipoles (zero where the
+// source cell is missing, inactive or empty) in shared memory.  A thread
+// owns a 4-target x 2-output register tile, so each n-step loads 6 table
+// values and 12 source values for 48 FMAs.  Accumulators stay in registers
+// across the offsets; the result is added once to the cell's b and g.
+//
+// Scaling: with h the cell size of the level, the tables hold
+// Dhat(k) h^(|k|+2) and the sources a(n) / (n! h^|n|), so both stay of order
+// one at every level and degree; the output is rescaled by h^-(|m'|+2).
+//
+// FP32C: tables and source coefficients in FP32, each offset's partial sums
+// in FP32, accumulated across offsets in FP64.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "dust_common.cuh"
+#include "fmm_internal.h"
+
+#define M2L_T 256
+
+struct M2LTabs {
+  const void *t[DUST_MAXLEV + 1];  // per-level dimensionless tables
+};
+
+// One CTA per batch descriptor (level, class, first target, count); the
+// batches of all levels >= 2 run in one launch (M2L of different levels is
+// independent; L2L follows level by level).
+//
+// Inside a CTA the warps are independent: warp w takes offsets w, w+W, ...;
+// lane i looks up the source of target i at that offset, the present ones
+// are compacted with a ballot, the warp stages the offset's table and (in
+// chunks of M2L_TC) the present sources in its own shared-memory slice and
+// evaluates them with __syncwarp only.  Results go to the CTA's shared
+// accumulators with shared-memory atomics (a few per lane per offset, against
+// thousands of FMAs).
+#define M2L_W 8
+#define M2L_TC 8
+template <typename T>
+__global__ void __launch_bounds__(M2L_W * 32) k_m2l_batch(FmmDev d, const int4 *batches,
+                                                          const uint32_t *list, int NB, int NW,
+                                                          int TC, M2LTabs tabs, const T *ahat,
+                                                          uint32_t c0, int isum_smem) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nm = d.nm, nm1 = d.nm1, nD = d.nD;
+  const int nout = d.use_vs ? nm1 : nm;
+  const int4 bd = batches[blockIdx.x];
+  const int l = bd.x, q = bd.y, t0 = bd.z, cnt = bd.w;
+  const T *dtab = (const T *)tabs.t[l];
+  double *s_acc = (double *)smraw;                  // NB x nout x 3
+  int *s_tc = (int *)(s_acc + (size_t)NB * nout * 3);  // NB x 3 target carts
+  const size_t wslice = (size_t)3 * nD + (size_t)TC * 3 * nm;  // per warp, in T
+  uint16_t *s_isum = (uint16_t *)(s_tc + 3 * NB);  // nm x nm1 index table (optional)
+  const uint16_t *isum = isum_smem ? s_isum : d.idxsum;
+  const size_t isz = isum_smem ? (size_t)nm * nm1 : 0;
+  T *s_w = (T *)(((uintptr_t)(s_isum + isz) + 15) & ~(uintptr_t)15);
+  __shared__ double s_hp[2 * DUST_MAXP + 6];  // (1/h)^d
+  const int bx = q & 1, by = (q >> 1) & 1, bz = (q >> 2) & 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t lo_l = d.G.lev_off[l];
+  const int sh = 3 * (d.G.ll - l);
+  if (tid == 0) {
+    double hi = 1.0 / d.G.csize[l], v = 1.0;
+    for (int e = 0; e < 2 * DUST_MAXP + 6; ++e, v *= hi) s_hp[e] = v;
+  }
+  for (int t = tid; t < NB; t += NW * 32) {
+    int i = -1000, j = -1000, k = -1000;
+    if (t < cnt) cart_of_key(d.G, l, d.act_key[list[t0 + t]], i, j, k);
+    s_tc[3 * t] = i;
+    s_tc[3 * t + 1] = j;
+    s_tc[3 * t + 2] = k;
+  }
+  for (int e = tid; e < NB * nout * 3; e += NW * 32) s_acc[e] = 0.0;
+  for (int e = tid; e < (int)isz; e += NW * 32) s_isum[e] = d.idxsum[e];
+  __syncthreads();
+  T *sD = s_w + (size_t)warp * wslice;
+  T *sA = sD + 3 * nD;
+  unsigned long long npairs = 0;
+  const int L = 3, W = 2 * L + 1;
+  for (int cand = warp; cand < 216; cand += NW) {
+    const int ox = cand % 6 - 2 - bx, oy = (cand / 6) % 6 - 2 - by, oz = cand / 36 - 2 - bz;
+    if (abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) continue;  // adjacent: near field
+    int src = -1;
+    if (lane < cnt) {
+      int si = s_tc[3 * lane] + ox, sj = s_tc[3 * lane + 1] + oy, sk = s_tc[3 * lane + 2] + oz;
+      if (cart_in(d.G, l, si, sj, sk)) {
+        uint32_t skey = key_of(d.G, l, si, sj, sk);
+        if ((d.flags[lo_l + skey] & FL_ACTIVE) &&
+            d.cstart[(skey + 1u) << sh] > d.cstart[skey << sh])
+          src = (int)d.cidx[lo_l + skey];
+      }
+    }
+    unsigned msk = __ballot_sync(0xffffffffu, src >= 0);
+    if (!msk) continue;
+    npairs += __popc(msk);
+    const int tab = (ox + L) + W * ((oy + L) + W * (oz + L));
+    const T *Dg = dtab + (size_t)tab * nD * 3;
+    __syncwarp();
+    for (int e = lane; e < 3 * nD; e += 32) sD[e] = Dg[e];
+    while (msk) {
+      // next chunk of present targets
+      int tl[M2L_TC], kc = 0;
+      while (msk && kc < TC) {
+        int t = __ffs(msk) - 1;
+        msk &= msk - 1;
+        tl[kc++] = t;
+      }
+      for (int c = 0; c < kc; ++c) {
+        int sc_ = __shfl_sync(0xffffffffu, src, tl[c]);
+        const T *ag = ahat + (size_t)(sc_ - c0) * 3 * nm;
+        for (int e = lane; e < 3 * nm; e += 32) sA[c * 3 * nm + e] = ag[e];
+      }
+      __syncwarp();
+      for (int m0 = lane; m0 < nout; m0 += 32) {
+        T pa[M2L_TC][3];
+#pragma unroll
+        for (int c = 0; c < M2L_TC; ++c) pa[c][0] = pa[c][1] = pa[c][2] = (T)0;
+        for (int n = 0; n < nm; ++n) {
+          const int k0 = isum[(size_t)n * nm1 + m0];
+          const T Dx = sD[3 * k0], Dy = sD[3 * k0 + 1], Dz = sD[3 * k0 + 2];
+#pragma unroll
+          for (int c = 0; c < M2L_TC; ++c) {
+            if (c < kc) {
+              const T ax = sA[c * 3 * nm + 3 * n], ay = sA[c * 3 * nm + 3 * n + 1],
+                      az = sA[c * 3 * nm + 3 * n + 2];
+              pa[c][0] += Dy * az - Dz * ay;
+              pa[c][1] += Dz * ax - Dx * az;
+              pa[c][2] += Dx * ay - Dy * ax;
+            }
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < M2L_TC; ++c)
+          if (c < kc) {
+            double *acc = s_acc + ((size_t)tl[c] * nout + m0) * 3;
+            atomicAdd(acc, (double)pa[c][0]);
+            atomicAdd(acc + 1, (double)pa[c][1]);
+            atomicAdd(acc + 2, (double)pa[c][2]);
+          }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (lane == 0 && d.counters) atomicAdd((unsigned long long *)d.counters, npairs);
+  for (int e = tid; e < cnt * nout; e += NW * 32) {
+    const int t = e / nout, mo = e - t * nout;
+    int oi, oj, ok;
+    mono_exp(mo, oi, oj, ok);
+    const double sc =
+        (((oi + oj + ok) & 1) ? -1.0 : 1.0) * d.inv_fact[mo] * s_hp[oi + oj + ok + 2];
+    const uint32_t ci = list[t0 + t];
+    const double *acc = s_acc + (size_t)t * nout * 3;
+    if (d.use_vs) {
+      double *g = d.Gx + (size_t)ci * 3 * nm1;
+      for (int c = 0; c < 3; ++c) g[3 * mo + c] += sc * acc[3 * mo + c];
+    }
+    if (mo < nm) {
+      double *bb = d.B + (size_t)ci * 3 * nm;
+      for (int c = 0; c < 3; ++c) bb[3 * mo + c] += sc * acc[3 * mo + c];
+    }
+  }
+}
+
+// ahat'(n) = a(n) / (n! h^|n|) for every active cell of levels >= 2
+template <typename T>
+__global__ void k_scale_a(FmmDev d, uint32_t c0, uint32_t nact, T *out) {
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = 3 * d.nm;
+  size_t tot = (size_t)(nact - c0) * w;
+  if (e >= tot) return;
+  uint32_t ci = c0 + (uint32_t)(e / w);
+  int r = (int)(e % w), nn = r / 3, ni, nj, nk;
+  mono_exp(nn, ni, nj, nk);
+  int l = d.act_lev[ci];
+  double hi = 1.0 / d.G.csize[l], hp = 1.0;
+  for (int q = 0; q < ni + nj + nk; ++q) hp *= hi;
+  out[e] = (T)(d.A[(size_t)ci * w + r] * d.inv_fact[nn] * hp);
+}
+
+// class keys of the active cells of levels >= 2: (level << 3 | key & 7) for
+// non-empty cells, 0xff for empty ones (dropped)
+__global__ void k_m2l_keys(FmmDev d, uint32_t c0, uint32_t nact, uint32_t *keys,
+                           uint32_t *vals, int *hist) {
+  uint32_t ci = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= nact) return;
+  int l = d.act_lev[ci];
+  uint32_t key = d.act_key[ci];
+  int sh = 3 * (d.G.ll - l);
+  bool ne = d.cstart[(key + 1u) << sh] > d.cstart[key << sh];
+  uint32_t k = ne ? (uint32_t)((l << 3) | (key & 7)) : 0xffu;
+  keys[ci - c0] = k;
+  vals[ci - c0] = ci;
+  if (ne) atomicAdd(hist + k, 1);
+}
+
+static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int m2l_batch_tables(dust_octree *o) {
+  // dimensionless tables Dhat(k) h^(|k|+2) for the batched kernel, FP64 and
+  // FP32 copies
+  int nD = o->nD;
+  std::vector<int> deg(nD);
+  for (int q = 0; q < nD; ++q) {
+    int i, j, k;
+    mono_exp(q, i, j, k);
+    deg[q] = i + j + k;
+  }
+  for (int l = 2; l <= o->G.ll; ++l) {
+    size_t n = (size_t)343 * nD * 3;
+    DUST_TRY(devbuf_grow(o->dtabs[l], n * 8));
+    DUST_TRY(devbuf_grow(o->dtab32[l], n * 4));
+    std::vector<double> h(n);
+    DUST_CUDA(cudaMemcpy(h.data(), o->dtab[l].p, n * 8, cudaMemcpyDeviceToHost));
+    double cs = o->G.csize[l];
+    std::vector<double> hp(2 * DUST_MAXP + 6, 1.0);
+    for (size_t e = 1; e < hp.size(); ++e) hp[e] = hp[e - 1] * cs;
+    std::vector<float> f(n);
+    for (size_t i = 0; i < n; ++i) {
+      size_t q = (i / 3) % nD;
+      h[i] *= hp[deg[q] + 2];
+      f[i] = (float)h[i];
+    }
+    DUST_CUDA(cudaMemcpy(o->dtabs[l].p, h.data(), n * 8, cudaMemcpyHostToDevice));
+    DUST_CUDA(cudaMemcpy(o->dtab32[l].p, f.data(), n * 4, cudaMemcpyHostToDevice));
+  }
+  return DUST_OK;
+}
+
+// Runs M2L for all levels >= 2 (level 1 is handled by the per-target kernel).
+// `before_level(l)` style ordering: L2L into level l must already be done, so
+// the caller invokes this per level.
+int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st) {
+  const int ll = o->G.ll;
+  uint32_t c0 = (uint32_t)o->act_off[2 <= ll ? 2 : ll + 1];
+  uint32_t nact = (uint32_t)o->n_active;
+  uint32_t m = nact > c0 ? nact - c0 : 0;
+  o->m2l_list = nullptr;
+  memset(o->m2l_cnt, 0, sizeof(o->m2l_cnt));
+  if (m == 0) return DUST_OK;
+  DUST_TRY(devbuf_grow(o->m2l_buf, (size_t)m * 16 + 4096));
+  uint32_t *k_in = (uint32_t *)o->m2l_buf.p, *v_in = k_in + m, *k_out = v_in + m,
+           *v_out = k_out + m;
+  int *hist = (int *)(v_out + m);
+  DUST_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(int), st));
+  k_m2l_keys<<<nblk(m, 256), 256, 0, st>>>(d, c0, nact, k_in, v_in, hist);
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, v_in, v_out, (int)m, 0, 8, st);
+  DUST_TRY(devbuf_grow(o->cub_tmp, tb));
+  DUST_CUDA(cub::DeviceRadixSort::SortPairs(o->cub_tmp.p, tb, k_in, k_out, v_in, v_out, (int)m,
+                                            0, 8, st));
+  int h[256];
+  DUST_CUDA(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  memcpy(o->m2l_cnt, h, sizeof(int) * 8 * (DUST_MAXLEV + 1));
+  o->m2l_list = v_out;
+  // pre-scaled source coefficients of all active cells of levels >= 2
+  bool f32 = o->prm.precision == DUST_PREC_FP32C;
+  size_t w = (size_t)3 * o->nm, tot = (size_t)m * w;
+  DUST_TRY(devbuf_grow(o->ahat, tot * (f32 ? 4 : 8) + 256));
+  o->ahat_c0 = c0;
+  return DUST_OK;
+}
+
+// fills the pre-scaled coefficients once the upward pass is complete
+int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
+  if (!o->m2l_list) return DUST_OK;
+  uint32_t c0 = o->ahat_c0, nact = (uint32_t)o->n_active;
+  size_t tot = (size_t)(nact - c0) * 3 * o->nm;
+  if (tot == 0) return DUST_OK;
+  if (o->prm.precision == DUST_PREC_FP32C)
+    k_scale_a<float><<<nblk(tot, 256), 256, 0, st>>>(d, c0, nact, (float *)o->ahat.p);
+  else
+    k_scale_a<double><<<nblk(tot, 256), 256, 0, st>>>(d, c0, nact, (double *)o->ahat.p);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st) {
+  if (!o->m2l_list) return DUST_OK;
+  // batch size, warps and chunk: the largest that fit 200 KB of shared memory
+  bool f32 = o->prm.precision == DUST_PREC_FP32C;
+  size_t esz = f32 ? 4 : 8;
+  int nout = o->prm.vortstretch ? o->nm1 : o->nm;
+  int NB = 8, NW = 2, TC = 2;
+  bool found = false;
+  const int isum_smem = (size_t)o->nm * o->nm1 * 2 <= 16 * 1024 ? 1 : 0;
+  const size_t isb = isum_smem ? (size_t)o->nm * o->nm1 * 2 + 16 : 0;
+  const int nbs[3] = {32, 16, 8}, nws[5] = {8, 6, 4, 3, 2}, tcs[3] = {8, 4, 2};
+  // two CTAs per SM when possible, else one
+  for (size_t cap : {(size_t)110 * 1024, (size_t)200 * 1024})
+    for (int b = 0; b < 5 && !found; ++b)
+      for (int a = 0; a < 3 && !found; ++a)
+        for (int c = 0; c < 3 && !found; ++c) {
+          size_t smx = (size_t)nbs[a] * nout * 24 + (size_t)nbs[a] * 12 + 32 + isb +
+                       esz * nws[b] * ((size_t)3 * o->nD + (size_t)tcs[c] * 3 * o->nm);
+          if (smx <= cap && (tcs[c] >= 4 || cap > 110 * 1024)) {
+            NB = nbs[a];
+            NW = nws[b];
+            TC = tcs[c];
+            found = true;
+          }
+        }
+  if (!found) return DUST_ERR_CAPACITY;
+  std::vector<int4> bs;
+  int start = 0;
+  for (int k = 0; k < 8 * (DUST_MAXLEV + 1); ++k) {
+    int c = o->m2l_cnt[k];
+    int l = k >> 3, q = k & 7;
+    if (l >= 2)
+      for (int b = 0; b < c; b += NB) bs.push_back(make_int4(l, q, start + b, std::min(NB, c - b)));
+    start += c;
+  }
+  if (bs.empty()) return DUST_OK;
+  DUST_TRY(devbuf_grow(o->m2l_bat, bs.size() * sizeof(int4)));
+  DUST_CUDA(cudaMemcpyAsync(o->m2l_bat.p, bs.data(), bs.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, st));
+  size_t sm = (size_t)NB * nout * 24 + (size_t)NB * 12 + 32 + isb +
+              esz * NW * ((size_t)3 * o->nD + (size_t)TC * 3 * o->nm);
+  M2LTabs tabs;
+  for (int l = 0; l <= DUST_MAXLEV; ++l)
+    tabs.t[l] = (l >= 2 && l <= o->G.ll) ? (f32 ? o->dtab32[l].p : o->dtabs[l].p) : nullptr;
+  unsigned grid = (unsigned)bs.size();
+  if (f32) {
+    if (sm > 48 * 1024)
+      DUST_CUDA(cudaFuncSetAttribute(k_m2l_batch<float>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_m2l_batch<float><<<grid, NW * 32, sm, st>>>(d, (const int4 *)o->m2l_bat.p, o->m2l_list,
+                                                NB, NW, TC, tabs, (const float *)o->ahat.p, o->ahat_c0,
+                                                isum_smem);
+  } else {
+    if (sm > 48 * 1024)
+      DUST_CUDA(cudaFuncSetAttribute(k_m2l_batch<double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_m2l_batch<double><<<grid, NW * 32, sm, st>>>(d, (const int4 *)o->m2l_bat.p, o->m2l_list,
+                                                 NB, NW, TC, tabs, (const double *)o->ahat.p,
+                                                 o->ahat_c0, isum_smem);
+  }
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}

@@ -50,6 +50,12 @@ class Linsys:
         check(lib().dust_linsys_assemble(self._h, C.byref(es), C.byref(ws)),
               "dust_linsys_assemble")
 
+    def sync(self):
+        """Wait for the handle's stream (assembly is asynchronous)."""
+        # dust_linsys_get_system with no outputs only synchronises the stream
+        check(lib().dust_linsys_get_system(self._h, abi.dptr(None), abi.dptr(None)),
+              "dust_linsys_get_system")
+
     def get_system(self):
         """dump_linsys: (A, b) as assembled (the static block holds its LU)."""
         A = np.empty(self.rank * self.rank)

@@ -111,6 +111,14 @@ class DeviceStepper:
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
         self.oc = Octree(params)
         self._ps = params.struct()
+        self.phase_events = False
+        self.events = []
+
+    def _mark(self):
+        if self.phase_events:
+            e = self.torch.cuda.Event(enable_timing=True)
+            e.record()
+            self.events.append(e)
 
     @staticmethod
     def _p(t, ctype=C.c_double):
@@ -121,6 +129,8 @@ class DeviceStepper:
         c = self.case
         P = self._p
         stream = torch.cuda.current_stream().cuda_stream
+        self.events = []
+        self._mark()
         el = abi.Panels(c.rank, P(self.env, C.c_int), P(self.ekind, C.c_int), P(self.ever),
                         P(self.emag), P(self.eub), P(self.euv))
         check(lib().dust_panels_centres_device(C.byref(el), P(self.ecen), C.c_void_p(stream)),
@@ -130,16 +140,21 @@ class DeviceStepper:
                                              P(self.cen), P(self.dir), P(self.mag), P(self.rv),
                                              C.byref(lines), P(self.euv), C.c_void_p(stream)),
               "dust_points_uvort_device")
+        self._mark()
         torch.cuda.current_stream().synchronize()
         wk = abi.WakeRows(abi.Panels(c.wake.n, P(self.wnv, C.c_int), P(self.wkind, C.c_int),
                                      P(self.wver), P(self.wmag), abi._dp(), abi._dp()),
                           c.n_impl, P(self.impl, C.c_int))
         check(lib().dust_linsys_assemble_device(self.ls._h, C.byref(el), C.byref(wk)),
               "dust_linsys_assemble_device")
+        if self.phase_events:
+            self.ls.sync()
+        self._mark()
         rep = abi.SolveReport()
         check(lib().dust_linsys_solve_device(self.ls._h, int(self.mode), P(self.res),
                                              C.byref(rep)), "dust_linsys_solve_device")
         self.last_report = {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+        self._mark()
         # element strengths and implicit wake panels (update_wake :881-889)
         self.emag.copy_(self.res)
         self.wmag.copy_(self.res[self.i1] - self.res[self.i2] * self.has2)
@@ -152,4 +167,5 @@ class DeviceStepper:
                                           P(self.mag), P(self.rv), C.byref(els), P(self.vel),
                                           P(self.str), P(self.rot), C.c_void_p(stream), 0),
               "dust_fmm_apply_device")
+        self._mark()
         return self.res

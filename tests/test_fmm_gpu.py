@@ -182,3 +182,75 @@ def test_edge_cases():
     ov, os_, _, _ = O.fmm_apply(prm, c, d, m, np.full(300, 0.02))
     v, s, _ = oc.apply_multipole(c, d, m, np.full(300, 0.02))
     assert rel(v, ov) < TOL64 and rel(s, os_) < TOL64
+
+
+TOL32 = 1e-6  # FP32 arithmetic with compensated accumulation, vs the FP64 oracle
+
+
+def _elements_case(rng):
+    wing, te = synth.flat_wing(span=2.0, chord=0.5, n_span=8, n_chord=4, alpha_deg=5.0)
+    wing.mag = rng.standard_normal(wing.n)
+    wing.kind[::3] = abi.DUST_ELEM_SURFPAN
+    wing.ub = rng.standard_normal((wing.n, 3)) * 0.1
+    wing.uvort = rng.standard_normal((wing.n, 3)) * 0.1
+    wake = wing.subset(te)
+    wake.ver = wake.ver + np.array([0.6, 0.0, 0.0])
+    wake.mag = rng.standard_normal(wake.n)
+    wake.kind[:] = abi.DUST_ELEM_VORTLATT
+    ev = abi.LineSet(np.array([[[1.1, -1.0, 0.0], [2.0, -1.0, 0.0]],
+                               [[1.1, 1.0, 0.0], [2.0, 1.0, 0.0]]]), np.array([0.3, -0.3]))
+    return abi.elements_struct(wing, wake, ev)
+
+
+@pytest.mark.parametrize("prec", [abi.DUST_PREC_FP64, abi.DUST_PREC_FP32C])
+def test_elements_far_field_path(prec):
+    """Particles far from small panels take the far-field fast path; the
+    result must equal the reference's tangent-frame formulas."""
+    rng = np.random.default_rng(8)
+    els = _elements_case(rng)
+    n = 3000
+    cen = rng.uniform(-8.0, 8.0, (n, 3))
+    dir_ = rng.standard_normal((n, 3))
+    dir_ /= np.linalg.norm(dir_, axis=1)[:, None]
+    mag = rng.uniform(1e-4, 2e-4, n)
+    rv = np.full(n, 0.1)
+    prm = FmmParams(box_length=16.0, origin=(-8.0, -8.0, -8.0), n_octree_levels=4,
+                    min_octree_part=5, multipole_degree=4, rankine_rad=0.1,
+                    u_inf=(0.0, 0.0, 0.0), precision=prec)
+    ov, _, _, _ = O.fmm_apply(prm, cen, dir_, mag, rv, els)
+    v, _, _ = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv, els)
+    tol = TOL64 if prec == abi.DUST_PREC_FP64 else TOL32
+    assert rel(v, ov) < tol
+
+
+def test_fp32c_uvort_and_elements():
+    rng = np.random.default_rng(5)
+    els = _elements_case(rng)
+    cen, dir_, mag, rv = ring(4000, seed=4)
+    prm = prm_ring(precision=abi.DUST_PREC_FP32C, rankine_rad=0.1, u_inf=(1.0, 0.0, 0.0))
+    ov, _, _, _ = O.fmm_apply(prm, cen, dir_, mag, rv, els)
+    v, _, _ = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv, els)
+    assert rel(v, ov) < TOL32
+    pts = rng.uniform(-1.5, 1.5, (500, 3))
+    ev = abi.LineSet(np.array([[[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]]]), np.array([0.7]))
+    uo = O.points_uvort(prm, pts, cen, dir_, mag, rv, ev)
+    ug = octree.points_uvort(prm, pts, cen, dir_, mag, rv, ev)
+    assert rel(ug, uo) < TOL32
+
+
+@pytest.mark.parametrize("p", [4, 6])
+def test_fmm_fp32c_matches_oracle(p):
+    cen, dir_, mag, rv = ring(4000, seed=12)
+    prm = prm_ring(multipole_degree=p, n_octree_levels=5, min_octree_part=5,
+                   precision=abi.DUST_PREC_FP32C)
+    ov, os_, orr, _ = O.fmm_apply(prm, cen, dir_, mag, rv)
+    v, s, r = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
+    assert rel(v, ov) < TOL32 and rel(s, os_) < TOL32 and rel(r, orr) < TOL32
+
+
+def test_fmm_degree8_matches_oracle():
+    cen, dir_, mag, rv = ring(2500, seed=13)
+    prm = prm_ring(multipole_degree=8, n_octree_levels=5, min_octree_part=5)
+    ov, os_, orr, _ = O.fmm_apply(prm, cen, dir_, mag, rv)
+    v, s, r = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
+    assert rel(v, ov) < TOL64 and rel(s, os_) < TOL64 and rel(r, orr) < TOL64
