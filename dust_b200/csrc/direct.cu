@@ -21,6 +21,8 @@
 // the CTA's particle tile (so no large-coordinate cancellation), partial
 // sums over a tile of sources are compensated (Knuth TwoSum) and then added
 // into FP64 accumulators; near pairs stay FP64.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cstring>
 
@@ -267,6 +269,85 @@ __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, in
   for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
 }
 
+// FP32C uvort on particles sorted along a Morton curve: a tile of 128
+// consecutive particles is spatially compact, so coordinates relative to the
+// tile's first particle are small and are rounded to FP32 once per tile.
+__global__ void k_uv_keys(int n, const double *cen, double x0, double y0, double z0,
+                          double inv_h, uint32_t *keys, uint32_t *vals) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  double c[3] = {cen[3 * (size_t)q] - x0, cen[3 * (size_t)q + 1] - y0, cen[3 * (size_t)q + 2] - z0};
+  uint32_t k[3];
+  for (int d = 0; d < 3; ++d) {
+    double v = c[d] * inv_h;
+    k[d] = v <= 0.0 ? 0u : (v >= 1023.0 ? 1023u : (uint32_t)v);
+  }
+  keys[q] = spread3(k[0]) | (spread3(k[1]) << 1) | (spread3(k[2]) << 2);
+  vals[q] = (uint32_t)q;
+}
+
+// sorted block: x y z (double), ax ay az s2 (float)
+__global__ void k_uv_gather(int n, const uint32_t *perm, const double *cen, const double *dir,
+                            const double *mag, const double *rv, double *X, float *F) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t q = perm[t];
+  double m = mag[q];
+  for (int d = 0; d < 3; ++d) {
+    X[(size_t)d * n + t] = cen[3 * (size_t)q + d];
+    F[(size_t)d * n + t] = (float)(m * dir[3 * (size_t)q + d]);
+  }
+  F[(size_t)3 * n + t] = (float)(rv[q] * rv[q]);
+}
+
+__global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *pts, int n,
+                                                        const double *X, const float *F,
+                                                        int chunk, double *uv) {
+  __shared__ float f_x[UV2_TILE][3], f_a[UV2_TILE][3], f_s2[UV2_TILE];
+  __shared__ double s_ref[3];
+  const int t = blockIdx.x * UV2_T + threadIdx.x;
+  const bool act = t < npts;
+  const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
+  double pos[3] = {0, 0, 0};
+  if (act)
+    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
+  double v[3] = {0, 0, 0};
+  for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
+    __syncthreads();
+    const int q = q0 + threadIdx.x;
+    const int m = min(UV2_TILE, q_hi - q0);
+    if (threadIdx.x < 3) s_ref[threadIdx.x] = X[(size_t)threadIdx.x * n + q0];
+    __syncthreads();
+    if (threadIdx.x < m) {
+      for (int c = 0; c < 3; ++c) {
+        f_x[threadIdx.x][c] = (float)(X[(size_t)c * n + q] - s_ref[c]);
+        f_a[threadIdx.x][c] = F[(size_t)c * n + q];
+      }
+      f_s2[threadIdx.x] = F[(size_t)3 * n + q];
+    }
+    __syncthreads();
+    if (!act) continue;
+    const float px = (float)(pos[0] - s_ref[0]), py = (float)(pos[1] - s_ref[1]),
+                pz = (float)(pos[2] - s_ref[2]);
+    f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
+    for (int u = 0; u < m; ++u) {
+      float dx = px - f_x[u][0], dy = py - f_x[u][1], dz = pz - f_x[u][2];
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, f_s2[u])));
+      float ir = rsqrtf(r2);
+      float c = -ir * ir * ir;
+      two_sum_acc(ax, c * (dy * f_a[u][2] - dz * f_a[u][1]));
+      two_sum_acc(ay, c * (dz * f_a[u][0] - dx * f_a[u][2]));
+      two_sum_acc(az, c * (dx * f_a[u][1] - dy * f_a[u][0]));
+    }
+    v[0] += (double)ax.s + (double)ax.c;
+    v[1] += (double)ay.s + (double)ay.c;
+    v[2] += (double)az.s + (double)az.c;
+  }
+  if (!act) return;
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
+}
+
 __global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts) return;
@@ -281,9 +362,9 @@ __global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv
   for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
 }
 
-int points_uvort_run(int precision, int n_pts, const double *pts, int n, const double *cen,
-                     const double *dir, const double *mag, const double *rv,
-                     const ElemDev &lines, double *uv, cudaStream_t st) {
+int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                     const double *cen, const double *dir, const double *mag, const double *rv,
+                     const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st) {
   if (n_pts <= 0) return DUST_OK;
   DUST_CUDA(cudaMemsetAsync(uv, 0, (size_t)n_pts * 24, st));
   if (n > 0) {
@@ -294,10 +375,31 @@ int points_uvort_run(int precision, int n_pts, const double *pts, int n, const d
     chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);
     int nch = (n + chunk - 1) / chunk;
     dim3 grd(pb, nch);
-    if (precision == DUST_PREC_FP32C)
-      k_uvort<true><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
-    else
+    if (prm->precision == DUST_PREC_FP32C) {
+      // Morton-sort the particles over the octree box (order only matters
+      // for accuracy of the tile-relative FP32 coordinates)
+      size_t N = (size_t)n;
+      size_t tb = 0;
+      uint32_t *dummy = nullptr;
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, dummy, dummy, dummy, dummy, n, 0, 30, st);
+      size_t off_f = (16 * N + 255) / 256 * 256;
+      size_t off_x = off_f + (16 * N + 255) / 256 * 256;
+      size_t off_t = off_x + (24 * N + 255) / 256 * 256;
+      DUST_TRY(devbuf_grow(scratch, off_t + tb + 256));
+      char *b = (char *)scratch.p;
+      uint32_t *k_in = (uint32_t *)b, *v_in = k_in + N, *k_out = v_in + N, *v_out = k_out + N;
+      float *F = (float *)(b + off_f);
+      double *X = (double *)(b + off_x);
+      double hbox = prm->box_length * std::max(prm->n_box[0], std::max(prm->n_box[1], prm->n_box[2]));
+      k_uv_keys<<<nblk(n, 256), 256, 0, st>>>(n, cen, prm->origin[0], prm->origin[1],
+                                               prm->origin[2], 1024.0 / hbox, k_in, v_in);
+      DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
+                                                st));
+      k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, rv, X, F);
+      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uv);
+    } else {
       k_uvort<false><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
+    }
   }
   if (lines.nline > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, lines, uv);
   DUST_CUDA(cudaGetLastError());

@@ -283,10 +283,12 @@ extern "C" int dust_elements_vel(const dust_fmm_params *prm, int n_pts, const do
   return DUST_OK;
 }
 
+static DevBuf g_uv_scratch;  // sort scratch of the uvort entry points (one host thread)
+
 int points_uvort_device(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                         const double *cen, const double *dir, const double *mag,
                         const double *rv, const ElemDev &lines, double *uv, cudaStream_t st) {
-  return points_uvort_run(prm->precision, n_pts, pts, n, cen, dir, mag, rv, lines, uv, st);
+  return points_uvort_run(prm, n_pts, pts, n, cen, dir, mag, rv, lines, g_uv_scratch, uv, st);
 }
 
 extern "C" int dust_points_uvort(const dust_fmm_params *prm, int n_pts, const double *pts,

@@ -100,6 +100,6 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
 // direct.cu
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
                        double *str, double *rot, cudaStream_t st);
-int points_uvort_run(int precision, int n_pts, const double *pts, int n, const double *cen,
-                     const double *dir, const double *mag, const double *rv,
-                     const ElemDev &lines, double *uv, cudaStream_t st);
+int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                     const double *cen, const double *dir, const double *mag, const double *rv,
+                     const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st);

@@ -17,6 +17,9 @@ struct dust_linsys {
   DevBuf A;     // column-major rank x rank, FP64; static block holds its LU
   DevBuf As;    // unfactored static block (nst x nst) for residuals
   DevBuf b, bst, piv, info, geo, raw, impl, work, A32, gm;
+  DevBuf ainv32;  // FP32 inverse of the static block (mixed solve)
+  DevBuf mx;      // mixed-solve work: Schur complement, coupling blocks, vectors
+  bool ainv_ready = false;
   LuWork lu;
   const PanelGeo *el = nullptr, *wk = nullptr;
   int nwake = 0, n_impl = 0;
@@ -25,6 +28,10 @@ struct dust_linsys {
 
 int linsys_solve_lu64(dust_linsys *L, double *res_dev);
 int linsys_solve_iterative(dust_linsys *L, int mode, double *x_dev, dust_solve_report *rep);
+// Static/moving Schur solve in FP32/TF32 refined to FP64 (tol on the
+// normwise backward error ||b-Ax|| / (||A|| ||x||), max_iter refinements).
+int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter,
+                             dust_solve_report *rep);
 void linsys_shift_pivots(cudaStream_t st, int *P, int n, int off);
 
 // Mixed-precision dense solve on device arrays: FP32 LU (tensor-core

@@ -243,6 +243,18 @@ int linsys_gmres_nn(dust_linsys *L, const double *Af, double *x, dust_solve_repo
 
 int linsys_solve_iterative(dust_linsys *L, int mode, double *x_dev, dust_solve_report *rep) {
   size_t n = L->n;
+  if (mode == DUST_SOLVE_MIXED) {
+    int s = linsys_solve_schur_mixed(L, x_dev, 1e-14, 30, rep);
+    if (s == DUST_OK) {
+      L->factored = true;
+      return DUST_OK;
+    }
+    if (s != DUST_ERR_NOT_CONVERGED && s != DUST_ERR_SINGULAR) return s;
+    if (rep) rep->fell_back = 1;
+    DUST_TRY(linsys_solve_lu64(L, x_dev));
+    if (rep) rep->mode_used = DUST_SOLVE_LU64;
+    return DUST_OK;
+  }
   DUST_TRY(devbuf_grow(L->gm, n * n * 8 + 256));
   double *Af = (double *)L->gm.p;
   DUST_TRY(linsys_full_matrix(L, Af));

@@ -274,6 +274,15 @@ DUST_API int dust_linsys_get_system(dust_linsys *ls, double *A, double *b);
 DUST_API int dust_dense_solve(int n, int nrhs, const double *A, const double *B,
                      double *X, int mode, double tol, dust_solve_report *rep);
 
+/* Tensor-core (tcgen05, kind::tf32) update C -= A B on device arrays
+ * (column-major FP32, read as TF32, FP32 accumulation): the trailing update
+ * of the mixed-precision LU (the dgemm of mod_linsys.f90:428-438 in its
+ * low-precision form).  Synchronises `stream`; DUST_ERR_TIMEOUT if a bounded
+ * wait inside the kernel gave up. */
+DUST_API int dust_tc_gemm_tf32_minus(int m, int n, int k, const float *A, int lda,
+                                     const float *B, int ldb, float *C, int ldc,
+                                     void *stream);
+
 /* ---------------------------------------------------------------- misc */
 DUST_API const char *dust_status_string(int status);
 DUST_API const char *dust_last_error(void); /* text of the last CUDA error seen      */

@@ -85,8 +85,34 @@ def test_linsys_body_rotor_matches_oracle():
     # mixed precision on the same system
     ls.assemble_linsys(els, wake, n_impl, ind)
     res3, rep3 = ls.solve_linsys(abi.DUST_SOLVE_MIXED)
-    assert rep3["residual"] <= 1e-12
+    assert rep3["mode_used"] == abi.DUST_SOLVE_MIXED and rep3["fell_back"] == 0
+    assert rep3["residual"] <= 1e-14
     assert rel(res3, ro2) < 1e-9
+    # mixed twice in a row, then plain again: the handle's LU stays usable
+    ls.assemble_linsys(els, wake, n_impl, ind)
+    res4, rep4 = ls.solve_linsys(abi.DUST_SOLVE_MIXED)
+    assert rep4["fell_back"] == 0 and rel(res4, ro2) < 1e-9
+    ls.assemble_linsys(els, wake, n_impl, ind)
+    res5, _ = ls.solve_linsys(abi.DUST_SOLVE_LU64)
+    assert rel(res5, ro2) < 1e-10
+
+
+@pytest.mark.parametrize("nst_frac", [1.0, 0.7, 0.0])
+def test_linsys_mixed_schur_matches_oracle(nst_frac):
+    prm = FmmParams(u_inf=(1.0, 0.0, 0.0), rankine_rad=0.1)
+    wing, wk, n_impl, ind = wing_case(n_span=20, n_chord=8)
+    rng = np.random.default_rng(5)
+    wing.uvort = rng.standard_normal((wing.n, 3)) * 0.05
+    n = wing.n
+    nst = int(n * nst_frac)
+    _, _, ro = O.linsys_run(prm, n, nst, wing, wing, (wk, n_impl, ind), (wk, n_impl, ind))
+    ls = linsys.initialize_linsys(prm, n, nst, wing, wk, n_impl, ind)
+    for _ in range(2):
+        ls.assemble_linsys(wing, wk, n_impl, ind)
+        res, rep = ls.solve_linsys(abi.DUST_SOLVE_MIXED)
+        assert rep["mode_used"] == abi.DUST_SOLVE_MIXED and rep["fell_back"] == 0
+        assert rep["residual"] <= 1e-14
+        assert rel(res, ro) < 1e-10
 
 
 @pytest.mark.parametrize("n,nrhs", [(1, 1), (63, 1), (64, 3), (200, 2), (1000, 4)])
