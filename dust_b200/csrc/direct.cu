@@ -405,3 +405,101 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }
+
+// ------------------------------------------------- uvort without allocation
+// dust_points_uvort_device_noalloc: the same sums as dust_points_uvort_device
+// (same kernels, same order of operations) for callers that must not
+// allocate device memory during a step.  Its only scratch (end-vortex
+// geometry, and in the FP32C mode the Morton keys, the sorted particle copy
+// and the radix-sort work space) lives in the fixed array below, reserved
+// when the library is loaded.
+static __device__ __align__(256) unsigned char g_uv_noalloc[DUST_UVORT_NOALLOC_SCRATCH];
+static void *g_uv_noalloc_ptr[64];  // per device, looked up on the first call there
+
+__global__ void k_line_build(int n, const double *ver, const double *mag, LineGeo *out);
+
+static inline size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int n_pts,
+                                                const double *pts, int n, const double *cen,
+                                                const double *dir, const double *mag,
+                                                const double *r_vortex,
+                                                const dust_lines *end_vort, double *uvort,
+                                                void *stream) {
+  if (!prm || n_pts < 0 || n < 0) return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  const int nl = end_vort ? end_vort->n : 0;
+  if (nl < 0) return DUST_ERR_BAD_ARG;
+  const bool f32 = prm->precision == DUST_PREC_FP32C && n > 0;
+  const size_t N = (size_t)n;
+  // scratch layout: [LineGeo x nl][keys/vals 16N][F 16N][X 24N][sort work]
+  const size_t off_p = round256(sizeof(LineGeo) * (size_t)nl);
+  const size_t off_f = off_p + (f32 ? round256(16 * N) : 0);
+  const size_t off_x = off_f + (f32 ? round256(16 * N) : 0);
+  const size_t off_t = off_x + (f32 ? round256(24 * N) : 0);
+  char msg[160];
+  if (off_t > DUST_UVORT_NOALLOC_SCRATCH) {
+    snprintf(msg, sizeof(msg), "uvort no-alloc scratch: %zu bytes needed, %u available", off_t,
+             (unsigned)DUST_UVORT_NOALLOC_SCRATCH);
+    dust_set_last_error(msg, __FILE__, __LINE__);
+    return DUST_ERR_CAPACITY;
+  }
+  size_t tb = 0;
+  if (f32) {
+    uint32_t *dummy = nullptr;
+    DUST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, dummy, dummy, dummy, dummy, n, 0, 30,
+                                              (cudaStream_t)stream));
+  }
+  const size_t need = off_t + round256(tb);
+  if (need > DUST_UVORT_NOALLOC_SCRATCH) {
+    snprintf(msg, sizeof(msg), "uvort no-alloc scratch: %zu bytes needed, %u available", need,
+             (unsigned)DUST_UVORT_NOALLOC_SCRATCH);
+    dust_set_last_error(msg, __FILE__, __LINE__);
+    return DUST_ERR_CAPACITY;
+  }
+  int dev = 0;
+  DUST_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return DUST_ERR_NO_DEVICE;
+  if (!g_uv_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    DUST_CUDA(cudaGetSymbolAddress(&p, g_uv_noalloc));
+    g_uv_noalloc_ptr[dev] = p;
+  }
+  char *b = (char *)g_uv_noalloc_ptr[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+  ElemDev e;
+  memset(&e, 0, sizeof(e));
+  e.rp = reg_params(prm);
+  e.nline = nl;
+  e.lines = (const LineGeo *)b;
+  if (nl > 0) k_line_build<<<nblk(nl, 128), 128, 0, st>>>(nl, end_vort->ver, end_vort->mag,
+                                                          (LineGeo *)b);
+  DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
+  if (n > 0) {
+    int pb = (int)nblk(n_pts, UV2_T);
+    int want = std::max(1, (148 * 8 + pb - 1) / pb);
+    int chunk = (n + want - 1) / want;
+    chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);
+    int nch = (n + chunk - 1) / chunk;
+    dim3 grd(pb, nch);
+    if (f32) {
+      uint32_t *k_in = (uint32_t *)(b + off_p), *v_in = k_in + N, *k_out = v_in + N,
+               *v_out = k_out + N;
+      float *F = (float *)(b + off_f);
+      double *X = (double *)(b + off_x);
+      double hbox =
+          prm->box_length * std::max(prm->n_box[0], std::max(prm->n_box[1], prm->n_box[2]));
+      k_uv_keys<<<nblk(n, 256), 256, 0, st>>>(n, cen, prm->origin[0], prm->origin[1],
+                                               prm->origin[2], 1024.0 / hbox, k_in, v_in);
+      DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
+                                                st));
+      k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, r_vortex, X, F);
+      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uvort);
+    } else {
+      k_uvort<false><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, r_vortex, chunk, uvort);
+    }
+  }
+  if (nl > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, e, uvort);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}

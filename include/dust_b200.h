@@ -187,6 +187,37 @@ DUST_API int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts,
                                       const dust_lines *end_vort, double *uvort,
                                       void *stream);
 
+/* No counterpart in the reference.  Same result as dust_points_uvort_device
+ * (same kernels and summation order) for callers that must not allocate
+ * device memory during a step: a host code that hands the whole device to
+ * its own pool or caching allocator (a cudaMalloc would fail or evict it), or
+ * one that cannot afford the device-wide synchronisation of cudaFree inside
+ * its time loop.  This entry point calls no cudaMalloc/cudaFree nor any
+ * allocating library routine: its scratch (end-vortex geometry, and in the
+ * FP32C mode the Morton keys, the sorted particle copy and the radix-sort
+ * work space, about 56 bytes per particle plus the sort work) is a fixed
+ * device array of DUST_UVORT_NOALLOC_SCRATCH bytes inside the library,
+ * reserved when the library is loaded.
+ *   - Sizes that need more scratch than that return DUST_ERR_CAPACITY before
+ *     anything is launched; dust_last_error() names the bytes needed.  The
+ *     FP64 mode needs scratch only for the end vortices (88 bytes each).
+ *   - Nothing has to start at zero: the scratch is written before it is
+ *     read, and uvort is overwritten (zeroed on `stream`, then summed).
+ *   - The scratch is one array per device, shared by every call: calls that
+ *     overlap in time (two streams, or two host threads) race on it and give
+ *     wrong results.  Serialise them.
+ *   - The first call on each device looks the array up
+ *     (cudaGetSymbolAddress, which also loads the library's device code); a
+ *     caller that records its stream into a graph should make that first
+ *     call before it starts capturing. */
+#define DUST_UVORT_NOALLOC_SCRATCH (4u << 20)
+DUST_API int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int n_pts,
+                                              const double *pts, int n,
+                                              const double *cen, const double *dir,
+                                              const double *mag, const double *r_vortex,
+                                              const dust_lines *end_vort, double *uvort,
+                                              void *stream);
+
 /* Panel centres (calc_geo_data) of a device-resident panel set into
  * cen(3,n) in device memory. */
 DUST_API int dust_panels_centres_device(const dust_panels *pan, double *cen,
