@@ -18,9 +18,10 @@
 //
 // Precision.  FP64 everywhere in the plain mode.  In the FP32C mode the far
 // field runs in FP32 on coordinates taken relative to a reference point of
-// the CTA's particle tile (so no large-coordinate cancellation), partial
-// sums over a tile of sources are compensated (Knuth TwoSum) and then added
-// into FP64 accumulators; near pairs stay FP64.
+// the CTA's particle tile (so no large-coordinate cancellation); partial
+// sums over one tile of sources are FP32 and are added into FP64
+// accumulators tile by tile; near pairs stay FP64 (queued and evaluated
+// apart from the FP32 loop, k_elem_out_split).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -179,6 +180,131 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
   }
 }
 
+// FP32C element sums with the near pairs split off.  The far-field test
+// and formula run in FP32 for EF2_PPT particles per thread against a
+// shared-memory tile of EF2_TILE panels; a pair that is not clearly far
+// (threshold widened by 1e-4 so a pair far in FP32 is far in FP64) is queued
+// in shared memory instead of being evaluated in the loop, and after each
+// tile the whole CTA evaluates the queued pairs densely with the reference's
+// exact FP64 formulas (vel_pan), accumulating per particle with shared
+// atomics.  Keeping the rare near pairs (about 0.5 % of all, but in a few
+// percent of the warp iterations) out of the FP32 loop removes the
+// divergence that otherwise dominates.  Far partial sums are FP32 over one
+// tile and FP64 across tiles.
+#define EF2_T 128
+#define EF2_PPT 2
+#define EF2_NP (EF2_T * EF2_PPT)
+#define EF2_TILE 32
+#define EF2_QCAP (EF2_NP * EF2_TILE)
+
+__global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, const FFRec *ff,
+                                                          double *vel, double *str, double *rot) {
+  __shared__ float4 s_cf[EF2_TILE];  // centre - ref, widened ff2
+  __shared__ float4 s_nm[EF2_TILE];  // normal, area * mag
+  __shared__ float s_as[EF2_TILE];   // area * sigma
+  __shared__ double s_pos[EF2_NP][3];
+  __shared__ double s_near[EF2_NP][3];
+  __shared__ uint16_t s_q[EF2_QCAP];  // (local particle << 5) | panel in tile
+  __shared__ int s_qn;
+  const size_t n = d.n;
+  const uint32_t t0 = blockIdx.x * EF2_NP;
+  const int tid = threadIdx.x;
+  const double ref[3] = {d.P[t0], d.P[n + t0], d.P[2 * n + t0]};
+  float px[EF2_PPT], py[EF2_PPT], pz[EF2_PPT];
+  bool act[EF2_PPT];
+  double v[EF2_PPT][3];
+#pragma unroll
+  for (int i = 0; i < EF2_PPT; ++i) {
+    const int lp = tid + i * EF2_T;
+    const uint32_t t = t0 + lp;
+    act[i] = t < n;
+    double pos[3] = {ref[0], ref[1], ref[2]};
+    if (act[i])
+      for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
+    px[i] = (float)(pos[0] - ref[0]);
+    py[i] = (float)(pos[1] - ref[1]);
+    pz[i] = (float)(pos[2] - ref[2]);
+    for (int c = 0; c < 3; ++c) {
+      s_pos[lp][c] = pos[c];
+      s_near[lp][c] = 0.0;
+      v[i][c] = 0.0;
+    }
+  }
+  const int ntot = e.nbody + e.nwake;
+  for (int p0 = 0; p0 < ntot; p0 += EF2_TILE) {
+    const int m = min(EF2_TILE, ntot - p0);
+    __syncthreads();
+    if (tid < m) {
+      const FFRec &r = ff[p0 + tid];
+      s_cf[tid] = make_float4((float)(r.c[0] - ref[0]), (float)(r.c[1] - ref[1]),
+                              (float)(r.c[2] - ref[2]), (float)r.ff2 * 1.0001f);
+      s_nm[tid] = make_float4((float)r.n[0], (float)r.n[1], (float)r.n[2], (float)r.amu);
+      s_as[tid] = (float)r.asig;
+    }
+    if (tid == 0) s_qn = 0;
+    __syncthreads();
+    float acc[EF2_PPT][3];
+#pragma unroll
+    for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
+    for (int q = 0; q < m; ++q) {
+      const float4 cf = s_cf[q], nm = s_nm[q];
+      const float as = s_as[q];
+#pragma unroll
+      for (int i = 0; i < EF2_PPT; ++i) {
+        const float rx = px[i] - cf.x, ry = py[i] - cf.y, rz = pz[i] - cf.z;
+        const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        if (r2 > cf.w) {
+          const float ir = rsqrtf(r2);
+          const float ir2 = ir * ir;
+          const float rn = fmaf(rx, nm.x, fmaf(ry, nm.y, rz * nm.z));
+          const float k3 = ir2 * ir;
+          const float coef = fmaf(3.0f * nm.w * rn, ir2, as);
+          acc[i][0] = fmaf(k3, fmaf(coef, rx, -nm.w * nm.x), acc[i][0]);
+          acc[i][1] = fmaf(k3, fmaf(coef, ry, -nm.w * nm.y), acc[i][1]);
+          acc[i][2] = fmaf(k3, fmaf(coef, rz, -nm.w * nm.z), acc[i][2]);
+        } else if (act[i]) {
+          const int slot = atomicAdd(&s_qn, 1);
+          s_q[slot] = (uint16_t)(((tid + i * EF2_T) << 5) | q);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < EF2_PPT; ++i)
+      for (int c = 0; c < 3; ++c) v[i][c] += (double)acc[i][c];
+    __syncthreads();
+    const int qn = s_qn;
+    for (int k = tid; k < qn; k += EF2_T) {
+      const int lp = s_q[k] >> 5, j = p0 + (s_q[k] & 31);
+      const PanelGeo *pg = j < e.nbody ? e.body + j : e.wake + (j - e.nbody);
+      double u[3];
+      vel_pan(e.rp, *pg, s_pos[lp], u);
+      for (int c = 0; c < 3; ++c) atomicAdd(&s_near[lp][c], u[c]);
+    }
+  }
+  __syncthreads();
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+#pragma unroll
+  for (int i = 0; i < EF2_PPT; ++i) {
+    if (!act[i]) continue;
+    const int lp = tid + i * EF2_T;
+    const uint32_t t = t0 + lp;
+    double w[3] = {v[i][0] + s_near[lp][0], v[i][1] + s_near[lp][1], v[i][2] + s_near[lp][2]};
+    for (int q = 0; q < e.nline; ++q) {
+      double u[3];
+      vel_line(e.rp, e.lines[q], s_pos[lp], u);
+      for (int c = 0; c < 3; ++c) w[c] += u[c];
+    }
+    const uint32_t ip = d.perm[t];
+    for (int c = 0; c < 3; ++c) {
+      vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + w[c] * k4pi + d.u_inf[c];
+      if (str)
+        str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
+      if (rot)
+        rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
+    }
+  }
+}
+
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
                        double *str, double *rot, cudaStream_t st) {
   int ntot = e.nbody + e.nwake;
@@ -189,7 +315,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision
     k_ffrec<<<nblk(e.nwake, 128), 128, 0, st>>>(e.wake, e.nwake, e.rp.ff_dou, ff + e.nbody);
   if (d.n > 0) {
     if (precision == DUST_PREC_FP32C)
-      k_elem_out<true><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
+      k_elem_out_split<<<nblk(d.n, EF2_NP), EF2_T, 0, st>>>(d, e, ff, vel, str, rot);
     else
       k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
   }
@@ -303,7 +429,10 @@ __global__ void k_uv_gather(int n, const uint32_t *perm, const double *cen, cons
 __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *pts, int n,
                                                         const double *X, const float *F,
                                                         int chunk, double *uv) {
-  __shared__ float f_x[UV2_TILE][3], f_a[UV2_TILE][3], f_s2[UV2_TILE];
+  // one tile of particles per pass: (x, y, z relative to the tile's first
+  // particle, core radius^2) and (alpha) as float4; partial sums over the
+  // tile in FP32, added into FP64 per tile
+  __shared__ float4 s_xs[UV2_TILE], s_al[UV2_TILE];
   __shared__ double s_ref[3];
   const int t = blockIdx.x * UV2_T + threadIdx.x;
   const bool act = t < npts;
@@ -319,29 +448,31 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
     if (threadIdx.x < 3) s_ref[threadIdx.x] = X[(size_t)threadIdx.x * n + q0];
     __syncthreads();
     if (threadIdx.x < m) {
-      for (int c = 0; c < 3; ++c) {
-        f_x[threadIdx.x][c] = (float)(X[(size_t)c * n + q] - s_ref[c]);
-        f_a[threadIdx.x][c] = F[(size_t)c * n + q];
-      }
-      f_s2[threadIdx.x] = F[(size_t)3 * n + q];
+      s_xs[threadIdx.x] = make_float4((float)(X[q] - s_ref[0]), (float)(X[(size_t)n + q] - s_ref[1]),
+                                      (float)(X[2 * (size_t)n + q] - s_ref[2]),
+                                      F[(size_t)3 * n + q]);
+      s_al[threadIdx.x] =
+          make_float4(F[q], F[(size_t)n + q], F[2 * (size_t)n + q], 0.f);
     }
     __syncthreads();
     if (!act) continue;
     const float px = (float)(pos[0] - s_ref[0]), py = (float)(pos[1] - s_ref[1]),
                 pz = (float)(pos[2] - s_ref[2]);
-    f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
     for (int u = 0; u < m; ++u) {
-      float dx = px - f_x[u][0], dy = py - f_x[u][1], dz = pz - f_x[u][2];
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, f_s2[u])));
-      float ir = rsqrtf(r2);
-      float c = -ir * ir * ir;
-      two_sum_acc(ax, c * (dy * f_a[u][2] - dz * f_a[u][1]));
-      two_sum_acc(ay, c * (dz * f_a[u][0] - dx * f_a[u][2]));
-      two_sum_acc(az, c * (dx * f_a[u][1] - dy * f_a[u][0]));
+      const float4 xs = s_xs[u], al = s_al[u];
+      const float dx = px - xs.x, dy = py - xs.y, dz = pz - xs.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xs.w)));
+      const float ir = rsqrtf(r2);
+      const float c = -ir * ir * ir;
+      ax = fmaf(c, fmaf(dy, al.z, -dz * al.y), ax);
+      ay = fmaf(c, fmaf(dz, al.x, -dx * al.z), ay);
+      az = fmaf(c, fmaf(dx, al.y, -dy * al.x), az);
     }
-    v[0] += (double)ax.s + (double)ax.c;
-    v[1] += (double)ay.s + (double)ay.c;
-    v[2] += (double)az.s + (double)az.c;
+    v[0] += (double)ax;
+    v[1] += (double)ay;
+    v[2] += (double)az;
   }
   if (!act) return;
   const double k4pi = 1.0 / (4.0 * DUST_PI);
