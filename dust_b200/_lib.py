@@ -8,7 +8,8 @@ import os
 import re
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-SO_PATH = os.path.join(_HERE, "_lib", "libdust_b200.so")
+# DUST_B200_LIB selects another build of the same library (same ABI)
+SO_PATH = os.environ.get("DUST_B200_LIB") or os.path.join(_HERE, "_lib", "libdust_b200.so")
 HEADER = os.path.join(os.path.dirname(_HERE), "include", "dust_b200.h")
 
 _lib = None

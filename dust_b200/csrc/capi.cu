@@ -95,8 +95,7 @@ extern "C" int dust_fmm_apply(dust_octree *o, int n, const double *cen, const do
     if (rotu) DUST_CUDA(cudaMemcpyAsync(rotu, orr, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
   }
   DUST_CUDA(cudaStreamSynchronize(st));
-  fmm_collect_stats(o, n, n_elem_of(elems));
-  return DUST_OK;
+  return fmm_collect_stats(o, n, n_elem_of(elems));
 }
 
 extern "C" int dust_fmm_apply_device(dust_octree *o, int n, const double *cen,
@@ -114,6 +113,6 @@ extern "C" int dust_fmm_apply_device(dust_octree *o, int n, const double *cen,
   DUST_TRY(fmm_run_device(o, n, cen, dir, mag, r_vortex, st));
   DUST_TRY(fmm_finish_device(o, n, e, vel, stretch, rotu, st));
   if (sync) DUST_CUDA(cudaStreamSynchronize(st));
-  if (o->timing || sync) fmm_collect_stats(o, n, n_elem_of(elems));
+  if (o->timing || sync) return fmm_collect_stats(o, n, n_elem_of(elems));
   return DUST_OK;
 }

@@ -184,27 +184,41 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
 // and formula run in FP32 for EF2_PPT particles per thread against a
 // shared-memory tile of EF2_TILE panels; a pair that is not clearly far
 // (threshold widened by 1e-4 so a pair far in FP32 is far in FP64) is queued
-// in shared memory instead of being evaluated in the loop, and after each
-// tile the whole CTA evaluates the queued pairs densely with the reference's
-// exact FP64 formulas (vel_pan), accumulating per particle with shared
-// atomics.  Keeping the rare near pairs (about 0.5 % of all, but in a few
-// percent of the warp iterations) out of the FP32 loop removes the
-// divergence that otherwise dominates.  Far partial sums are FP32 over one
-// tile and FP64 across tiles.
+// in shared memory instead of being evaluated in the loop.  Whenever the
+// queue could not take another full tile, and once at the end, the whole CTA
+// evaluates the queued pairs densely with the reference's exact FP64
+// formulas (vel_pan), accumulating per particle with shared atomics.  Keeping
+// the rare near pairs (about 0.5 % of all, but in a few percent of the warp
+// iterations) out of the FP32 loop removes the divergence that otherwise
+// dominates.  Far partial sums are FP32 over one tile, FP64 across tiles.
 #define EF2_T 128
+#ifndef EF2_PPT
 #define EF2_PPT 2
+#endif
 #define EF2_NP (EF2_T * EF2_PPT)
-#define EF2_TILE 32
-#define EF2_QCAP (EF2_NP * EF2_TILE)
+#define EF2_TILE 16
+#define EF2_QCAP (2 * EF2_NP * EF2_TILE)
+
+__device__ __forceinline__ void ef2_flush(const ElemDev &e, const uint32_t *s_q, int qn,
+                                          const double (*s_pos)[3], double (*s_near)[3]) {
+  for (int k = threadIdx.x; k < qn; k += EF2_T) {
+    const uint32_t en = s_q[k];
+    const int lp = en & 0x3ff, j = (int)(en >> 10);
+    const PanelGeo *pg = j < e.nbody ? e.body + j : e.wake + (j - e.nbody);
+    double u[3];
+    vel_pan(e.rp, *pg, s_pos[lp], u);
+    for (int c = 0; c < 3; ++c) atomicAdd(&s_near[lp][c], u[c]);
+  }
+}
 
 __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, const FFRec *ff,
                                                           double *vel, double *str, double *rot) {
   __shared__ float4 s_cf[EF2_TILE];  // centre - ref, widened ff2
-  __shared__ float4 s_nm[EF2_TILE];  // normal, area * mag
-  __shared__ float s_as[EF2_TILE];   // area * sigma
+  __shared__ float4 s_nm[EF2_TILE];  // normal, 3 * area * mag
+  __shared__ float4 s_mn[EF2_TILE];  // -area * mag * normal, area * sigma
   __shared__ double s_pos[EF2_NP][3];
   __shared__ double s_near[EF2_NP][3];
-  __shared__ uint16_t s_q[EF2_QCAP];  // (local particle << 5) | panel in tile
+  __shared__ uint32_t s_q[EF2_QCAP];  // (panel << 10) | local particle
   __shared__ int s_qn;
   const size_t n = d.n;
   const uint32_t t0 = blockIdx.x * EF2_NP;
@@ -230,25 +244,31 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
       v[i][c] = 0.0;
     }
   }
+  if (tid == 0) s_qn = 0;
   const int ntot = e.nbody + e.nwake;
   for (int p0 = 0; p0 < ntot; p0 += EF2_TILE) {
     const int m = min(EF2_TILE, ntot - p0);
     __syncthreads();
+    // a full tile can add up to EF2_NP * EF2_TILE entries
+    if (s_qn > EF2_QCAP - EF2_NP * EF2_TILE) {
+      ef2_flush(e, s_q, s_qn, s_pos, s_near);
+      __syncthreads();
+      if (tid == 0) s_qn = 0;
+    }
     if (tid < m) {
       const FFRec &r = ff[p0 + tid];
       s_cf[tid] = make_float4((float)(r.c[0] - ref[0]), (float)(r.c[1] - ref[1]),
                               (float)(r.c[2] - ref[2]), (float)r.ff2 * 1.0001f);
-      s_nm[tid] = make_float4((float)r.n[0], (float)r.n[1], (float)r.n[2], (float)r.amu);
-      s_as[tid] = (float)r.asig;
+      s_nm[tid] = make_float4((float)r.n[0], (float)r.n[1], (float)r.n[2], (float)(3.0 * r.amu));
+      s_mn[tid] = make_float4((float)(-r.amu * r.n[0]), (float)(-r.amu * r.n[1]),
+                              (float)(-r.amu * r.n[2]), (float)r.asig);
     }
-    if (tid == 0) s_qn = 0;
     __syncthreads();
     float acc[EF2_PPT][3];
 #pragma unroll
     for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
     for (int q = 0; q < m; ++q) {
-      const float4 cf = s_cf[q], nm = s_nm[q];
-      const float as = s_as[q];
+      const float4 cf = s_cf[q], nm = s_nm[q], mn = s_mn[q];
 #pragma unroll
       for (int i = 0; i < EF2_PPT; ++i) {
         const float rx = px[i] - cf.x, ry = py[i] - cf.y, rz = pz[i] - cf.z;
@@ -258,29 +278,22 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
           const float ir2 = ir * ir;
           const float rn = fmaf(rx, nm.x, fmaf(ry, nm.y, rz * nm.z));
           const float k3 = ir2 * ir;
-          const float coef = fmaf(3.0f * nm.w * rn, ir2, as);
-          acc[i][0] = fmaf(k3, fmaf(coef, rx, -nm.w * nm.x), acc[i][0]);
-          acc[i][1] = fmaf(k3, fmaf(coef, ry, -nm.w * nm.y), acc[i][1]);
-          acc[i][2] = fmaf(k3, fmaf(coef, rz, -nm.w * nm.z), acc[i][2]);
+          const float coef = fmaf(nm.w * rn, ir2, mn.w);
+          acc[i][0] = fmaf(k3, fmaf(coef, rx, mn.x), acc[i][0]);
+          acc[i][1] = fmaf(k3, fmaf(coef, ry, mn.y), acc[i][1]);
+          acc[i][2] = fmaf(k3, fmaf(coef, rz, mn.z), acc[i][2]);
         } else if (act[i]) {
           const int slot = atomicAdd(&s_qn, 1);
-          s_q[slot] = (uint16_t)(((tid + i * EF2_T) << 5) | q);
+          s_q[slot] = ((uint32_t)(p0 + q) << 10) | (uint32_t)(tid + i * EF2_T);
         }
       }
     }
 #pragma unroll
     for (int i = 0; i < EF2_PPT; ++i)
       for (int c = 0; c < 3; ++c) v[i][c] += (double)acc[i][c];
-    __syncthreads();
-    const int qn = s_qn;
-    for (int k = tid; k < qn; k += EF2_T) {
-      const int lp = s_q[k] >> 5, j = p0 + (s_q[k] & 31);
-      const PanelGeo *pg = j < e.nbody ? e.body + j : e.wake + (j - e.nbody);
-      double u[3];
-      vel_pan(e.rp, *pg, s_pos[lp], u);
-      for (int c = 0; c < 3; ++c) atomicAdd(&s_near[lp][c], u[c]);
-    }
   }
+  __syncthreads();
+  ef2_flush(e, s_q, s_qn, s_pos, s_near);
   __syncthreads();
   const double k4pi = 1.0 / (4.0 * DUST_PI);
 #pragma unroll
@@ -314,7 +327,8 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision
   if (e.nwake)
     k_ffrec<<<nblk(e.nwake, 128), 128, 0, st>>>(e.wake, e.nwake, e.rp.ff_dou, ff + e.nbody);
   if (d.n > 0) {
-    if (precision == DUST_PREC_FP32C)
+    // the near-pair queue packs the panel index in 22 bits
+    if (precision == DUST_PREC_FP32C && ntot < (1 << 22))
       k_elem_out_split<<<nblk(d.n, EF2_NP), EF2_T, 0, st>>>(d, e, ff, vel, str, rot);
     else
       k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
@@ -430,9 +444,14 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
                                                         const double *X, const float *F,
                                                         int chunk, double *uv) {
   // one tile of particles per pass: (x, y, z relative to the tile's first
-  // particle, core radius^2) and (alpha) as float4; partial sums over the
-  // tile in FP32, added into FP64 per tile
-  __shared__ float4 s_xs[UV2_TILE], s_al[UV2_TILE];
+  // particle, core radius^2), alpha and w = x cross alpha as float4/float2.
+  // With d = p - x_q,  d x alpha_q = p x alpha_q - w_q, so the tile's sum is
+  //   sum_q c_q (d x alpha_q) = p x (sum_q c_q alpha_q) - sum_q c_q w_q,
+  // two 3-vector FMA accumulations per pair instead of a cross product
+  // (|x_q| is bounded by the tile's extent, so nothing cancels).  Partial
+  // sums over the tile in FP32, added into FP64 per tile.
+  __shared__ float4 s_xs[UV2_TILE], s_aw[UV2_TILE];
+  __shared__ float2 s_w2[UV2_TILE];
   __shared__ double s_ref[3];
   const int t = blockIdx.x * UV2_T + threadIdx.x;
   const bool act = t < npts;
@@ -448,31 +467,37 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
     if (threadIdx.x < 3) s_ref[threadIdx.x] = X[(size_t)threadIdx.x * n + q0];
     __syncthreads();
     if (threadIdx.x < m) {
-      s_xs[threadIdx.x] = make_float4((float)(X[q] - s_ref[0]), (float)(X[(size_t)n + q] - s_ref[1]),
-                                      (float)(X[2 * (size_t)n + q] - s_ref[2]),
-                                      F[(size_t)3 * n + q]);
-      s_al[threadIdx.x] =
-          make_float4(F[q], F[(size_t)n + q], F[2 * (size_t)n + q], 0.f);
+      const float x = (float)(X[q] - s_ref[0]), y = (float)(X[(size_t)n + q] - s_ref[1]),
+                  z = (float)(X[2 * (size_t)n + q] - s_ref[2]);
+      const float ax = F[q], ay = F[(size_t)n + q], az = F[2 * (size_t)n + q];
+      s_xs[threadIdx.x] = make_float4(x, y, z, F[(size_t)3 * n + q]);
+      s_aw[threadIdx.x] = make_float4(ax, ay, az, fmaf(y, az, -z * ay));
+      s_w2[threadIdx.x] = make_float2(fmaf(z, ax, -x * az), fmaf(x, ay, -y * ax));
     }
     __syncthreads();
     if (!act) continue;
     const float px = (float)(pos[0] - s_ref[0]), py = (float)(pos[1] - s_ref[1]),
                 pz = (float)(pos[2] - s_ref[2]);
-    float ax = 0.f, ay = 0.f, az = 0.f;
+    float Ax = 0.f, Ay = 0.f, Az = 0.f, Wx = 0.f, Wy = 0.f, Wz = 0.f;
 #pragma unroll 4
     for (int u = 0; u < m; ++u) {
-      const float4 xs = s_xs[u], al = s_al[u];
+      const float4 xs = s_xs[u], aw = s_aw[u];
+      const float2 w2 = s_w2[u];
       const float dx = px - xs.x, dy = py - xs.y, dz = pz - xs.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xs.w)));
       const float ir = rsqrtf(r2);
-      const float c = -ir * ir * ir;
-      ax = fmaf(c, fmaf(dy, al.z, -dz * al.y), ax);
-      ay = fmaf(c, fmaf(dz, al.x, -dx * al.z), ay);
-      az = fmaf(c, fmaf(dx, al.y, -dy * al.x), az);
+      const float c = ir * ir * ir;
+      Ax = fmaf(c, aw.x, Ax);
+      Ay = fmaf(c, aw.y, Ay);
+      Az = fmaf(c, aw.z, Az);
+      Wx = fmaf(c, aw.w, Wx);
+      Wy = fmaf(c, w2.x, Wy);
+      Wz = fmaf(c, w2.y, Wz);
     }
-    v[0] += (double)ax;
-    v[1] += (double)ay;
-    v[2] += (double)az;
+    // velocity kernel coefficient is -1/rho^3
+    v[0] -= (double)(fmaf(py, Az, -pz * Ay) - Wx);
+    v[1] -= (double)(fmaf(pz, Ax, -px * Az) - Wy);
+    v[2] -= (double)(fmaf(px, Ay, -py * Ax) - Wz);
   }
   if (!act) return;
   const double k4pi = 1.0 / (4.0 * DUST_PI);

@@ -34,6 +34,8 @@
 #include "elements.cuh"
 #include "fmm_internal.h"
 
+static int build_shift_tables(dust_octree *o);
+
 // ===================================================================== host
 static int grow(DevBuf &b, size_t bytes) {
   if (bytes <= b.cap) return DUST_OK;
@@ -189,6 +191,7 @@ extern "C" int dust_octree_create(const dust_fmm_params *prm, dust_octree **out)
   }
   for (int e = 0; e < 8; ++e) cudaEventCreate(&o->ev[e]);
   st = build_tables(o);
+  if (st == DUST_OK) st = build_shift_tables(o);
   if (st == DUST_OK) st = m2l_batch_tables(o);
   if (st != DUST_OK) {
     dust_octree_destroy(o);
@@ -209,6 +212,9 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
   devbuf_free(o->m2l_buf);
   devbuf_free(o->ahat);
   devbuf_free(o->m2l_bat);
+  devbuf_free(o->m2l_img);
+  devbuf_free(o->m2l_src);
+  devbuf_free(o->shift);
   devbuf_free(o->ffbuf);
   DevBuf *bufs[] = {&o->idxsum, &o->keys,   &o->keys_s, &o->vals,   &o->perm,
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
@@ -458,6 +464,208 @@ __global__ void k_m2m(FmmDev d, int l, uint32_t act_lo) {
   ap[3 * m] = acc[0];
   ap[3 * m + 1] = acc[1];
   ap[3 * m + 2] = acc[2];
+}
+
+// ------------------------------------------------ M2M / L2L from tables
+// The child-parent displacement is (+-delta, +-delta, +-delta), delta = half
+// the child's cell size, with the signs given by the child's octant.  So the
+// weights of M2M_multipole (mod_multipole.f90:256-278)
+//   a_par(m) += sum_{s <= m} C(m,s) d^(m-s) a_child(s)
+// and of L2L_multipole (:360-384)
+//   b_child(m) += sum_{s >= m, |s| <= p} C(s,m) d^(s-m) b_par(s)
+// are per level the same up to the sign (-1)^(sum of the exponents along the
+// axes where d < 0).  The host lists, per output m, the terms (s, exponent,
+// unsigned weight); the kernels apply the octant's sign.
+struct ShiftTerm {
+  double w;
+  uint16_t s;
+  uint8_t ex, ey, ez, pad[3];
+};
+
+__device__ __forceinline__ double shift_w(const ShiftTerm &t, uint32_t oct) {
+  const int par = ((oct & 1u) ? 0 : t.ex) + ((oct & 2u) ? 0 : t.ey) + ((oct & 4u) ? 0 : t.ez);
+  return (par & 1) ? -t.w : t.w;
+}
+
+#define SH_T 128
+// M2M into the active branch cells of level l: one warp per parent, lanes
+// over the output coefficient m; terms and offsets staged in shared memory
+__global__ void __launch_bounds__(SH_T) k_m2m_t(FmmDev d, int l, uint32_t act_lo, uint32_t na,
+                                                const ShiftTerm *terms, const int *off, int nterm) {
+  extern __shared__ __align__(16) unsigned char shm[];
+  ShiftTerm *st = (ShiftTerm *)shm;
+  int *so = (int *)(st + nterm);
+  for (int e = threadIdx.x; e < nterm; e += SH_T) st[e] = terms[e];
+  for (int e = threadIdx.x; e <= d.nm; e += SH_T) so[e] = off[e];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t c = blockIdx.x * (SH_T / 32) + warp; c < na; c += gridDim.x * (SH_T / 32)) {
+    const uint32_t ci = act_lo + c;
+    const uint32_t key = d.act_key[ci];
+    if (!(d.flags[d.G.lev_off[l] + key] & FL_BRANCH)) continue;
+    uint32_t cc[8];
+    for (int ch = 0; ch < 8; ++ch) cc[ch] = d.cidx[d.G.lev_off[l + 1] + 8u * key + (uint32_t)ch];
+    for (int m = lane; m < d.nm; m += 32) {
+      double acc[3] = {0, 0, 0};
+      for (int ch = 0; ch < 8; ++ch) {
+        const double *a = d.A + (size_t)cc[ch] * 3 * d.nm;
+        for (int t = so[m]; t < so[m + 1]; ++t) {
+          const double w = shift_w(st[t], (uint32_t)ch);
+          const int s3 = 3 * st[t].s;
+          acc[0] += w * a[s3];
+          acc[1] += w * a[s3 + 1];
+          acc[2] += w * a[s3 + 2];
+        }
+      }
+      double *ap = d.A + (size_t)ci * 3 * d.nm;
+      ap[3 * m] = acc[0];
+      ap[3 * m + 1] = acc[1];
+      ap[3 * m + 2] = acc[2];
+    }
+  }
+}
+
+// L2L into the active cells of level l (>= 2) from their parents: one warp
+// per child; b terms (|s| <= p) and, with stretching, g terms (|s| <= p+1)
+__global__ void __launch_bounds__(SH_T) k_l2l_t(FmmDev d, int l, uint32_t act_lo, uint32_t na,
+                                                const ShiftTerm *tb, const int *ob, int ntb,
+                                                const ShiftTerm *tg, const int *og, int ntg) {
+  extern __shared__ __align__(16) unsigned char shm[];
+  ShiftTerm *sb = (ShiftTerm *)shm;
+  ShiftTerm *sg = sb + ntb;
+  int *sob = (int *)(sg + ntg);
+  int *sog = sob + d.nm + 1;
+  for (int e = threadIdx.x; e < ntb; e += SH_T) sb[e] = tb[e];
+  for (int e = threadIdx.x; e < ntg; e += SH_T) sg[e] = tg[e];
+  for (int e = threadIdx.x; e <= d.nm; e += SH_T) sob[e] = ob[e];
+  for (int e = threadIdx.x; e <= d.nm1 && ntg > 0; e += SH_T) sog[e] = og[e];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t c = blockIdx.x * (SH_T / 32) + warp; c < na; c += gridDim.x * (SH_T / 32)) {
+    const uint32_t ci = act_lo + c;
+    const uint32_t key = d.act_key[ci];
+    const uint32_t oct = key & 7u;
+    const uint32_t pc = d.cidx[d.G.lev_off[l - 1] + (key >> 3)];
+    const double *bp = d.B + (size_t)pc * 3 * d.nm;
+    double *b = d.B + (size_t)ci * 3 * d.nm;
+    for (int m = lane; m < d.nm; m += 32) {
+      double acc[3] = {0, 0, 0};
+      for (int t = sob[m]; t < sob[m + 1]; ++t) {
+        const double w = shift_w(sb[t], oct);
+        const int s3 = 3 * sb[t].s;
+        acc[0] += w * bp[s3];
+        acc[1] += w * bp[s3 + 1];
+        acc[2] += w * bp[s3 + 2];
+      }
+      for (int e = 0; e < 3; ++e) b[3 * m + e] += acc[e];
+    }
+    if (ntg > 0) {
+      const double *gp = d.Gx + (size_t)pc * 3 * d.nm1;
+      double *g = d.Gx + (size_t)ci * 3 * d.nm1;
+      for (int m = lane; m < d.nm1; m += 32) {
+        double acc[3] = {0, 0, 0};
+        for (int t = sog[m]; t < sog[m + 1]; ++t) {
+          const double w = shift_w(sg[t], oct);
+          const int s3 = 3 * sg[t].s;
+          acc[0] += w * gp[s3];
+          acc[1] += w * gp[s3 + 1];
+          acc[2] += w * gp[s3 + 2];
+        }
+        for (int e = 0; e < 3; ++e) g[3 * m + e] += acc[e];
+      }
+    }
+  }
+}
+
+static double binom_h(int n, int k) {
+  double r = 1.0;
+  for (int q = 1; q <= k; ++q) r = r * (double)(n - k + q) / (double)q;
+  return r;
+}
+
+// term lists of one shift: up = false: s <= m (M2M, deg <= p); up = true:
+// s >= m with |s| <= q (L2L of a degree-q expansion)
+static void shift_terms(int nout, int q, bool up, double delta, std::vector<ShiftTerm> &t,
+                        std::vector<int> &off) {
+  t.clear();
+  off.assign(1, 0);
+  for (int m = 0; m < nout; ++m) {
+    int mi, mj, mk;
+    mono_exp(m, mi, mj, mk);
+    for (int s = 0; s < n_mon(q); ++s) {
+      int si, sj, sk;
+      mono_exp(s, si, sj, sk);
+      int ex, ey, ez;
+      double w;
+      if (!up) {
+        if (si > mi || sj > mj || sk > mk) continue;
+        ex = mi - si;
+        ey = mj - sj;
+        ez = mk - sk;
+        w = binom_h(mi, si) * binom_h(mj, sj) * binom_h(mk, sk);
+      } else {
+        if (si < mi || sj < mj || sk < mk) continue;
+        ex = si - mi;
+        ey = sj - mj;
+        ez = sk - mk;
+        w = binom_h(si, mi) * binom_h(sj, mj) * binom_h(sk, mk);
+      }
+      double dp = 1.0;
+      for (int e = 0; e < ex + ey + ez; ++e) dp *= delta;
+      ShiftTerm x;
+      memset(&x, 0, sizeof(x));
+      x.w = w * dp;
+      x.s = (uint16_t)s;
+      x.ex = (uint8_t)ex;
+      x.ey = (uint8_t)ey;
+      x.ez = (uint8_t)ez;
+      t.push_back(x);
+    }
+    off.push_back((int)t.size());
+  }
+}
+
+// per level l: [0] M2M into level l, [1] L2L b into level l, [2] L2L g
+static int build_shift_tables(dust_octree *o) {
+  std::vector<char> blob;
+  auto put = [&](const void *p, size_t n) {
+    size_t at = (blob.size() + 15) / 16 * 16;
+    blob.resize(at + n);
+    memcpy(blob.data() + at, p, n);
+    return at;
+  };
+  std::vector<ShiftTerm> t;
+  std::vector<int> off;
+  size_t at_t[DUST_MAXLEV + 1][3], at_o[DUST_MAXLEV + 1][3];
+  for (int l = 1; l <= o->G.ll; ++l)
+    for (int k = 0; k < 3; ++k) {
+      o->shift_n[l][k] = 0;
+      at_t[l][k] = at_o[l][k] = 0;
+      if (k == 0 && l >= o->G.ll) continue;
+      if (k > 0 && l < 2) continue;
+      if (k == 0)
+        shift_terms(o->nm, o->p, false, 0.5 * o->G.csize[l + 1], t, off);
+      else if (k == 1)
+        shift_terms(o->nm, o->p, true, 0.5 * o->G.csize[l], t, off);
+      else
+        shift_terms(o->nm1, o->p + 1, true, 0.5 * o->G.csize[l], t, off);
+      o->shift_n[l][k] = (int)t.size();
+      at_t[l][k] = put(t.data(), t.size() * sizeof(ShiftTerm));
+      at_o[l][k] = put(off.data(), off.size() * sizeof(int));
+    }
+  DUST_TRY(devbuf_grow(o->shift, blob.size() + 16));
+  DUST_CUDA(cudaMemcpy(o->shift.p, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  for (int l = 1; l <= o->G.ll; ++l)
+    for (int k = 0; k < 3; ++k) {
+      o->shift_t[l][k] = (const char *)o->shift.p + at_t[l][k];
+      o->shift_o[l][k] = (const char *)o->shift.p + at_o[l][k];
+    }
+  return DUST_OK;
+}
+
+static unsigned shift_grid(int64_t na) {
+  int64_t w = (na + SH_T / 32 - 1) / (SH_T / 32);
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(w, 148 * 16));
 }
 
 // M2L (mod_multipole.f90:282-356): one CTA per active target cell of level
@@ -1117,8 +1325,16 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   }
   for (int l = ll - 1; l >= 1; --l) {
     int64_t na = o->act_off[l + 1] - o->act_off[l];
-    if (na > 0)
-      k_m2m<<<(unsigned)na, (o->nm + 31) / 32 * 32, 0, st>>>(d, l, (uint32_t)o->act_off[l]);
+    if (na > 0) {
+      const int nt = o->shift_n[l][0];
+      const size_t shm = (size_t)nt * sizeof(ShiftTerm) + (size_t)(o->nm + 1) * 4;
+      if (shm > 48 * 1024)
+        DUST_CUDA(cudaFuncSetAttribute(k_m2m_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)shm));
+      k_m2m_t<<<shift_grid(na), SH_T, shm, st>>>(d, l, (uint32_t)o->act_off[l], (uint32_t)na,
+                                                  (const ShiftTerm *)o->shift_t[l][0],
+                                                  (const int *)o->shift_o[l][0], nt);
+    }
   }
   DUST_TRY(m2l_scale_sources(o, d, st));
   if (o->timing) cudaEventRecord(o->ev[2], st);
@@ -1136,8 +1352,15 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   for (int l = 2; l <= ll; ++l) {
     int64_t na = o->act_off[l + 1] - o->act_off[l];
     if (na <= 0) continue;
-    int thr = ((d.use_vs ? o->nm1 : o->nm) + 31) / 32 * 32;
-    k_l2l<<<(unsigned)na, thr, 0, st>>>(d, l, (uint32_t)o->act_off[l]);
+    const int ntb = o->shift_n[l][1], ntg = d.use_vs ? o->shift_n[l][2] : 0;
+    const size_t shm = (size_t)(ntb + ntg) * sizeof(ShiftTerm) + (size_t)(o->nm + o->nm1 + 2) * 4;
+    if (shm > 48 * 1024)
+      DUST_CUDA(cudaFuncSetAttribute(k_l2l_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)shm));
+    k_l2l_t<<<shift_grid(na), SH_T, shm, st>>>(
+        d, l, (uint32_t)o->act_off[l], (uint32_t)na, (const ShiftTerm *)o->shift_t[l][1],
+        (const int *)o->shift_o[l][1], ntb, (const ShiftTerm *)o->shift_t[l][2],
+        (const int *)o->shift_o[l][2], ntg);
   }
   if (o->timing) cudaEventRecord(o->ev[3], st);
   // leaves: L2P + P2P
@@ -1176,15 +1399,17 @@ int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, doub
   return DUST_OK;
 }
 
-void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
+int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
   dust_fmm_stats &s = o->stats;
   memset(&s, 0, sizeof(s));
   cudaStreamSynchronize(o->last_stream);
+  int status = DUST_OK;
   if (o->dev.counters) {
     int64_t c[4] = {0, 0, 0, 0};
     cudaMemcpy(c, o->dev.counters, sizeof(c), cudaMemcpyDeviceToHost);
     s.n_m2l_pairs = c[0];
     s.n_p2p_pairs = c[1];
+    if (c[2]) status = DUST_ERR_TIMEOUT;  // a bounded wait of the tensor-core M2L gave up
   }
   s.n_particles = n;
   s.n_leaves = o->n_leaves;
@@ -1200,4 +1425,5 @@ void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
     cudaEventElapsedTime(&s.ms_elems, o->ev[4], o->ev[5]);
     cudaEventElapsedTime(&s.ms_total, o->ev[0], o->ev[5]);
   }
+  return status;
 }

@@ -69,6 +69,11 @@ struct dust_octree {
   DevBuf m2l_bat;                      // M2L batch descriptors
   uint32_t *m2l_list = nullptr;
   DevBuf ahat;                         // pre-scaled M2L source coefficients
+  DevBuf m2l_img;                      // tensor-core M2L table images (FP32C)
+  DevBuf m2l_src;                      // tensor-core M2L interaction lists + masks
+  DevBuf shift;                        // M2M / L2L term tables of every level
+  const void *shift_t[DUST_MAXLEV + 1][3], *shift_o[DUST_MAXLEV + 1][3];
+  int shift_n[DUST_MAXLEV + 1][3];
   uint32_t ahat_c0 = 0;
   int m2l_cnt[8 * (DUST_MAXLEV + 1)];
   int64_t n_active = 0, n_leaves = 0;
@@ -82,7 +87,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
                    const double *mag, const double *rv, cudaStream_t st);
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st);
-void fmm_collect_stats(dust_octree *o, int n, int64_t n_elem);
+int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem);
 
 // elements.cu
 int elem_build_device(const dust_panels *body, const dust_panels *wake,
@@ -96,6 +101,13 @@ int m2l_batch_tables(dust_octree *o);
 int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st);
 int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st);
 int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
+
+// m2l_tc.cu: tensor-core M2L of levels >= 2 (FP32C mode, degree <= 4)
+bool m2l_tc_usable(const dust_octree *o);
+int m2l_tc_tables(dust_octree *o);
+size_t m2l_tc_ahat_bytes(size_t ncells);
+int m2l_tc_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
+int m2l_tc_run(dust_octree *o, FmmDev &d, cudaStream_t st);
 
 // direct.cu
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,

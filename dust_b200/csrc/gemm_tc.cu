@@ -20,47 +20,17 @@
 
 #include "dust_common.cuh"
 #include "fmm_internal.h"
+#include "tc_common.cuh"
 
 #define TC_BM 128
 #define TC_BN 128
 #define TC_BK 32
 #define TC_THREADS 128
 #define TC_STAGE_BYTES (TC_BM * TC_BK * 4 + TC_BN * TC_BK * 4)  // 32 KiB
-#define TC_SPIN_LIMIT (1ll << 24)
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
 
 // byte offset of element (row r, k) in a K-major no-swizzle tile of 128 rows
 __device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
   return (uint32_t)((k >> 2) * 2048 + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4);
-}
-
-__device__ __forceinline__ uint64_t make_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
-  // base offset 0, LBO mode 0, layout type 0 = no swizzle
-  return d;
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-  long long it = 0;
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (++it > TC_SPIN_LIMIT) return false;
-  }
 }
 
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tf32_minus(int m, int n, int k, const float *A,

@@ -238,7 +238,7 @@ int m2l_batch_tables(dust_octree *o) {
     DUST_CUDA(cudaMemcpy(o->dtabs[l].p, h.data(), n * 8, cudaMemcpyHostToDevice));
     DUST_CUDA(cudaMemcpy(o->dtab32[l].p, f.data(), n * 4, cudaMemcpyHostToDevice));
   }
-  return DUST_OK;
+  return m2l_tc_tables(o);
 }
 
 // Runs M2L for all levels >= 2 (level 1 is handled by the per-target kernel).
@@ -271,7 +271,9 @@ int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st) {
   // pre-scaled source coefficients of all active cells of levels >= 2
   bool f32 = o->prm.precision == DUST_PREC_FP32C;
   size_t w = (size_t)3 * o->nm, tot = (size_t)m * w;
-  DUST_TRY(devbuf_grow(o->ahat, tot * (f32 ? 4 : 8) + 256));
+  size_t ab = tot * (f32 ? 4 : 8) + 256;
+  if (m2l_tc_usable(o)) ab = std::max(ab, m2l_tc_ahat_bytes(m) + 256);
+  DUST_TRY(devbuf_grow(o->ahat, ab));
   o->ahat_c0 = c0;
   return DUST_OK;
 }
@@ -282,6 +284,7 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
   uint32_t c0 = o->ahat_c0, nact = (uint32_t)o->n_active;
   size_t tot = (size_t)(nact - c0) * 3 * o->nm;
   if (tot == 0) return DUST_OK;
+  if (m2l_tc_usable(o)) return m2l_tc_scale_sources(o, d, st);
   if (o->prm.precision == DUST_PREC_FP32C)
     k_scale_a<float><<<nblk(tot, 256), 256, 0, st>>>(d, c0, nact, (float *)o->ahat.p);
   else
@@ -292,6 +295,7 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
 
 int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st) {
   if (!o->m2l_list) return DUST_OK;
+  if (m2l_tc_usable(o)) return m2l_tc_run(o, d, st);
   // batch size, warps and chunk: the largest that fit 200 KB of shared memory
   bool f32 = o->prm.precision == DUST_PREC_FP32C;
   size_t esz = f32 ? 4 : 8;

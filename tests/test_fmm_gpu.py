@@ -238,7 +238,7 @@ def test_fp32c_uvort_and_elements():
     assert rel(ug, uo) < TOL32
 
 
-@pytest.mark.parametrize("p", [4, 6])
+@pytest.mark.parametrize("p", [2, 4, 6])
 def test_fmm_fp32c_matches_oracle(p):
     cen, dir_, mag, rv = ring(4000, seed=12)
     prm = prm_ring(multipole_degree=p, n_octree_levels=5, min_octree_part=5,
