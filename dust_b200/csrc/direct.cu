@@ -180,46 +180,52 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
   }
 }
 
-// FP32C element sums with the near pairs split off.  The far-field test
-// and formula run in FP32 for EF2_PPT particles per thread against a
-// shared-memory tile of EF2_TILE panels; a pair that is not clearly far
-// (threshold widened by 1e-4 so a pair far in FP32 is far in FP64) is queued
-// in shared memory instead of being evaluated in the loop.  Whenever the
-// queue could not take another full tile, and once at the end, the whole CTA
-// evaluates the queued pairs densely with the reference's exact FP64
-// formulas (vel_pan), accumulating per particle with shared atomics.  Keeping
-// the rare near pairs (about 0.5 % of all, but in a few percent of the warp
-// iterations) out of the FP32 loop removes the divergence that otherwise
-// dominates.  Far partial sums are FP32 over one tile, FP64 across tiles.
+// FP32C element sums, far and near pairs in separate kernels.
+//
+// k_elem_far runs the far-field test and formula in FP32 for EF2_PPT
+// particles per thread against a shared-memory tile of EF2_TILE panels; the
+// tile's partial sums are FP32, added into FP64 per tile.  A pair that is
+// not clearly far (threshold widened by 1e-4 so a pair far in FP32 is far in
+// FP64) is queued in shared memory and the queue is appended to a global list
+// of near pairs.  k_elem_near evaluates that list with the reference's exact
+// FP64 formulas (vel_pan), one pair per thread, and k_elem_fin adds the end
+// vortices and writes the outputs in the caller's order.  Keeping the heavy
+// FP64 formulas out of the FP32 kernel keeps its register count, and so its
+// occupancy, at the level of the far-field arithmetic.
 #define EF2_T 128
-#ifndef EF2_PPT
 #define EF2_PPT 2
-#endif
 #define EF2_NP (EF2_T * EF2_PPT)
 #define EF2_TILE 16
 #define EF2_QCAP (2 * EF2_NP * EF2_TILE)
 
-__device__ __forceinline__ void ef2_flush(const ElemDev &e, const uint32_t *s_q, int qn,
-                                          const double (*s_pos)[3], double (*s_near)[3]) {
+struct NearPair {
+  uint32_t t, j;  // particle (sorted order), panel
+};
+
+__device__ __forceinline__ void ef2_flush(const uint32_t *s_q, int qn, uint32_t t0,
+                                          unsigned long long *count, NearPair *list,
+                                          unsigned long long cap, unsigned long long *s_base) {
+  if (threadIdx.x == 0) *s_base = atomicAdd(count, (unsigned long long)qn);
+  __syncthreads();
+  const unsigned long long base = *s_base;
   for (int k = threadIdx.x; k < qn; k += EF2_T) {
-    const uint32_t en = s_q[k];
-    const int lp = en & 0x3ff, j = (int)(en >> 10);
-    const PanelGeo *pg = j < e.nbody ? e.body + j : e.wake + (j - e.nbody);
-    double u[3];
-    vel_pan(e.rp, *pg, s_pos[lp], u);
-    for (int c = 0; c < 3; ++c) atomicAdd(&s_near[lp][c], u[c]);
+    const unsigned long long at = base + (unsigned long long)k;
+    if (at < cap) {
+      const uint32_t en = s_q[k];
+      list[at] = NearPair{t0 + (en & 0x3ffu), en >> 10};
+    }
   }
 }
 
-__global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, const FFRec *ff,
-                                                          double *vel, double *str, double *rot) {
+__global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const FFRec *ff,
+                                                    double *farv, unsigned long long *count,
+                                                    NearPair *list, unsigned long long cap) {
   __shared__ float4 s_cf[EF2_TILE];  // centre - ref, widened ff2
   __shared__ float4 s_nm[EF2_TILE];  // normal, 3 * area * mag
   __shared__ float4 s_mn[EF2_TILE];  // -area * mag * normal, area * sigma
-  __shared__ double s_pos[EF2_NP][3];
-  __shared__ double s_near[EF2_NP][3];
   __shared__ uint32_t s_q[EF2_QCAP];  // (panel << 10) | local particle
   __shared__ int s_qn;
+  __shared__ unsigned long long s_base;
   const size_t n = d.n;
   const uint32_t t0 = blockIdx.x * EF2_NP;
   const int tid = threadIdx.x;
@@ -229,8 +235,7 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
   double v[EF2_PPT][3];
 #pragma unroll
   for (int i = 0; i < EF2_PPT; ++i) {
-    const int lp = tid + i * EF2_T;
-    const uint32_t t = t0 + lp;
+    const uint32_t t = t0 + tid + i * EF2_T;
     act[i] = t < n;
     double pos[3] = {ref[0], ref[1], ref[2]};
     if (act[i])
@@ -238,11 +243,7 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
     px[i] = (float)(pos[0] - ref[0]);
     py[i] = (float)(pos[1] - ref[1]);
     pz[i] = (float)(pos[2] - ref[2]);
-    for (int c = 0; c < 3; ++c) {
-      s_pos[lp][c] = pos[c];
-      s_near[lp][c] = 0.0;
-      v[i][c] = 0.0;
-    }
+    v[i][0] = v[i][1] = v[i][2] = 0.0;
   }
   if (tid == 0) s_qn = 0;
   const int ntot = e.nbody + e.nwake;
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
     __syncthreads();
     // a full tile can add up to EF2_NP * EF2_TILE entries
     if (s_qn > EF2_QCAP - EF2_NP * EF2_TILE) {
-      ef2_flush(e, s_q, s_qn, s_pos, s_near);
+      ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
       __syncthreads();
       if (tid == 0) s_qn = 0;
     }
@@ -293,33 +294,90 @@ __global__ void __launch_bounds__(EF2_T) k_elem_out_split(FmmDev d, ElemDev e, c
       for (int c = 0; c < 3; ++c) v[i][c] += (double)acc[i][c];
   }
   __syncthreads();
-  ef2_flush(e, s_q, s_qn, s_pos, s_near);
-  __syncthreads();
-  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
 #pragma unroll
   for (int i = 0; i < EF2_PPT; ++i) {
     if (!act[i]) continue;
-    const int lp = tid + i * EF2_T;
-    const uint32_t t = t0 + lp;
-    double w[3] = {v[i][0] + s_near[lp][0], v[i][1] + s_near[lp][1], v[i][2] + s_near[lp][2]};
-    for (int q = 0; q < e.nline; ++q) {
-      double u[3];
-      vel_line(e.rp, e.lines[q], s_pos[lp], u);
-      for (int c = 0; c < 3; ++c) w[c] += u[c];
-    }
-    const uint32_t ip = d.perm[t];
-    for (int c = 0; c < 3; ++c) {
-      vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + w[c] * k4pi + d.u_inf[c];
-      if (str)
-        str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
-      if (rot)
-        rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
-    }
+    const uint32_t t = t0 + tid + i * EF2_T;
+    for (int c = 0; c < 3; ++c) farv[(size_t)c * n + t] = v[i][c];
   }
 }
 
-int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
-                       double *str, double *rot, cudaStream_t st) {
+// the queued near pairs, exact FP64 (one pair per thread)
+__global__ void k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count,
+                            const NearPair *list, unsigned long long cap, double *farv) {
+  const unsigned long long nq = min(*count, cap);
+  const size_t n = d.n;
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < nq;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const NearPair np = list[k];
+    const double pos[3] = {d.P[np.t], d.P[n + np.t], d.P[2 * n + np.t]};
+    const PanelGeo *pg = (int)np.j < e.nbody ? e.body + np.j : e.wake + (np.j - e.nbody);
+    double u[3];
+    vel_pan(e.rp, *pg, pos, u);
+    for (int c = 0; c < 3; ++c) atomicAdd(farv + (size_t)c * n + np.t, u[c]);
+  }
+}
+
+// end vortices, wind, FMM outputs; scatter to the caller's order
+__global__ void k_elem_fin(FmmDev d, ElemDev e, const double *farv, double *vel, double *str,
+                           double *rot) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n = d.n;
+  if (t >= n) return;
+  const double pos[3] = {d.P[t], d.P[n + t], d.P[2 * n + t]};
+  double w[3] = {farv[t], farv[n + t], farv[2 * n + t]};
+  for (int q = 0; q < e.nline; ++q) {
+    double u[3];
+    vel_line(e.rp, e.lines[q], pos, u);
+    for (int c = 0; c < 3; ++c) w[c] += u[c];
+  }
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  const uint32_t ip = d.perm[t];
+  for (int c = 0; c < 3; ++c) {
+    vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + w[c] * k4pi + d.u_inf[c];
+    if (str) str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
+    if (rot) rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
+  }
+}
+
+// FP32C path: far kernel, (grow and redo if the near list overflowed), near
+// kernel, outputs
+static int elem_output_split(FmmDev &d, const ElemDev &e, const FFRec *ff, DevBuf &work,
+                             size_t &near_cap, double *vel, double *str, double *rot,
+                             cudaStream_t st) {
+  const size_t n = d.n;
+  if (near_cap == 0) near_cap = std::max<size_t>(1 << 20, n * 96);
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    const size_t off_l = (n * 24 + 255) / 256 * 256 + 256;
+    DUST_TRY(devbuf_grow(work, off_l + near_cap * sizeof(NearPair)));
+    double *farv = (double *)work.p;
+    unsigned long long *count = (unsigned long long *)((char *)work.p + off_l - 256);
+    NearPair *list = (NearPair *)((char *)work.p + off_l);
+    DUST_CUDA(cudaMemsetAsync(count, 0, 8, st));
+    k_elem_far<<<nblk(n, EF2_NP), EF2_T, 0, st>>>(d, e, ff, farv, count, list,
+                                                    (unsigned long long)near_cap);
+    unsigned long long h = 0;
+    DUST_CUDA(cudaMemcpyAsync(&h, count, 8, cudaMemcpyDeviceToHost, st));
+    DUST_CUDA(cudaStreamSynchronize(st));
+    if (h > near_cap) {
+      near_cap = (size_t)(h + h / 4 + 1024);
+      continue;
+    }
+    if (h > 0) {
+      const unsigned grid = (unsigned)std::min<unsigned long long>((h + 127) / 128, 148ull * 64);
+      k_elem_near<<<grid, 128, 0, st>>>(d, e, count, list, (unsigned long long)near_cap, farv);
+    }
+    k_elem_fin<<<nblk(n, 128), 128, 0, st>>>(d, e, farv, vel, str, rot);
+    DUST_CUDA(cudaGetLastError());
+    return DUST_OK;
+  }
+  return DUST_ERR_CAPACITY;
+}
+
+int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
+                       size_t &near_cap, int precision, double *vel, double *str, double *rot,
+                       cudaStream_t st) {
   int ntot = e.nbody + e.nwake;
   DUST_TRY(devbuf_grow(ffbuf, sizeof(FFRec) * (size_t)std::max(ntot, 1)));
   FFRec *ff = (FFRec *)ffbuf.p;
@@ -329,7 +387,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision
   if (d.n > 0) {
     // the near-pair queue packs the panel index in 22 bits
     if (precision == DUST_PREC_FP32C && ntot < (1 << 22))
-      k_elem_out_split<<<nblk(d.n, EF2_NP), EF2_T, 0, st>>>(d, e, ff, vel, str, rot);
+      return elem_output_split(d, e, ff, work, near_cap, vel, str, rot, st);
     else
       k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
   }

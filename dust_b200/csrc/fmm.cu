@@ -216,6 +216,7 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
   devbuf_free(o->m2l_src);
   devbuf_free(o->shift);
   devbuf_free(o->ffbuf);
+  devbuf_free(o->elem_work);
   DevBuf *bufs[] = {&o->idxsum, &o->keys,   &o->keys_s, &o->vals,   &o->perm,
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
                     &o->cidx,   &o->lidx,   &o->act_key, &o->act_lev, &o->leaf_ci,
@@ -1393,7 +1394,9 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
 
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st) {
-  if (n > 0) DUST_TRY(elem_output_device(o->dev, e, o->ffbuf, o->prm.precision, vel, str, rot, st));
+  if (n > 0)
+    DUST_TRY(elem_output_device(o->dev, e, o->ffbuf, o->elem_work, o->near_cap, o->prm.precision,
+                                vel, str, rot, st));
   if (o->timing) cudaEventRecord(o->ev[5], st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;

@@ -63,6 +63,8 @@ struct dust_octree {
   DevBuf act_key, act_lev, leaf_ci, mp, outs, cub_tmp, small;
   DevBuf h_in, h_out, el_geo, el_raw;  // staging of host-API calls
   DevBuf ffbuf;                        // far-field panel records
+  DevBuf elem_work;                    // FP32C element sums: far sums, near-pair list
+  size_t near_cap = 0;                 // capacity of the near-pair list
   DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless M2L tables (FP64)
   DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless M2L tables (FP32)
   DevBuf m2l_buf;                      // class-sorted M2L target lists
@@ -110,8 +112,9 @@ int m2l_tc_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
 int m2l_tc_run(dust_octree *o, FmmDev &d, cudaStream_t st);
 
 // direct.cu
-int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, int precision, double *vel,
-                       double *str, double *rot, cudaStream_t st);
+int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
+                       size_t &near_cap, int precision, double *vel, double *str, double *rot,
+                       cudaStream_t st);
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st);
