@@ -498,6 +498,8 @@ __global__ void k_uv_gather(int n, const uint32_t *perm, const double *cen, cons
   F[(size_t)3 * n + t] = (float)(rv[q] * rv[q]);
 }
 
+// UV2_PPT points per thread (consecutive CTA slices of UV2_T points)
+#define UV2_PPT 2
 __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *pts, int n,
                                                         const double *X, const float *F,
                                                         int chunk, double *uv) {
@@ -511,13 +513,17 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
   __shared__ float4 s_xs[UV2_TILE], s_aw[UV2_TILE];
   __shared__ float2 s_w2[UV2_TILE];
   __shared__ double s_ref[3];
-  const int t = blockIdx.x * UV2_T + threadIdx.x;
-  const bool act = t < npts;
+  int t[UV2_PPT];
+  double pos[UV2_PPT][3], v[UV2_PPT][3];
+#pragma unroll
+  for (int i = 0; i < UV2_PPT; ++i) {
+    t[i] = (blockIdx.x * UV2_PPT + i) * UV2_T + threadIdx.x;
+    for (int c = 0; c < 3; ++c) {
+      pos[i][c] = t[i] < npts ? pts[3 * (size_t)t[i] + c] : 0.0;
+      v[i][c] = 0.0;
+    }
+  }
   const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
-  double pos[3] = {0, 0, 0};
-  if (act)
-    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
-  double v[3] = {0, 0, 0};
   for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
     __syncthreads();
     const int q = q0 + threadIdx.x;
@@ -533,33 +539,46 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
       s_w2[threadIdx.x] = make_float2(fmaf(z, ax, -x * az), fmaf(x, ay, -y * ax));
     }
     __syncthreads();
-    if (!act) continue;
-    const float px = (float)(pos[0] - s_ref[0]), py = (float)(pos[1] - s_ref[1]),
-                pz = (float)(pos[2] - s_ref[2]);
-    float Ax = 0.f, Ay = 0.f, Az = 0.f, Wx = 0.f, Wy = 0.f, Wz = 0.f;
-#pragma unroll 4
+    float px[UV2_PPT], py[UV2_PPT], pz[UV2_PPT];
+    float A[UV2_PPT][3], W[UV2_PPT][3];
+#pragma unroll
+    for (int i = 0; i < UV2_PPT; ++i) {
+      px[i] = (float)(pos[i][0] - s_ref[0]);
+      py[i] = (float)(pos[i][1] - s_ref[1]);
+      pz[i] = (float)(pos[i][2] - s_ref[2]);
+      A[i][0] = A[i][1] = A[i][2] = W[i][0] = W[i][1] = W[i][2] = 0.f;
+    }
+#pragma unroll 2
     for (int u = 0; u < m; ++u) {
       const float4 xs = s_xs[u], aw = s_aw[u];
       const float2 w2 = s_w2[u];
-      const float dx = px - xs.x, dy = py - xs.y, dz = pz - xs.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xs.w)));
-      const float ir = rsqrtf(r2);
-      const float c = ir * ir * ir;
-      Ax = fmaf(c, aw.x, Ax);
-      Ay = fmaf(c, aw.y, Ay);
-      Az = fmaf(c, aw.z, Az);
-      Wx = fmaf(c, aw.w, Wx);
-      Wy = fmaf(c, w2.x, Wy);
-      Wz = fmaf(c, w2.y, Wz);
+#pragma unroll
+      for (int i = 0; i < UV2_PPT; ++i) {
+        const float dx = px[i] - xs.x, dy = py[i] - xs.y, dz = pz[i] - xs.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, xs.w)));
+        const float ir = rsqrtf(r2);
+        const float c = ir * ir * ir;
+        A[i][0] = fmaf(c, aw.x, A[i][0]);
+        A[i][1] = fmaf(c, aw.y, A[i][1]);
+        A[i][2] = fmaf(c, aw.z, A[i][2]);
+        W[i][0] = fmaf(c, aw.w, W[i][0]);
+        W[i][1] = fmaf(c, w2.x, W[i][1]);
+        W[i][2] = fmaf(c, w2.y, W[i][2]);
+      }
     }
     // velocity kernel coefficient is -1/rho^3
-    v[0] -= (double)(fmaf(py, Az, -pz * Ay) - Wx);
-    v[1] -= (double)(fmaf(pz, Ax, -px * Az) - Wy);
-    v[2] -= (double)(fmaf(px, Ay, -py * Ax) - Wz);
+#pragma unroll
+    for (int i = 0; i < UV2_PPT; ++i) {
+      v[i][0] -= (double)(fmaf(py[i], A[i][2], -pz[i] * A[i][1]) - W[i][0]);
+      v[i][1] -= (double)(fmaf(pz[i], A[i][0], -px[i] * A[i][2]) - W[i][1]);
+      v[i][2] -= (double)(fmaf(px[i], A[i][1], -py[i] * A[i][0]) - W[i][2]);
+    }
   }
-  if (!act) return;
   const double k4pi = 1.0 / (4.0 * DUST_PI);
-  for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
+#pragma unroll
+  for (int i = 0; i < UV2_PPT; ++i)
+    if (t[i] < npts)
+      for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t[i] + c, v[i][c] * k4pi);
 }
 
 __global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv) {
@@ -582,7 +601,9 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
   if (n_pts <= 0) return DUST_OK;
   DUST_CUDA(cudaMemsetAsync(uv, 0, (size_t)n_pts * 24, st));
   if (n > 0) {
-    int pb = (int)nblk(n_pts, UV2_T);
+    // point blocks: UV2_T points (UV2_T * UV2_PPT for the sorted FP32 kernel)
+    const bool srt = prm->precision == DUST_PREC_FP32C;
+    int pb = (int)nblk(n_pts, srt ? UV2_T * UV2_PPT : UV2_T);
     // enough CTAs for every SM several times over; chunks of whole tiles
     int want = std::max(1, (148 * 8 + pb - 1) / pb);
     int chunk = (n + want - 1) / want;
@@ -690,7 +711,7 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
                                                           (LineGeo *)b);
   DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
   if (n > 0) {
-    int pb = (int)nblk(n_pts, UV2_T);
+    int pb = (int)nblk(n_pts, f32 ? UV2_T * UV2_PPT : UV2_T);
     int want = std::max(1, (148 * 8 + pb - 1) / pb);
     int chunk = (n + want - 1) / want;
     chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);

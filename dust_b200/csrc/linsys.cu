@@ -98,13 +98,19 @@ __global__ void __launch_bounds__(AIC_RX *AIC_CY)
   }
 }
 
-// static columns of static rows: b(ie) += sum_j bst(ie,j) nor_j.(-wind - uvort_j)
+// static columns of static rows: b(ie) += sum_j bst(ie,j) nor_j.(-wind - uvort_j);
+// blockIdx.y takes a chunk of RS_COLS columns (partial sums added atomically)
+#define RS_COLS 256
 __global__ void k_rhs_static(const PanelGeo *el, const double *bst, int nst, double *b) {
-  int ie = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double s_sig[RS_COLS];
+  const int j0 = blockIdx.y * RS_COLS, j1 = min(nst, j0 + RS_COLS);
+  for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) s_sig[j - j0] = el[j].sig0;
+  __syncthreads();
+  const int ie = blockIdx.x * blockDim.x + threadIdx.x;
   if (ie >= nst) return;
   double s = 0.0;
-  for (int j = 0; j < nst; ++j) s += bst[(size_t)ie + (size_t)j * nst] * el[j].sig0;
-  b[ie] += s;
+  for (int j = j0; j < j1; ++j) s += bst[(size_t)ie + (size_t)j * nst] * s_sig[j - j0];
+  atomicAdd(b + ie, s);
 }
 
 // add_wake_surfpan (mod_surfpan.f90:489-535) / add_wake_vortlatt
@@ -269,8 +275,8 @@ static int assemble(dust_linsys *L, const dust_panels *elems, const dust_wake_ro
   DUST_CUDA(cudaMemsetAsync(L->b.p, 0, (size_t)n * 8, L->st));
   // build_row: static rows get the moving columns, moving rows all columns
   if (nst > 0) {
-    k_rhs_static<<<nblk(nst, 128), 128, 0, L->st>>>(L->el, (const double *)L->bst.p, nst,
-                                                     (double *)L->b.p);
+    k_rhs_static<<<dim3(nblk(nst, 128), nblk(nst, RS_COLS)), 128, 0, L->st>>>(
+        L->el, (const double *)L->bst.p, nst, (double *)L->b.p);
     launch_aic(L, 0, nst, nst, n, 1);
   }
   launch_aic(L, nst, n, 0, n, 1);
