@@ -259,7 +259,7 @@ extern "C" int dust_linsys_destroy(dust_linsys *L) {
   if (!L) return DUST_OK;
   if (L->st) cudaStreamSynchronize(L->st);
   DevBuf *bufs[] = {&L->A,  &L->As, &L->b,    &L->bst,  &L->piv, &L->info, &L->geo,
-                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->A32, &L->gm, &L->ainv32, &L->mx};
+                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->A32, &L->gm, &L->ainv32, &L->mx, &L->kr};
   for (DevBuf *b : bufs) devbuf_free(*b);
   if (L->cb) cublasDestroy(L->cb);
   if (L->st) cudaStreamDestroy(L->st);

@@ -6,6 +6,7 @@
 #include "dust_common.cuh"
 #include "elements.cuh"
 #include "fmm_internal.h"
+#include "gnn_internal.h"
 #include "lu.cuh"
 
 struct dust_linsys {
@@ -20,6 +21,8 @@ struct dust_linsys {
   DevBuf ainv32;  // FP32 inverse of the static block (mixed solve)
   DevBuf mx;      // mixed-solve work: Schur complement, coupling blocks, vectors
   bool ainv_ready = false;
+  struct dust_precond *pc = nullptr;  // learned preconditioner (GMRES_NN)
+  DevBuf kr;                          // GMRES Krylov basis and vectors
   LuWork lu;
   const PanelGeo *el = nullptr, *wk = nullptr;
   int nwake = 0, n_impl = 0;
@@ -40,3 +43,9 @@ int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w
                        DevBuf &wrk, int n, int nrhs, const double *A64, const double *B,
                        double *X, double tol, int max_iter, int use_tc,
                        dust_solve_report *rep);
+
+// the assembled (unfactored) system as a view, and Y = A X through it
+SysView linsys_view(const dust_linsys *L);
+int linsys_matmat(const dust_linsys *L, int ncols, const double *X, int ldx, double *Y, int ldy,
+                  cudaStream_t st, cublasHandle_t cb);
+int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep);

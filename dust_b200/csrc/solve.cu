@@ -219,61 +219,21 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
   return s;
 }
 
-// Mixed / learned solves of the linsys handle (full unfactored FP64 matrix).
-__global__ void k_put_static(int n, int nst, const double *As, double *Af) {
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  size_t tot = (size_t)nst * nst;
-  if (idx >= tot) return;
-  int j = (int)(idx / nst), i = (int)(idx % nst);
-  Af[(size_t)i + (size_t)j * n] = As[idx];
-}
-
-int linsys_full_matrix(dust_linsys *L, double *Af) {
-  size_t n = L->n;
-  DUST_CUDA(cudaMemcpyAsync(Af, L->A.p, n * n * 8, cudaMemcpyDeviceToDevice, L->st));
-  if (L->nst > 0) {
-    size_t tot = (size_t)L->nst * L->nst;
-    k_put_static<<<nblk(tot, 256), 256, 0, L->st>>>(L->n, L->nst, (const double *)L->As.p, Af);
-  }
-  DUST_CUDA(cudaGetLastError());
-  return DUST_OK;
-}
-
-int linsys_gmres_nn(dust_linsys *L, const double *Af, double *x, dust_solve_report *rep);
 
 int linsys_solve_iterative(dust_linsys *L, int mode, double *x_dev, dust_solve_report *rep) {
-  size_t n = L->n;
-  if (mode == DUST_SOLVE_MIXED) {
-    int s = linsys_solve_schur_mixed(L, x_dev, 1e-14, 30, rep);
-    if (s == DUST_OK) {
-      L->factored = true;
-      return DUST_OK;
-    }
-    if (s != DUST_ERR_NOT_CONVERGED && s != DUST_ERR_SINGULAR) return s;
-    if (rep) rep->fell_back = 1;
-    DUST_TRY(linsys_solve_lu64(L, x_dev));
-    if (rep) rep->mode_used = DUST_SOLVE_LU64;
+  int s = DUST_ERR_BAD_ARG;
+  if (mode == DUST_SOLVE_MIXED)
+    s = linsys_solve_schur_mixed(L, x_dev, 1e-14, 30, rep);
+  else if (mode == DUST_SOLVE_GMRES_NN)
+    s = linsys_gmres_nn(L, x_dev, rep);
+  if (s == DUST_OK) {
+    L->factored = true;
     return DUST_OK;
   }
-  DUST_TRY(devbuf_grow(L->gm, n * n * 8 + 256));
-  double *Af = (double *)L->gm.p;
-  DUST_TRY(linsys_full_matrix(L, Af));
-  if (mode == DUST_SOLVE_GMRES_NN) {
-    int s = linsys_gmres_nn(L, Af, x_dev, rep);
-    if (s == DUST_OK) {
-      L->factored = true;
-      return DUST_OK;
-    }
-    if (rep) rep->fell_back = 1;
-    // plain LU remains the fallback (the step's result is then exact LU)
-    DUST_TRY(linsys_solve_lu64(L, x_dev));
-    if (rep) rep->mode_used = DUST_SOLVE_LU64;
-    return DUST_OK;
-  }
-  DevBuf wrk;
-  int s = mixed_solve_device(L->cb, L->st, L->lu, L->A32, wrk, L->n, 1, Af,
-                             (const double *)L->b.p, x_dev, 1e-14, 30, 1, rep);
-  devbuf_free(wrk);
-  L->factored = true;
-  return s;
+  if (s != DUST_ERR_NOT_CONVERGED && s != DUST_ERR_SINGULAR) return s;
+  // plain LU remains the fallback (the step's result is then exact LU)
+  if (rep) rep->fell_back = 1;
+  DUST_TRY(linsys_solve_lu64(L, x_dev));
+  if (rep) rep->mode_used = DUST_SOLVE_LU64;
+  return DUST_OK;
 }

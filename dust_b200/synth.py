@@ -196,6 +196,25 @@ def cylinder(n_target=6000, length=4.0, radius=0.3, center=(0.0, 0.0, -0.6)):
     return _orient_outward(ps)
 
 
+def rotor_fuselage(n_fus=6000, n_blades=4, n_span=30, n_chord=8, phase=0.0, omega=40.0,
+                   inflow=(0.0, 0.0, 0.0)):
+    """Moving-body case of the learned preconditioner: a rotor (radius 1,
+    linear twist -8 deg, `n_blades` blades of n_span x n_chord vortex-lattice
+    panels) at azimuth `phase` above a closed cylindrical fuselage of about
+    n_fus surface panels.  Returns (elems, nstatic) with the fuselage (static)
+    first; the rotor panels carry their body velocity omega x r (+ inflow
+    subtracted as a relative wind is the caller's u_inf)."""
+    body = cylinder(n_target=n_fus, length=4.0, radius=0.3, center=(0.0, 0.0, -0.6))
+    rot, _ = rotor_blades(n_blades=n_blades, radius=1.0, root=0.2, chord=0.1, n_span=n_span,
+                          n_chord=n_chord, twist_deg=-8.0, phase=phase, center=(0.0, 0.0, 0.0))
+    els = concat_panels(body, rot)
+    ub = np.zeros((els.n, 3))
+    cen = rot.ver.mean(axis=1)
+    ub[body.n:] = np.cross([0.0, 0.0, omega], cen) - np.asarray(inflow)
+    els.ub = ub
+    return els, body.n
+
+
 def te_wake(panels, te_idx, offset, second=None, mag=None):
     """One row of wake panels behind trailing-edge panels: the trailing edge
     of panel i is the edge ver[1] -> ver[2] (chordwise-last vertices of the

@@ -252,7 +252,8 @@ typedef struct dust_solve_report {
   int    mode_used;       /* DUST_SOLVE_* that produced the solution         */
   int    iterations;      /* refinement / GMRES iterations                   */
   int    fell_back;       /* 1 if GMRES stalled and LU was used              */
-  double residual;        /* final ||b - A x||_inf / (||A||_inf ||x||_inf)   */
+  double residual;        /* final ||b - A x||_inf / (||A||_inf ||x||_inf);
+                             GMRES: ||b - A x||_2 / ||b||_2                  */
   float  ms_factor, ms_solve;
 } dust_solve_report;
 
@@ -313,6 +314,51 @@ DUST_API int dust_dense_solve(int n, int nrhs, const double *A, const double *B,
 DUST_API int dust_tc_gemm_tf32_minus(int m, int n, int k, const float *A, int lda,
                                      const float *B, int ldb, float *C, int ldc,
                                      void *stream);
+
+/* ------------------------------------------------ learned preconditioner */
+/* No counterpart in the reference (it refactors the moving block every step,
+ * mod_linsys.f90:352-482).  A 3-layer, width-64 graph network over the
+ * k-nearest-neighbour graph of the panel centres maps the current matrix to
+ * a sparse approximate inverse M = (I + O) D^-1 (D = diag A, O on the graph's
+ * edges) that right-preconditions the FP64 GMRES of DUST_SOLVE_GMRES_NN and
+ * gives its warm start M b.  Untrained (output weights zero) M is Jacobi.
+ * Training runs on the GPU: the loss of a stored system is
+ * ||M [A Z, b] - [Z, x]||_F^2 / (n C) over 7 random +-1 probe columns Z and
+ * the solution x, minimised with Adam. */
+typedef struct dust_precond dust_precond;
+
+/* Graph of n panel centres (host, 3n): each panel's k nearest others. */
+DUST_API int dust_precond_create(int n, int k, const double *centres,
+                                 unsigned long long seed, dust_precond **out);
+DUST_API int dust_precond_destroy(dust_precond *p);
+DUST_API int dust_precond_num_params(void);
+DUST_API int dust_precond_get_params(const dust_precond *p, float *w, int count);
+DUST_API int dust_precond_set_params(dust_precond *p, const float *w, int count);
+
+/* Stores a training sample: `ls` assembled and not yet solved, x_dev its
+ * solution (device, n doubles). */
+DUST_API int dust_precond_add_sample(dust_precond *p, dust_linsys *ls,
+                                     const double *x_dev, unsigned long long seed);
+DUST_API int dust_precond_num_samples(const dust_precond *p);
+
+/* Loss (and gradient, count = dust_precond_num_params()) of sample `si` at
+ * the current weights; grad may be NULL. */
+DUST_API int dust_precond_loss_grad(dust_precond *p, int si, float *loss,
+                                    float *grad, int count);
+
+/* The stored inputs of sample `si` (host arrays, any may be NULL):
+ * x[n*8], ef[n*(k+1)*4], w[n*(k+1)], nbr[n*(k+1)], Y[n*8], T[n*8]. */
+DUST_API int dust_precond_get_sample(const dust_precond *p, int si, float *x,
+                                     float *ef, float *w, int *nbr, float *Y,
+                                     float *T);
+
+/* `iters` Adam steps cycling over the samples; *loss_out = mean loss of the
+ * last pass. */
+DUST_API int dust_precond_train(dust_precond *p, int iters, float lr,
+                                float *loss_out);
+
+/* Attaches p (NULL detaches) to the system for DUST_SOLVE_GMRES_NN. */
+DUST_API int dust_linsys_set_precond(dust_linsys *ls, dust_precond *p);
 
 /* ---------------------------------------------------------------- misc */
 DUST_API const char *dust_status_string(int status);
