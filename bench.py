@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="small case (smoke)")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-preconditioner mode (and its training)")
+    ap.add_argument("--train-iters", type=int, default=400)
     ap.add_argument("--profile-step", action="store_true",
                     help="run warm-up + one step only (for ncu launch lists)")
     return ap.parse_args()
@@ -226,7 +229,8 @@ def run_reference(args, rank, ws):
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
             "n_gpus": args.gpus, "steps": len(vals), "warmup": 0, "ms_per_step": round(v, 1),
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
             "data": "synthetic",
             "config": {"workload": "full step: 2x3-blade VLM rotors (1,920 moving) + "
                        "12,000-panel wing, 2M particles, FMM p=%d" % args.degree,
@@ -255,11 +259,23 @@ def main():
     params = case.fmm_params(degree=args.degree)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     modes = [("plain", abi.DUST_SOLVE_LU64), ("mixed", abi.DUST_SOLVE_MIXED)]
+    learned = None
+    if not args.no_learned:
+        # the learned preconditioner trains (untimed) on the plain solutions
+        # of the same geometry at rotor azimuths other than the benchmarked one
+        from dust_b200 import precond
+        period = 2 * np.pi / 3
+        angles = (np.arange(12) + 0.5) * period / 12
+        pc, info = precond.train_for_case(case, params, angles, iters=args.train_iters)
+        learned = {"precond": pc, "info": info}
+        modes.append(("learned", abi.DUST_SOLVE_GMRES_NN))
     results = {}
     steppers = {}
     for name, mode in modes:
         prm = params if name == "plain" else params.replace(precision=abi.DUST_PREC_FP32C)
         st = step.DeviceStepper(case, prm, mode)
+        if name == "learned":
+            learned["precond"].attach(st.ls)
         steppers[name] = st
         for _ in range(max(args.warmup, 1 if args.profile_step else 3)):
             st.step()
@@ -278,14 +294,17 @@ def main():
         return
     # phase breakdown (plain and mixed share the FMM): one timed step with events
     ph = {k: phase_breakdown(steppers[k], case, params) for k in steppers}
-    best = min(results, key=lambda k: results[k]["ms"])
     lp = results["plain"]["loads"]
     load_err = {k: float(np.max(np.abs(results[k]["loads"] - lp) / np.maximum(np.abs(lp), 1e-30)))
                 for k in results}
+    # the headline mode: the fastest whose loads are within 1e-6 of FP64
+    best = min((k for k in results if load_err[k] <= 1e-6), key=lambda k: results[k]["ms"])
     # end to end through the host API (pinned buffers)
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(case, params, dict(modes)[best], args, ws)
+        prm_best = params if best == "plain" else params.replace(precision=abi.DUST_PREC_FP32C)
+        e2e = run_e2e(case, prm_best, dict(modes)[best], args, ws,
+                      learned["precond"] if best == "learned" else None)
     cpu = None
     if not args.no_cpu and rank == 0 and ws == 1:
         ms_cpu, parts = cpu_baseline(case, params)
@@ -298,7 +317,8 @@ def main():
         line = {
             "metric": METRIC, "value": round(r["ms"] / ws, 3), "unit": "ms", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"], 3),
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
             "data": "synthetic (seeded FullStepCase)",
             "config": {"workload": "full step: 2x3-blade VLM rotors (1,920 moving unknowns) + "
                        "12,000-panel surface-panel wing, 338 wake panels, %d particles, "
@@ -309,8 +329,9 @@ def main():
             "plain_fp64_ms": round(results["plain"]["ms"], 3),
             "speedup_vs_plain_fp64": round(results["plain"]["ms"] / r["ms"], 3),
             "load_error_vs_fp64": load_err[best],
-            "modes": {k: {"ms": round(v["ms"], 3), "solve": v["report"]} for k, v in
-                      results.items()},
+            "modes": {k: {"ms": round(v["ms"], 3), "load_error_vs_fp64": load_err[k],
+                          "solve": v["report"]} for k, v in results.items()},
+            "learned_training": learned["info"] if learned else None,
             "phases_ms": ph,
             "clocks": r["clocks"],
             "roofline": rf,
@@ -372,7 +393,7 @@ def count_launches(st):
         return None
 
 
-def run_e2e(case, params, mode, args, ws):
+def run_e2e(case, params, mode, args, ws, pc=None):
     """Same step through the host API with pinned host buffers: every step
     copies particles and panels in and velocities/strengths out."""
     import torch
@@ -381,6 +402,8 @@ def run_e2e(case, params, mode, args, ws):
     case.cen, case.dir, case.mag, case.r_vortex = (pin(case.cen), pin(case.dir),
                                                   pin(case.mag), pin(case.r_vortex))
     hs = step.HostStepper(case, params, mode)
+    if pc is not None:
+        pc.attach(hs.ls)
     for _ in range(2):
         hs.step()
     torch.cuda.synchronize()
