@@ -87,6 +87,8 @@ class FmmStats(C.Structure):
         ("ms_p2p", C.c_float),
         ("ms_elems", C.c_float),
         ("ms_total", C.c_float),
+        ("ms_m2l_kernel", C.c_float),
+        ("ms_elem_far", C.c_float),
     ]
 
 

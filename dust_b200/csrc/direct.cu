@@ -345,7 +345,7 @@ __global__ void k_elem_fin(FmmDev d, ElemDev e, const double *farv, double *vel,
 // kernel, outputs
 static int elem_output_split(FmmDev &d, const ElemDev &e, const FFRec *ff, DevBuf &work,
                              size_t &near_cap, double *vel, double *str, double *rot,
-                             cudaStream_t st) {
+                             cudaStream_t st, cudaEvent_t *kev, bool *kev_done) {
   const size_t n = d.n;
   if (near_cap == 0) near_cap = std::max<size_t>(1 << 20, n * 96);
   for (int attempt = 0; attempt < 3; ++attempt) {
@@ -355,8 +355,13 @@ static int elem_output_split(FmmDev &d, const ElemDev &e, const FFRec *ff, DevBu
     unsigned long long *count = (unsigned long long *)((char *)work.p + off_l - 256);
     NearPair *list = (NearPair *)((char *)work.p + off_l);
     DUST_CUDA(cudaMemsetAsync(count, 0, 8, st));
+    if (kev) cudaEventRecord(kev[0], st);
     k_elem_far<<<nblk(n, EF2_NP), EF2_T, 0, st>>>(d, e, ff, farv, count, list,
                                                     (unsigned long long)near_cap);
+    if (kev) {
+      cudaEventRecord(kev[1], st);
+      if (kev_done) *kev_done = true;
+    }
     unsigned long long h = 0;
     DUST_CUDA(cudaMemcpyAsync(&h, count, 8, cudaMemcpyDeviceToHost, st));
     DUST_CUDA(cudaStreamSynchronize(st));
@@ -377,7 +382,8 @@ static int elem_output_split(FmmDev &d, const ElemDev &e, const FFRec *ff, DevBu
 
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
                        size_t &near_cap, int precision, double *vel, double *str, double *rot,
-                       cudaStream_t st) {
+                       cudaStream_t st, cudaEvent_t *kev, bool *kev_done) {
+  if (kev_done) *kev_done = false;
   int ntot = e.nbody + e.nwake;
   DUST_TRY(devbuf_grow(ffbuf, sizeof(FFRec) * (size_t)std::max(ntot, 1)));
   FFRec *ff = (FFRec *)ffbuf.p;
@@ -387,7 +393,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
   if (d.n > 0) {
     // the near-pair queue packs the panel index in 22 bits
     if (precision == DUST_PREC_FP32C && ntot < (1 << 22))
-      return elem_output_split(d, e, ff, work, near_cap, vel, str, rot, st);
+      return elem_output_split(d, e, ff, work, near_cap, vel, str, rot, st, kev, kev_done);
     else
       k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
   }

@@ -189,7 +189,7 @@ extern "C" int dust_octree_create(const dust_fmm_params *prm, dust_octree **out)
     delete o;
     return DUST_ERR_CUDA;
   }
-  for (int e = 0; e < 8; ++e) cudaEventCreate(&o->ev[e]);
+  for (int e = 0; e < 10; ++e) cudaEventCreate(&o->ev[e]);
   st = build_tables(o);
   if (st == DUST_OK) st = build_shift_tables(o);
   if (st == DUST_OK) st = m2l_batch_tables(o);
@@ -223,7 +223,7 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
                     &o->mp,     &o->outs,   &o->cub_tmp, &o->small,  &o->h_in,
                     &o->h_out,  &o->el_geo, &o->el_raw};
   for (DevBuf *b : bufs) devbuf_free(*b);
-  for (int e = 0; e < 8; ++e) cudaEventDestroy(o->ev[e]);
+  for (int e = 0; e < 10; ++e) cudaEventDestroy(o->ev[e]);
   cudaStreamDestroy(o->stream);
   delete o;
   return DUST_OK;
@@ -1245,6 +1245,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   int64_t *small = (int64_t *)o->small.p;
   int *err = (int *)(small + 40);
 
+  o->kev_m2l = false;
   if (o->timing) cudaEventRecord(o->ev[0], st);
   DUST_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(nfine + 1) * 4, st));
   int big = 0x7fffffff;
@@ -1396,7 +1397,7 @@ int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, doub
                       double *rot, cudaStream_t st) {
   if (n > 0)
     DUST_TRY(elem_output_device(o->dev, e, o->ffbuf, o->elem_work, o->near_cap, o->prm.precision,
-                                vel, str, rot, st));
+                                vel, str, rot, st, o->timing ? &o->ev[8] : nullptr, &o->kev_far));
   if (o->timing) cudaEventRecord(o->ev[5], st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
@@ -1427,6 +1428,8 @@ int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
     cudaEventElapsedTime(&s.ms_p2p, o->ev[3], o->ev[4]);
     cudaEventElapsedTime(&s.ms_elems, o->ev[4], o->ev[5]);
     cudaEventElapsedTime(&s.ms_total, o->ev[0], o->ev[5]);
+    if (o->kev_m2l) cudaEventElapsedTime(&s.ms_m2l_kernel, o->ev[6], o->ev[7]);
+    if (o->kev_far) cudaEventElapsedTime(&s.ms_elem_far, o->ev[8], o->ev[9]);
   }
   return status;
 }

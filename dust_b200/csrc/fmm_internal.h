@@ -53,7 +53,8 @@ struct dust_octree {
   uint64_t ncell_tot = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t last_stream = nullptr;  // stream of the last evaluation
-  cudaEvent_t ev[8];
+  cudaEvent_t ev[10];  // phases [0..5], M2L kernel [6, 7], far element kernel [8, 9]
+  bool kev_m2l = false, kev_far = false;  // whether [6, 7] / [8, 9] were recorded
   bool timing = false;
   DevBuf dtab[DUST_MAXLEV + 1];
   int kdlen[DUST_MAXLEV + 1][3];
@@ -114,7 +115,7 @@ int m2l_tc_run(dust_octree *o, FmmDev &d, cudaStream_t st);
 // direct.cu
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
                        size_t &near_cap, int precision, double *vel, double *str, double *rot,
-                       cudaStream_t st);
+                       cudaStream_t st, cudaEvent_t *kev = nullptr, bool *kev_done = nullptr);
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st);

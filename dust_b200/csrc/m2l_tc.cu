@@ -548,9 +548,12 @@ int m2l_tc_run(dust_octree *o, FmmDev &d, cudaStream_t st) {
     attr = true;
   }
   // counters[2] is the kernel's timeout flag (cleared with the counters)
+  o->kev_m2l = o->timing;
+  if (o->timing) cudaEventRecord(o->ev[6], st);
   k_m2l_tc<<<(unsigned)nb, MT_THREADS2, smem, st>>>(
       d, (const int4 *)o->m2l_bat.p, o->m2l_list, srcl, maskl, (const float *)o->m2l_img.p,
       (const float *)o->ahat.p, o->ahat_c0, nout, scr, (unsigned long long *)(d.counters + 2));
+  if (o->timing) cudaEventRecord(o->ev[7], st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }

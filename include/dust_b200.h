@@ -5,7 +5,8 @@
  * The reference (DUST, Fortran 2008 + OpenMP) reaches this path through
  * module procedures of mod_octree and mod_linsys.  Every entry point below
  * replaces one of them and is meant to be bound from Fortran with
- * ISO_C_BINDING (see INTEGRATION.md for the interface module).  Arrays are
+ * ISO_C_BINDING (an interface module with one BIND(C) interface per
+ * function, value arguments for ints, type(c_ptr) for handles).  Arrays are
  * plain host (or, for the *_device variants, device) pointers in the
  * Fortran layout: a particle/panel coordinate array `x(3,n)` is passed as a
  * double* of length 3*n with the three components of one item contiguous.
@@ -52,8 +53,12 @@ extern "C" {
 
 /* ------------------------------------------------------ precision modes */
 #define DUST_PREC_FP64   0     /* plain: FP64 everywhere                      */
-#define DUST_PREC_FP32C  1     /* FP32 arithmetic with compensated (two-sum)
-                                  accumulation; FP64 root-level translations */
+#define DUST_PREC_FP32C  1     /* FP32 pair arithmetic on tile-relative
+                                  coordinates, partial sums per tile in FP32
+                                  and across tiles in FP64; M2L of levels >= 2
+                                  on the tensor cores (3xTF32, p <= 4); tables,
+                                  level-1 M2L, M2M, L2L and near element pairs
+                                  stay FP64                                   */
 
 /* Octree / FMM parameters.  One field per DUST input key
  * (src/general/mod_sim_param.f90:376-452, read at :772-804). */
@@ -118,6 +123,8 @@ typedef struct dust_fmm_stats {
   int64_t n_elem_pairs;      /* particle x element evaluations               */
   int     n_levels;
   float   ms_tree, ms_upward, ms_m2l, ms_p2p, ms_elems, ms_total;
+  float   ms_m2l_kernel;     /* tensor-core M2L kernel alone (FP32C), else 0  */
+  float   ms_elem_far;       /* FP32 far-field element kernel alone, else 0   */
 } dust_fmm_stats;
 
 typedef struct dust_octree dust_octree;
