@@ -1180,6 +1180,219 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
   }
 }
 
+// ------------------------------------------- L2P + P2P, FP32C (warp per leaf)
+// Leaves hold a few particles (6 on average in the full-step case), so a
+// CTA per leaf leaves most lanes idle.  Here one warp owns one leaf: lanes
+// are split into G groups of TPR = (targets rounded up to a power of two)
+// lanes, lane (tl, grp) accumulates target tl over the sources u = grp mod
+// G of each 32-source tile staged in the warp's own shared memory, and the
+// groups are combined with shuffles.  Pair arithmetic is p2p_pair_f (FP32 on
+// coordinates relative to the leaf centre) with the FP32 partial sums folded
+// into FP64 after every 128 sources; L2P stays FP64.
+#define P2W_WARPS 4
+#define P2W_TILE 32
+#define P2W_MAXR 320
+
+template <bool VS, bool DF, bool VD, bool TV>
+__global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
+  __shared__ float s_src[P2W_WARPS][7][P2W_TILE];
+  __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
+  __shared__ uint32_t s_rlo[P2W_WARPS][P2W_MAXR];
+  __shared__ uint32_t s_rcum[P2W_WARPS][P2W_MAXR + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t leaf = blockIdx.x * P2W_WARPS + w;
+  if (leaf >= d.n_leaves) return;  // warp-uniform: no CTA-wide barriers below
+  const uint32_t ci = d.leaf_ci[leaf];
+  const int l = d.act_lev[ci];
+  const uint32_t key = d.act_key[ci];
+  int ci_, cj, ck;
+  cart_of_key(d.G, l, key, ci_, cj, ck);
+  double cc[3];
+  cell_center(d.G, l, ci_, cj, ck, cc);
+  const uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
+  if (hi == lo) return;
+  uint32_t *rlo = s_rlo[w], *rcum = s_rcum[w];
+  // near-field source ranges, in the order of k_p2p
+  int nr = 0;
+  for (int lev = l; lev >= 1; --lev) {
+    const int sh = l - lev;
+    const int ai = ci_ >> sh, aj = cj >> sh, ak = ck >> sh;
+    bool pred = false;
+    uint32_t a0 = 0, a1 = 0;
+    if (lane < 27 && lane != 13) {
+      const int di = lane % 3 - 1, dj = (lane / 3) % 3 - 1, dk = lane / 9 - 1;
+      if (cart_in(d.G, lev, ai + di, aj + dj, ak + dk)) {
+        const uint32_t nk = key_of(d.G, lev, ai + di, aj + dj, ak + dk);
+        const uint8_t f = d.flags[d.G.lev_off[lev] + nk];
+        const bool want = (lev == l) ? (f & FL_ACTIVE) != 0 : (f & FL_LEAF) != 0;
+        if (want) {
+          a0 = cell_lo(d.G, d.cstart, lev, nk);
+          a1 = cell_hi(d.G, d.cstart, lev, nk);
+          pred = a1 > a0;
+        }
+      }
+    }
+    const unsigned msk = __ballot_sync(0xffffffffu, pred);
+    if (pred && nr + __popc(msk) < P2W_MAXR) {
+      const int pos = nr + __popc(msk & ((1u << lane) - 1u));
+      rlo[pos] = a0;
+      rcum[pos] = a1 - a0;
+    }
+    nr = min(nr + __popc(msk), P2W_MAXR - 1);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    rlo[nr] = lo;
+    rcum[nr] = hi - lo;
+    ++nr;
+    uint32_t run = 0;
+    for (int r = 0; r < nr; ++r) {
+      const uint32_t len = rcum[r];
+      rcum[r] = run;
+      run += len;
+    }
+    rcum[nr] = run;
+  }
+  nr = __shfl_sync(0xffffffffu, nr, 0);  // lane 0 appended the own leaf
+  __syncwarp();
+  const uint32_t S = rcum[nr];
+  const size_t n = d.n;
+  const int nt = (int)(hi - lo), nm = d.nm, nm1 = d.nm1;
+  if (lane == 0 && d.counters)
+    atomicAdd((unsigned long long *)d.counters + 1, (unsigned long long)nt * (S - 1));
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  const double *bl = d.B + (size_t)ci * 3 * nm, *gl = d.Gx + (size_t)ci * 3 * nm1;
+  // L2P of one target (FP64): velocity and the gradient of the local field
+  auto l2p = [&](uint32_t ti, double *lv, double *g) {
+    const double x = d.P[ti] - cc[0], y = d.P[n + ti] - cc[1], z = d.P[2 * n + ti] - cc[2];
+    double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
+    px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+    for (int e = 1; e <= DUST_MAXP; ++e) {
+      px[e] = px[e - 1] * x;
+      py[e] = py[e - 1] * y;
+      pz[e] = pz[e - 1] * z;
+    }
+    for (int e = 0; e < 3; ++e) lv[e] = 0.0;
+    for (int e = 0; e < 9; ++e) g[e] = 0.0;
+    for (int m = 0; m < nm; ++m) {
+      int mi, mj, mk;
+      mono_exp(m, mi, mj, mk);
+      const double pr = px[mi] * py[mj] * pz[mk];
+      for (int e = 0; e < 3; ++e) lv[e] += __ldg(bl + 3 * m + e) * pr;
+      if (VS) {
+        const double *g0 = gl + 3 * mono_idx(mi + 1, mj, mk), *g1 = gl + 3 * mono_idx(mi, mj + 1, mk),
+                     *g2 = gl + 3 * mono_idx(mi, mj, mk + 1);
+        const double f0 = (mi + 1) * pr, f1 = (mj + 1) * pr, f2 = (mk + 1) * pr;
+        for (int e = 0; e < 3; ++e) {
+          g[0 + 3 * e] += f0 * __ldg(g0 + e);
+          g[1 + 3 * e] += f1 * __ldg(g1 + e);
+          g[2 + 3 * e] += f2 * __ldg(g2 + e);
+        }
+      }
+    }
+  };
+  double ave_ros = 0.0;
+  if (TV) {
+    // leaf average of |sym(grad)|^2 from the local expansion (:1214-1230)
+    double part = 0.0;
+    for (int t = lane; t < nt; t += 32) {
+      double lv[3], g[9];
+      l2p(lo + t, lv, g);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const double sy = 0.5 * (g[a + 3 * b] + g[b + 3 * a]);
+          part += sy * sy;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    ave_ros = part / (double)nt;
+  }
+  float *fs = &s_src[w][0][0];
+  for (int t0 = 0; t0 < nt; t0 += 32) {
+    const int cnt = min(32, nt - t0);
+    int TPR = 1;
+    while (TPR < cnt) TPR <<= 1;
+    const int G = 32 / TPR, tl = lane & (TPR - 1), grp = lane / TPR;
+    const bool act = tl < cnt;
+    const uint32_t ti = lo + t0 + (act ? tl : 0);
+    const double tp[3] = {d.P[ti], d.P[n + ti], d.P[2 * n + ti]};
+    const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
+    const float ftp[3] = {(float)(tp[0] - cc[0]), (float)(tp[1] - cc[1]), (float)(tp[2] - cc[2])};
+    const float fta[3] = {(float)ta[0], (float)ta[1], (float)ta[2]};
+    P2PAcc A;
+    for (int e = 0; e < 3; ++e) A.v[e] = A.s[e] = A.r[e] = A.f[e] = 0.0;
+    P2PAccF B;
+    for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+    int since = 0;
+    for (uint32_t s0 = 0; s0 < S; s0 += P2W_TILE) {
+      __syncwarp();
+      const uint32_t v = s0 + lane;
+      if (v < S) {
+        int a = 0, b = nr - 1;
+        while (a < b) {  // last r with rcum[r] <= v
+          const int mid = (a + b + 1) >> 1;
+          if (rcum[mid] <= v) a = mid; else b = mid - 1;
+        }
+        const uint32_t sidx = rlo[a] + (v - rcum[a]);
+        s_sid[w][lane] = sidx;
+        for (int q = 0; q < 3; ++q) fs[q * P2W_TILE + lane] = (float)(d.P[(size_t)q * n + sidx] - cc[q]);
+        for (int q = 3; q < 7; ++q) fs[q * P2W_TILE + lane] = (float)d.P[(size_t)q * n + sidx];
+      }
+      __syncwarp();
+      const int m = (int)min((uint32_t)P2W_TILE, S - s0);
+      if (act)
+        for (int u = grp; u < m; u += G) {
+          if (s_sid[w][u] == ti) continue;
+          p2p_pair_f<VS, DF, VD>(ftp, fta, fs[u], fs[P2W_TILE + u], fs[2 * P2W_TILE + u],
+                                 fs[3 * P2W_TILE + u], fs[4 * P2W_TILE + u], fs[5 * P2W_TILE + u],
+                                 fs[6 * P2W_TILE + u], B);
+        }
+      if (++since == 4 || s0 + P2W_TILE >= S) {
+        // FP32 partial sums of up to 128 sources folded into FP64
+        since = 0;
+        for (int e = 0; e < 3; ++e) {
+          A.v[e] += (double)B.v[e];
+          A.s[e] += (double)B.s[e];
+          A.r[e] += (double)B.r[e];
+          A.f[e] += (double)B.f[e];
+          B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+        }
+      }
+    }
+    // combine the groups of each target
+    for (int o = TPR; o < 32; o <<= 1)
+      for (int e = 0; e < 3; ++e) {
+        A.v[e] += __shfl_xor_sync(0xffffffffu, A.v[e], o);
+        A.s[e] += __shfl_xor_sync(0xffffffffu, A.s[e], o);
+        A.r[e] += __shfl_xor_sync(0xffffffffu, A.r[e], o);
+        A.f[e] += __shfl_xor_sync(0xffffffffu, A.f[e], o);
+      }
+    if (act && grp == 0) {
+      double lv[3], g[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
+      l2p(ti, lv, g);
+      if (VS) {
+        for (int e = 0; e < 3; ++e) ls[e] = ta[0] * g[e] + ta[1] * g[e + 3] + ta[2] * g[e + 6];
+        if (DF) {
+          lr[0] = g[1 + 6] - g[2 + 3];
+          lr[1] = g[2 + 0] - g[0 + 6];
+          lr[2] = g[0 + 3] - g[1 + 0];
+        }
+      }
+      double nu = d.nu_inf;
+      if (TV) {
+        const double rv = d.P[6 * n + ti];
+        nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave_ros);
+      }
+      for (int e = 0; e < 3; ++e) {
+        d.out[(size_t)e * n + ti] = lv[e] + A.v[e] * k4pi;
+        d.out[(size_t)(3 + e) * n + ti] = ls[e] + A.s[e] * k4pi + (VD ? A.f[e] * nu : 0.0);
+        d.out[(size_t)(6 + e) * n + ti] = lr[e] + A.r[e] * k4pi;
+      }
+    }
+  }
+}
+
 // ======================================================== host orchestration
 static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -1308,6 +1521,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   d.act_key = (const uint32_t *)o->act_key.p;
   d.act_lev = (const uint8_t *)o->act_lev.p;
   d.leaf_ci = (const uint32_t *)o->leaf_ci.p;
+  d.n_leaves = (uint32_t)o->n_leaves;
   double *mp = (double *)o->mp.p;
   d.A = mp;
   d.B = mp + (size_t)nact * 3 * o->nm;
@@ -1373,7 +1587,8 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
 #define LAUNCH_P2P(A, B, C, D)                                                   \
   do {                                                                         \
     if (f32)                                                                   \
-      k_p2p<A, B, C, D, true><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);    \
+      k_p2p_w<A, B, C, D><<<(unsigned)((o->n_leaves + P2W_WARPS - 1) / P2W_WARPS), \
+                            P2W_WARPS * 32, 0, st>>>(d);                        \
     else                                                                       \
       k_p2p<A, B, C, D, false><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);   \
   } while (0)

@@ -33,6 +33,7 @@ struct FmmDev {
   const uint32_t *act_key;
   const uint8_t *act_lev;
   const uint32_t *leaf_ci;
+  uint32_t n_leaves;
   double *A, *B, *Gx;  // multipole a, local b (deg p), local g (deg p+1)
   double *out;         // sorted-order vel(3), stretch(3), rotu(3), SoA
   int64_t *counters;   // [0] M2L pairs, [1] P2P pairs
