@@ -20,8 +20,8 @@
 // field runs in FP32 on coordinates taken relative to a reference point of
 // the CTA's particle tile (so no large-coordinate cancellation); partial
 // sums over one tile of sources are FP32 and are added into FP64
-// accumulators tile by tile; near pairs stay FP64 (queued and evaluated
-// apart from the FP32 loop, k_elem_out_split).
+// accumulators tile by tile; near pairs stay FP64 (listed by the FP32
+// kernel and evaluated apart from it, k_elem_far / k_elem_near).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -68,24 +68,19 @@ __device__ inline void near_pan(const RegParams &rp, const PanelGeo *pg, int j,
 #define EF_T 128
 #define EF_TILE 64
 
-template <bool F32>
+// FP64 element sums (plain mode): far field by the closed form above, near
+// pairs by the reference's formulas; then end vortices, wind and the scatter
+// of all outputs to the caller's order.
 __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FFRec *ff,
                                                    double *vel, double *str, double *rot) {
   __shared__ double s_c[EF_TILE][3], s_n[EF_TILE][3];
   __shared__ double s_amu[EF_TILE], s_asig[EF_TILE], s_ff2[EF_TILE];
-  __shared__ float f_c[EF_TILE][3], f_n[EF_TILE][3], f_amu[EF_TILE], f_asig[EF_TILE],
-      f_ff2[EF_TILE];
   const uint32_t t = blockIdx.x * EF_T + threadIdx.x;
   const size_t n = d.n;
   const bool act = t < n;
-  const uint32_t t0 = blockIdx.x * EF_T;
-  // reference point of the tile (first particle of the CTA)
-  const double ref[3] = {d.P[t0], d.P[n + t0], d.P[2 * n + t0]};
-  double pos[3] = {ref[0], ref[1], ref[2]};
+  double pos[3] = {0.0, 0.0, 0.0};
   if (act)
     for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
-  const float px = (float)(pos[0] - ref[0]), py = (float)(pos[1] - ref[1]),
-              pz = (float)(pos[2] - ref[2]);
   double v[3] = {0, 0, 0};
   const int ntot = e.nbody + e.nwake;
   for (int p0 = 0; p0 < ntot; p0 += EF_TILE) {
@@ -93,75 +88,35 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
     const int m = min(EF_TILE, ntot - p0);
     for (int q = threadIdx.x; q < m; q += EF_T) {
       const FFRec &r = ff[p0 + q];
-      if (F32) {
-        for (int c = 0; c < 3; ++c) {
-          f_c[q][c] = (float)(r.c[c] - ref[c]);
-          f_n[q][c] = (float)r.n[c];
-        }
-        f_amu[q] = (float)r.amu;
-        f_asig[q] = (float)r.asig;
-        // squared far-field radius, rounded up so a far pair in FP32 is far
-        // in FP64 too; pairs within rounding of the threshold go near
-        f_ff2[q] = (float)r.ff2 * 1.000001f;
-      } else {
-        for (int c = 0; c < 3; ++c) {
-          s_c[q][c] = r.c[c];
-          s_n[q][c] = r.n[c];
-        }
-        s_amu[q] = r.amu;
-        s_asig[q] = r.asig;
-        s_ff2[q] = r.ff2;
+      for (int c = 0; c < 3; ++c) {
+        s_c[q][c] = r.c[c];
+        s_n[q][c] = r.n[c];
       }
+      s_amu[q] = r.amu;
+      s_asig[q] = r.asig;
+      s_ff2[q] = r.ff2;
     }
     __syncthreads();
     if (!act) continue;
-    if (F32) {
-      f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
-      for (int q = 0; q < m; ++q) {
-        float rx = px - f_c[q][0], ry = py - f_c[q][1], rz = pz - f_c[q][2];
-        float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-        if (r2 > f_ff2[q]) {
-          float ir = rsqrtf(r2);
-          float ir2 = ir * ir;
-          float rn = fmaf(rx, f_n[q][0], fmaf(ry, f_n[q][1], rz * f_n[q][2]));
-          float k3 = ir2 * ir;
-          float coef = fmaf(3.0f * f_amu[q] * rn, ir2, f_asig[q]);
-          two_sum_acc(ax, k3 * fmaf(coef, rx, -f_amu[q] * f_n[q][0]));
-          two_sum_acc(ay, k3 * fmaf(coef, ry, -f_amu[q] * f_n[q][1]));
-          two_sum_acc(az, k3 * fmaf(coef, rz, -f_amu[q] * f_n[q][2]));
-        } else {
-          int j = p0 + q;
-          const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
-          int jj = j < e.nbody ? j : j - e.nbody;
-          double u[3];
-          near_pan(e.rp, pg, jj, pos, u);
-          for (int c = 0; c < 3; ++c) v[c] += u[c];
-        }
-      }
-      v[0] += (double)ax.s + (double)ax.c;
-      v[1] += (double)ay.s + (double)ay.c;
-      v[2] += (double)az.s + (double)az.c;
-    } else {
-      for (int q = 0; q < m; ++q) {
-        double rx = pos[0] - s_c[q][0], ry = pos[1] - s_c[q][1], rz = pos[2] - s_c[q][2];
-        double r2 = rx * rx + ry * ry + rz * rz;
-        if (r2 > s_ff2[q]) {
-          double ir = rsqrt(r2);
-          double ir2 = ir * ir;
-          double rn = rx * s_n[q][0] + ry * s_n[q][1] + rz * s_n[q][2];
-          double k3 = ir2 * ir;
-          double coef = 3.0 * s_amu[q] * rn * ir2 + s_asig[q];
-          v[0] += k3 * (coef * rx - s_amu[q] * s_n[q][0]);
-          v[1] += k3 * (coef * ry - s_amu[q] * s_n[q][1]);
-          v[2] += k3 * (coef * rz - s_amu[q] * s_n[q][2]);
-        } else {
-          int j = p0 + q;
-          const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
-          int jj = j < e.nbody ? j : j - e.nbody;
-          double u[3];
-          near_pan(e.rp, pg, jj, pos, u);
-          for (int c = 0; c < 3; ++c) v[c] += u[c];
-        }
+    for (int q = 0; q < m; ++q) {
+      double rx = pos[0] - s_c[q][0], ry = pos[1] - s_c[q][1], rz = pos[2] - s_c[q][2];
+      double r2 = rx * rx + ry * ry + rz * rz;
+      if (r2 > s_ff2[q]) {
+        double ir = rsqrt(r2);
+        double ir2 = ir * ir;
+        double rn = rx * s_n[q][0] + ry * s_n[q][1] + rz * s_n[q][2];
+        double k3 = ir2 * ir;
+        double coef = 3.0 * s_amu[q] * rn * ir2 + s_asig[q];
+        v[0] += k3 * (coef * rx - s_amu[q] * s_n[q][0]);
+        v[1] += k3 * (coef * ry - s_amu[q] * s_n[q][1]);
+        v[2] += k3 * (coef * rz - s_amu[q] * s_n[q][2]);
+      } else {
+        int j = p0 + q;
+        const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
+        int jj = j < e.nbody ? j : j - e.nbody;
+        double u[3];
+        near_pan(e.rp, pg, jj, pos, u);
+        for (int c = 0; c < 3; ++c) v[c] += u[c];
       }
     }
   }
@@ -395,7 +350,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
     if (precision == DUST_PREC_FP32C && ntot < (1 << 22))
       return elem_output_split(d, e, ff, work, near_cap, vel, str, rot, st, kev, kev_done);
     else
-      k_elem_out<false><<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
+      k_elem_out<<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
   }
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
@@ -407,16 +362,12 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
 #define UV2_T 128
 #define UV2_TILE 128
 
-template <bool F32>
+// FP64 uvort (plain mode): particles in the caller's order
 __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, int n,
                                                  const double *cen, const double *dir,
                                                  const double *mag, const double *rv,
                                                  int chunk, double *uv) {
-  // particles arrive in the caller's order, so a tile is not spatially
-  // compact: the FP32 path takes the point-particle difference in FP64 and
-  // rounds only the difference
   __shared__ double s_x[UV2_TILE][3], s_a[UV2_TILE][3], s_s[UV2_TILE];
-  __shared__ float f_a[UV2_TILE][3], f_s2[UV2_TILE];
   const int t = blockIdx.x * UV2_T + threadIdx.x;
   const bool act = t < npts;
   const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
@@ -431,41 +382,19 @@ __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, in
     if (threadIdx.x < m) {
       double mg = mag[q];
       for (int c = 0; c < 3; ++c) s_x[threadIdx.x][c] = cen[3 * (size_t)q + c];
-      if (F32) {
-        for (int c = 0; c < 3; ++c) f_a[threadIdx.x][c] = (float)(mg * dir[3 * (size_t)q + c]);
-        f_s2[threadIdx.x] = (float)(rv[q] * rv[q]);
-      } else {
-        for (int c = 0; c < 3; ++c) s_a[threadIdx.x][c] = mg * dir[3 * (size_t)q + c];
-        s_s[threadIdx.x] = rv[q];
-      }
+      for (int c = 0; c < 3; ++c) s_a[threadIdx.x][c] = mg * dir[3 * (size_t)q + c];
+      s_s[threadIdx.x] = rv[q];
     }
     __syncthreads();
     if (!act) continue;
-    if (F32) {
-      f32c ax = {0.f, 0.f}, ay = {0.f, 0.f}, az = {0.f, 0.f};
-      for (int u = 0; u < m; ++u) {
-        float dx = (float)(pos[0] - s_x[u][0]), dy = (float)(pos[1] - s_x[u][1]),
-              dz = (float)(pos[2] - s_x[u][2]);
-        float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, f_s2[u])));
-        float ir = rsqrtf(r2);
-        float c = -ir * ir * ir;
-        two_sum_acc(ax, c * (dy * f_a[u][2] - dz * f_a[u][1]));
-        two_sum_acc(ay, c * (dz * f_a[u][0] - dx * f_a[u][2]));
-        two_sum_acc(az, c * (dx * f_a[u][1] - dy * f_a[u][0]));
-      }
-      v[0] += (double)ax.s + (double)ax.c;
-      v[1] += (double)ay.s + (double)ay.c;
-      v[2] += (double)az.s + (double)az.c;
-    } else {
-      for (int u = 0; u < m; ++u) {
-        double dx = pos[0] - s_x[u][0], dy = pos[1] - s_x[u][1], dz = pos[2] - s_x[u][2];
-        double r2 = dx * dx + dy * dy + dz * dz + s_s[u] * s_s[u];
-        double ir = rsqrt(r2);
-        double c = -ir * ir * ir;
-        v[0] += c * (dy * s_a[u][2] - dz * s_a[u][1]);
-        v[1] += c * (dz * s_a[u][0] - dx * s_a[u][2]);
-        v[2] += c * (dx * s_a[u][1] - dy * s_a[u][0]);
-      }
+    for (int u = 0; u < m; ++u) {
+      double dx = pos[0] - s_x[u][0], dy = pos[1] - s_x[u][1], dz = pos[2] - s_x[u][2];
+      double r2 = dx * dx + dy * dy + dz * dz + s_s[u] * s_s[u];
+      double ir = rsqrt(r2);
+      double c = -ir * ir * ir;
+      v[0] += c * (dy * s_a[u][2] - dz * s_a[u][1]);
+      v[1] += c * (dz * s_a[u][0] - dx * s_a[u][2]);
+      v[2] += c * (dx * s_a[u][1] - dy * s_a[u][0]);
     }
   }
   if (!act) return;
@@ -505,7 +434,7 @@ __global__ void k_uv_gather(int n, const uint32_t *perm, const double *cen, cons
 }
 
 // UV2_PPT points per thread (consecutive CTA slices of UV2_T points)
-#define UV2_PPT 2
+#define UV2_PPT 4
 __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *pts, int n,
                                                         const double *X, const float *F,
                                                         int chunk, double *uv) {
@@ -639,7 +568,7 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
       k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, rv, X, F);
       k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uv);
     } else {
-      k_uvort<false><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
+      k_uvort<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
     }
   }
   if (lines.nline > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, lines, uv);
@@ -737,7 +666,7 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
       k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, r_vortex, X, F);
       k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uvort);
     } else {
-      k_uvort<false><<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, r_vortex, chunk, uvort);
+      k_uvort<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, r_vortex, chunk, uvort);
     }
   }
   if (nl > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, e, uvort);

@@ -129,15 +129,3 @@ __host__ __device__ inline bool cart_in(const TreeGeom &G, int l, int i, int j, 
 #define FL_BRANCH 2
 #define FL_ACTIVE 4
 
-// ------------------------------------------------------------- FP helpers
-// Error-free transformation (Knuth two-sum) for compensated FP32 sums.
-struct f32c {
-  float s, c;
-};
-__device__ __forceinline__ void two_sum_acc(f32c &a, float x) {
-  float t = a.s + x;
-  float bp = t - a.s;
-  float e = (a.s - (t - bp)) + (x - bp);
-  a.s = t;
-  a.c += e;
-}

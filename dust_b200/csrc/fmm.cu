@@ -1194,11 +1194,12 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
 #define P2W_MAXR 320
 
 template <bool VS, bool DF, bool VD, bool TV>
-__global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
+__global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
   __shared__ float s_src[P2W_WARPS][7][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
   __shared__ uint32_t s_rlo[P2W_WARPS][P2W_MAXR];
   __shared__ uint32_t s_rcum[P2W_WARPS][P2W_MAXR + 1];
+  __shared__ double s_acc[P2W_WARPS][12][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t leaf = blockIdx.x * P2W_WARPS + w;
   if (leaf >= d.n_leaves) return;  // warp-uniform: no CTA-wide barriers below
@@ -1309,6 +1310,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
     ave_ros = part / (double)nt;
   }
   float *fs = &s_src[w][0][0];
+  double *acc = &s_acc[w][0][lane];  // this lane's 12 FP64 sums, stride 32
   for (int t0 = 0; t0 < nt; t0 += 32) {
     const int cnt = min(32, nt - t0);
     int TPR = 1;
@@ -1316,12 +1318,10 @@ __global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
     const int G = 32 / TPR, tl = lane & (TPR - 1), grp = lane / TPR;
     const bool act = tl < cnt;
     const uint32_t ti = lo + t0 + (act ? tl : 0);
-    const double tp[3] = {d.P[ti], d.P[n + ti], d.P[2 * n + ti]};
-    const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
-    const float ftp[3] = {(float)(tp[0] - cc[0]), (float)(tp[1] - cc[1]), (float)(tp[2] - cc[2])};
-    const float fta[3] = {(float)ta[0], (float)ta[1], (float)ta[2]};
-    P2PAcc A;
-    for (int e = 0; e < 3; ++e) A.v[e] = A.s[e] = A.r[e] = A.f[e] = 0.0;
+    const float ftp[3] = {(float)(d.P[ti] - cc[0]), (float)(d.P[n + ti] - cc[1]),
+                          (float)(d.P[2 * n + ti] - cc[2])};
+    const float fta[3] = {(float)d.P[3 * n + ti], (float)d.P[4 * n + ti], (float)d.P[5 * n + ti]};
+    for (int e = 0; e < 12; ++e) acc[32 * e] = 0.0;
     P2PAccF B;
     for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
     int since = 0;
@@ -1352,23 +1352,22 @@ __global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
         // FP32 partial sums of up to 128 sources folded into FP64
         since = 0;
         for (int e = 0; e < 3; ++e) {
-          A.v[e] += (double)B.v[e];
-          A.s[e] += (double)B.s[e];
-          A.r[e] += (double)B.r[e];
-          A.f[e] += (double)B.f[e];
+          acc[32 * e] += (double)B.v[e];
+          acc[32 * (3 + e)] += (double)B.s[e];
+          acc[32 * (6 + e)] += (double)B.r[e];
+          acc[32 * (9 + e)] += (double)B.f[e];
           B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
         }
       }
     }
     // combine the groups of each target
-    for (int o = TPR; o < 32; o <<= 1)
-      for (int e = 0; e < 3; ++e) {
-        A.v[e] += __shfl_xor_sync(0xffffffffu, A.v[e], o);
-        A.s[e] += __shfl_xor_sync(0xffffffffu, A.s[e], o);
-        A.r[e] += __shfl_xor_sync(0xffffffffu, A.r[e], o);
-        A.f[e] += __shfl_xor_sync(0xffffffffu, A.f[e], o);
-      }
+    double A[12];
+    for (int e = 0; e < 12; ++e) {
+      A[e] = acc[32 * e];
+      for (int o = TPR; o < 32; o <<= 1) A[e] += __shfl_xor_sync(0xffffffffu, A[e], o);
+    }
     if (act && grp == 0) {
+      const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
       double lv[3], g[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
       l2p(ti, lv, g);
       if (VS) {
@@ -1385,9 +1384,9 @@ __global__ void __launch_bounds__(P2W_WARPS * 32) k_p2p_w(FmmDev d) {
         nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave_ros);
       }
       for (int e = 0; e < 3; ++e) {
-        d.out[(size_t)e * n + ti] = lv[e] + A.v[e] * k4pi;
-        d.out[(size_t)(3 + e) * n + ti] = ls[e] + A.s[e] * k4pi + (VD ? A.f[e] * nu : 0.0);
-        d.out[(size_t)(6 + e) * n + ti] = lr[e] + A.r[e] * k4pi;
+        d.out[(size_t)e * n + ti] = lv[e] + A[e] * k4pi;
+        d.out[(size_t)(3 + e) * n + ti] = ls[e] + A[3 + e] * k4pi + (VD ? A[9 + e] * nu : 0.0);
+        d.out[(size_t)(6 + e) * n + ti] = lr[e] + A[6 + e] * k4pi;
       }
     }
   }
