@@ -275,18 +275,91 @@ __global__ void k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count
 }
 
 // end vortices, wind, FMM outputs; scatter to the caller's order
-__global__ void k_elem_fin(FmmDev d, ElemDev e, const double *farv, double *vel, double *str,
-                           double *rot) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t n = d.n;
-  if (t >= n) return;
-  const double pos[3] = {d.P[t], d.P[n + t], d.P[2 * n + t]};
-  double w[3] = {farv[t], farv[n + t], farv[2 * n + t]};
-  for (int q = 0; q < e.nline; ++q) {
-    double u[3];
-    vel_line(e.rp, e.lines[q], pos, u);
-    for (int c = 0; c < 3; ++c) w[c] += u[c];
+// End vortices in FP32 (k_elem_fin): segment (v0, v1) of circulation mag at
+// a point p.  With a = p - v0,
+// b = p - v1, e the unit direction and c = e x a (so |c| = h, the distance
+// to the line, without the cancellation of a - (a.e) e), the reference's
+// ((L - ai)/|b| + ai/|a|) c / h^2 is used while the projection ai = a.e lies
+// on the segment (both terms positive), and the equivalent
+// L c (|a| + |b|) / (|a||b|(|a||b| + a.b)) beyond its ends (a.b > 0 there), so
+// neither form cancels.  Inside the Rankine core the result is scaled by
+// h^2 / (r_rankine L)^2 as in the reference's core formula.
+__device__ __forceinline__ void line_vel_f(const double *vv, const float *q, const double *pos,
+                                           float rr2, float rc, float *u) {
+  // vv: v0 (3), v1 (3) in FP64; q: e (3), L, mag.  a and b are formed in
+  // FP64 and rounded once, so their accuracy does not depend on the spread
+  // of the CTA's particles.
+  const float ax = (float)(pos[0] - vv[0]), ay = (float)(pos[1] - vv[1]),
+              az = (float)(pos[2] - vv[2]);
+  const float bx = (float)(pos[0] - vv[3]), by = (float)(pos[1] - vv[4]),
+              bz = (float)(pos[2] - vv[5]);
+  const float L = q[3];
+  const float ra = sqrtf(fmaf(ax, ax, fmaf(ay, ay, az * az)));
+  const float rb = sqrtf(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+  const float ai = fmaf(ax, q[0], fmaf(ay, q[1], az * q[2]));
+  const float cx = q[1] * az - q[2] * ay, cy = q[2] * ax - q[0] * az, cz = q[0] * ay - q[1] * ax;
+  const float hi2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+  float f;
+  if (ai > 0.f && ai < L) {
+    f = hi2 > 0.f ? ((L - ai) / rb + ai / ra) / hi2 : 0.f;
+  } else {
+    const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
+    const float den = ra * rb * fmaf(ra, rb, ab);
+    f = den > 0.f ? L * (ra + rb) / den : 0.f;
   }
+  const float rrL2 = rr2 * L * L;
+  if (!(hi2 > rrL2)) {
+    // Rankine core (or the cutoff around the end points)
+    f = (ra > L * rc && rb > L * rc) ? f * hi2 / rrL2 : 0.f;
+  }
+  f *= q[4];
+  u[0] = f * cx;
+  u[1] = f * cy;
+  u[2] = f * cz;
+}
+
+#define EL_T 128
+#define EL_TILE 64
+__global__ void __launch_bounds__(EL_T) k_elem_fin(FmmDev d, ElemDev e, const double *farv,
+                                                   double *vel, double *str, double *rot) {
+  __shared__ double s_v[EL_TILE][6];
+  __shared__ float s_l[EL_TILE][5];
+  const uint32_t t0 = blockIdx.x * EL_T, t = t0 + threadIdx.x;
+  const size_t n = d.n;
+  const bool act = t < n;
+  double pos[3] = {0.0, 0.0, 0.0};
+  if (act)
+    for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
+  const float rr2 = (float)(e.rp.r_rankine * e.rp.r_rankine), rc = (float)e.rp.r_cutoff;
+  double w[3] = {0.0, 0.0, 0.0};
+  if (act)
+    for (int c = 0; c < 3; ++c) w[c] = farv[(size_t)c * n + t];
+  for (int q0 = 0; q0 < e.nline; q0 += EL_TILE) {
+    const int m = min(EL_TILE, e.nline - q0);
+    __syncthreads();
+    if (threadIdx.x < m) {
+      const LineGeo &L = e.lines[q0 + threadIdx.x];
+      float *q = s_l[threadIdx.x];
+      for (int c = 0; c < 3; ++c) {
+        s_v[threadIdx.x][c] = L.ver[0][c];
+        s_v[threadIdx.x][3 + c] = L.ver[1][c];
+        q[c] = (float)L.edge_uni[c];
+      }
+      q[3] = (float)L.edge_len;
+      q[4] = (float)L.mag;
+    }
+    __syncthreads();
+    float a[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < m; ++k) {
+      float u[3];
+      line_vel_f(s_v[k], s_l[k], pos, rr2, rc, u);
+      a[0] += u[0];
+      a[1] += u[1];
+      a[2] += u[2];
+    }
+    for (int c = 0; c < 3; ++c) w[c] += (double)a[c];
+  }
+  if (!act) return;
   const double k4pi = 1.0 / (4.0 * DUST_PI);
   const uint32_t ip = d.perm[t];
   for (int c = 0; c < 3; ++c) {
@@ -328,7 +401,7 @@ static int elem_output_split(FmmDev &d, const ElemDev &e, const FFRec *ff, DevBu
       const unsigned grid = (unsigned)std::min<unsigned long long>((h + 127) / 128, 148ull * 64);
       k_elem_near<<<grid, 128, 0, st>>>(d, e, count, list, (unsigned long long)near_cap, farv);
     }
-    k_elem_fin<<<nblk(n, 128), 128, 0, st>>>(d, e, farv, vel, str, rot);
+    k_elem_fin<<<nblk(n, EL_T), EL_T, 0, st>>>(d, e, farv, vel, str, rot);
     DUST_CUDA(cudaGetLastError());
     return DUST_OK;
   }
