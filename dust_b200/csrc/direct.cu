@@ -62,7 +62,7 @@ __global__ void k_ffrec(const PanelGeo *pg, int n, double ff_dou, FFRec *out) {
 // exact reference evaluation of one panel (x 4 pi)
 __device__ inline void near_pan(const RegParams &rp, const PanelGeo *pg, int j,
                                 const double *pos, double *v) {
-  vel_pan(rp, pg[j], pos, v);
+  vel_pan_near(rp, pg[j], pos, v);
 }
 
 #define EF_T 128
@@ -143,19 +143,35 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
 // not clearly far (threshold widened by 1e-4 so a pair far in FP32 is far in
 // FP64) is queued in shared memory and the queue is appended to a global list
 // of near pairs.  k_elem_near evaluates that list with the reference's exact
-// FP64 formulas (vel_pan), one pair per thread, and k_elem_fin adds the end
+// FP64 formulas (vel_pan_near), one pair per thread, and k_elem_fin adds the end
 // vortices and writes the outputs in the caller's order.  Keeping the heavy
 // FP64 formulas out of the FP32 kernel keeps its register count, and so its
 // occupancy, at the level of the far-field arithmetic.
-#define EF2_T 128
+//
+// Most tiles lie beyond the far-field radius of every particle of the CTA:
+// the loader threads test each panel against the bounding box of the CTA's
+// particles (with a further 1e-4 margin, so the box test never calls far a
+// pair the per-pair test would queue) and such tiles run a loop without the
+// per-pair test.  A tile shorter than EF2_TILE is padded with null panels
+// (no strength, 1e6 away) so both loops are fully unrolled.
+#ifndef EF2_PPT
 #define EF2_PPT 2
+#endif
+#define EF2_T 128
 #define EF2_NP (EF2_T * EF2_PPT)
 #define EF2_TILE 16
-#define EF2_QCAP (2 * EF2_NP * EF2_TILE)
+#define EF2_QCAP (EF2_NP * EF2_TILE)  // one tile's worst case
+static_assert(EF2_NP <= 1024, "local particle index is packed in 10 bits");
 
 struct NearPair {
   uint32_t t, j;  // particle (sorted order), panel
 };
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 __device__ __forceinline__ void ef2_flush(const uint32_t *s_q, int qn, uint32_t t0,
                                           unsigned long long *count, NearPair *list,
@@ -172,13 +188,52 @@ __device__ __forceinline__ void ef2_flush(const uint32_t *s_q, int qn, uint32_t 
   }
 }
 
+// far-field term of a panel at r = p - c, added to acc:
+//   nm = 3 A mu n, mn = -A mu n, as = A sigma:
+//   acc += (1/r^3) (r (r.nm / r^2 + as) + mn)
+__device__ __forceinline__ void ef2_term(float rx, float ry, float rz, float r2, float nmx,
+                                         float nmy, float nmz, float mnx, float mny, float mnz,
+                                         float as, float *acc) {
+  const float ir = rsqrt_approx(r2);
+  const float ir2 = ir * ir;
+  const float k3 = ir2 * ir;
+  const float rn = fmaf(rx, nmx, fmaf(ry, nmy, rz * nmz));
+  const float coef = fmaf(rn, ir2, as);
+  acc[0] = fmaf(k3, fmaf(coef, rx, mnx), acc[0]);
+  acc[1] = fmaf(k3, fmaf(coef, ry, mny), acc[1]);
+  acc[2] = fmaf(k3, fmaf(coef, rz, mnz), acc[2]);
+}
+
+// The same term for two panels at once in packed FP32 (f32x2) arithmetic.
+__device__ __forceinline__ void ef2_term2(float2 px, float2 py, float2 pz, float2 ncx, float2 ncy,
+                                          float2 ncz, float2 nmx, float2 nmy, float2 nmz,
+                                          float2 mnx, float2 mny, float2 mnz, float2 as,
+                                          float2 *acc) {
+  const float2 rx = __fadd2_rn(px, ncx), ry = __fadd2_rn(py, ncy), rz = __fadd2_rn(pz, ncz);
+  const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+  const float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+  const float2 ir2 = __fmul2_rn(ir, ir);
+  const float2 k3 = __fmul2_rn(ir2, ir);
+  const float2 rn = __ffma2_rn(rx, nmx, __ffma2_rn(ry, nmy, __fmul2_rn(rz, nmz)));
+  const float2 coef = __ffma2_rn(rn, ir2, as);
+  acc[0] = __ffma2_rn(k3, __ffma2_rn(coef, rx, mnx), acc[0]);
+  acc[1] = __ffma2_rn(k3, __ffma2_rn(coef, ry, mny), acc[1]);
+  acc[2] = __ffma2_rn(k3, __ffma2_rn(coef, rz, mnz), acc[2]);
+}
+
+// Shared-memory tile: panels in pairs (q, q+1); the ten values of a pair
+// (-cx, -cy, -cz, nm x/y/z, mn x/y/z, as) are stored interleaved, value k of
+// panel q at [q / 2][2 k + q % 2], so five float4 loads give the ten float2
+// operands of ef2_term2.
+#define EF2_PK 20
+
 __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const FFRec *ff,
                                                     double *farv, unsigned long long *count,
                                                     NearPair *list, unsigned long long cap) {
-  __shared__ float4 s_cf[EF2_TILE];  // centre - ref, widened ff2
-  __shared__ float4 s_nm[EF2_TILE];  // normal, 3 * area * mag
-  __shared__ float4 s_mn[EF2_TILE];  // -area * mag * normal, area * sigma
+  __shared__ __align__(16) float s_pk[EF2_TILE / 2][EF2_PK];
+  __shared__ float s_ff[EF2_TILE];  // widened ff2
   __shared__ uint32_t s_q[EF2_QCAP];  // (panel << 10) | local particle
+  __shared__ float s_box[EF2_T / 32][6];
   __shared__ int s_qn;
   __shared__ unsigned long long s_base;
   const size_t n = d.n;
@@ -188,6 +243,7 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
   float px[EF2_PPT], py[EF2_PPT], pz[EF2_PPT];
   bool act[EF2_PPT];
   double v[EF2_PPT][3];
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
   for (int i = 0; i < EF2_PPT; ++i) {
     const uint32_t t = t0 + tid + i * EF2_T;
@@ -198,9 +254,27 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
     px[i] = (float)(pos[0] - ref[0]);
     py[i] = (float)(pos[1] - ref[1]);
     pz[i] = (float)(pos[2] - ref[2]);
+    if (act[i]) {
+      lo[0] = fminf(lo[0], px[i]), hi[0] = fmaxf(hi[0], px[i]);
+      lo[1] = fminf(lo[1], py[i]), hi[1] = fmaxf(hi[1], py[i]);
+      lo[2] = fminf(lo[2], pz[i]), hi[2] = fmaxf(hi[2], pz[i]);
+    }
     v[i][0] = v[i][1] = v[i][2] = 0.0;
   }
+  // bounding box of the CTA's particles
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+  if ((tid & 31) == 0)
+    for (int c = 0; c < 3; ++c) s_box[tid >> 5][c] = lo[c], s_box[tid >> 5][3 + c] = hi[c];
   if (tid == 0) s_qn = 0;
+  __syncthreads();
+  for (int w = 0; w < EF2_T / 32; ++w)
+    for (int c = 0; c < 3; ++c)
+      lo[c] = fminf(lo[c], s_box[w][c]), hi[c] = fmaxf(hi[c], s_box[w][3 + c]);
   const int ntot = e.nbody + e.nwake;
   for (int p0 = 0; p0 < ntot; p0 += EF2_TILE) {
     const int m = min(EF2_TILE, ntot - p0);
@@ -211,42 +285,79 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
       __syncthreads();
       if (tid == 0) s_qn = 0;
     }
-    if (tid < m) {
-      const FFRec &r = ff[p0 + tid];
-      s_cf[tid] = make_float4((float)(r.c[0] - ref[0]), (float)(r.c[1] - ref[1]),
-                              (float)(r.c[2] - ref[2]), (float)r.ff2 * 1.0001f);
-      s_nm[tid] = make_float4((float)r.n[0], (float)r.n[1], (float)r.n[2], (float)(3.0 * r.amu));
-      s_mn[tid] = make_float4((float)(-r.amu * r.n[0]), (float)(-r.amu * r.n[1]),
-                              (float)(-r.amu * r.n[2]), (float)r.asig);
+    bool near_box = false;
+    if (tid < EF2_TILE) {
+      float val[10] = {-1.0e6f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float ffw = 0.f;
+      if (tid < m) {
+        const FFRec &r = ff[p0 + tid];
+        const float cx = (float)(r.c[0] - ref[0]), cy = (float)(r.c[1] - ref[1]),
+                    cz = (float)(r.c[2] - ref[2]);
+        ffw = (float)r.ff2 * 1.0001f;
+        const float a3 = (float)(3.0 * r.amu);
+        val[0] = -cx, val[1] = -cy, val[2] = -cz;
+        for (int c = 0; c < 3; ++c) {
+          val[3 + c] = a3 * (float)r.n[c];
+          val[6 + c] = (float)(-r.amu * r.n[c]);
+        }
+        val[9] = (float)r.asig;
+        const float dx = fmaxf(fmaxf(lo[0] - cx, cx - hi[0]), 0.f);
+        const float dy = fmaxf(fmaxf(lo[1] - cy, cy - hi[1]), 0.f);
+        const float dz = fmaxf(fmaxf(lo[2] - cz, cz - hi[2]), 0.f);
+        near_box = !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ffw * 1.0001f);
+      }
+      for (int k = 0; k < 10; ++k) s_pk[tid >> 1][2 * k + (tid & 1)] = val[k];
+      s_ff[tid] = ffw;
     }
-    __syncthreads();
-    float acc[EF2_PPT][3];
+    const bool tile_near = __syncthreads_or(near_box);
+    double tv[EF2_PPT][3];
+    if (!tile_near) {
+      float2 acc[EF2_PPT][3];
 #pragma unroll
-    for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
-    for (int q = 0; q < m; ++q) {
-      const float4 cf = s_cf[q], nm = s_nm[q], mn = s_mn[q];
+      for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int i = 0; i < EF2_PPT; ++i) {
-        const float rx = px[i] - cf.x, ry = py[i] - cf.y, rz = pz[i] - cf.z;
-        const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-        if (r2 > cf.w) {
-          const float ir = rsqrtf(r2);
-          const float ir2 = ir * ir;
-          const float rn = fmaf(rx, nm.x, fmaf(ry, nm.y, rz * nm.z));
-          const float k3 = ir2 * ir;
-          const float coef = fmaf(nm.w * rn, ir2, mn.w);
-          acc[i][0] = fmaf(k3, fmaf(coef, rx, mn.x), acc[i][0]);
-          acc[i][1] = fmaf(k3, fmaf(coef, ry, mn.y), acc[i][1]);
-          acc[i][2] = fmaf(k3, fmaf(coef, rz, mn.z), acc[i][2]);
-        } else if (act[i]) {
-          const int slot = atomicAdd(&s_qn, 1);
-          s_q[slot] = ((uint32_t)(p0 + q) << 10) | (uint32_t)(tid + i * EF2_T);
+      for (int pr = 0; pr < EF2_TILE / 2; ++pr) {
+        const float4 A = *(const float4 *)&s_pk[pr][0], B = *(const float4 *)&s_pk[pr][4],
+                     C = *(const float4 *)&s_pk[pr][8], D = *(const float4 *)&s_pk[pr][12],
+                     E = *(const float4 *)&s_pk[pr][16];
+#pragma unroll
+        for (int i = 0; i < EF2_PPT; ++i)
+          ef2_term2(make_float2(px[i], px[i]), make_float2(py[i], py[i]),
+                    make_float2(pz[i], pz[i]), make_float2(A.x, A.y), make_float2(A.z, A.w),
+                    make_float2(B.x, B.y), make_float2(B.z, B.w), make_float2(C.x, C.y),
+                    make_float2(C.z, C.w), make_float2(D.x, D.y), make_float2(D.z, D.w),
+                    make_float2(E.x, E.y), make_float2(E.z, E.w), acc[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < EF2_PPT; ++i)
+        for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c].x + (double)acc[i][c].y;
+    } else {
+      float acc[EF2_PPT][3];
+#pragma unroll
+      for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
+#pragma unroll 2
+      for (int q = 0; q < EF2_TILE; ++q) {
+        const float *pk = &s_pk[q >> 1][q & 1];
+        const float ffw = s_ff[q];
+#pragma unroll
+        for (int i = 0; i < EF2_PPT; ++i) {
+          const float rx = px[i] + pk[0], ry = py[i] + pk[2], rz = pz[i] + pk[4];
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          if (r2 > ffw) {
+            ef2_term(rx, ry, rz, r2, pk[6], pk[8], pk[10], pk[12], pk[14], pk[16], pk[18], acc[i]);
+          } else if (act[i]) {
+            const int slot = atomicAdd(&s_qn, 1);
+            s_q[slot] = ((uint32_t)(p0 + q) << 10) | (uint32_t)(tid + i * EF2_T);
+          }
         }
       }
+#pragma unroll
+      for (int i = 0; i < EF2_PPT; ++i)
+        for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c];
     }
 #pragma unroll
     for (int i = 0; i < EF2_PPT; ++i)
-      for (int c = 0; c < 3; ++c) v[i][c] += (double)acc[i][c];
+      for (int c = 0; c < 3; ++c) v[i][c] += tv[i][c];
   }
   __syncthreads();
   ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
@@ -269,7 +380,7 @@ __global__ void k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count
     const double pos[3] = {d.P[np.t], d.P[n + np.t], d.P[2 * n + np.t]};
     const PanelGeo *pg = (int)np.j < e.nbody ? e.body + np.j : e.wake + (np.j - e.nbody);
     double u[3];
-    vel_pan(e.rp, *pg, pos, u);
+    vel_pan_near(e.rp, *pg, pos, u);
     for (int c = 0; c < 3; ++c) atomicAdd(farv + (size_t)c * n + np.t, u[c]);
   }
 }

@@ -299,3 +299,122 @@ __device__ inline void vel_pan(const RegParams &rp, const PanelGeo &p, const dou
     for (int d = 0; d < 3; ++d) v[d] = vd[d] * p.mag;
   }
 }
+
+// vel_pan for a point inside the panel's far-field radius, with the
+// per-vertex quantities shared between the edges: the distances to the
+// vertices and to the projected vertices are computed once per vertex (the
+// reference's loops recompute each at both of its edges), reciprocal
+// distances replace the divisions by them, the solid angle's atan2 takes its
+// two arguments unscaled (atan2(y/d, x/d) = atan2(y, x) for d > 0), and the
+// Rankine-core test compares squares.  Same branches and formulas as
+// vel_pan (vel_dou, vel_sou, pot_dou), equal up to rounding; points beyond
+// the far-field radii go to vel_pan.
+template <int NV>
+__device__ inline void vel_pan_near_t(const RegParams &rp, const PanelGeo &p, const double *pos,
+                                      double *v) {
+  const double rv[3] = {pos[0] - p.cen[0], pos[1] - p.cen[1], pos[2] - p.cen[2]};
+  const double r2 = d3dot(rv, rv);
+  const double radius = sqrt(r2);
+  const bool sp = p.kind == DUST_ELEM_SURFPAN;
+  const bool dou_far = radius > rp.ff_dou * p.max_edge;
+  const bool sou_far = radius > 10.0 * p.max_edge;
+  if (dou_far && (!sp || sou_far)) {
+    vel_pan(rp, p, pos, v);
+    return;
+  }
+  constexpr int nv = NV;
+  double dv[NV][3], R[NV], iR[NV];
+#pragma unroll
+  for (int i = 0; i < nv; ++i) {
+    for (int d = 0; d < 3; ++d) dv[i][d] = pos[d] - p.ver[i][d];
+    const double q = d3dot(dv[i], dv[i]);
+    R[i] = sqrt(q);
+    iR[i] = 1.0 / R[i];
+  }
+  double vd[3] = {0.0, 0.0, 0.0};
+  if (dou_far) {
+    vel_dou(rp, p, pos, vd);
+  } else {
+#pragma unroll
+    for (int i1 = 0; i1 < nv; ++i1) {
+      const int ip1 = i1 + 1 == nv ? 0 : i1 + 1;
+      const double *eu = p.edge_uni[i1];
+      const double L = p.edge_len[i1];
+      const double ai = d3dot(dv[i1], eu);
+      double hv[3], cr[3];
+      for (int d = 0; d < 3; ++d) hv[d] = dv[i1][d] - ai * eu[d];
+      const double hi2 = d3dot(hv, hv);
+      d3cross(eu, hv, cr);
+      const double rr = rp.r_rankine * L;
+      double f;
+      if (hi2 > rr * rr) {
+        f = ((L - ai) * iR[ip1] + ai * iR[i1]) / hi2;
+      } else if (R[i1] > L * rp.r_cutoff && R[ip1] > L * rp.r_cutoff) {
+        f = ((L - ai) * iR[ip1] + ai * iR[i1]) / (rr * rr);
+      } else {
+        continue;
+      }
+      for (int d = 0; d < 3; ++d) vd[d] += f * cr[d];
+    }
+  }
+  if (!sp) {
+    for (int d = 0; d < 3; ++d) v[d] = vd[d] * p.mag;
+    return;
+  }
+  double vs[3];
+  if (sou_far) {
+    vel_sou(rp, p, pos, vs);
+  } else {
+    double Rp[NV];
+#pragma unroll
+    for (int i = 0; i < nv; ++i) {
+      const double a[3] = {pos[0] - p.verp[i][0], pos[1] - p.verp[i][1], pos[2] - p.verp[i][2]};
+      Rp[i] = sqrt(d3dot(a, a));
+    }
+    double phix = 0.0, phiy = 0.0;
+#pragma unroll
+    for (int i1 = 0; i1 < nv; ++i1) {
+      const int ip1 = i1 + 1 == nv ? 0 : i1 + 1;
+      const double L = p.edge_len[i1], s = Rp[i1] + Rp[ip1];
+      const double souLog = (s - L < 1e-12) ? 0.0 : log((s + L) / (s - L));
+      phix += p.sinTi[i1] * souLog;
+      phiy -= p.cosTi[i1] * souLog;
+    }
+    double pdou;
+    if (dou_far) {
+      pdou = d3dot(rv, p.nor) * p.area / (radius * radius * radius);
+    } else {
+      double dou = 0.0;
+#pragma unroll
+    for (int i1 = 0; i1 < nv; ++i1) {
+        const int im1 = i1 == 0 ? nv - 1 : i1 - 1;
+        double ei[3], ap1[3], am1[3], cr[3];
+        for (int d = 0; d < 3; ++d) ei[d] = -dv[i1][d] * iR[i1];
+        const double ep = d3dot(ei, p.edge_vec[i1]), em = d3dot(ei, p.edge_vec[im1]);
+        for (int d = 0; d < 3; ++d) {
+          ap1[d] = p.edge_vec[i1][d] - ei[d] * ep;
+          am1[d] = -p.edge_vec[im1][d] + ei[d] * em;
+        }
+        d3cross(am1, ap1, cr);
+        dou += atan2(d3dot(ei, cr), d3dot(am1, ap1));
+      }
+      const double gb = (double)(nv - 2) * DUST_PI;
+      if (dou < -gb + 1.0e-5)
+        dou += gb;
+      else if (dou > gb - 1.0e-5)
+        dou -= gb;
+      pdou = dou;
+    }
+    for (int d = 0; d < 3; ++d)
+      vs[d] = -(p.tang[0][d] * phix + p.tang[1][d] * phiy + p.nor[d] * pdou);
+  }
+  for (int d = 0; d < 3; ++d) v[d] = vd[d] * p.mag - vs[d] * p.sig;
+}
+
+__device__ inline void vel_pan_near(const RegParams &rp, const PanelGeo &p, const double *pos,
+                                    double *v) {
+  if (p.nv == 4)
+    vel_pan_near_t<4>(rp, p, pos, v);
+  else
+    vel_pan_near_t<3>(rp, p, pos, v);
+}
