@@ -16,6 +16,8 @@
 // instead of hanging.
 #include <climits>
 
+#include <cooperative_groups.h>
+
 #include "lu.cuh"
 
 #define PAN_T 256
@@ -219,6 +221,236 @@ __global__ void __launch_bounds__(PAN_T) k_panel(PanelArgs<T> a) {
   }
 }
 
+// Cluster panel factorisation: the panel's rows are split over the C CTAs
+// of one thread-block cluster, each CTA keeping its rows in shared memory.
+// Per column every CTA publishes its local pivot candidate (|value|, row and
+// the row's jb entries) in its own shared memory, one hardware cluster
+// barrier follows, and every CTA then reads the C candidates (and the
+// diagonal row) through distributed shared memory and makes the same
+// choice.  Published buffers alternate between two copies, so a CTA one
+// column ahead never overwrites data another CTA still reads; a final
+// cluster barrier keeps every CTA's shared memory alive until the last
+// remote read.  No spin waits: the cluster's CTAs are co-scheduled and all
+// take the same barriers.
+#define CPAN_T 256
+
+template <typename T>
+struct CPanelShared {  // published per column, two copies
+  T cval[2];
+  int crow[2];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(CPAN_T) k_panel_cluster(PanelArgs<T> a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int jb = a.jb, LD = jb + 1;
+  T *sp = (T *)smraw;                        // R rows x LD, row-major
+  T *s_crowv = sp + (size_t)a.R * LD;        // [2][jb] candidate row
+  T *s_srow = s_crowv + 2 * jb;              // [2][jb] diagonal row (owner only)
+  T *s_prow = s_srow + 2 * jb;               // [jb] pivot row (local copy)
+  __shared__ CPanelShared<T> s_pub;
+  __shared__ T s_wv[CPAN_T / 32];
+  __shared__ int s_wr[CPAN_T / 32], s_wg[CPAN_T / 32];
+  __shared__ int s_p;
+  const int g = (int)cl.block_rank(), C = (int)cl.num_blocks();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int NW = CPAN_T / 32;
+  const int r0 = g * a.R, r1 = min(a.m, r0 + a.R), nr = max(0, r1 - r0);
+  T *Ap = a.A + (size_t)a.k + (size_t)a.k * a.lda;
+  for (int idx = tid; idx < nr * jb; idx += CPAN_T) {
+    const int c = idx / nr, r = idx % nr;
+    sp[r * LD + c] = Ap[(size_t)(r0 + r) + (size_t)c * a.lda];
+  }
+  __syncthreads();
+  for (int j = 0; j < jb; ++j) {
+    const int buf = j & 1;
+    // local maximum of |a(r, j)| over own rows r >= j (first index on ties)
+    T best = (T)-1;
+    int brow = INT_MAX;
+    for (int r = tid; r < nr; r += CPAN_T) {
+      const int gr = r0 + r;
+      if (gr < j) continue;
+      T v = fabs(sp[r * LD + j]);
+      if (v != v) v = (T)-0.5;  // NaN: still a candidate, below every number
+      if (v > best || (v == best && gr < brow)) {
+        best = v;
+        brow = gr;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const T ov = __shfl_down_sync(0xffffffffu, best, o);
+      const int orr = __shfl_down_sync(0xffffffffu, brow, o);
+      if (ov > best || (ov == best && orr < brow)) {
+        best = ov;
+        brow = orr;
+      }
+    }
+    if (lane == 0) {
+      s_wv[warp] = best;
+      s_wr[warp] = brow;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      T b = s_wv[0];
+      int br = s_wr[0];
+      for (int w = 1; w < NW; ++w)
+        if (s_wv[w] > b || (s_wv[w] == b && s_wr[w] < br)) {
+          b = s_wv[w];
+          br = s_wr[w];
+        }
+      s_p = br;
+      s_pub.crow[buf] = br;
+      s_pub.cval[buf] = (br == INT_MAX) ? (T)-1 : b;
+    }
+    __syncthreads();
+    const int mybest = s_p;
+    if (mybest != INT_MAX)
+      for (int c = tid; c < jb; c += CPAN_T) s_crowv[buf * jb + c] = sp[(mybest - r0) * LD + c];
+    if (j >= r0 && j < r1)
+      for (int c = tid; c < jb; c += CPAN_T) s_srow[buf * jb + c] = sp[(j - r0) * LD + c];
+    cl.sync();
+    // global pivot: the maximum over the C published candidates (warp 0)
+    if (warp == 0) {
+      T bv = (T)-1;
+      int br = INT_MAX, bg = -1;
+      for (int q = lane; q < C; q += 32) {
+        const CPanelShared<T> *rp = cl.map_shared_rank(&s_pub, q);
+        const int rr = rp->crow[buf];
+        const T vv = rp->cval[buf];
+        if (rr != INT_MAX && (vv > bv || (vv == bv && rr < br))) {
+          bv = vv;
+          br = rr;
+          bg = q;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, bv, o);
+        const int orr = __shfl_down_sync(0xffffffffu, br, o);
+        const int og = __shfl_down_sync(0xffffffffu, bg, o);
+        if (ov > bv || (ov == bv && orr < br)) {
+          bv = ov;
+          br = orr;
+          bg = og;
+        }
+      }
+      if (lane == 0) {
+        s_wr[0] = br;
+        s_wg[0] = bg;
+      }
+    }
+    __syncthreads();
+    int p = s_wr[0], gw = s_wg[0];
+    if (gw < 0 || gw >= C || p < j || p >= a.m) {
+      // cannot happen while some CTA owns a row >= j; keep the indices in
+      // bounds and report instead of reading outside the published buffers
+      if (tid == 0) atomicExch(a.err, 2);
+      gw = g;
+      p = j;
+    }
+    const T *prow_src = cl.map_shared_rank(s_crowv, gw) + buf * jb;
+    for (int c = tid; c < jb; c += CPAN_T) s_prow[c] = prow_src[c];
+    if (p != j && p >= r0 && p < r1) {
+      // the diagonal row j moves to row p: fetch it from its owner
+      const T *srow_src = cl.map_shared_rank(s_srow, j / a.R) + buf * jb;
+      for (int c = tid; c < jb; c += CPAN_T) sp[(p - r0) * LD + c] = srow_src[c];
+    }
+    __syncthreads();
+    const T pv = s_prow[j];
+    if (g == 0 && tid == 0) {
+      a.ipiv[a.k + j] = a.k + p + 1;
+      if (pv == (T)0 && *a.info == 0) *a.info = a.k + j + 1;
+    }
+    if (p != j && j >= r0 && j < r1)
+      for (int c = tid; c < jb; c += CPAN_T) sp[(j - r0) * LD + c] = s_prow[c];
+    __syncthreads();
+    if (pv != (T)0) {
+      const T rinv = (T)1 / pv;
+      for (int r = warp; r < nr; r += NW) {
+        if (r0 + r <= j) continue;
+        const T l = sp[r * LD + j] * rinv;
+        for (int c = j + 1 + lane; c < jb; c += 32) sp[r * LD + c] -= l * s_prow[c];
+        __syncwarp();
+        if (lane == 0) sp[r * LD + j] = l;
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < nr * jb; idx += CPAN_T) {
+    const int c = idx / nr, r = idx % nr;
+    Ap[(size_t)(r0 + r) + (size_t)c * a.lda] = sp[r * LD + c];
+  }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Launches the cluster panel when the panel fits in the shared memory of a
+// cluster of 8 (or, where the device allows it, 16) CTAs; returns false to
+// fall back to the grid-wide version.  The kernel attributes and whether a
+// cluster of each size with the full shared memory can be resident are set
+// up once per element type.
+template <typename T>
+static bool panel_cluster_launch(cudaStream_t st, PanelArgs<T> pa, int *status) {
+  static int max_sm = -1;
+  static bool ok[2] = {false, false};
+  if (max_sm < 0) {
+    int dev = 0, opt = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&opt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    max_sm = opt - 2048;  // room for the static shared variables
+    bool attrs = cudaFuncSetAttribute(k_panel_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      max_sm) == cudaSuccess;
+    const bool np = attrs && cudaFuncSetAttribute(k_panel_cluster<T>,
+                                                  cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                                  1) == cudaSuccess;
+    for (int i = 0; i < 2 && attrs; ++i) {
+      const int C = i == 0 ? 8 : 16;
+      if (C > 8 && !np) break;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(C);
+      cfg.blockDim = dim3(CPAN_T);
+      cfg.dynamicSmemBytes = (size_t)max_sm;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = C;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      ok[i] = cudaOccupancyMaxActiveClusters(&ncl, k_panel_cluster<T>, &cfg) == cudaSuccess &&
+              ncl >= 1;
+    }
+    cudaGetLastError();
+  }
+  const int jb = pa.jb, m = pa.m;
+  const size_t fixed = (size_t)5 * jb * sizeof(T) + 1024;
+  for (int i = 0; i < 2; ++i) {
+    const int C = i == 0 ? 8 : 16;
+    const int R = (m + C - 1) / C;
+    const size_t sm = (size_t)R * (jb + 1) * sizeof(T) + fixed;
+    if (!ok[i] || sm > (size_t)max_sm) continue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(CPAN_T);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    pa.G = C;
+    pa.R = R;
+    *status = cudaLaunchKernelEx(&cfg, k_panel_cluster<T>, pa) == cudaSuccess ? DUST_OK
+                                                                               : DUST_ERR_CUDA;
+    return true;
+  }
+  return false;
+}
+
 template <typename T>
 __global__ void k_laswp(T *A, int lda, int c0, int c1, int k1, int k2, const int *ipiv) {
   int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,9 +544,18 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
       DUST_CUDA(cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sm));
     PanelArgs<T> pa{A, lda, k, jb, m, G, R, ipiv, info_dev, bar, err, cval, crow, crowv, srow};
-    void *args[] = {&pa};
-    DUST_CUDA(cudaMemsetAsync(bar, 0, 8, st));
-    DUST_CUDA(cudaLaunchCooperativeKernel((void *)k_panel<T>, dim3(G), dim3(PAN_T), args, sm, st));
+    int cst = DUST_OK;
+    if (panel_cluster_launch<T>(st, pa, &cst)) {
+      if (cst != DUST_OK) {
+        dust_set_last_error("cluster panel launch failed", __FILE__, __LINE__);
+        return cst;
+      }
+    } else {
+      void *args[] = {&pa};
+      DUST_CUDA(cudaMemsetAsync(bar, 0, 8, st));
+      DUST_CUDA(
+          cudaLaunchCooperativeKernel((void *)k_panel<T>, dim3(G), dim3(PAN_T), args, sm, st));
+    }
     lu_laswp<T>(st, A, lda, 0, k, k, k + jb, ipiv);
     lu_laswp<T>(st, A, lda, k + jb, n, k, k + jb, ipiv);
     if (k + jb < n) {

@@ -124,6 +124,28 @@ def test_dense_lu64_matches_numpy(n, nrhs):
     assert rel(X, np.linalg.solve(A, B)) < 1e-10
 
 
+@pytest.mark.parametrize("n", [300, 2500, 4000, 7000])
+def test_dense_lu64_pivoting(n):
+    """Random matrices without a dominant diagonal: every column pivots.
+    The panel runs on a cluster of 8 CTAs (n = 300, 2500), of 16 (4000) and
+    on the grid-wide kernel (7000 rows do not fit a cluster's shared memory)."""
+    rng = np.random.default_rng(n + 1)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, 2))
+    X, rep = linsys.dense_solve(A, B, abi.DUST_SOLVE_LU64)
+    assert rel(X, np.linalg.solve(A, B)) < 1e-9
+
+
+@pytest.mark.parametrize("n", [500, 1920])
+def test_dense_mixed_pivoting(n):
+    rng = np.random.default_rng(n + 2)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, 3))
+    X, rep = linsys.dense_solve(A, B, abi.DUST_SOLVE_MIXED, tol=1e-12)
+    assert rep["fell_back"] == 0 and rep["residual"] <= 1e-12
+    assert rel(X, np.linalg.solve(A, B)) < 1e-9
+
+
 def test_dense_mixed_refines_to_fp64():
     rng = np.random.default_rng(5)
     n = 700
