@@ -159,8 +159,13 @@ __global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FF
 #endif
 #define EF2_T 128
 #define EF2_NP (EF2_T * EF2_PPT)
-#define EF2_TILE 16
+#define EF2_TILE 16  // panels per FP32 partial sum and per near-queue check
+#ifndef EF2_SUB
+#define EF2_SUB 4  // sub-tiles staged per barrier pair
+#endif
+#define EF2_LOAD (EF2_TILE * EF2_SUB)
 #define EF2_QCAP (EF2_NP * EF2_TILE)  // one tile's worst case
+static_assert(EF2_LOAD % 32 == 0 && EF2_LOAD <= EF2_T && EF2_SUB <= 32, "staging layout");
 static_assert(EF2_NP <= 1024, "local particle index is packed in 10 bits");
 
 struct NearPair {
@@ -230,8 +235,9 @@ __device__ __forceinline__ void ef2_term2(float2 px, float2 py, float2 pz, float
 __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const FFRec *ff,
                                                     double *farv, unsigned long long *count,
                                                     NearPair *list, unsigned long long cap) {
-  __shared__ __align__(16) float s_pk[EF2_TILE / 2][EF2_PK];
-  __shared__ float s_ff[EF2_TILE];  // widened ff2
+  __shared__ __align__(16) float s_pk[EF2_LOAD / 2][EF2_PK];
+  __shared__ float s_ff[EF2_LOAD];  // widened ff2
+  __shared__ unsigned s_nearw[EF2_LOAD / 32];
   __shared__ uint32_t s_q[EF2_QCAP];  // (panel << 10) | local particle
   __shared__ float s_box[EF2_T / 32][6];
   __shared__ int s_qn;
@@ -276,20 +282,14 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
     for (int c = 0; c < 3; ++c)
       lo[c] = fminf(lo[c], s_box[w][c]), hi[c] = fmaxf(hi[c], s_box[w][3 + c]);
   const int ntot = e.nbody + e.nwake;
-  for (int p0 = 0; p0 < ntot; p0 += EF2_TILE) {
-    const int m = min(EF2_TILE, ntot - p0);
+  for (int p0 = 0; p0 < ntot; p0 += EF2_LOAD) {
     __syncthreads();
-    // a full tile can add up to EF2_NP * EF2_TILE entries
-    if (s_qn > EF2_QCAP - EF2_NP * EF2_TILE) {
-      ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
-      __syncthreads();
-      if (tid == 0) s_qn = 0;
-    }
+    // stage EF2_LOAD panels (EF2_SUB sub-tiles) with one barrier pair
     bool near_box = false;
-    if (tid < EF2_TILE) {
+    if (tid < EF2_LOAD) {
       float val[10] = {-1.0e6f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       float ffw = 0.f;
-      if (tid < m) {
+      if (p0 + tid < ntot) {
         const FFRec &r = ff[p0 + tid];
         const float cx = (float)(r.c[0] - ref[0]), cy = (float)(r.c[1] - ref[1]),
                     cz = (float)(r.c[2] - ref[2]);
@@ -309,55 +309,82 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
       for (int k = 0; k < 10; ++k) s_pk[tid >> 1][2 * k + (tid & 1)] = val[k];
       s_ff[tid] = ffw;
     }
-    const bool tile_near = __syncthreads_or(near_box);
-    double tv[EF2_PPT][3];
-    if (!tile_near) {
-      float2 acc[EF2_PPT][3];
+    // near flag of each sub-tile, one bit per sub-tile
+    const unsigned nb = __ballot_sync(0xffffffffu, near_box);
+    if ((tid & 31) == 0 && tid < EF2_LOAD) s_nearw[tid >> 5] = nb;
+    __syncthreads();
+    unsigned near_bits = 0;
 #pragma unroll
-      for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = make_float2(0.f, 0.f);
+    for (int w = 0; w < EF2_LOAD / 32; ++w) {
+      const unsigned bw = s_nearw[w];
 #pragma unroll
-      for (int pr = 0; pr < EF2_TILE / 2; ++pr) {
-        const float4 A = *(const float4 *)&s_pk[pr][0], B = *(const float4 *)&s_pk[pr][4],
-                     C = *(const float4 *)&s_pk[pr][8], D = *(const float4 *)&s_pk[pr][12],
-                     E = *(const float4 *)&s_pk[pr][16];
+      for (int sb = 0; sb < 32 / EF2_TILE; ++sb)
+        if ((bw >> (sb * EF2_TILE)) & ((1u << EF2_TILE) - 1u)) near_bits |= 1u << (w * (32 / EF2_TILE) + sb);
+    }
+    const int nsub = min(EF2_SUB, (ntot - p0 + EF2_TILE - 1) / EF2_TILE);
+    for (int sb = 0; sb < nsub; ++sb) {
+      const int q0 = p0 + sb * EF2_TILE;
+      double tv[EF2_PPT][3];
+      if (!((near_bits >> sb) & 1u)) {
+        float2 acc[EF2_PPT][3];
+#pragma unroll
+        for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int pr = 0; pr < EF2_TILE / 2; ++pr) {
+          const float *pk = s_pk[sb * (EF2_TILE / 2) + pr];
+          const float4 A = *(const float4 *)&pk[0], B = *(const float4 *)&pk[4],
+                       C = *(const float4 *)&pk[8], D = *(const float4 *)&pk[12],
+                       E = *(const float4 *)&pk[16];
+#pragma unroll
+          for (int i = 0; i < EF2_PPT; ++i)
+            ef2_term2(make_float2(px[i], px[i]), make_float2(py[i], py[i]),
+                      make_float2(pz[i], pz[i]), make_float2(A.x, A.y), make_float2(A.z, A.w),
+                      make_float2(B.x, B.y), make_float2(B.z, B.w), make_float2(C.x, C.y),
+                      make_float2(C.z, C.w), make_float2(D.x, D.y), make_float2(D.z, D.w),
+                      make_float2(E.x, E.y), make_float2(E.z, E.w), acc[i]);
+        }
 #pragma unroll
         for (int i = 0; i < EF2_PPT; ++i)
-          ef2_term2(make_float2(px[i], px[i]), make_float2(py[i], py[i]),
-                    make_float2(pz[i], pz[i]), make_float2(A.x, A.y), make_float2(A.z, A.w),
-                    make_float2(B.x, B.y), make_float2(B.z, B.w), make_float2(C.x, C.y),
-                    make_float2(C.z, C.w), make_float2(D.x, D.y), make_float2(D.z, D.w),
-                    make_float2(E.x, E.y), make_float2(E.z, E.w), acc[i]);
-      }
+          for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c].x + (double)acc[i][c].y;
+      } else {
+        // the queue must hold one sub-tile's worst case: flush first if not
+        // (the near bits are the same in every thread, so are these barriers)
+        __syncthreads();
+        if (s_qn > EF2_QCAP - EF2_NP * EF2_TILE) {
+          ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
+          __syncthreads();
+          if (tid == 0) s_qn = 0;
+          __syncthreads();
+        }
+        float acc[EF2_PPT][3];
 #pragma unroll
-      for (int i = 0; i < EF2_PPT; ++i)
-        for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c].x + (double)acc[i][c].y;
-    } else {
-      float acc[EF2_PPT][3];
-#pragma unroll
-      for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
+        for (int i = 0; i < EF2_PPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
 #pragma unroll 2
-      for (int q = 0; q < EF2_TILE; ++q) {
-        const float *pk = &s_pk[q >> 1][q & 1];
-        const float ffw = s_ff[q];
+        for (int q = 0; q < EF2_TILE; ++q) {
+          const int ql = sb * EF2_TILE + q;
+          const float *pk = &s_pk[ql >> 1][ql & 1];
+          const float ffw = s_ff[ql];
 #pragma unroll
-        for (int i = 0; i < EF2_PPT; ++i) {
-          const float rx = px[i] + pk[0], ry = py[i] + pk[2], rz = pz[i] + pk[4];
-          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-          if (r2 > ffw) {
-            ef2_term(rx, ry, rz, r2, pk[6], pk[8], pk[10], pk[12], pk[14], pk[16], pk[18], acc[i]);
-          } else if (act[i]) {
-            const int slot = atomicAdd(&s_qn, 1);
-            s_q[slot] = ((uint32_t)(p0 + q) << 10) | (uint32_t)(tid + i * EF2_T);
+          for (int i = 0; i < EF2_PPT; ++i) {
+            const float rx = px[i] + pk[0], ry = py[i] + pk[2], rz = pz[i] + pk[4];
+            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            if (r2 > ffw) {
+              ef2_term(rx, ry, rz, r2, pk[6], pk[8], pk[10], pk[12], pk[14], pk[16], pk[18],
+                       acc[i]);
+            } else if (act[i]) {
+              const int slot = atomicAdd(&s_qn, 1);
+              s_q[slot] = ((uint32_t)(q0 + q) << 10) | (uint32_t)(tid + i * EF2_T);
+            }
           }
         }
+#pragma unroll
+        for (int i = 0; i < EF2_PPT; ++i)
+          for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c];
       }
 #pragma unroll
       for (int i = 0; i < EF2_PPT; ++i)
-        for (int c = 0; c < 3; ++c) tv[i][c] = (double)acc[i][c];
+        for (int c = 0; c < 3; ++c) v[i][c] += tv[i][c];
     }
-#pragma unroll
-    for (int i = 0; i < EF2_PPT; ++i)
-      for (int c = 0; c < 3; ++c) v[i][c] += tv[i][c];
   }
   __syncthreads();
   ef2_flush(s_q, s_qn, t0, count, list, cap, &s_base);
@@ -370,7 +397,10 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
 }
 
 // the queued near pairs, exact FP64 (one pair per thread)
-__global__ void k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count,
+#ifndef EN_MINB
+#define EN_MINB 6
+#endif
+__global__ void __launch_bounds__(128, EN_MINB) k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count,
                             const NearPair *list, unsigned long long cap, double *farv) {
   const unsigned long long nq = min(*count, cap);
   const size_t n = d.n;

@@ -259,10 +259,8 @@ __global__ void __launch_bounds__(CPAN_T) k_panel_cluster(PanelArgs<T> a) {
   const int NW = CPAN_T / 32;
   const int r0 = g * a.R, r1 = min(a.m, r0 + a.R), nr = max(0, r1 - r0);
   T *Ap = a.A + (size_t)a.k + (size_t)a.k * a.lda;
-  for (int idx = tid; idx < nr * jb; idx += CPAN_T) {
-    const int c = idx / nr, r = idx % nr;
-    sp[r * LD + c] = Ap[(size_t)(r0 + r) + (size_t)c * a.lda];
-  }
+  for (int c = 0; c < jb; ++c)
+    for (int r = tid; r < nr; r += CPAN_T) sp[r * LD + c] = Ap[(size_t)(r0 + r) + (size_t)c * a.lda];
   __syncthreads();
   for (int j = 0; j < jb; ++j) {
     const int buf = j & 1;
@@ -366,21 +364,21 @@ __global__ void __launch_bounds__(CPAN_T) k_panel_cluster(PanelArgs<T> a) {
       for (int c = tid; c < jb; c += CPAN_T) sp[(j - r0) * LD + c] = s_prow[c];
     __syncthreads();
     if (pv != (T)0) {
+      // one thread per row (LD = jb + 1 words apart: no bank conflicts)
       const T rinv = (T)1 / pv;
-      for (int r = warp; r < nr; r += NW) {
+      for (int r = tid; r < nr; r += CPAN_T) {
         if (r0 + r <= j) continue;
-        const T l = sp[r * LD + j] * rinv;
-        for (int c = j + 1 + lane; c < jb; c += 32) sp[r * LD + c] -= l * s_prow[c];
-        __syncwarp();
-        if (lane == 0) sp[r * LD + j] = l;
+        T *row = sp + (size_t)r * LD;
+        const T l = row[j] * rinv;
+        row[j] = l;
+#pragma unroll 4
+        for (int c = j + 1; c < jb; ++c) row[c] -= l * s_prow[c];
       }
     }
     __syncthreads();
   }
-  for (int idx = tid; idx < nr * jb; idx += CPAN_T) {
-    const int c = idx / nr, r = idx % nr;
-    Ap[(size_t)(r0 + r) + (size_t)c * a.lda] = sp[r * LD + c];
-  }
+  for (int c = 0; c < jb; ++c)
+    for (int r = tid; r < nr; r += CPAN_T) Ap[(size_t)(r0 + r) + (size_t)c * a.lda] = sp[r * LD + c];
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
