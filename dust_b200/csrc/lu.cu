@@ -382,6 +382,258 @@ __global__ void __launch_bounds__(CPAN_T) k_panel_cluster(PanelArgs<T> a) {
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
+// Single-CTA panel factorisation for panels of moderate height.  The CTA
+// factors the panel in sub-panels of W columns; thread t keeps rows t,
+// t + NT, ... (RPT of them) of the sub-panel in registers, so the rank-1
+// updates of a column touch no memory and a pivot search needs only CTA
+// barriers; the pivot row is exchanged through shared memory.  After a
+// sub-panel: its row interchanges are applied to the panel's other columns
+// (as one net permutation of the touched rows), U12 right of it is solved
+// with its unit lower triangle, and the panel's remaining columns get the
+// rank-W update from the rows still in registers.  Pivot choice, ipiv and
+// info are those of the column-by-column algorithm (first maximum wins).
+#define P1_T 512
+#define P1_NW (P1_T / 32)
+#define P1_JB 64  // widest panel
+
+template <typename T, int W, int RPT>
+__global__ void __launch_bounds__(P1_T) k_panel_1cta(PanelArgs<T> a) {
+  constexpr int VEC = 16 / (int)sizeof(T);  // U12 columns per vector load
+  const int m = a.m, jb = a.jb, lda = a.lda;
+  __shared__ __align__(16) T s_u[W * P1_JB];  // U12 of the current sub-panel
+  __shared__ T s_l11[W][W + 1];
+  __shared__ __align__(16) T s_prow[W], s_jrow[W];
+  __shared__ T s_wv[P1_NW];
+  __shared__ int s_wr[P1_NW];
+  __shared__ int s_piv[W], s_pos[2 * W], s_src[2 * W];
+  __shared__ int s_np;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  T *Ap = a.A + (size_t)a.k + (size_t)a.k * lda;
+  T x[RPT][W];
+  for (int s0 = 0; s0 < jb; s0 += W) {
+    const int w = min(W, jb - s0);
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int r = tid + k * P1_T;
+#pragma unroll
+      for (int c = 0; c < W; ++c)
+        x[k][c] = (r < m && c < w) ? Ap[r + (size_t)(s0 + c) * lda] : (T)0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < W; ++jj) {
+      if (jj >= w) break;
+      const int j = s0 + jj;
+      // maximum of |a(r, j)| over rows r >= j (first index on ties)
+      T best = (T)-1;
+      int brow = INT_MAX;
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * P1_T;
+        if (r >= j && r < m) {
+          T v = fabs(x[k][jj]);
+          if (v != v) v = (T)-0.5;  // NaN: still a candidate, below every number
+          if (v > best || (v == best && r < brow)) {
+            best = v;
+            brow = r;
+          }
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, best, o);
+        const int orr = __shfl_down_sync(0xffffffffu, brow, o);
+        if (ov > best || (ov == best && orr < brow)) {
+          best = ov;
+          brow = orr;
+        }
+      }
+      if (lane == 0) {
+        s_wv[warp] = best;
+        s_wr[warp] = brow;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        best = lane < P1_NW ? s_wv[lane] : (T)-1;
+        brow = lane < P1_NW ? s_wr[lane] : INT_MAX;
+        for (int o = 16; o > 0; o >>= 1) {
+          const T ov = __shfl_down_sync(0xffffffffu, best, o);
+          const int orr = __shfl_down_sync(0xffffffffu, brow, o);
+          if (ov > best || (ov == best && orr < brow)) {
+            best = ov;
+            brow = orr;
+          }
+        }
+        if (lane == 0) s_piv[jj] = (brow == INT_MAX) ? j : brow;
+      }
+      __syncthreads();
+      const int p = s_piv[jj];
+      // exchange rows j and p through shared memory
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * P1_T;
+        if (r == p)
+#pragma unroll
+          for (int c = 0; c < W; ++c) s_prow[c] = x[k][c];
+        if (r == j)
+#pragma unroll
+          for (int c = 0; c < W; ++c) s_jrow[c] = x[k][c];
+      }
+      __syncthreads();
+      T prow[W];
+#pragma unroll
+      for (int c = 0; c < W; ++c) prow[c] = s_prow[c];
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * P1_T;
+        if (r == j)
+#pragma unroll
+          for (int c = 0; c < W; ++c) x[k][c] = prow[c];
+        else if (r == p)
+#pragma unroll
+          for (int c = 0; c < W; ++c) x[k][c] = s_jrow[c];
+      }
+      const T pv = prow[jj];
+      if (tid == 0) {
+        a.ipiv[a.k + j] = a.k + p + 1;
+        if (pv == (T)0 && *a.info == 0) *a.info = a.k + j + 1;
+      }
+      if (pv != (T)0) {
+        const T rinv = (T)1 / pv;
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          const int r = tid + k * P1_T;
+          if (r > j && r < m) {
+            const T l = x[k][jj] * rinv;
+            x[k][jj] = l;
+#pragma unroll
+            for (int c = jj + 1; c < W; ++c) x[k][c] -= l * prow[c];
+          }
+        }
+      }
+      __syncthreads();  // s_prow / s_jrow are rewritten by the next column
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int r = tid + k * P1_T;
+      if (r < m) {
+#pragma unroll
+        for (int c = 0; c < W; ++c)
+          if (c < w) Ap[r + (size_t)(s0 + c) * lda] = x[k][c];
+        if (r >= s0 && r < s0 + w)
+#pragma unroll
+          for (int c = 0; c < W; ++c) s_l11[r - s0][c] = x[k][c];
+      }
+    }
+    // net permutation of the rows the sub-panel's interchanges touched:
+    // position s_pos[q] receives the content of row s_src[q]
+    if (tid == 0) {
+      int np = 0;
+      for (int jj = 0; jj < w; ++jj) {
+        const int j = s0 + jj, p = s_piv[jj];
+        if (p == j) continue;
+        int ij = -1, ip = -1;
+        for (int q = 0; q < np; ++q) {
+          if (s_pos[q] == j) ij = q;
+          if (s_pos[q] == p) ip = q;
+        }
+        if (ij < 0) {
+          s_pos[np] = j;
+          s_src[np] = j;
+          ij = np++;
+        }
+        if (ip < 0) {
+          s_pos[np] = p;
+          s_src[np] = p;
+          ip = np++;
+        }
+        const int t = s_src[ij];
+        s_src[ij] = s_src[ip];
+        s_src[ip] = t;
+      }
+      s_np = np;
+    }
+    __syncthreads();
+    {
+      // the other columns of the panel: at most 2W rows x (P1_JB - 1) columns
+      const int np = s_np, nco = jb - w;
+      T vals[(2 * W * (P1_JB - 1) + P1_T - 1) / P1_T];
+      int cnt = 0;
+      for (int e = tid; e < np * nco; e += P1_T) {
+        const int q = e % np, ci = e / np, c = ci < s0 ? ci : ci + w;
+        vals[cnt++] = Ap[s_src[q] + (size_t)c * lda];
+      }
+      __syncthreads();
+      cnt = 0;
+      for (int e = tid; e < np * nco; e += P1_T) {
+        const int q = e % np, ci = e / np, c = ci < s0 ? ci : ci + w;
+        Ap[s_pos[q] + (size_t)c * lda] = vals[cnt++];
+      }
+    }
+    __syncthreads();
+    const int c1 = s0 + w, nc = jb - c1;
+    if (nc > 0) {
+      // U12 = L11^-1 A12: one lane per column, the column in registers
+      if (tid < nc) {
+        T u[W];
+        const size_t cb = (size_t)(c1 + tid) * lda;
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          if (i < w) {
+            T sacc = Ap[s0 + i + cb];
+#pragma unroll
+            for (int q = 0; q < i; ++q) sacc -= s_l11[i][q] * u[q];
+            u[i] = sacc;
+            s_u[i * P1_JB + tid] = sacc;
+            Ap[s0 + i + cb] = sacc;
+          }
+        }
+      }
+      __syncthreads();
+      // A22 -= L21 U12 for the rows below the sub-panel, from the registers
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = tid + k * P1_T;
+        if (r < c1 || r >= m) continue;
+        for (int c = 0; c < nc; c += VEC) {
+          T v[VEC];
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) v[e] = c + e < nc ? Ap[r + (size_t)(c1 + c + e) * lda] : (T)0;
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            T uu[VEC];
+            *(float4 *)uu = *(const float4 *)&s_u[q * P1_JB + c];
+            const T lq = q < w ? x[k][q] : (T)0;
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) v[e] -= lq * uu[e];
+          }
+#pragma unroll
+          for (int e = 0; e < VEC; ++e)
+            if (c + e < nc) Ap[r + (size_t)(c1 + c + e) * lda] = v[e];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int W, int RPT>
+static bool panel_1cta_try(cudaStream_t st, const PanelArgs<T> &pa, int *status) {
+  if (pa.jb > P1_JB || pa.m > RPT * P1_T) return false;
+  k_panel_1cta<T, W, RPT><<<1, P1_T, 0, st>>>(pa);
+  *status = cudaGetLastError() == cudaSuccess ? DUST_OK : DUST_ERR_CUDA;
+  return true;
+}
+
+// rows per thread from the panel height: up to 2 rows per thread with
+// sub-panels of 16 (FP32) or 8 (FP64) columns; FP32 up to 4 with 8 columns
+// (taller FP64 panels go to the cluster kernel)
+template <typename T>
+static bool panel_1cta_launch(cudaStream_t st, const PanelArgs<T> &pa, int *status) {
+  if constexpr (sizeof(T) == 4)
+    return panel_1cta_try<T, 16, 2>(st, pa, status) || panel_1cta_try<T, 8, 4>(st, pa, status);
+  else
+    return panel_1cta_try<T, 8, 2>(st, pa, status);
+}
+
 // Launches the cluster panel when the panel fits in the shared memory of a
 // cluster of 8 (or, where the device allows it, 16) CTAs; returns false to
 // fall back to the grid-wide version.  The kernel attributes and whether a
@@ -543,9 +795,9 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
                                      (int)sm));
     PanelArgs<T> pa{A, lda, k, jb, m, G, R, ipiv, info_dev, bar, err, cval, crow, crowv, srow};
     int cst = DUST_OK;
-    if (panel_cluster_launch<T>(st, pa, &cst)) {
+    if (panel_1cta_launch<T>(st, pa, &cst) || panel_cluster_launch<T>(st, pa, &cst)) {
       if (cst != DUST_OK) {
-        dust_set_last_error("cluster panel launch failed", __FILE__, __LINE__);
+        dust_set_last_error("panel launch failed", __FILE__, __LINE__);
         return cst;
       }
     } else {
