@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(EF2_T) k_elem_far(FmmDev d, ElemDev e, const F
 
 // the queued near pairs, exact FP64 (one pair per thread)
 #ifndef EN_MINB
-#define EN_MINB 6
+#define EN_MINB 8
 #endif
 __global__ void __launch_bounds__(128, EN_MINB) k_elem_near(FmmDev d, ElemDev e, const unsigned long long *count,
                             const NearPair *list, unsigned long long cap, double *farv) {

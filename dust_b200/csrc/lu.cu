@@ -716,6 +716,63 @@ __global__ void k_laswp(T *A, int lda, int c0, int c1, int k1, int k2, const int
   }
 }
 
+// Row interchanges of one panel (pivots ipiv[k .. k+jb)) on the columns
+// outside it, [0, k) and [k + jb, n): the jb transpositions, applied in
+// order, permute at most 2 jb rows; every CTA derives that net permutation
+// (position <- source row) in shared memory and moves the touched rows of
+// its LW_C columns, reading them all before writing any.
+#define LW_C 32
+#define LW_T 256
+template <typename T>
+__global__ void __launch_bounds__(LW_T) k_laswp_net(T *A, int lda, int n, int k, int jb,
+                                                    const int *ipiv) {
+  extern __shared__ int s_map[];  // [n - k]: slot of a touched row, or -1
+  __shared__ int s_pos[2 * P1_JB], s_src[2 * P1_JB];
+  __shared__ int s_np;
+  const int m = n - k, tid = threadIdx.x;
+  for (int r = tid; r < m; r += LW_T) s_map[r] = -1;
+  __syncthreads();
+  if (tid == 0) {
+    int np = 0;
+    for (int jj = 0; jj < jb; ++jj) {
+      const int p = ipiv[k + jj] - 1 - k;
+      if (p == jj || p < 0 || p >= m) continue;
+      int ij = s_map[jj], ip = s_map[p];
+      if (ij < 0) {
+        s_pos[np] = jj;
+        s_src[np] = jj;
+        s_map[jj] = ij = np++;
+      }
+      if (ip < 0) {
+        s_pos[np] = p;
+        s_src[np] = p;
+        s_map[p] = ip = np++;
+      }
+      const int t = s_src[ij];
+      s_src[ij] = s_src[ip];
+      s_src[ip] = t;
+    }
+    s_np = np;
+  }
+  __syncthreads();
+  const int np = s_np, ncol = n - jb;
+  const int c0 = blockIdx.x * LW_C, cn = min(LW_C, ncol - c0);
+  if (cn <= 0 || np == 0) return;
+  constexpr int PER = (2 * P1_JB * LW_C + LW_T - 1) / LW_T;
+  T v[PER];
+  int cnt = 0;
+  for (int e = tid; e < np * cn; e += LW_T) {
+    const int q = e % np, ci = c0 + e / np, c = ci < k ? ci : ci + jb;
+    v[cnt++] = A[(size_t)k + s_src[q] + (size_t)c * lda];
+  }
+  __syncthreads();
+  cnt = 0;
+  for (int e = tid; e < np * cn; e += LW_T) {
+    const int q = e % np, ci = c0 + e / np, c = ci < k ? ci : ci + jb;
+    A[(size_t)k + s_pos[q] + (size_t)c * lda] = v[cnt++];
+  }
+}
+
 template <typename T>
 void lu_laswp(cudaStream_t st, T *A, int lda, int c0, int c1, int k1, int k2,
               const int *ipiv) {
@@ -806,8 +863,21 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
       DUST_CUDA(
           cudaLaunchCooperativeKernel((void *)k_panel<T>, dim3(G), dim3(PAN_T), args, sm, st));
     }
-    lu_laswp<T>(st, A, lda, 0, k, k, k + jb, ipiv);
-    lu_laswp<T>(st, A, lda, k + jb, n, k, k + jb, ipiv);
+    if (n > jb) {
+      const size_t msm = (size_t)(n - k) * sizeof(int);
+      static size_t opened = 48 * 1024;  // per element type
+      if (msm > 200 * 1024) {
+        lu_laswp<T>(st, A, lda, 0, k, k, k + jb, ipiv);
+        lu_laswp<T>(st, A, lda, k + jb, n, k, k + jb, ipiv);
+      } else {
+        if (msm > opened) {
+          DUST_CUDA(cudaFuncSetAttribute(k_laswp_net<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+          opened = 200 * 1024;
+        }
+        k_laswp_net<T><<<(n - jb + LW_C - 1) / LW_C, LW_T, msm, st>>>(A, lda, n, k, jb, ipiv);
+      }
+    }
     if (k + jb < n) {
       CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_UNIT, jb,
                       n - k - jb, A + k + (size_t)k * lda, lda, A + k + (size_t)(k + jb) * lda,
