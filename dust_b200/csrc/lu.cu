@@ -386,7 +386,8 @@ __global__ void __launch_bounds__(CPAN_T) k_panel_cluster(PanelArgs<T> a) {
 // factors the panel in sub-panels of W columns; thread t keeps rows t,
 // t + NT, ... (RPT of them) of the sub-panel in registers, so the rank-1
 // updates of a column touch no memory and a pivot search needs only CTA
-// barriers; the pivot row is exchanged through shared memory.  After a
+// barriers (two per column); the pivot row is exchanged through shared
+// memory.  After a
 // sub-panel: its row interchanges are applied to the panel's other columns
 // (as one net permutation of the touched rows), U12 right of it is solved
 // with its unit lower triangle, and the panel's remaining columns get the
@@ -402,14 +403,17 @@ __global__ void __launch_bounds__(P1_T) k_panel_1cta(PanelArgs<T> a) {
   const int m = a.m, jb = a.jb, lda = a.lda;
   __shared__ __align__(16) T s_u[W * P1_JB];  // U12 of the current sub-panel
   __shared__ T s_l11[W][W + 1];
-  __shared__ __align__(16) T s_prow[W], s_jrow[W];
-  __shared__ T s_wv[P1_NW];
-  __shared__ int s_wr[P1_NW];
+  // per column, alternating between two copies (a column's readers finish
+  // before any thread passes the next column's second barrier)
+  __shared__ __align__(16) T s_prow[2][W], s_jrow[2][W];
+  __shared__ T s_wv[2][P1_NW];
+  __shared__ int s_wr[2][P1_NW];
   __shared__ int s_piv[W], s_pos[2 * W], s_src[2 * W];
   __shared__ int s_np;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   T *Ap = a.A + (size_t)a.k + (size_t)a.k * lda;
   T x[RPT][W];
+  int par = 0;
   for (int s0 = 0; s0 < jb; s0 += W) {
     const int w = min(W, jb - s0);
 #pragma unroll
@@ -439,48 +443,44 @@ __global__ void __launch_bounds__(P1_T) k_panel_1cta(PanelArgs<T> a) {
         }
       }
       for (int o = 16; o > 0; o >>= 1) {
-        const T ov = __shfl_down_sync(0xffffffffu, best, o);
-        const int orr = __shfl_down_sync(0xffffffffu, brow, o);
+        const T ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int orr = __shfl_xor_sync(0xffffffffu, brow, o);
         if (ov > best || (ov == best && orr < brow)) {
           best = ov;
           brow = orr;
         }
       }
       if (lane == 0) {
-        s_wv[warp] = best;
-        s_wr[warp] = brow;
+        s_wv[par][warp] = best;
+        s_wr[par][warp] = brow;
       }
       __syncthreads();
-      if (warp == 0) {
-        best = lane < P1_NW ? s_wv[lane] : (T)-1;
-        brow = lane < P1_NW ? s_wr[lane] : INT_MAX;
-        for (int o = 16; o > 0; o >>= 1) {
-          const T ov = __shfl_down_sync(0xffffffffu, best, o);
-          const int orr = __shfl_down_sync(0xffffffffu, brow, o);
-          if (ov > best || (ov == best && orr < brow)) {
-            best = ov;
-            brow = orr;
-          }
+      // every warp reduces the warps' candidates itself
+      best = lane < P1_NW ? s_wv[par][lane] : (T)-1;
+      brow = lane < P1_NW ? s_wr[par][lane] : INT_MAX;
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int orr = __shfl_xor_sync(0xffffffffu, brow, o);
+        if (ov > best || (ov == best && orr < brow)) {
+          best = ov;
+          brow = orr;
         }
-        if (lane == 0) s_piv[jj] = (brow == INT_MAX) ? j : brow;
       }
-      __syncthreads();
-      const int p = s_piv[jj];
-      // exchange rows j and p through shared memory
+      const int p = (brow == INT_MAX) ? j : brow;
+      // rows j and p through shared memory
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
         const int r = tid + k * P1_T;
         if (r == p)
 #pragma unroll
-          for (int c = 0; c < W; ++c) s_prow[c] = x[k][c];
+          for (int c = 0; c < W; ++c) s_prow[par][c] = x[k][c];
         if (r == j)
 #pragma unroll
-          for (int c = 0; c < W; ++c) s_jrow[c] = x[k][c];
+          for (int c = 0; c < W; ++c) s_jrow[par][c] = x[k][c];
       }
+      if (tid == 0) s_piv[jj] = p;
       __syncthreads();
-      T prow[W];
-#pragma unroll
-      for (int c = 0; c < W; ++c) prow[c] = s_prow[c];
+      const T *prow = s_prow[par];
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
         const int r = tid + k * P1_T;
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(P1_T) k_panel_1cta(PanelArgs<T> a) {
           for (int c = 0; c < W; ++c) x[k][c] = prow[c];
         else if (r == p)
 #pragma unroll
-          for (int c = 0; c < W; ++c) x[k][c] = s_jrow[c];
+          for (int c = 0; c < W; ++c) x[k][c] = s_jrow[par][c];
       }
       const T pv = prow[jj];
       if (tid == 0) {
@@ -509,8 +509,9 @@ __global__ void __launch_bounds__(P1_T) k_panel_1cta(PanelArgs<T> a) {
           }
         }
       }
-      __syncthreads();  // s_prow / s_jrow are rewritten by the next column
+      par ^= 1;
     }
+    __syncthreads();
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
       const int r = tid + k * P1_T;
@@ -623,15 +624,15 @@ static bool panel_1cta_try(cudaStream_t st, const PanelArgs<T> &pa, int *status)
   return true;
 }
 
-// rows per thread from the panel height: up to 2 rows per thread with
-// sub-panels of 16 (FP32) or 8 (FP64) columns; FP32 up to 4 with 8 columns
-// (taller FP64 panels go to the cluster kernel)
+// rows per thread from the panel height (up to 4, so panels of up to 2048
+// rows), sub-panels of 16 (FP32) or 8 (FP64) columns; taller panels go to
+// the cluster kernel
 template <typename T>
 static bool panel_1cta_launch(cudaStream_t st, const PanelArgs<T> &pa, int *status) {
   if constexpr (sizeof(T) == 4)
-    return panel_1cta_try<T, 16, 2>(st, pa, status) || panel_1cta_try<T, 8, 4>(st, pa, status);
+    return panel_1cta_try<T, 16, 2>(st, pa, status) || panel_1cta_try<T, 16, 4>(st, pa, status);
   else
-    return panel_1cta_try<T, 8, 2>(st, pa, status);
+    return panel_1cta_try<T, 8, 2>(st, pa, status) || panel_1cta_try<T, 8, 4>(st, pa, status);
 }
 
 // Launches the cluster panel when the panel fits in the shared memory of a

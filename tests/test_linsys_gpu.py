@@ -127,8 +127,8 @@ def test_dense_lu64_matches_numpy(n, nrhs):
 @pytest.mark.parametrize("n", [300, 2500, 4000, 7000])
 def test_dense_lu64_pivoting(n):
     """Random matrices without a dominant diagonal: every column pivots.
-    FP64 panels of up to 1024 rows run on one CTA (n = 300 and the last
-    panels of the others), taller ones on a cluster of 8 CTAs (2500) or 16
+    Panels of up to 2048 rows run on one CTA (n = 300 and the last panels
+    of the others), taller FP64 ones on a cluster of 8 CTAs (2500) or 16
     (4000), and on the grid-wide kernel when they do not fit a cluster's
     shared memory (7000)."""
     rng = np.random.default_rng(n + 1)
