@@ -721,12 +721,13 @@ __global__ void k_laswp(T *A, int lda, int c0, int c1, int k1, int k2, const int
 // outside it, [0, k) and [k + jb, n): the jb transpositions, applied in
 // order, permute at most 2 jb rows; every CTA derives that net permutation
 // (position <- source row) in shared memory and moves the touched rows of
-// its LW_C columns, reading them all before writing any.
+// its LW_C columns, reading them all before writing any.  CTA 0 also
+// applies it to `perm` (when given), the factorisation's row permutation.
 #define LW_C 32
 #define LW_T 256
 template <typename T>
 __global__ void __launch_bounds__(LW_T) k_laswp_net(T *A, int lda, int n, int k, int jb,
-                                                    const int *ipiv) {
+                                                    const int *ipiv, int *perm) {
   extern __shared__ int s_map[];  // [n - k]: slot of a touched row, or -1
   __shared__ int s_pos[2 * P1_JB], s_src[2 * P1_JB];
   __shared__ int s_np;
@@ -757,6 +758,12 @@ __global__ void __launch_bounds__(LW_T) k_laswp_net(T *A, int lda, int n, int k,
   }
   __syncthreads();
   const int np = s_np, ncol = n - jb;
+  if (perm && blockIdx.x == 0) {
+    // the running row permutation of the factorisation (for lu_getrs)
+    const int pv = tid < np ? perm[k + s_src[tid]] : 0;
+    __syncthreads();
+    if (tid < np) perm[k + s_pos[tid]] = pv;
+  }
   const int c0 = blockIdx.x * LW_C, cn = min(LW_C, ncol - c0);
   if (cn <= 0 || np == 0) return;
   constexpr int PER = (2 * P1_JB * LW_C + LW_T - 1) / LW_T;
@@ -805,6 +812,23 @@ static cublasStatus_t gemm_minus_(cublasHandle_t h, int m, int n, int k, const f
   return cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &mone, A, lda, B, ldb, &one, C, ldc);
 }
 
+__global__ void k_iota(int n, int *v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+// B(:, c) = B(perm, c) for each column: one CTA per column through shared
+// memory
+template <typename T>
+__global__ void k_permute_rows(T *B, int ldb, int n, const int *perm) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T *s = (T *)smraw;
+  T *col = B + (size_t)blockIdx.x * ldb;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = col[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) col[i] = s[perm[i]];
+}
+
 // tcgen05 TF32 trailing update (gemm_tc.cu); C -= A B, FP32 column-major.
 int gemm_tf32_minus(cudaStream_t st, int m, int n, int k, const float *A, int lda,
                     const float *B, int ldb, float *C, int ldc);
@@ -819,8 +843,12 @@ int gemm_tf32_minus(cudaStream_t st, int m, int n, int k, const float *A, int ld
 
 template <typename T>
 int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
-             int *ipiv, int *info_dev, int gemm_update) {
+             int *ipiv, int *info_dev, int gemm_update, int *perm) {
   if (n <= 0) return DUST_OK;
+  if (perm) {
+    if ((size_t)n * sizeof(int) > 200 * 1024) return DUST_ERR_BAD_ARG;
+    k_iota<<<(n + 255) / 256, 256, 0, st>>>(n, perm);
+  }
   const int nb = 64;
   if (w.nsm == 0) {
     int dev = 0;
@@ -864,7 +892,7 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
       DUST_CUDA(
           cudaLaunchCooperativeKernel((void *)k_panel<T>, dim3(G), dim3(PAN_T), args, sm, st));
     }
-    if (n > jb) {
+    if (n > jb || perm) {
       const size_t msm = (size_t)(n - k) * sizeof(int);
       static size_t opened = 48 * 1024;  // per element type
       if (msm > 200 * 1024) {
@@ -876,7 +904,8 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
           opened = 200 * 1024;
         }
-        k_laswp_net<T><<<(n - jb + LW_C - 1) / LW_C, LW_T, msm, st>>>(A, lda, n, k, jb, ipiv);
+        k_laswp_net<T><<<std::max(1, (n - jb + LW_C - 1) / LW_C), LW_T, msm, st>>>(A, lda, n, k,
+                                                                                  jb, ipiv, perm);
       }
     }
     if (k + jb < n) {
@@ -906,10 +935,21 @@ int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda
 
 template <typename T>
 int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, int lda,
-             const int *ipiv, T *B, int ldb) {
+             const int *ipiv, T *B, int ldb, const int *perm) {
   if (n <= 0 || nrhs <= 0) return DUST_OK;
   CUBLAS_OK(cublasSetStream(cb, st));
-  lu_laswp<T>(st, B, ldb, 0, nrhs, 0, n, ipiv);
+  const size_t psm = (size_t)n * sizeof(T);
+  if (perm && psm <= 200 * 1024) {
+    static size_t opened = 48 * 1024;  // per element type
+    if (psm > opened) {
+      DUST_CUDA(cudaFuncSetAttribute(k_permute_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+      opened = 200 * 1024;
+    }
+    k_permute_rows<T><<<nrhs, 512, psm, st>>>(B, ldb, n, perm);
+  } else {
+    lu_laswp<T>(st, B, ldb, 0, nrhs, 0, n, ipiv);
+  }
   CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_UNIT, n, nrhs, A,
                   lda, B, ldb));
   CUBLAS_OK(trsm_(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, n, nrhs,
@@ -919,12 +959,12 @@ int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, in
 }
 
 template int lu_getrf<double>(cublasHandle_t, cudaStream_t, LuWork &, int, double *, int, int *,
-                              int *, int);
+                              int *, int, int *);
 template int lu_getrf<float>(cublasHandle_t, cudaStream_t, LuWork &, int, float *, int, int *,
-                             int *, int);
+                             int *, int, int *);
 template void lu_laswp<double>(cudaStream_t, double *, int, int, int, int, int, const int *);
 template void lu_laswp<float>(cudaStream_t, float *, int, int, int, int, int, const int *);
 template int lu_getrs<double>(cublasHandle_t, cudaStream_t, int, int, const double *, int,
-                              const int *, double *, int);
+                              const int *, double *, int, const int *);
 template int lu_getrs<float>(cublasHandle_t, cudaStream_t, int, int, const float *, int,
-                             const int *, float *, int);
+                             const int *, float *, int, const int *);

@@ -21,10 +21,12 @@ struct LuWork {
 // relative to A's first row) as LAPACK.  *info_dev receives the first zero
 // pivot (1-based) or stays 0; the returned status reports launch errors and
 // barrier timeouts.  `gemm_update` selects the trailing update:
-// 0 = cuBLAS DGEMM/SGEMM (plain), 1 = tcgen05 TF32 (FP32 only).
+// 0 = cuBLAS DGEMM/SGEMM (plain), 1 = tcgen05 TF32 (FP32 only).  With
+// `perm` (n ints, n <= 51,200) the row permutation is also accumulated
+// (perm[i] = original row now at row i), for lu_getrs.
 template <typename T>
 int lu_getrf(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
-             int *ipiv, int *info_dev, int gemm_update);
+             int *ipiv, int *info_dev, int gemm_update, int *perm = nullptr);
 
 // Row interchanges of rows [k1, k2) (0-based) given ipiv (1-based, absolute
 // row numbers relative to A), applied to columns [c0, c1) of A.
@@ -32,7 +34,8 @@ template <typename T>
 void lu_laswp(cudaStream_t st, T *A, int lda, int c0, int c1, int k1, int k2,
               const int *ipiv);
 
-// Solves A X = B with the factors (nrhs columns, ldb).
+// Solves A X = B with the factors (nrhs columns, ldb); the row interchanges
+// from `perm` (lu_getrf's) in one gather when given, else from ipiv.
 template <typename T>
 int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, int lda,
-             const int *ipiv, T *B, int ldb);
+             const int *ipiv, T *B, int ldb, const int *perm = nullptr);

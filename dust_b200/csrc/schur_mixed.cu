@@ -100,7 +100,7 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   // work: Y (nst x nmv), S (nmv x nmv), Ads32 (nmv x nst), Asd32 (nst x nmv),
   // vectors
   size_t need = 4 * ((size_t)nst * nmv * 3 + (size_t)nmv * nmv + (size_t)n * 4) + 8 * (size_t)n * 4 +
-                (size_t)nmv * 4 + 1024;
+                (size_t)nmv * 8 + 2048;
   DUST_TRY(devbuf_grow(L->mx, need));
   char *b = (char *)L->mx.p;
   auto take = [&](size_t bytes) {
@@ -119,6 +119,8 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   double *rs = (double *)take((size_t)n * 8);
   int *piv = (int *)take((size_t)nmv * 4 + 64);
   int *info = piv + nmv;
+  int *perm = (int *)take((size_t)nmv * 4);
+  const bool use_perm = (size_t)nmv * 4 <= 200 * 1024;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -132,7 +134,8 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
       DUST_TRY(gemm_tf32_acc(st, nst, nmv, nst, Ainv, nst, Asd, nst, Y, nst, 1.0f));
       DUST_TRY(gemm_tf32_acc(st, nmv, nmv, nst, Ads, nmv, Y, nst, S, nmv, -1.0f));
     }
-    DUST_TRY(lu_getrf<float>(L->cb, st, L->lu, nmv, S, nmv, piv, info, 1));
+    DUST_TRY(lu_getrf<float>(L->cb, st, L->lu, nmv, S, nmv, piv, info, 1,
+                             use_perm ? perm : nullptr));
     DUST_TRY(gemm_tf32_error(st));
     int hinfo = 0;
     DUST_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -194,7 +197,8 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
       if (nst > 0 && cublasSgemv(L->cb, CUBLAS_OP_N, nmv, nst, &monef, Ads, nmv, d32, 1, &onef,
                                  t32, 1) != CUBLAS_STATUS_SUCCESS)
         return DUST_ERR_CUDA;
-      DUST_TRY(lu_getrs<float>(L->cb, st, nmv, 1, S, nmv, piv, t32, nmv));
+      DUST_TRY(lu_getrs<float>(L->cb, st, nmv, 1, S, nmv, piv, t32, nmv,
+                               use_perm ? perm : nullptr));
       DUST_CUDA(cudaMemcpyAsync(d32 + nst, t32, (size_t)nmv * 4, cudaMemcpyDeviceToDevice, st));
       if (nst > 0 && cublasSgemv(L->cb, CUBLAS_OP_N, nst, nmv, &monef, Y, nst, t32, 1, &onef, d32,
                                  1) != CUBLAS_STATUS_SUCCESS)
