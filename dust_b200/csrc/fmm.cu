@@ -489,27 +489,37 @@ __device__ __forceinline__ double shift_w(const ShiftTerm &t, uint32_t oct) {
 }
 
 #define SH_T 128
+#define SH_W (SH_T / 32)
 // M2M into the active branch cells of level l: one warp per parent, lanes
-// over the output coefficient m; terms and offsets staged in shared memory
+// over the output coefficient m; terms and offsets staged in shared memory,
+// and each warp stages its parent's 8 children's coefficients (missing
+// children as zeros) before the term loops
 __global__ void __launch_bounds__(SH_T) k_m2m_t(FmmDev d, int l, uint32_t act_lo, uint32_t na,
                                                 const ShiftTerm *terms, const int *off, int nterm) {
   extern __shared__ __align__(16) unsigned char shm[];
-  ShiftTerm *st = (ShiftTerm *)shm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w3 = 3 * d.nm;
+  double *sa = (double *)shm + (size_t)warp * 8 * w3;  // [8][3 nm]
+  ShiftTerm *st = (ShiftTerm *)((double *)shm + (size_t)SH_W * 8 * w3);
   int *so = (int *)(st + nterm);
   for (int e = threadIdx.x; e < nterm; e += SH_T) st[e] = terms[e];
   for (int e = threadIdx.x; e <= d.nm; e += SH_T) so[e] = off[e];
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t c = blockIdx.x * (SH_T / 32) + warp; c < na; c += gridDim.x * (SH_T / 32)) {
+  for (uint32_t c = blockIdx.x * SH_W + warp; c < na; c += gridDim.x * SH_W) {
     const uint32_t ci = act_lo + c;
     const uint32_t key = d.act_key[ci];
     if (!(d.flags[d.G.lev_off[l] + key] & FL_BRANCH)) continue;
-    uint32_t cc[8];
-    for (int ch = 0; ch < 8; ++ch) cc[ch] = d.cidx[d.G.lev_off[l + 1] + 8u * key + (uint32_t)ch];
+    __syncwarp();
+    for (int ch = 0; ch < 8; ++ch) {
+      const uint32_t cc = d.cidx[d.G.lev_off[l + 1] + 8u * key + (uint32_t)ch];
+      const double *a = d.A + (size_t)cc * w3;
+      for (int e = lane; e < w3; e += 32) sa[ch * w3 + e] = a[e];
+    }
+    __syncwarp();
     for (int m = lane; m < d.nm; m += 32) {
       double acc[3] = {0, 0, 0};
       for (int ch = 0; ch < 8; ++ch) {
-        const double *a = d.A + (size_t)cc[ch] * 3 * d.nm;
+        const double *a = sa + ch * w3;
         for (int t = so[m]; t < so[m + 1]; ++t) {
           const double w = shift_w(st[t], (uint32_t)ch);
           const int s3 = 3 * st[t].s;
@@ -518,7 +528,7 @@ __global__ void __launch_bounds__(SH_T) k_m2m_t(FmmDev d, int l, uint32_t act_lo
           acc[2] += w * a[s3 + 2];
         }
       }
-      double *ap = d.A + (size_t)ci * 3 * d.nm;
+      double *ap = d.A + (size_t)ci * w3;
       ap[3 * m] = acc[0];
       ap[3 * m + 1] = acc[1];
       ap[3 * m + 2] = acc[2];
@@ -527,12 +537,43 @@ __global__ void __launch_bounds__(SH_T) k_m2m_t(FmmDev d, int l, uint32_t act_lo
 }
 
 // L2L into the active cells of level l (>= 2) from their parents: one warp
-// per child; b terms (|s| <= p) and, with stretching, g terms (|s| <= p+1)
+// per parent (an active branch cell of level l - 1), lanes over the output
+// coefficient m.  The 8 children's weights differ only in sign (the octant's
+// parity of the exponents), so each term's products are formed once and
+// added to all 8 children's sums; the parent's b and g are staged in shared
+// memory; only active children are written.  b terms (|s| <= p) and, with
+// stretching, g terms (|s| <= p+1).
+__device__ __forceinline__ void l2l_terms(const ShiftTerm *tt, int t0, int t1, const double *src,
+                                          double (*acc)[3]) {
+#pragma unroll
+  for (int ch = 0; ch < 8; ++ch) acc[ch][0] = acc[ch][1] = acc[ch][2] = 0.0;
+  for (int t = t0; t < t1; ++t) {
+    const ShiftTerm tm = tt[t];
+    const int s3 = 3 * tm.s;
+    const double v0 = tm.w * src[s3], v1 = tm.w * src[s3 + 1], v2 = tm.w * src[s3 + 2];
+    const unsigned px = tm.ex & 1u, py = tm.ey & 1u, pz = tm.ez & 1u;
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      // sign of shift_w for octant ch
+      const unsigned neg = ((ch & 1) ? 0u : px) ^ ((ch & 2) ? 0u : py) ^ ((ch & 4) ? 0u : pz);
+      if (neg) {
+        acc[ch][0] -= v0, acc[ch][1] -= v1, acc[ch][2] -= v2;
+      } else {
+        acc[ch][0] += v0, acc[ch][1] += v1, acc[ch][2] += v2;
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(SH_T) k_l2l_t(FmmDev d, int l, uint32_t act_lo, uint32_t na,
                                                 const ShiftTerm *tb, const int *ob, int ntb,
                                                 const ShiftTerm *tg, const int *og, int ntg) {
   extern __shared__ __align__(16) unsigned char shm[];
-  ShiftTerm *sb = (ShiftTerm *)shm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wb = 3 * d.nm, wg = ntg > 0 ? 3 * d.nm1 : 0;
+  double *sbp = (double *)shm + (size_t)warp * (wb + wg);  // parent's b, then g
+  double *sgp = sbp + wb;
+  ShiftTerm *sb = (ShiftTerm *)((double *)shm + (size_t)SH_W * (wb + wg));
   ShiftTerm *sg = sb + ntb;
   int *sob = (int *)(sg + ntg);
   int *sog = sob + d.nm + 1;
@@ -541,38 +582,47 @@ __global__ void __launch_bounds__(SH_T) k_l2l_t(FmmDev d, int l, uint32_t act_lo
   for (int e = threadIdx.x; e <= d.nm; e += SH_T) sob[e] = ob[e];
   for (int e = threadIdx.x; e <= d.nm1 && ntg > 0; e += SH_T) sog[e] = og[e];
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t c = blockIdx.x * (SH_T / 32) + warp; c < na; c += gridDim.x * (SH_T / 32)) {
-    const uint32_t ci = act_lo + c;
-    const uint32_t key = d.act_key[ci];
-    const uint32_t oct = key & 7u;
-    const uint32_t pc = d.cidx[d.G.lev_off[l - 1] + (key >> 3)];
-    const double *bp = d.B + (size_t)pc * 3 * d.nm;
-    double *b = d.B + (size_t)ci * 3 * d.nm;
-    for (int m = lane; m < d.nm; m += 32) {
-      double acc[3] = {0, 0, 0};
-      for (int t = sob[m]; t < sob[m + 1]; ++t) {
-        const double w = shift_w(sb[t], oct);
-        const int s3 = 3 * sb[t].s;
-        acc[0] += w * bp[s3];
-        acc[1] += w * bp[s3 + 1];
-        acc[2] += w * bp[s3 + 2];
-      }
-      for (int e = 0; e < 3; ++e) b[3 * m + e] += acc[e];
+  // act_lo / na: the active cells of level l - 1 (the candidate parents)
+  for (uint32_t c = blockIdx.x * SH_W + warp; c < na; c += gridDim.x * SH_W) {
+    const uint32_t pc = act_lo + c;
+    const uint32_t key = d.act_key[pc];
+    if (!(d.flags[d.G.lev_off[l - 1] + key] & FL_BRANCH)) continue;
+    uint32_t cc[8];
+    unsigned live = 0;
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      const uint32_t ck = 8u * key + (uint32_t)ch;
+      if (d.flags[d.G.lev_off[l] + ck] & FL_ACTIVE) live |= 1u << ch;
+      cc[ch] = d.cidx[d.G.lev_off[l] + ck];
     }
-    if (ntg > 0) {
-      const double *gp = d.Gx + (size_t)pc * 3 * d.nm1;
-      double *g = d.Gx + (size_t)ci * 3 * d.nm1;
-      for (int m = lane; m < d.nm1; m += 32) {
-        double acc[3] = {0, 0, 0};
-        for (int t = sog[m]; t < sog[m + 1]; ++t) {
-          const double w = shift_w(sg[t], oct);
-          const int s3 = 3 * sg[t].s;
-          acc[0] += w * gp[s3];
-          acc[1] += w * gp[s3 + 1];
-          acc[2] += w * gp[s3 + 2];
+    if (!live) continue;
+    __syncwarp();
+    const double *bp = d.B + (size_t)pc * wb;
+    for (int e = lane; e < wb; e += 32) sbp[e] = bp[e];
+    if (wg > 0) {
+      const double *gp = d.Gx + (size_t)pc * wg;
+      for (int e = lane; e < wg; e += 32) sgp[e] = gp[e];
+    }
+    __syncwarp();
+    double acc[8][3];
+    for (int m = lane; m < d.nm; m += 32) {
+      l2l_terms(sb, sob[m], sob[m + 1], sbp, acc);
+#pragma unroll
+      for (int ch = 0; ch < 8; ++ch)
+        if ((live >> ch) & 1u) {
+          double *b = d.B + (size_t)cc[ch] * wb + 3 * m;
+          b[0] += acc[ch][0], b[1] += acc[ch][1], b[2] += acc[ch][2];
         }
-        for (int e = 0; e < 3; ++e) g[3 * m + e] += acc[e];
+    }
+    if (wg > 0) {
+      for (int m = lane; m < d.nm1; m += 32) {
+        l2l_terms(sg, sog[m], sog[m + 1], sgp, acc);
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch)
+          if ((live >> ch) & 1u) {
+            double *g = d.Gx + (size_t)cc[ch] * wg + 3 * m;
+            g[0] += acc[ch][0], g[1] += acc[ch][1], g[2] += acc[ch][2];
+          }
       }
     }
   }
@@ -1542,7 +1592,8 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
     int64_t na = o->act_off[l + 1] - o->act_off[l];
     if (na > 0) {
       const int nt = o->shift_n[l][0];
-      const size_t shm = (size_t)nt * sizeof(ShiftTerm) + (size_t)(o->nm + 1) * 4;
+      const size_t shm = (size_t)SH_W * 8 * 3 * o->nm * 8 + (size_t)nt * sizeof(ShiftTerm) +
+                         (size_t)(o->nm + 1) * 4;
       if (shm > 48 * 1024)
         DUST_CUDA(cudaFuncSetAttribute(k_m2m_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)shm));
@@ -1568,12 +1619,14 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
     int64_t na = o->act_off[l + 1] - o->act_off[l];
     if (na <= 0) continue;
     const int ntb = o->shift_n[l][1], ntg = d.use_vs ? o->shift_n[l][2] : 0;
-    const size_t shm = (size_t)(ntb + ntg) * sizeof(ShiftTerm) + (size_t)(o->nm + o->nm1 + 2) * 4;
+    const size_t shm = (size_t)SH_W * 3 * (o->nm + (ntg > 0 ? o->nm1 : 0)) * 8 +
+                       (size_t)(ntb + ntg) * sizeof(ShiftTerm) + (size_t)(o->nm + o->nm1 + 2) * 4;
     if (shm > 48 * 1024)
       DUST_CUDA(cudaFuncSetAttribute(k_l2l_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)shm));
-    k_l2l_t<<<shift_grid(na), SH_T, shm, st>>>(
-        d, l, (uint32_t)o->act_off[l], (uint32_t)na, (const ShiftTerm *)o->shift_t[l][1],
+    const int64_t npar = o->act_off[l] - o->act_off[l - 1];
+    k_l2l_t<<<shift_grid(npar), SH_T, shm, st>>>(
+        d, l, (uint32_t)o->act_off[l - 1], (uint32_t)npar, (const ShiftTerm *)o->shift_t[l][1],
         (const int *)o->shift_o[l][1], ntb, (const ShiftTerm *)o->shift_t[l][2],
         (const int *)o->shift_o[l][2], ntg);
   }
