@@ -425,33 +425,41 @@ __global__ void __launch_bounds__(128, EN_MINB) k_elem_near(FmmDev d, ElemDev e,
 // L c (|a| + |b|) / (|a||b|(|a||b| + a.b)) beyond its ends (a.b > 0 there), so
 // neither form cancels.  Inside the Rankine core the result is scaled by
 // h^2 / (r_rankine L)^2 as in the reference's core formula.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ void line_vel_f(const double *vv, const float *q, const double *pos,
                                            float rr2, float rc, float *u) {
-  // vv: v0 (3), v1 (3) in FP64; q: e (3), L, mag.  a and b are formed in
-  // FP64 and rounded once, so their accuracy does not depend on the spread
-  // of the CTA's particles.
+  // vv: v0 (3), v1 (3) in FP64; q: e (3), L, mag, 1 / (r_rankine L)^2.  a and
+  // b are formed in FP64 and rounded once, so their accuracy does not depend
+  // on the spread of the CTA's particles.  Distances and quotients by the
+  // approximate reciprocal (square root) instructions.
   const float ax = (float)(pos[0] - vv[0]), ay = (float)(pos[1] - vv[1]),
               az = (float)(pos[2] - vv[2]);
   const float bx = (float)(pos[0] - vv[3]), by = (float)(pos[1] - vv[4]),
               bz = (float)(pos[2] - vv[5]);
   const float L = q[3];
-  const float ra = sqrtf(fmaf(ax, ax, fmaf(ay, ay, az * az)));
-  const float rb = sqrtf(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+  const float a2 = fmaf(ax, ax, fmaf(ay, ay, az * az));
+  const float b2 = fmaf(bx, bx, fmaf(by, by, bz * bz));
+  const float ira = rsqrt_approx(a2), irb = rsqrt_approx(b2);
+  const float ra = a2 * ira, rb = b2 * irb;
   const float ai = fmaf(ax, q[0], fmaf(ay, q[1], az * q[2]));
   const float cx = q[1] * az - q[2] * ay, cy = q[2] * ax - q[0] * az, cz = q[0] * ay - q[1] * ax;
   const float hi2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
   float f;
   if (ai > 0.f && ai < L) {
-    f = hi2 > 0.f ? ((L - ai) / rb + ai / ra) / hi2 : 0.f;
+    f = hi2 > 0.f ? fmaf(L - ai, irb, ai * ira) * rcp_approx(hi2) : 0.f;
   } else {
     const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
     const float den = ra * rb * fmaf(ra, rb, ab);
-    f = den > 0.f ? L * (ra + rb) / den : 0.f;
+    f = den > 0.f ? L * (ra + rb) * rcp_approx(den) : 0.f;
   }
-  const float rrL2 = rr2 * L * L;
-  if (!(hi2 > rrL2)) {
+  if (!(hi2 > rr2 * L * L)) {
     // Rankine core (or the cutoff around the end points)
-    f = (ra > L * rc && rb > L * rc) ? f * hi2 / rrL2 : 0.f;
+    f = (ra > L * rc && rb > L * rc) ? f * hi2 * q[5] : 0.f;
   }
   f *= q[4];
   u[0] = f * cx;
@@ -464,7 +472,7 @@ __device__ __forceinline__ void line_vel_f(const double *vv, const float *q, con
 __global__ void __launch_bounds__(EL_T) k_elem_fin(FmmDev d, ElemDev e, const double *farv,
                                                    double *vel, double *str, double *rot) {
   __shared__ double s_v[EL_TILE][6];
-  __shared__ float s_l[EL_TILE][5];
+  __shared__ float s_l[EL_TILE][6];
   const uint32_t t0 = blockIdx.x * EL_T, t = t0 + threadIdx.x;
   const size_t n = d.n;
   const bool act = t < n;
@@ -488,6 +496,8 @@ __global__ void __launch_bounds__(EL_T) k_elem_fin(FmmDev d, ElemDev e, const do
       }
       q[3] = (float)L.edge_len;
       q[4] = (float)L.mag;
+      const double rl = e.rp.r_rankine * L.edge_len;
+      q[5] = (float)(1.0 / (rl * rl));
     }
     __syncthreads();
     float a[3] = {0.f, 0.f, 0.f};
