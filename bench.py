@@ -289,7 +289,8 @@ def main():
         ms = max_over_ranks(float(np.mean(times)), ws)
         res = st.res.cpu().numpy()
         results[name] = {"ms": ms, "times": times, "loads": case.loads(res),
-                         "report": st.last_report, "clocks": clk.summary(), "res": res}
+                         "report": st.last_report, "clocks": clk.summary(), "res": res,
+                         "fmm": [t.cpu().numpy() for t in (st.vel, st.str, st.rot)]}
     if args.profile_step:
         return
     # phase breakdown (plain and mixed share the FMM): one timed step with events
@@ -297,6 +298,15 @@ def main():
     lp = results["plain"]["loads"]
     load_err = {k: float(np.max(np.abs(results[k]["loads"] - lp) / np.maximum(np.abs(lp), 1e-30)))
                 for k in results}
+    # particle outputs of the step (velocity without the wind, stretching,
+    # div-filter curl) against the FP64 step: relative L2 norms
+    uinf = np.asarray(params.u_inf)
+    def fmm_err(k):
+        a, b = results[k]["fmm"], results["plain"]["fmm"]
+        rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        return {"vel_induced": rel(a[0] - uinf, b[0] - uinf), "stretch": rel(a[1], b[1]),
+                "rot": rel(a[2], b[2])}
+    fmm_errs = {k: fmm_err(k) for k in results}
     # the headline mode: the fastest whose loads are within 1e-6 of FP64
     best = min((k for k in results if load_err[k] <= 1e-6), key=lambda k: results[k]["ms"])
     # end to end through the host API (pinned buffers)
@@ -330,7 +340,8 @@ def main():
             "speedup_vs_plain_fp64": round(results["plain"]["ms"] / r["ms"], 3),
             "load_error_vs_fp64": load_err[best],
             "modes": {k: {"ms": round(v["ms"], 3), "load_error_vs_fp64": load_err[k],
-                          "solve": v["report"]} for k, v in results.items()},
+                          "particle_error_vs_fp64": fmm_errs[k], "solve": v["report"]}
+                      for k, v in results.items()},
             "learned_training": learned["info"] if learned else None,
             "phases_ms": ph,
             "clocks": r["clocks"],
@@ -452,10 +463,12 @@ def run_e2e(case, params, mode, args, ws, pc=None):
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     case.cen, case.dir, case.mag, case.r_vortex = (pin(case.cen), pin(case.dir),
                                                   pin(case.mag), pin(case.r_vortex))
-    hs = step.HostStepper(case, params, mode)
+    n = case.mag.shape[0]
+    out = tuple(pin(np.empty((n, 3))) for _ in range(3))  # page-locked outputs
+    hs = step.HostStepper(case, params, mode, out=out)
     if pc is not None:
         pc.attach(hs.ls)
-    for _ in range(2):
+    for _ in range(3):
         hs.step()
     torch.cuda.synchronize()
     barrier(ws)
@@ -470,11 +483,10 @@ def run_e2e(case, params, mode, args, ws, pc=None):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     ms = max_over_ranks(float(np.mean(times)), ws)
-    n = case.mag.shape[0]
     h2d = n * 8 * 8 + case.rank * 8 * (12 + 3 + 3 + 1) + case.wake.n * 8 * 13 + case.end_vort.n * 56
     d2h = n * 9 * 8 + case.rank * 8
     return {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h)}
+            "d2h_bytes_per_step": int(d2h), "step_ms": [round(t, 2) for t in times]}
 
 
 if __name__ == "__main__":

@@ -234,7 +234,9 @@ __device__ __forceinline__ void mt_epilogue(const FmmDev &d, int h, int r, bool 
 #define MT_THREADS2 (MT_P + 64)
 // offsets accumulated in one TMEM set before it is drained to FP64 (the
 // tensor core's FP32 accumulation truncates, so its runs are kept short)
+#ifndef MT_GROUP
 #define MT_GROUP 4
+#endif
 
 __global__ void __launch_bounds__(MT_THREADS2, 1)
     k_m2l_tc(FmmDev d, const int4 *batches, const uint32_t *list, const int *srcl,

@@ -46,15 +46,24 @@ class Octree:
         return {k: getattr(s, k) for k, _ in abi.FmmStats._fields_}
 
     def apply_multipole(self, cen, dir_, mag, r_vortex, elements=None,
-                        want_stretch=True, want_rotu=True):
+                        want_stretch=True, want_rotu=True, out=None):
         """Velocity (incl. u_inf), stretching and div-filter curl at every
-        particle, in the caller's particle order."""
+        particle, in the caller's particle order.  ``out``: optional
+        (vel, stretch, rotu) host arrays (n x 3 float64, C order) to write,
+        e.g. page-locked buffers reused across steps."""
         cen, dir_, mag, rv = (abi.f64(cen), abi.f64(dir_), abi.f64(mag), abi.f64(r_vortex))
         n = mag.shape[0]
         est, keep = elements if elements is not None else abi.elements_struct()
-        vel = np.empty((n, 3))
-        st = np.empty((n, 3)) if want_stretch else None
-        ro = np.empty((n, 3)) if want_rotu else None
+        if out is not None:
+            vel, st, ro = out
+            for a in (vel, st, ro):
+                if a is not None and (a.dtype != np.float64 or a.shape != (n, 3)
+                                      or not a.flags.c_contiguous):
+                    raise ValueError("out arrays must be C-contiguous float64 (n, 3)")
+        else:
+            vel = np.empty((n, 3))
+            st = np.empty((n, 3)) if want_stretch else None
+            ro = np.empty((n, 3)) if want_rotu else None
         check(lib().dust_fmm_apply(self._h, n, abi.dptr(cen), abi.dptr(dir_), abi.dptr(mag),
                                    abi.dptr(rv), C.byref(est), abi.dptr(vel), abi.dptr(st),
                                    abi.dptr(ro)), "dust_fmm_apply")

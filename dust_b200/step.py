@@ -31,10 +31,13 @@ from .octree import Octree
 
 
 class HostStepper:
-    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64):
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None):
+        """``out``: optional (vel, stretch, rotu) host arrays the particle
+        outputs are written to every step (e.g. page-locked buffers)."""
         self.case = case
         self.params = params
         self.mode = mode
+        self.out = out
         c = case
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
         self.oc = Octree(params)
@@ -64,7 +67,7 @@ class HostStepper:
         m2 = np.where(self.ind[:, 1] >= 0, res[np.maximum(self.ind[:, 1], 0)], 0.0)
         c.wake.mag = res[self.ind[:, 0]] - m2
         els = abi.elements_struct(c.elems, c.wake, c.end_vort)
-        vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els)
+        vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els, out=self.out)
         return res, vel, st, ro
 
 
