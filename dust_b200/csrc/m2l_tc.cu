@@ -17,15 +17,16 @@
 // the FP32 remainder, and a product is Ah Bh + Ah Bl + Al Bh, which keeps
 // about FP32 accuracy; the tables are split from their FP64 values.
 //
-// Roles (192 threads):
-//  warps 0-3  producers: per offset look up the 128 source cells (empty,
+// Roles (320 threads):
+//  warps 0-7  producers: per offset look up the 128 source cells (empty,
 //             inactive or missing ones give zero rows), then per component
 //             gather their coefficients into shared memory as TF32 high/low
-//             parts in the canonical no-swizzle K-major layout; at the end
-//             they read TMEM (one row = one target per thread) and add the
-//             rescaled locals to the FP64 b and g arrays;
-//  warp 4     lane 0 issues the 90 tcgen05.mma of an offset and commits;
-//  warp 5     lane 0 streams the offset's table image (61,440 B, prepared
+//             parts in the canonical no-swizzle K-major layout.  They also
+//             drain the TMEM accumulators to FP64 (one row = one target per
+//             thread, half the columns per warp) every MT_GROUP offsets and
+//             at the end add the rescaled locals to the FP64 b and g;
+//  warp 8     lane 0 issues the 90 tcgen05.mma of an offset and commits;
+//  warp 9     lane 0 streams the offset's table image (61,440 B, prepared
 //             once per level in the operand layout) with one bulk copy.
 // Two A buffers (one component each) and two B buffers overlap gathering,
 // copying and the tensor core.  Offsets where no target of the CTA has a
@@ -227,11 +228,16 @@ __device__ __forceinline__ void mt_epilogue(const FmmDev &d, int h, int r, bool 
   }
 }
 
-// producers / drainers: 8 warps; the MMA issuer and the table loader: one
-// warp each
-#define MT_PW 8
+// producers (MT_PW warps, MT_DW of them also drainers); the MMA issuer and
+// the table loader: one warp each
+#ifndef MT_PW
+#define MT_PW 8  // producer warps (gathers); 10 and 20 measured slower
+#endif
+#define MT_DW 8  // of which drain the TMEM accumulators (4 lane quarters x 2 column halves)
 #define MT_P (MT_PW * 32)
+#define MT_D (MT_DW * 32)
 #define MT_THREADS2 (MT_P + 64)
+static_assert((MT_M * MT_KCH) % MT_P == 0 && MT_PW >= MT_DW, "producer layout");
 // offsets accumulated in one TMEM set before it is drained to FP64 (the
 // tensor core's FP32 accumulation truncates, so its runs are kept short)
 #ifndef MT_GROUP
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
       mbar_init(&s_afull[b], MT_P);
       mbar_init(&s_aempty[b], 1);
       mbar_init(&s_cfull[b], 1);
-      mbar_init(&s_cempty[b], MT_P);
+      mbar_init(&s_cempty[b], MT_D);
     }
     mbar_init(&s_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;");
@@ -301,8 +307,9 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
   if (warp < MT_PW) {
     // ------------------------------------------------ producers / drainers
     // drain role: target row r (TMEM lane), columns m' in [28 h, 28 h + 28)
+    const bool drainer = warp < MT_DW;
     const int r = (warp & 3) * 32 + lane, h = warp >> 2;
-    const bool valid = r < cnt;
+    const bool valid = drainer && r < cnt;
     const uint32_t ci = valid ? list[t0 + r] : 0u;
     int ntot = 0;  // present offsets
     for (int w = 0; w < 7; ++w) ntot += __popc(s_mask[w]);
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
       if (!ok) break;
       // a group's set is drained once the next group has started (its MMAs
       // then overlap the drain), the last group after the loop
-      if (oi % MT_GROUP == 0 && oi >= MT_GROUP) {
+      if (drainer && oi % MT_GROUP == 0 && oi >= MT_GROUP) {
         const int g = oi / MT_GROUP - 1;
         if (!mbar_wait_f(smem_u32(&s_cfull[g & 1]), (uint32_t)((g >> 1) & 1), fail)) {
           ok = false;
@@ -381,7 +388,7 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
       ++oi;
       cand = ncand;
     }
-    if (ok && ntot > 0) {
+    if (drainer && ok && ntot > 0) {
       const int g = (ntot - 1) / MT_GROUP;
       if (mbar_wait_f(smem_u32(&s_cfull[g & 1]), (uint32_t)((g >> 1) & 1), fail)) {
         asm volatile("tcgen05.fence::after_thread_sync;");
