@@ -1,8 +1,12 @@
 // gmres.cu -- learned-preconditioned FP64 GMRES for the time-stepping system.
 //
-// Restarted GMRES(m) with right preconditioning A M u = b, x = M u, where
-// M = (I + O) D^-1 comes from the graph network of gnn.cu evaluated on the
-// current matrix; the warm start is x0 = M b.  Matrix-vector products use
+// Restarted GMRES(m) with right preconditioning A P u = b, x = P u.  With a
+// static block, P is block lower-triangular on the static/moving split:
+//   z_s = Ainv v_s,   z_d = [M (0; v_d - A_ds z_s)]_d,
+// with Ainv = A_ss^-1 (FP32, built once from the static LU, as the mixed
+// solve uses it) and M = (I + O) D^-1 from the graph network of gnn.cu
+// evaluated on the current matrix, so the network only has to approximate
+// the moving bodies' part; without one, P = M.  The warm start is x0 = P b.  Matrix-vector products use
 // the assembled blocks directly (static block from its unfactored copy), so
 // nothing is refactored.  Orthogonalisation is classical Gram-Schmidt applied
 // twice; the small Hessenberg least-squares problem is solved on the host
@@ -81,6 +85,43 @@ int pc_pack_sample(int n, int C, const double *dinv, const double *AZ, const dou
   return DUST_OK;
 }
 
+__global__ void k_to_f32(int n, const double *a, float *b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_to_f64(int n, const float *a, double *b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+
+// z = P v (see the file comment); tmp: 2 n doubles + 2 nst floats
+static int gm_precond(dust_linsys *L, dust_precond *P, const double *v, double *z, char *tmp,
+                      cudaStream_t st, cublasHandle_t cb) {
+  const int n = L->n, nst = L->nst, nmv = L->nmv;
+  if (nst == 0) {
+    pc_apply(P, v, z, st);
+    return DUST_OK;
+  }
+  double *t = (double *)tmp, *y = t + n;
+  float *v32 = (float *)(y + n), *z32 = v32 + nst;
+  const float onef = 1.0f, zerof = 0.0f;
+  const double one = 1.0, mone = -1.0;
+  k_to_f32<<<nblk(nst, 256), 256, 0, st>>>(nst, v, v32);
+  if (cublasSgemv(cb, CUBLAS_OP_N, nst, nst, &onef, (const float *)L->ainv32.p, nst, v32, 1,
+                  &zerof, z32, 1) != CUBLAS_STATUS_SUCCESS)
+    return DUST_ERR_CUDA;
+  k_to_f64<<<nblk(nst, 256), 256, 0, st>>>(nst, z32, z);
+  if (nmv == 0) return DUST_OK;
+  DUST_CUDA(cudaMemsetAsync(t, 0, (size_t)nst * 8, st));
+  DUST_CUDA(cudaMemcpyAsync(t + nst, v + nst, (size_t)nmv * 8, cudaMemcpyDeviceToDevice, st));
+  if (cublasDgemv(cb, CUBLAS_OP_N, nmv, nst, &mone, (const double *)L->A.p + nst, n, z, 1, &one,
+                  t + nst, 1) != CUBLAS_STATUS_SUCCESS)
+    return DUST_ERR_CUDA;
+  pc_apply(P, t, y, st);
+  DUST_CUDA(cudaMemcpyAsync(z + nst, y + nst, (size_t)nmv * 8, cudaMemcpyDeviceToDevice, st));
+  return DUST_OK;
+}
+
 __global__ void k_scale(int n, double a, const double *x, double *y) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = a * x[i];
@@ -112,9 +153,13 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
   cudaEventDestroy(ev);
   if (s != DUST_OK) return s;
   // V (n x (m+1)), z, w, r, u and the projections h (m+1) on the device
-  DUST_TRY(devbuf_grow(L->kr, (size_t)n * 8 * (m + 1 + 4) + (size_t)(m + 2) * 8 + 256));
+  if (L->nst > 0 && !L->ainv_ready) DUST_TRY(build_static_inverse(L));
+  DUST_TRY(devbuf_grow(L->kr, (size_t)n * 8 * (m + 1 + 6) + (size_t)(m + 2) * 8 +
+                                  (size_t)L->nst * 8 + 512));
   double *V = (double *)L->kr.p, *z = V + (size_t)n * (m + 1), *w = z + n, *r = w + n,
          *u = r + n, *hd = u + n;
+  char *ptmp = (char *)(hd + m + 2);  // gm_precond scratch
+  auto precond = [&](const double *v, double *out) { return gm_precond(L, P, v, out, ptmp, st, cb); };
   const double *b = (const double *)L->b.p;
   const double one = 1.0, mone = -1.0, zero = 0.0;
   cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST);
@@ -133,7 +178,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
     if (rep) rep->mode_used = DUST_SOLVE_GMRES_NN;
     return DUST_OK;
   }
-  pc_apply(P, b, x, st);  // warm start x0 = M b
+  DUST_TRY(precond(b, x));  // warm start x0 = P b
   DUST_TRY(resid());
   double beta = 0.0;
   if (!nrm2(r, &beta)) return DUST_ERR_CUDA;
@@ -146,7 +191,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
     int k = 0;
     bool done = false;
     while (k < m && it < GM_MAXIT && !done) {
-      pc_apply(P, V + (size_t)k * n, z, st);
+      DUST_TRY(precond(V + (size_t)k * n, z));
       DUST_TRY(linsys_matmat(L, 1, z, n, w, n, st, cb));
       double *hc = &H[(size_t)k * (m + 1)];
       std::fill(hc, hc + m + 1, 0.0);
@@ -183,7 +228,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
       ++it;
       if (std::fabs(g[k]) <= GM_TOL * bnorm || hn == 0.0) done = true;
     }
-    // y = H(1:k,1:k) \ g(1:k); x += M (V y)
+    // y = H(1:k,1:k) \ g(1:k); x += P (V y)
     for (int q = k - 1; q >= 0; --q) {
       double sum = g[q];
       for (int c = q + 1; c < k; ++c) sum -= H[(size_t)c * (m + 1) + q] * y[c];
@@ -193,7 +238,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
     DUST_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
     if (cublasDgemv(cb, CUBLAS_OP_N, n, k, &one, V, n, hd, 1, &zero, u, 1) != CUBLAS_STATUS_SUCCESS)
       return DUST_ERR_CUDA;
-    pc_apply(P, u, z, st);
+    DUST_TRY(precond(u, z));
     k_add<<<nblk(n, 256), 256, 0, st>>>(n, z, x);
     DUST_TRY(resid());
     if (!nrm2(r, &beta)) return DUST_ERR_CUDA;

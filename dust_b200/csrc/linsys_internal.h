@@ -49,3 +49,5 @@ SysView linsys_view(const dust_linsys *L);
 int linsys_matmat(const dust_linsys *L, int ncols, const double *X, int ldx, double *Y, int ldy,
                   cudaStream_t st, cublasHandle_t cb);
 int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep);
+// Ainv = A_ss^-1 (FP32) from the static block's FP64 LU, once per handle
+int build_static_inverse(dust_linsys *L);

@@ -69,7 +69,7 @@ __global__ void k_rowabs_blocks(int n, int nst, const double *As, const double *
   atomicAdd(rs + i, s);
 }
 
-static int build_static_inverse(dust_linsys *L) {
+int build_static_inverse(dust_linsys *L) {
   const int nst = L->nst, n = L->n;
   size_t nn = (size_t)nst * nst;
   DevBuf X;
