@@ -51,6 +51,25 @@ int linsys_matmat(const dust_linsys *L, int nc, const double *X, int ldx, double
                        ldy) == CUBLAS_STATUS_SUCCESS;
   };
   bool ok = true;
+  if (nc == 1) {
+    // one vector: matrix-vector products (bandwidth bound)
+    auto gemv = [&](int m, int k, const double *Ap, int lda, const double *Xp, double *Yp,
+                    const double *beta) {
+      return cublasDgemv(cb, CUBLAS_OP_N, m, k, &one, Ap, lda, Xp, 1, beta, Yp, 1) ==
+             CUBLAS_STATUS_SUCCESS;
+    };
+    if (nst == 0) {
+      ok = gemv(n, n, A, n, X, Y, &zero);
+    } else {
+      ok = gemv(nst, nst, As, nst, X, Y, &zero);
+      if (nmv > 0) {
+        ok = ok && gemv(nst, nmv, A + (size_t)nst * n, n, X + nst, Y, &one);
+        ok = ok && gemv(nmv, nst, A + nst, n, X, Y + nst, &zero);
+        ok = ok && gemv(nmv, nmv, A + nst + (size_t)nst * n, n, X + nst, Y + nst, &one);
+      }
+    }
+    return ok ? DUST_OK : DUST_ERR_CUDA;
+  }
   if (nst == 0) {
     ok = gemm(n, n, A, n, X, Y, &zero);
   } else {
@@ -154,11 +173,12 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
   if (s != DUST_OK) return s;
   // V (n x (m+1)), z, w, r, u and the projections h (m+1) on the device
   if (L->nst > 0 && !L->ainv_ready) DUST_TRY(build_static_inverse(L));
-  DUST_TRY(devbuf_grow(L->kr, (size_t)n * 8 * (m + 1 + 6) + (size_t)(m + 2) * 8 +
-                                  (size_t)L->nst * 8 + 512));
+  // hd: two Gram-Schmidt projections of m+1 and the new norm, read in one copy
+  const size_t nhd = 2 * (size_t)(m + 1) + 2;
+  DUST_TRY(devbuf_grow(L->kr, (size_t)n * 8 * (m + 1 + 6) + nhd * 8 + (size_t)L->nst * 8 + 512));
   double *V = (double *)L->kr.p, *z = V + (size_t)n * (m + 1), *w = z + n, *r = w + n,
          *u = r + n, *hd = u + n;
-  char *ptmp = (char *)(hd + m + 2);  // gm_precond scratch
+  char *ptmp = (char *)(hd + nhd);  // gm_precond scratch
   auto precond = [&](const double *v, double *out) { return gm_precond(L, P, v, out, ptmp, st, cb); };
   const double *b = (const double *)L->b.p;
   const double one = 1.0, mone = -1.0, zero = 0.0;
@@ -183,7 +203,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
   double beta = 0.0;
   if (!nrm2(r, &beta)) return DUST_ERR_CUDA;
   int it = 0;
-  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(m + 1);
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hh(nhd);
   while (beta > GM_TOL * bnorm && it < GM_MAXIT) {
     k_scale<<<nblk(n, 256), 256, 0, st>>>(n, 1.0 / beta, r, V);
     std::fill(g.begin(), g.end(), 0.0);
@@ -195,20 +215,24 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
       DUST_TRY(linsys_matmat(L, 1, z, n, w, n, st, cb));
       double *hc = &H[(size_t)k * (m + 1)];
       std::fill(hc, hc + m + 1, 0.0);
-      // classical Gram-Schmidt, twice
+      // classical Gram-Schmidt, twice; both projections and the norm of the
+      // result stay on the device until one copy to the host
       for (int pass = 0; pass < 2; ++pass) {
-        if (cublasDgemv(cb, CUBLAS_OP_T, n, k + 1, &one, V, n, w, 1, &zero, hd, 1) !=
+        double *hp = hd + (size_t)pass * (m + 1);
+        if (cublasDgemv(cb, CUBLAS_OP_T, n, k + 1, &one, V, n, w, 1, &zero, hp, 1) !=
                 CUBLAS_STATUS_SUCCESS ||
-            cublasDgemv(cb, CUBLAS_OP_N, n, k + 1, &mone, V, n, hd, 1, &one, w, 1) !=
+            cublasDgemv(cb, CUBLAS_OP_N, n, k + 1, &mone, V, n, hp, 1, &one, w, 1) !=
                 CUBLAS_STATUS_SUCCESS)
           return DUST_ERR_CUDA;
-        DUST_CUDA(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * (k + 1),
-                                  cudaMemcpyDeviceToHost, st));
-        DUST_CUDA(cudaStreamSynchronize(st));
-        for (int q = 0; q <= k; ++q) hc[q] += hh[q];
       }
-      double hn = 0.0;
-      if (!nrm2(w, &hn)) return DUST_ERR_CUDA;
+      cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_DEVICE);
+      const bool nok = cublasDnrm2(cb, n, w, 1, hd + 2 * (m + 1)) == CUBLAS_STATUS_SUCCESS;
+      cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST);
+      if (!nok) return DUST_ERR_CUDA;
+      DUST_CUDA(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * nhd, cudaMemcpyDeviceToHost, st));
+      DUST_CUDA(cudaStreamSynchronize(st));
+      for (int q = 0; q <= k; ++q) hc[q] = hh[q] + hh[(size_t)(m + 1) + q];
+      const double hn = hh[2 * (size_t)(m + 1)];
       hc[k + 1] = hn;
       if (hn > 0.0) k_scale<<<nblk(n, 256), 256, 0, st>>>(n, 1.0 / hn, w, V + (size_t)(k + 1) * n);
       // Givens rotations on the new column
