@@ -1233,10 +1233,10 @@ __global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
 // ------------------------------------------- L2P + P2P, FP32C (warp per leaf)
 // Leaves hold a few particles (6 on average in the full-step case), so a
 // CTA per leaf leaves most lanes idle.  Here one warp owns one leaf: lanes
-// are split into G groups of TPR = (targets rounded up to a power of two)
-// lanes, lane (tl, grp) accumulates target tl over the sources u = grp mod
-// G of each 32-source tile staged in the warp's own shared memory, and the
-// groups are combined with shuffles.  Pair arithmetic is p2p_pair_f (FP32 on
+// are split into G = 32 / cnt groups of cnt lanes (cnt targets, at most 32
+// at a time), lane (tl, grp) accumulates target tl over the sources
+// u = grp mod G of each 32-source tile staged in the warp's own shared
+// memory, and group 0 adds the other groups' sums from shared memory.  Pair arithmetic is p2p_pair_f (FP32 on
 // coordinates relative to the leaf centre) with the FP32 partial sums folded
 // into FP64 after every 128 sources; L2P stays FP64.
 #define P2W_WARPS 4
@@ -1362,11 +1362,11 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
   float *fs = &s_src[w][0][0];
   double *acc = &s_acc[w][0][lane];  // this lane's 12 FP64 sums, stride 32
   for (int t0 = 0; t0 < nt; t0 += 32) {
+    // G groups of cnt lanes (one lane per target) split the sources; lanes
+    // beyond G * cnt idle
     const int cnt = min(32, nt - t0);
-    int TPR = 1;
-    while (TPR < cnt) TPR <<= 1;
-    const int G = 32 / TPR, tl = lane & (TPR - 1), grp = lane / TPR;
-    const bool act = tl < cnt;
+    const int TPR = cnt, G = 32 / TPR, tl = lane % TPR, grp = lane / TPR;
+    const bool act = grp < G;
     const uint32_t ti = lo + t0 + (act ? tl : 0);
     const float ftp[3] = {(float)(d.P[ti] - cc[0]), (float)(d.P[n + ti] - cc[1]),
                           (float)(d.P[2 * n + ti] - cc[2])};
@@ -1410,12 +1410,16 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
         }
       }
     }
-    // combine the groups of each target
+    // combine the groups of each target (group 0's lane sums the others'
+    // shared-memory sums)
+    __syncwarp();
     double A[12];
     for (int e = 0; e < 12; ++e) {
       A[e] = acc[32 * e];
-      for (int o = TPR; o < 32; o <<= 1) A[e] += __shfl_xor_sync(0xffffffffu, A[e], o);
+      if (grp == 0)
+        for (int g = 1; g < G; ++g) A[e] += acc[32 * e + g * TPR];
     }
+    __syncwarp();
     if (act && grp == 0) {
       const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
       double lv[3], g[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
