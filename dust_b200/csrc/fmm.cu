@@ -373,12 +373,17 @@ __device__ inline double ipow_d(double x, int e) {
   return r;
 }
 
-// P2M (leaf_M_multipole, mod_multipole.f90:224-251): one CTA per leaf.
-__global__ void k_p2m(FmmDev d) {
-  extern __shared__ double sh[];
-  const int CH = 64;
-  double *sx = sh, *sy = sh + CH, *sz = sh + 2 * CH, *sa = sh + 3 * CH;  // sa: 3*CH
-  uint32_t ci = d.leaf_ci[blockIdx.x];
+// P2M (leaf_M_multipole, mod_multipole.f90:224-251): one warp per leaf.
+#define P2M_W 4
+__global__ void __launch_bounds__(P2M_W * 32) k_p2m(FmmDev d) {
+  // one warp per leaf: the leaf's particles in chunks of 32 in the warp's
+  // shared memory, lanes over the output coefficients m (32 at a time); each
+  // coefficient sums its particles in the same order as a serial loop
+  __shared__ double sh[P2M_W][6][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t leaf = blockIdx.x * P2M_W + w;
+  if (leaf >= d.n_leaves) return;  // warp-uniform
+  uint32_t ci = d.leaf_ci[leaf];
   int l = d.act_lev[ci];
   uint32_t key = d.act_key[ci];
   int ci_, cj, ck;
@@ -387,37 +392,40 @@ __global__ void k_p2m(FmmDev d) {
   cell_center(d.G, l, ci_, cj, ck, c);
   uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
   if (hi == lo) return;  // empty leaf: a = 0 (block zeroed before the pass)
-  int m = threadIdx.x;
-  int mi = 0, mj = 0, mk = 0;
-  if (m < d.nm) mono_exp(m, mi, mj, mk);
-  double ax = 0, ay = 0, az = 0;
   const size_t n = d.n;
-  for (uint32_t s0 = lo; s0 < hi; s0 += CH) {
-    int cnt = min((int)(hi - s0), CH);
-    __syncthreads();
-    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-      uint32_t s = s0 + t;
-      sx[t] = d.P[s] - c[0];
-      sy[t] = d.P[n + s] - c[1];
-      sz[t] = d.P[2 * n + s] - c[2];
-      sa[3 * t] = d.P[3 * n + s];
-      sa[3 * t + 1] = d.P[4 * n + s];
-      sa[3 * t + 2] = d.P[5 * n + s];
-    }
-    __syncthreads();
-    if (m < d.nm)
-      for (int t = 0; t < cnt; ++t) {
-        double pr = ipow_d(sx[t], mi) * ipow_d(sy[t], mj) * ipow_d(sz[t], mk);
-        ax += pr * sa[3 * t];
-        ay += pr * sa[3 * t + 1];
-        az += pr * sa[3 * t + 2];
+  double(*sp)[32] = sh[w];
+  for (int m0 = 0; m0 < d.nm; m0 += 32) {
+    const int m = m0 + lane;
+    int mi = 0, mj = 0, mk = 0;
+    if (m < d.nm) mono_exp(m, mi, mj, mk);
+    double ax = 0, ay = 0, az = 0;
+    for (uint32_t s0 = lo; s0 < hi; s0 += 32) {
+      const int cnt = min((int)(hi - s0), 32);
+      __syncwarp();
+      if (lane < cnt) {
+        const uint32_t s = s0 + lane;
+        sp[0][lane] = d.P[s] - c[0];
+        sp[1][lane] = d.P[n + s] - c[1];
+        sp[2][lane] = d.P[2 * n + s] - c[2];
+        sp[3][lane] = d.P[3 * n + s];
+        sp[4][lane] = d.P[4 * n + s];
+        sp[5][lane] = d.P[5 * n + s];
       }
-  }
-  if (m < d.nm) {
-    double *a = d.A + (size_t)ci * 3 * d.nm;
-    a[3 * m] = ax;
-    a[3 * m + 1] = ay;
-    a[3 * m + 2] = az;
+      __syncwarp();
+      if (m < d.nm)
+        for (int t = 0; t < cnt; ++t) {
+          double pr = ipow_d(sp[0][t], mi) * ipow_d(sp[1][t], mj) * ipow_d(sp[2][t], mk);
+          ax += pr * sp[3][t];
+          ay += pr * sp[4][t];
+          az += pr * sp[5][t];
+        }
+    }
+    if (m < d.nm) {
+      double *a = d.A + (size_t)ci * 3 * d.nm;
+      a[3 * m] = ax;
+      a[3 * m + 1] = ay;
+      a[3 * m + 2] = az;
+    }
   }
 }
 
@@ -1589,8 +1597,7 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   o->dev = d;
   DUST_TRY(m2l_prepare(o, d, st));
   if (o->n_leaves > 0) {
-    int thr = std::max(64, (o->nm + 31) / 32 * 32);
-    k_p2m<<<(unsigned)o->n_leaves, thr, 6 * 64 * 8, st>>>(d);
+    k_p2m<<<(unsigned)((o->n_leaves + P2M_W - 1) / P2M_W), P2M_W * 32, 0, st>>>(d);
   }
   for (int l = ll - 1; l >= 1; --l) {
     int64_t na = o->act_off[l + 1] - o->act_off[l];
