@@ -139,6 +139,15 @@ def barrier(ws):
         dist.barrier()
 
 
+def workload(case, degree):
+    """The benchmark's workload description (both arms)."""
+    nmv = case.rank - case.nstatic
+    return ("full step: 2x3-blade VLM rotors (%s moving unknowns) + %s-panel surface-panel "
+            "wing, %d wake panels, %d particles, FMM p=%d, leaves<=64"
+            % (format(nmv, ","), format(case.nstatic, ","), case.wake.n, case.mag.shape[0],
+               degree))
+
+
 def make_case(args):
     from dust_b200 import synth
     if args.quick:
@@ -193,10 +202,11 @@ def cpu_baseline(case, params, budget_s=20.0):
     O.fmm_apply(params, case.cen[sub], case.dir[sub], case.mag[sub], case.r_vortex[sub])
     parts["fmm"] = (time.perf_counter() - t) * 20
     # (4) assembly + Schur LU per step: a reduced system, scaled by flop count
-    m = 1200
+    m = min(1200, case.nstatic)
+    nmv_s = min(160, case.rank - case.nstatic)
     sl = np.arange(m)
     sub_el = case.elems.subset(np.concatenate([sl, np.arange(case.nstatic,
-                                                             case.nstatic + 160)]))
+                                                             case.nstatic + nmv_s)]))
     nst_s = m
     t = time.perf_counter()
     O.linsys_run(params, sub_el.n, nst_s, sub_el, sub_el, (abi.empty_panels(), 0, None),
@@ -206,7 +216,7 @@ def cpu_baseline(case, params, budget_s=20.0):
     def step_flops(nst, nmv):
         return 2 * nst * nst * nmv + 2 * nmv * nmv * nst + 2 / 3 * nmv ** 3
     # the sample also paid its static LU (2/3 nst^3); scale by total flops
-    fl_small = 2 / 3 * nst_s ** 3 + step_flops(nst_s, 160)
+    fl_small = 2 / 3 * nst_s ** 3 + step_flops(nst_s, nmv_s)
     parts["linsys"] = t_small * step_flops(case.nstatic, case.rank - case.nstatic) / fl_small
     total_ms = 1e3 * sum(parts.values())
     return total_ms, {k: round(v * 1e3, 1) for k, v in parts.items()}
@@ -220,8 +230,7 @@ def run_reference(args, rank, ws):
     case = synth.FullStepCase(n_particles=args.particles) if not args.quick else make_case(args)
     params = case.fmm_params(degree=args.degree)
     vals = []
-    for _ in range(max(1, args.warmup if args.warmup < 2 else 1)):
-        pass
+    # each step is a bounded sample (about 20 s of host work); at most 2
     for _ in range(max(1, min(args.steps, 2))):
         ms, parts = cpu_baseline(case, params)
         vals.append(ms)
@@ -230,11 +239,11 @@ def run_reference(args, rank, ws):
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
             "n_gpus": args.gpus, "steps": len(vals), "warmup": 0, "ms_per_step": round(v, 1),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
-            "data": "synthetic",
-            "config": {"workload": "full step: 2x3-blade VLM rotors (1,920 moving) + "
-                       "12,000-panel wing, 2M particles, FMM p=%d" % args.degree,
-                       "parallelism": "replicas"},
+            "dtype": "f64",
+            "data": "synthetic (seeded FullStepCase)",
+            "config": {"workload": workload(case, args.degree), "mode": "reference (FP64 CPU)",
+                       "levels": params.n_octree_levels,
+                       "parallelism": "rank 0 only" if ws > 1 else "host cores"},
             "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": cores, "kind": "port",
                              "sample": "per-phase samples scaled to one step: " +
                              json.dumps(parts)},
@@ -330,9 +339,7 @@ def main():
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
             "data": "synthetic (seeded FullStepCase)",
-            "config": {"workload": "full step: 2x3-blade VLM rotors (1,920 moving unknowns) + "
-                       "12,000-panel surface-panel wing, 338 wake panels, %d particles, "
-                       "FMM p=%d, leaves<=64" % (case.mag.shape[0], args.degree),
+            "config": {"workload": workload(case, args.degree),
                        "mode": best, "levels": params.n_octree_levels,
                        "l2": "256 MB flush between timed steps; A is 1.55 GB",
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
