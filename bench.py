@@ -257,6 +257,9 @@ def main():
     rank, ws, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, rank, ws)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import torch
     from dust_b200 import abi, step
