@@ -116,8 +116,12 @@ def dist_init(args):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # gloo without a GPU: only the reference arm (host cores) runs there
+        cuda = torch.cuda.is_available()
+        if cuda:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if cuda else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, ws, local

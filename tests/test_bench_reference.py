@@ -24,3 +24,18 @@ def test_reference_arm_json_line():
     assert d["e2e"] == {"value": d["value"], "unit": "ms", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert "particles" in d["config"]["workload"]
+
+
+def test_reference_arm_two_ranks():
+    """Under torchrun only rank 0 runs the reference arm and prints; the other
+    rank exits 0 without work (gloo here, no GPU needed)."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr", "127.0.0.1", "--master-port", "29617",
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--quick", "--steps", "1",
+           "--warmup", "0", "--gpus", "2"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
