@@ -117,3 +117,61 @@ def test_oracle_fmm_out_of_box():
     with pytest.raises(RuntimeError):
         O.fmm_apply(FmmParams(box_length=1.0), np.array([[2.0, 0.5, 0.5]]),
                     np.array([[0, 0, 1.0]]), np.array([1.0]), np.array([0.1]))
+
+
+def test_vortex_particle_pair_analytic():
+    """Two particles: the regularised Biot-Savart velocity and the stretching
+    term of the reference's kernel (rho^2 = r^2 + sigma_q^2 with the SOURCE
+    particle's core, c = -rho^-3, d = 3 rho^-5), written out by hand."""
+    rng = np.random.default_rng(7)
+    cen = rng.uniform(-0.3, 0.3, (2, 3))
+    dir_ = rng.standard_normal((2, 3))
+    dir_ /= np.linalg.norm(dir_, axis=1)[:, None]
+    mag = np.array([0.7, 1.3])
+    rv = np.array([0.05, 0.11])
+    prm = FmmParams(box_length=2.0, origin=(-1.0, -1.0, -1.0), vortstretch=True,
+                    divergence_filtering=False, diffusion=False)
+    vel, st, _ = O.direct_particles(prm, cen, dir_, mag, rv)
+    al = mag[:, None] * dir_
+    for p, q in ((0, 1), (1, 0)):
+        r = cen[p] - cen[q]
+        rho2 = r @ r + rv[q] ** 2
+        c, d = -rho2 ** -1.5, 3.0 * rho2 ** -2.5
+        u = c * np.cross(r, al[q]) / (4 * np.pi)
+        v = np.cross(al[p], al[q])
+        s = -(c * v + d * r * (r @ v)) / (4 * np.pi)
+        assert rel(vel[p], u) < 1e-12
+        assert rel(st[p], s) < 1e-12
+
+
+def test_vortex_segment_analytic():
+    """A straight vortex segment (end vortex) at a point beside it: the
+    Biot-Savart law Gamma / (4 pi h) (cos t1 - cos t2) about the segment."""
+    L, gam = 0.8, 1.7
+    lines = abi.LineSet(np.array([[[0.0, 0.0, 0.0], [L, 0.0, 0.0]]]), np.array([gam]))
+    prm = FmmParams()
+    for a, h in ((0.3, 0.2), (-0.4, 0.5), (1.1, 0.35)):
+        pos = np.array([[a, h, 0.0]])
+        v = O.elements_vel(prm, pos, abi.elements_struct(end_vort=lines))[0]
+        r1, r2 = np.hypot(a, h), np.hypot(L - a, h)
+        mag_v = gam / (4 * np.pi * h) * (a / r1 + (L - a) / r2)
+        assert rel(v, np.array([0.0, 0.0, mag_v])) < 1e-12
+
+
+@pytest.mark.parametrize("kind", [abi.DUST_ELEM_VORTLATT, abi.DUST_ELEM_SURFPAN])
+def test_panel_velocity_far_near_consistency(kind):
+    """Just inside and just outside the far-field radius (10 x max edge) the
+    exact doublet/source formulas and the point dipole/source agree to the
+    expansion error (edge / r)^2."""
+    pan = abi.PanelSet(np.array([[[0, 0, 0], [0.1, 0, 0], [0.1, 0.1, 0], [0, 0.1, 0]]]),
+                       kind=np.array([kind]))
+    prm = FmmParams()
+    cen = np.array([0.05, 0.05, 0.0])
+    d = np.array([0.3, -0.2, 0.93])
+    d /= np.linalg.norm(d)
+    inside, outside = cen + 0.999 * d, cen + 1.001 * d
+    vd_in, vd_out = O.velocity_doublet(prm, pan, 0, inside), O.velocity_doublet(prm, pan, 0, outside)
+    assert rel(vd_in, vd_out) < 2e-2
+    if kind == abi.DUST_ELEM_SURFPAN:
+        vs_in, vs_out = O.velocity_source(prm, pan, 0, inside), O.velocity_source(prm, pan, 0, outside)
+        assert rel(vs_in, vs_out) < 2e-2
