@@ -5,15 +5,24 @@
 // swapped across the whole matrix, L unit lower, U upper, info = first
 // zero pivot.
 //
-// Panel factorisation: one cooperative launch of G CTAs; CTA g keeps rows
-// [g*R, (g+1)*R) of the panel in shared memory.  Per column there is a
-// single grid-wide barrier: before it every CTA publishes its local maximum
-// and that row, and the owner of the diagonal row publishes it; after it
-// every CTA selects the same pivot, performs its part of the swap from the
-// published rows and updates its rows.  Published buffers alternate between
-// two copies so a CTA one column ahead never overwrites data still read.
-// The barrier spins with an iteration limit and raises an error flag
-// instead of hanging.
+// Panel factorisation (64 columns), by the panel's height:
+//  * up to 2048 rows: one CTA (k_panel_1cta) holding 16- (FP32) or 8-column
+//    (FP64) sub-panels in registers, two CTA barriers per column;
+//  * taller panels that fit the shared memory of a cluster of 8 or 16 CTAs:
+//    k_panel_cluster, one cluster barrier per column, candidates exchanged
+//    through distributed shared memory;
+//  * otherwise one cooperative launch of G CTAs (k_panel): CTA g keeps rows
+//    [g*R, (g+1)*R) of the panel in shared memory, one grid-wide barrier per
+//    column (before it every CTA publishes its local maximum and that row,
+//    and the owner of the diagonal row publishes it; after it every CTA
+//    selects the same pivot, performs its part of the swap from the
+//    published rows and updates its rows).  Published buffers alternate
+//    between two copies so a CTA one column ahead never overwrites data
+//    still read.  The barrier spins with an iteration limit and raises an
+//    error flag instead of hanging.
+// The panel's row interchanges reach the other columns as one net
+// permutation per panel (k_laswp_net); trailing updates are GEMMs (cuBLAS,
+// or the tcgen05 TF32 kernel of gemm_tc.cu for FP32).
 #include <climits>
 
 #include <cooperative_groups.h>

@@ -2,9 +2,9 @@
 //
 // Blocked right-looking LU as LAPACK dgetrf (partial pivoting, first
 // maximum wins like idamax), used by solve_linsys's sequence
-// (src/linsys/mod_linsys.f90:352-482).  The panel is factored by one
-// cooperative kernel that keeps its rows in shared memory, one grid-wide
-// barrier per column; trailing updates are GEMMs.
+// (src/linsys/mod_linsys.f90:352-482).  Panels are factored by one CTA
+// (rows in registers), a thread-block cluster or a cooperative grid,
+// whichever the panel's height allows (lu.cu); trailing updates are GEMMs.
 #pragma once
 
 #include <cublas_v2.h>
