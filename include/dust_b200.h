@@ -327,8 +327,12 @@ DUST_API int dust_tc_gemm_tf32_minus(int m, int n, int k, const float *A, int ld
  * mod_linsys.f90:352-482).  A 3-layer, width-64 graph network over the
  * k-nearest-neighbour graph of the panel centres maps the current matrix to
  * a sparse approximate inverse M = (I + O) D^-1 (D = diag A, O on the graph's
- * edges) that right-preconditions the FP64 GMRES of DUST_SOLVE_GMRES_NN and
- * gives its warm start M b.  Untrained (output weights zero) M is Jacobi.
+ * edges).  DUST_SOLVE_GMRES_NN right-preconditions its FP64 GMRES with M, or,
+ * when the system has static rows, with the block lower-triangular operator
+ * that applies the FP32 inverse of the static block to the static part and M
+ * to the moving part (the static inverse is built once, on first use); the
+ * warm start is that operator applied to b.  Untrained (output weights zero)
+ * M is Jacobi.
  * Training runs on the GPU: the loss of a stored system is
  * ||M [A Z, b] - [Z, x]||_F^2 / (n C) over 7 random +-1 probe columns Z and
  * the solution x, minimised with Adam. */
