@@ -39,3 +39,23 @@ def test_reference_arm_two_ranks():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_roofline_fields():
+    """The roofline object of the bench line (dominant kernel: the FP32C
+    element far field) from a phase breakdown: achieved = algorithmic flops /
+    kernel time, frac = achieved / peak, traffic scaled by the particles."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from dust_b200 import synth
+    case = synth.FullStepCase(n_particles=10_000)
+    params = case.fmm_params()
+    ph = {"mixed": {"k_elem_far_ms": 2.0, "n_elem_pairs": 10_000 * 14_596, "k_m2l_tc_ms": 1.0,
+                    "n_m2l_pairs": 1000, "uvort": 1.5}}
+    rf = bench.roofline(ph, case, params, "mixed")
+    for k in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
+        assert k in rf
+    ach = bench.FLOP_ELEM_PAIR * 10_000 * 14_596 / 2e-3 / 1e12
+    assert abs(rf["achieved"] - ach) <= 0.01 and abs(rf["frac"] - ach / rf["peak"]) <= 1e-3
+    assert rf["unit"] == "TFLOP/s" and rf["traffic"] > 0
+    assert [o["kernel"] for o in rf["others"]][0] == "k_m2l_tc"
