@@ -52,6 +52,35 @@ class FmmParams(C.Structure):
     ]
 
 
+class UpdateParams(C.Structure):
+    """dust_update_params: the particles' Euler step of complete_wake."""
+    _fields_ = [
+        ("dt", C.c_double),
+        ("ndt_update_wake", C.c_int),
+        ("box_min", C.c_double * 3),
+        ("box_max", C.c_double * 3),
+        ("vortstretch", C.c_int),
+        ("diffusion", C.c_int),
+        ("divergence_filtering", C.c_int),
+        ("filt_eta", C.c_double),
+    ]
+
+
+def update_params(dt, box_min, box_max, ndt_update_wake=1, vortstretch=True, diffusion=True,
+                  divergence_filtering=False, filt_eta=0.0):
+    u = UpdateParams()
+    u.dt = float(dt)
+    u.ndt_update_wake = int(ndt_update_wake)
+    for d in range(3):
+        u.box_min[d] = float(box_min[d])
+        u.box_max[d] = float(box_max[d])
+    u.vortstretch = int(bool(vortstretch))
+    u.diffusion = int(bool(diffusion))
+    u.divergence_filtering = int(bool(divergence_filtering))
+    u.filt_eta = float(filt_eta)
+    return u
+
+
 class Panels(C.Structure):
     _fields_ = [
         ("n", C.c_int),

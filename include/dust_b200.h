@@ -371,13 +371,55 @@ DUST_API int dust_precond_train(dust_precond *p, int iters, float lr,
 /* Attaches p (NULL detaches) to the system for DUST_SOLVE_GMRES_NN. */
 DUST_API int dust_linsys_set_precond(dust_linsys *ls, dust_precond *p);
 
+/* ------------------------------------------------------ particle update */
+/* Parameters of the particles' explicit Euler step in complete_wake
+ * (src/aeroel/mod_wake.f90:1309-1355): dt and ndt_update_wake as
+ * sim_param%dt and %ndt_update_wake, the box as wake%part_box_min/max
+ * (particles_box_min/max), the switches as sim_param%use_vs, %use_vd and
+ * %use_divfilt, filt_eta as sim_param%filt_eta. */
+typedef struct dust_update_params {
+  double dt;
+  int    ndt_update_wake;
+  double box_min[3], box_max[3];
+  int    vortstretch;            /* use_vs                                    */
+  int    diffusion;              /* use_vd                                    */
+  int    divergence_filtering;   /* use_divfilt                               */
+  double filt_eta;
+} dust_update_params;
+
+/* The particle loop of complete_wake (src/aeroel/mod_wake.f90:1309-1355),
+ * penetration avoidance (use_pa, off by default, :1313-1318) excepted.
+ * Arrays as in dust_fmm_apply: cen, dir, vel, stretch, rotu (3, n), mag (n),
+ * free_flag (n; 0 = live, 1 = free slot).  For every live particle:
+ *   p = cen + vel dt ndt; if p is inside the box (bounds included):
+ *     cen = p, and with vortstretch or diffusion:
+ *       with divergence_filtering:
+ *         stretch -= filt_eta / ndt (dir mag - rotu mag / |rotu|)
+ *       alpha = dir mag + stretch dt ndt; dir = alpha / |alpha| if |alpha| != 0
+ *     (mag is left unchanged, as in the reference);
+ *   else free_flag = 1.
+ * *n_freed receives the number of particles set free (the reference
+ * decrements wake%n_prt by it).  Same operation order as the reference, no
+ * fused multiply-adds.  Host arrays; allocates device memory for the call. */
+DUST_API int dust_particles_update(const dust_update_params *u, int n, double *cen,
+                                   double *dir, const double *mag, const double *vel,
+                                   double *stretch, const double *rotu, int *free_flag,
+                                   int *n_freed);
+/* The same on device arrays (n_freed a device int, overwritten), queued on
+ * `stream` (NULL: the default stream), not synchronised; allocates nothing. */
+DUST_API int dust_particles_update_device(const dust_update_params *u, int n, double *cen,
+                                          double *dir, const double *mag, const double *vel,
+                                          double *stretch, const double *rotu,
+                                          int *free_flag, int *n_freed, void *stream);
+
 /* ---------------------------------------------------------------- misc */
 DUST_API const char *dust_status_string(int status);
 DUST_API const char *dust_last_error(void); /* text of the last CUDA error seen      */
 DUST_API int dust_device_ok(void);   /* DUST_OK if a usable sm_100 device is present */
 /* sizeof() of the ABI structs in declaration order (dust_fmm_params,
  * dust_panels, dust_lines, dust_elements, dust_fmm_stats, dust_solve_report,
- * dust_wake_rows), for binding checks; returns the number of sizes. */
+ * dust_wake_rows, dust_update_params), for binding checks; returns the
+ * number of sizes. */
 DUST_API int dust_abi_sizes(int64_t *out, int n);
 
 #ifdef __cplusplus

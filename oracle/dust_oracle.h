@@ -16,6 +16,7 @@
  *   src/aeroel/mod_vortlatt.f90  vortex-lattice rows
  *   src/aeroel/mod_vortline.f90  vortex line velocity
  *   src/linsys/mod_linsys.f90    static/moving block LU sequence
+ *   src/aeroel/mod_wake.f90      particle loop of complete_wake
  *
  * Parity pins: the reference is Fortran and cannot be compiled here (no
  * Fortran compiler, LAPACK or HDF5), and it has no unit-level golden vectors
@@ -99,6 +100,12 @@ void or_dtrsm_llnu(int m, int n, const double *A, int lda, double *B, int ldb);
 void or_dtrsm_runn(int m, int n, const double *A, int lda, double *B, int ldb);
 void or_dgemm_nn_minus(int m, int n, int k, const double *A, int lda,
                        const double *B, int ldb, double *C, int ldc);
+
+/* Particle loop of complete_wake (mod_wake.f90:1309-1355), arguments as
+ * dust_particles_update. */
+int or_particles_update(const dust_update_params *u, int n, double *cen, double *dir,
+                        const double *mag, const double *vel, double *stretch,
+                        const double *rotu, int *free_flag, int *n_freed);
 
 #ifdef __cplusplus
 }

@@ -38,6 +38,7 @@ def lib():
         L.or_dgetrf.restype = C.c_int
         L.or_linsys_run.restype = C.c_int
         L.or_last_tree_flags.restype = C.c_int
+        L.or_particles_update.restype = C.c_int
     return _lib
 
 
@@ -178,3 +179,21 @@ def linsys_run(prm, rank, nstatic, elems_init, elems_step, wake_init, wake_step)
     if rc != 0:
         raise RuntimeError(f"oracle linsys status {rc}")
     return A.reshape(rank, rank).T.copy(), b, res
+
+
+def particles_update(u, cen, dir_, mag, vel, stretch, rotu, free):
+    """complete_wake's particle loop on copies; returns (cen, dir, stretch,
+    free, n_freed)."""
+    cen, dir_, stretch = (np.array(abi.f64(a), dtype=np.float64, order="C")
+                          for a in (cen, dir_, stretch))
+    mag, vel, rotu = abi.f64(mag), abi.f64(vel), abi.f64(rotu)
+    free = np.array(free, dtype=np.int32, order="C")
+    nf = C.c_int(0)
+    rc = lib().or_particles_update(C.byref(u), mag.shape[0], abi.dptr(cen), abi.dptr(dir_),
+                                   abi.dptr(mag), abi.dptr(vel), abi.dptr(stretch),
+                                   abi.dptr(rotu), free.ctypes.data_as(C.POINTER(C.c_int)),
+                                   C.byref(nf))
+    if rc != 0:
+        raise RuntimeError(f"oracle particles_update status {rc}")
+    return cen, dir_, stretch, free, nf.value
+

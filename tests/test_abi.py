@@ -25,7 +25,8 @@ def test_struct_sizes_match_header():
     sizes = (C.c_int64 * 16)()
     n = L.dust_abi_sizes(sizes, 16)
     mine = [C.sizeof(t) for t in (abi.FmmParams, abi.Panels, abi.Lines, abi.Elements,
-                                   abi.FmmStats, abi.SolveReport, abi.WakeRows)]
+                                   abi.FmmStats, abi.SolveReport, abi.WakeRows,
+                                   abi.UpdateParams)]
     assert n == len(mine)
     assert list(sizes)[:n] == mine
 
