@@ -235,3 +235,65 @@ def test_oracle_particles_update_matches_numpy(vs, vd, df, ndt):
         assert np.array_equal(g, r)
     assert got[4] == ref[4] > 0
     assert np.array_equal(got[1][1], dir_[1]) or not (vs or vd)
+
+
+def _segment_4pi(v0, v1, p):
+    """4 pi x the velocity of a unit-circulation straight segment v0 -> v1 at
+    p (Biot-Savart, no core)."""
+    e = v1 - v0
+    L = np.linalg.norm(e)
+    e = e / L
+    a = p - v0
+    ai = a @ e
+    h = np.linalg.norm(a - ai * e)
+    r1, r2 = np.linalg.norm(p - v0), np.linalg.norm(p - v1)
+    mag = (ai / r1 + (L - ai) / r2) / h
+    return mag * np.cross(e, a) / np.linalg.norm(np.cross(e, a))
+
+
+def test_doublet_velocity_equals_vortex_ring():
+    """A constant-strength doublet panel induces the velocity of the vortex
+    ring along its edges: inside the far-field radius the oracle's
+    velocity_calc_doublet equals the sum of the four straight-segment laws
+    (points away from the edges' cores)."""
+    rng = np.random.default_rng(11)
+    ver = np.array([[0.0, 0.0, 0.0], [0.3, 0.02, 0.01], [0.32, 0.25, -0.02], [0.01, 0.22, 0.0]])
+    pan = abi.PanelSet(ver[None], kind=np.array([abi.DUST_ELEM_VORTLATT]))
+    prm = FmmParams()
+    for _ in range(20):
+        pos = ver.mean(axis=0) + rng.uniform(-0.8, 0.8, 3)
+        if np.linalg.norm(pos - ver.mean(axis=0)) > 2.5:
+            continue
+        v = O.velocity_doublet(prm, pan, 0, pos)
+        ring = sum(_segment_4pi(ver[i], ver[(i + 1) % 4], pos) for i in range(4))
+        assert rel(v, ring) < 1e-12
+
+
+def _solid_angle_tri(a, b, c):
+    """Van Oosterom-Strackee solid angle of triangle (a, b, c) seen from the
+    origin."""
+    na, nb, nc = np.linalg.norm(a), np.linalg.norm(b), np.linalg.norm(c)
+    num = a @ np.cross(b, c)
+    den = na * nb * nc + (a @ b) * nc + (a @ c) * nb + (b @ c) * na
+    return 2.0 * np.arctan2(num, den)
+
+
+def test_doublet_potential_is_solid_angle():
+    """potential_calc_doublet inside the far-field radius is the solid angle
+    the panel subtends (an independent formula: Van Oosterom-Strackee on the
+    two triangles of the planar quad), with the reference's sign."""
+    rng = np.random.default_rng(12)
+    ver = np.array([[0.0, 0.0, 0.0], [0.3, 0.0, 0.0], [0.35, 0.25, 0.0], [0.02, 0.22, 0.0]])
+    pan = abi.PanelSet(ver[None], kind=np.array([abi.DUST_ELEM_SURFPAN]))
+    prm = FmmParams()
+    signs = set()
+    for _ in range(20):
+        pos = ver.mean(axis=0) + rng.uniform(-0.8, 0.8, 3)
+        pos[2] = np.sign(pos[2]) * max(abs(pos[2]), 0.05)
+        rel_v = ver - pos
+        om = _solid_angle_tri(rel_v[0], rel_v[1], rel_v[2]) + \
+            _solid_angle_tri(rel_v[0], rel_v[2], rel_v[3])
+        dou = O.potential_doublet(prm, pan, 0, pos)
+        assert min(abs(dou - om), abs(dou + om)) < 1e-12
+        signs.add(np.sign(dou * om))
+    assert len(signs) == 1  # one fixed sign convention
