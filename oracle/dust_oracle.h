@@ -22,8 +22,12 @@
  * Fortran compiler, LAPACK or HDF5), and it has no unit-level golden vectors
  * for this path.  The LU sequence is pinned against LAPACK itself (the
  * reference's third-party solver) through scipy; the FMM and the influence
- * kernels are pinned only by analytic known answers (solid-angle sums,
- * FMM -> direct-sum convergence).  Parity of those parts is "unpinned".
+ * kernels are pinned only by analytic known answers and independent
+ * formulas (solid-angle sums and the Van Oosterom-Strackee solid angle,
+ * vortex-ring and straight-segment Biot-Savart laws, quadrature of the
+ * source potential, the particle-pair kernel, FMM -> direct-sum
+ * convergence).  Parity of those parts against the reference's own outputs
+ * is "unpinned".
  */
 #ifndef DUST_ORACLE_H
 #define DUST_ORACLE_H

@@ -297,3 +297,30 @@ def test_doublet_potential_is_solid_angle():
         assert min(abs(dou - om), abs(dou + om)) < 1e-12
         signs.add(np.sign(dou * om))
     assert len(signs) == 1  # one fixed sign convention
+
+
+def test_source_potential_equals_quadrature():
+    """potential_calc_sou_surfpan inside the far-field radius is the integral
+    of 1/r over the flat panel (Hess-Smith closed form): checked against
+    Gauss-Legendre quadrature on the bilinear map of the quad."""
+    ver = np.array([[0.0, 0.0, 0.0], [0.3, 0.0, 0.0], [0.35, 0.25, 0.0], [0.02, 0.22, 0.0]])
+    pan = abi.PanelSet(ver[None], kind=np.array([abi.DUST_ELEM_SURFPAN]))
+    prm = FmmParams()
+    x, w = np.polynomial.legendre.leggauss(60)
+    s, t = (x + 1) / 2, w / 2
+    S, T = np.meshgrid(s, s, indexing="ij")
+    W = np.outer(t, t)
+    # bilinear map q(s, t) and its Jacobian |q_s x q_t|
+    q = ((1 - S) * (1 - T))[..., None] * ver[0] + (S * (1 - T))[..., None] * ver[1] + \
+        (S * T)[..., None] * ver[2] + ((1 - S) * T)[..., None] * ver[3]
+    qs = (1 - T)[..., None] * (ver[1] - ver[0]) + T[..., None] * (ver[2] - ver[3])
+    qt = (1 - S)[..., None] * (ver[3] - ver[0]) + S[..., None] * (ver[2] - ver[1])
+    jac = np.linalg.norm(np.cross(qs, qt), axis=-1)
+    rng = np.random.default_rng(13)
+    for _ in range(10):
+        pos = ver.mean(axis=0) + rng.uniform(-0.5, 0.5, 3)
+        pos[2] = np.sign(pos[2]) * max(abs(pos[2]), 0.15)
+        quad = np.sum(W * jac / np.linalg.norm(q - pos, axis=-1))
+        dou = O.potential_doublet(prm, pan, 0, pos)
+        sou = O.potential_source(prm, pan, 0, dou, pos)
+        assert abs(sou - quad) < 1e-9 * abs(quad)
