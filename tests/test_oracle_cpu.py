@@ -324,3 +324,32 @@ def test_source_potential_equals_quadrature():
         dou = O.potential_doublet(prm, pan, 0, pos)
         sou = O.potential_source(prm, pan, 0, dou, pos)
         assert abs(sou - quad) < 1e-9 * abs(quad)
+
+
+def test_panel_velocities_are_potential_gradients():
+    """Inside the far-field radius the doublet and source velocities are the
+    gradients of the corresponding potentials (central differences, one sign
+    convention each)."""
+    ver = np.array([[0.0, 0.0, 0.0], [0.3, 0.0, 0.0], [0.35, 0.25, 0.0], [0.02, 0.22, 0.0]])
+    pan = abi.PanelSet(ver[None], kind=np.array([abi.DUST_ELEM_SURFPAN]))
+    prm = FmmParams()
+    rng = np.random.default_rng(14)
+    h = 1e-5
+    sd, ss = set(), set()
+    for _ in range(10):
+        pos = ver.mean(axis=0) + rng.uniform(-0.5, 0.5, 3)
+        pos[2] = np.sign(pos[2]) * max(abs(pos[2]), 0.1)
+        gd, gs = np.zeros(3), np.zeros(3)
+        for k in range(3):
+            e = np.zeros(3)
+            e[k] = h
+            dp, dm = O.potential_doublet(prm, pan, 0, pos + e), O.potential_doublet(prm, pan, 0, pos - e)
+            gd[k] = (dp - dm) / (2 * h)
+            gs[k] = (O.potential_source(prm, pan, 0, dp, pos + e) -
+                     O.potential_source(prm, pan, 0, dm, pos - e)) / (2 * h)
+        vd, vs = O.velocity_doublet(prm, pan, 0, pos), O.velocity_source(prm, pan, 0, pos)
+        for v, g, signs in ((vd, gd, sd), (vs, gs, ss)):
+            sg = 1.0 if np.linalg.norm(v - g) < np.linalg.norm(v + g) else -1.0
+            assert rel(v, sg * g) < 1e-6
+            signs.add(sg)
+    assert len(sd) == 1 and len(ss) == 1
