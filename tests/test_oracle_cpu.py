@@ -353,3 +353,34 @@ def test_panel_velocities_are_potential_gradients():
             assert rel(v, sg * g) < 1e-6
             signs.add(sg)
     assert len(sd) == 1 and len(ss) == 1
+
+
+def test_vortex_particle_pair_curl_and_diffusion():
+    """The divergence-filter curl (-2 c alpha_q + d r x (r x alpha_q)) and the
+    PSE diffusion term ((vol alpha_q - vol alpha_p) / sigma^2 eta(r, sigma)
+    (nu), eta = 105 / (8 pi) / ((r / sigma)^2 + 1)^(9/2) / sigma^3, both with
+    the source particle's core) of two particles, written out by hand."""
+    rng = np.random.default_rng(9)
+    cen = rng.uniform(-0.3, 0.3, (2, 3))
+    dir_ = rng.standard_normal((2, 3))
+    dir_ /= np.linalg.norm(dir_, axis=1)[:, None]
+    mag = np.array([0.9, 0.4])
+    rv = np.array([0.07, 0.13])
+    nu = 2.5e-3
+    prm = FmmParams(box_length=2.0, origin=(-1.0, -1.0, -1.0), vortstretch=True,
+                    divergence_filtering=True, diffusion=True, nu_inf=nu)
+    vel, st, ro = O.direct_particles(prm, cen, dir_, mag, rv)
+    al = mag[:, None] * dir_
+    for p, q in ((0, 1), (1, 0)):
+        r = cen[p] - cen[q]
+        rn = np.linalg.norm(r)
+        rho2 = rn * rn + rv[q] ** 2
+        c, d = -rho2 ** -1.5, 3.0 * rho2 ** -2.5
+        v = np.cross(al[p], al[q])
+        s = -(c * v + d * r * (r @ v)) / (4 * np.pi)
+        rot = (-2.0 * c * al[q] + d * np.cross(r, np.cross(r, al[q]))) / (4 * np.pi)
+        vol = 4.0 / 3.0 * np.pi * rv[q] ** 3
+        eta = 105.0 / (8.0 * np.pi) / ((rn / rv[q]) ** 2 + 1) ** 4.5 / rv[q] ** 3
+        diff = (vol * al[q] - vol * al[p]) / rv[q] ** 2 * eta
+        assert rel(ro[p], rot) < 1e-12
+        assert rel(st[p], s + diff * nu) < 1e-12
