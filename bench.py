@@ -55,6 +55,12 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=400)
     ap.add_argument("--profile-step", action="store_true",
                     help="run warm-up + one step only (for ncu launch lists)")
+    ap.add_argument("--workload", default="full", choices=["full", "fmm", "dense"],
+                    help="full: the full-step line (with the fmm and dense workloads as "
+                         "sub-objects); fmm / dense: that workload's own line")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="full step only, without the fmm / dense sub-objects")
+    ap.add_argument("--degrees", default="4,6,8", help="FMM degrees of the fmm workload")
     return ap.parse_args()
 
 
@@ -155,8 +161,8 @@ def workload(case, degree):
 def make_case(args):
     from dust_b200 import synth
     if args.quick:
-        return synth.FullStepCase(n_particles=200_000, wing_span=20, wing_around=40,
-                                  n_span_blade=10, n_chord_blade=4)
+        return synth.FullStepCase(n_particles=min(200_000, args.particles), wing_span=20,
+                                  wing_around=40, n_span_blade=10, n_chord_blade=4)
     return synth.FullStepCase(n_particles=args.particles)
 
 
@@ -174,86 +180,138 @@ def time_steps(stepper, steps, flush):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def cpu_baseline(case, params, budget_s=20.0):
-    """The oracle (C restatement of the reference, OpenMP on all host cores)
-    on a bounded sample of one step, scaled to a full step."""
+def host_cores():
+    """Physical host cores (the CPU baseline's thread count)."""
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def cpu_baseline(case, params, m2l_pairs, fmm_stride=32, uvort_stride=64):
+    """The reference's step on the host cores (the oracle's C loops with
+    OpenMP and LAPACK/BLAS through scipy, oracle/cpu_step.py) on a bounded
+    sample of the full-step workload, scaled to one step phase by phase by
+    the exact ratio of work:
+
+    * uvort: every `uvort_stride`-th collocation point (all particles and end
+      vortices), scaled by the point count;
+    * assembly: 8 moving rows over all columns through the oracle's row
+      builder, scaled by the entries a step rebuilds
+      (nstatic x nmoving + nmoving x rank);
+    * solve: the reference's LAPACK sequence (dlaswp, dtrsm x 2, dgemm,
+      dgetrf, dlaswp, dgetrs) on blocks of the full sizes, timed in full
+      (its time does not depend on the values);
+    * FMM: tree, P2M, M2M and L2L in full; M2L for every `fmm_stride`-th
+      target cell scaled by the M2L pair count; L2P + P2P + element sums for
+      every `fmm_stride`-th leaf scaled by the particle count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu_step
     import oracle as O
     from dust_b200 import abi
-    rng = np.random.default_rng(0)
+    cores = host_cores()
+    cpu_step.set_threads(cores)
     n = case.mag.shape[0]
-    cen_el = case.elems.ver.mean(axis=1)
-    tri = case.elems.n_ver == 3
-    cen_el[tri] = case.elems.ver[tri, :3].mean(axis=1)
     parts = {}
-    # (1) uvort: sample of collocation points, all particles
-    ns = 24
-    idx = rng.choice(case.rank, ns, replace=False)
+    cen_el = np.where(case.elems.n_ver[:, None] == 4, case.elems.ver.mean(axis=1),
+                      case.elems.ver[:, :3].mean(axis=1))
+    # (1) uvort
+    pts = np.ascontiguousarray(cen_el[::uvort_stride])
     t = time.perf_counter()
-    O.points_uvort(params, cen_el[idx], case.cen, case.dir, case.mag, case.r_vortex,
-                   case.end_vort)
-    parts["uvort"] = (time.perf_counter() - t) * case.rank / ns
-    # (2) element -> particle sums: sample of particles, all elements
-    npart = 400
-    pid = rng.choice(n, npart, replace=False)
+    O.points_uvort(params, pts, case.cen, case.dir, case.mag, case.r_vortex, case.end_vort)
+    parts["uvort"] = (time.perf_counter() - t) * case.rank / len(pts)
+    # (2) assembly: moving rows
+    nst, rank = case.nstatic, case.rank
+    nmv = rank - nst
+    rows = np.arange(nst, rank, max(1, nmv // 8))[:8]
+    t = time.perf_counter()
+    O.linsys_rows(params, case.elems, rows, (case.wake, case.n_impl, case.impl_ind))
+    per_entry = (time.perf_counter() - t) / (len(rows) * rank)
+    parts["assemble"] = per_entry * (nst * nmv + nmv * rank)
+    # (3) solve: LAPACK sequence at the full sizes on a well-conditioned
+    # stand-in (an LU of the static block as the reference keeps it)
+    rng = np.random.default_rng(0)
+    A = np.asfortranarray(rng.standard_normal((rank, rank)) * (1.0 / rank))
+    A[np.arange(rank), np.arange(rank)] += 1.0
+    P = np.arange(rank, dtype=np.int32)
+    t = time.perf_counter()
+    cpu_step.solve_linsys_lapack(A, P, nst, np.ones(rank))
+    parts["solve"] = time.perf_counter() - t
+    del A
+    # (4) FMM with the element sums
     els = abi.elements_struct(case.elems, case.wake, case.end_vort)
-    t = time.perf_counter()
-    O.elements_vel(params, case.cen[pid], els)
-    parts["elements"] = (time.perf_counter() - t) * n / npart
-    # (3) FMM tree + multipoles + near field on a 1/20 particle subsample
-    sub = rng.choice(n, n // 20, replace=False)
-    t = time.perf_counter()
-    O.fmm_apply(params, case.cen[sub], case.dir[sub], case.mag[sub], case.r_vortex[sub])
-    parts["fmm"] = (time.perf_counter() - t) * 20
-    # (4) assembly + Schur LU per step: a reduced system, scaled by flop count
-    m = min(1200, case.nstatic)
-    nmv_s = min(160, case.rank - case.nstatic)
-    sl = np.arange(m)
-    sub_el = case.elems.subset(np.concatenate([sl, np.arange(case.nstatic,
-                                                             case.nstatic + nmv_s)]))
-    nst_s = m
-    t = time.perf_counter()
-    O.linsys_run(params, sub_el.n, nst_s, sub_el, sub_el, (abi.empty_panels(), 0, None),
-                 (abi.empty_panels(), 0, None))
-    t_small = time.perf_counter() - t
-    # per-step flops: trsm x2 (nst^2 nmv each) + gemm (2 nmv^2 nst) + getrf(nmv)
-    def step_flops(nst, nmv):
-        return 2 * nst * nst * nmv + 2 * nmv * nmv * nst + 2 / 3 * nmv ** 3
-    # the sample also paid its static LU (2/3 nst^3); scale by total flops
-    fl_small = 2 / 3 * nst_s ** 3 + step_flops(nst_s, nmv_s)
-    parts["linsys"] = t_small * step_flops(case.nstatic, case.rank - case.nstatic) / fl_small
+    O.set_sample_stride(fmm_stride)
+    try:
+        O.fmm_apply(params, case.cen, case.dir, case.mag, case.r_vortex, els)
+        (t_tree, t_up, t_m2l, t_app), (m2l_s, npart_s) = O.last_fmm_times()
+    finally:
+        O.set_sample_stride(1)
+    parts["fmm"] = (t_tree + t_up + t_m2l * m2l_pairs / max(m2l_s, 1)
+                    + t_app * n / max(npart_s, 1))
     total_ms = 1e3 * sum(parts.values())
-    return total_ms, {k: round(v * 1e3, 1) for k, v in parts.items()}
+    sample = ("bounded sample scaled to one step per phase by the exact work ratio: uvort at "
+              "1/%d of the collocation points; assembly from 8 moving rows (per entry); "
+              "LAPACK solve in full; FMM tree/P2M/M2M/L2L in full, M2L at 1/%d of the target "
+              "cells (by pair count), L2P+P2P+elements at 1/%d of the leaves (by particle "
+              "count); phase s: %s" % (uvort_stride, fmm_stride, fmm_stride,
+                                       json.dumps({k: round(v, 2) for k, v in parts.items()})))
+    return total_ms, cores, sample
 
 
 def run_reference(args, rank, ws):
-    """--impl reference: the reference's algorithm on the host cores."""
+    """--impl reference: whole steps of the reference's algorithm on the host
+    cores (the oracle's C loops with OpenMP + LAPACK/BLAS, oracle/cpu_step.py),
+    timed in full.  initialize_linsys (static rows + static LU) runs once
+    before the timed steps.  A step of the full-size workload takes minutes
+    on the host, so the arm runs one whole step (``steps`` reports the steps
+    that ran)."""
     if rank != 0:
         return
-    from dust_b200 import synth
-    case = synth.FullStepCase(n_particles=args.particles) if not args.quick else make_case(args)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu_step
+    case = make_case(args)
     params = case.fmm_params(degree=args.degree)
-    vals = []
-    # each step is a bounded sample (about 20 s of host work); at most 2
-    for _ in range(max(1, min(args.steps, 2))):
-        ms, parts = cpu_baseline(case, params)
-        vals.append(ms)
-    cores = os.cpu_count()
-    v = float(np.median(vals))
+    cores = host_cores()
+    cpu_step.set_threads(cores)
+    t0 = time.perf_counter()
+    cs = cpu_step.CpuStep(case, params)
+    t_init = time.perf_counter() - t0
+    nsteps = 1 if not args.quick else max(1, min(args.steps, 2))
+    times, phases = [], []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        ph = cs.step()
+        times.append((time.perf_counter() - t0) * 1e3)
+        phases.append({k: round(v * 1e3, 1) for k, v in ph.items()})
+    v = float(np.mean(times))
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
-            "n_gpus": args.gpus, "steps": len(vals), "warmup": 0, "ms_per_step": round(v, 1),
+            "n_gpus": args.gpus, "steps": nsteps, "warmup": 0, "ms_per_step": round(v, 1),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64",
-            "data": "synthetic (seeded FullStepCase)",
-            "config": {"workload": workload(case, args.degree), "mode": "reference (FP64 CPU)",
-                       "levels": params.n_octree_levels,
-                       "parallelism": "rank 0 only" if ws > 1 else "host cores"},
-            "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": cores, "kind": "port",
-                             "sample": "per-phase samples scaled to one step: " +
-                             json.dumps(parts)},
+            "dtype": "f64", "data": "synthetic (seeded FullStepCase)",
+            "config": config_of(case, args, params),
+            "mode": "reference algorithm on the host cores (FP64)",
+            "phases_ms": phases, "init_s": round(t_init, 1),
+            "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": cores,
+                             "kind": "port",
+                             "sample": "%d whole step(s), timed in full, after "
+                                       "initialize_linsys (%.1f s, untimed); oracle C loops "
+                                       "(OpenMP, %d threads) + OpenBLAS LAPACK/BLAS"
+                                       % (nsteps, t_init, cores)},
             "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config_of(case, args, params):
+    """The workload description both arms print (identical dicts)."""
+    return {"workload": workload(case, args.degree), "levels": params.n_octree_levels,
+            "l2": "256 MB flush between timed steps; A is %.2f GB"
+                  % (case.rank * case.rank * 8 / 1e9),
+            "parallelism": "single GPU or host; replicas under torchrun"}
 
 
 def main():
@@ -261,6 +319,14 @@ def main():
     rank, ws, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, rank, ws)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.workload != "full":
+        line = workload_line(args, ws, args.workload)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
         if ws > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -333,11 +399,17 @@ def main():
                       learned["precond"] if best == "learned" else None)
     cpu = None
     if not args.no_cpu and rank == 0 and ws == 1:
-        ms_cpu, parts = cpu_baseline(case, params)
-        cpu = {"value": round(ms_cpu, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
-               "sample": "oracle per-phase samples scaled to one step: " + json.dumps(parts)}
+        ms_cpu, cores, sample = cpu_baseline(case, params, ph[best]["n_m2l_pairs"])
+        cpu = {"value": round(ms_cpu, 1), "unit": "ms", "cores": cores, "kind": "port",
+               "sample": sample}
     launches = count_launches(steppers[best])
     rf = roofline(ph, case, params, best)
+    subs = None
+    if not args.no_workloads and not args.quick:
+        # the other named workloads at their full sizes, 5 timed calls each
+        # after 3 warm-ups (time per call, not per step)
+        subs = {"fmm": run_fmm_workload(5, 3, flush=flush),
+                "dense": run_dense_workload(5, 3, flush=flush)}
     if rank == 0:
         r = results[best]
         line = {
@@ -346,10 +418,8 @@ def main():
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
             "data": "synthetic (seeded FullStepCase)",
-            "config": {"workload": workload(case, args.degree),
-                       "mode": best, "levels": params.n_octree_levels,
-                       "l2": "256 MB flush between timed steps; A is 1.55 GB",
-                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "config": config_of(case, args, params),
+            "mode": best,
             "plain_fp64_ms": round(results["plain"]["ms"], 3),
             "speedup_vs_plain_fp64": round(results["plain"]["ms"] / r["ms"], 3),
             "load_error_vs_fp64": load_err[best],
@@ -363,11 +433,259 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
+            "workloads": subs,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _peaks():
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(pk)) if os.path.exists(pk) else {}
+    mhz = peaks.get("sm_max_mhz", 1965.0)
+    return {
+        "hbm_gbs": peaks.get("hbm_gbs", 6650.0),
+        "bf16": peaks.get("bf16_tflops", 1590.0),
+        "fp32": 148 * 128 * 2 * mhz * 1e6 / 1e12,
+        "fp64": 148 * 64 * 2 * mhz * 1e6 / 1e12,
+        "src": "of measured" if peaks else "of fallback",
+        "mhz": mhz,
+    }
+
+
+def _event_times(fn, reps, flush):
+    """CUDA-event times (ms) of `reps` calls of fn on the current stream, with
+    a 256 MB write between calls (L2 holds nothing of the previous one)."""
+    import torch
+    out = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def nmon(p):
+    return (p + 1) * (p + 2) * (p + 3) // 6
+
+
+# P2P flops per particle pair with stretching, divergence-filter curl and PSE
+# diffusion on (the reference defaults): 27 + 30 + 18 + 20
+FLOP_P2P_PAIR = 95
+
+
+def run_fmm_workload(reps, warm, degrees=(4, 6, 8), n_truth=32768, flush=None):
+    """Standalone wake FMM: 1M ring + 100k background particles, velocity,
+    stretching, div-filter curl and PSE diffusion in FP64 and FP32C at each
+    degree; errors against the FP64 direct sum at a seeded 32k-particle
+    subset (all 1.1M sources); M2L roofline in HBM GB/s (source a, target b
+    read and write, stretching c: 27 n_mon(p) words per pair) and P2P in
+    FLOP/s (95 per pair)."""
+    import torch
+    from dust_b200 import octree as OCT
+    from dust_b200 import synth
+    pk = _peaks()
+    case = synth.RingCase()
+    case = case.permuted(case.truth_order(n_truth))
+    n = case.n
+    dev = torch.device("cuda")
+    T = lambda a: torch.as_tensor(a, device=dev)
+    cen, dir_, mag, rv = T(case.cen), T(case.dir), T(case.mag), T(case.r_vortex)
+    vel, st, ro = (torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(3))
+    if flush is None:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    t0 = time.perf_counter()
+    tv, ts, _ = OCT.direct_particles(case.fmm_params(4), case.cen, case.dir, case.mag,
+                                     case.r_vortex, n_tgt=n_truth)
+    t_direct = time.perf_counter() - t0
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    stream = torch.cuda.current_stream().cuda_stream
+    out = {}
+    for p in degrees:
+        full64 = None
+        for name, prec in (("fp64", 0), ("fp32c", 1)):
+            prm = case.fmm_params(p, prec)
+            oc = OCT.Octree(prm)
+            call = lambda: oc.apply_multipole_device(cen, dir_, mag, rv, vel, st, ro,
+                                                     stream=stream, sync=False)
+            for _ in range(warm):
+                call()
+            torch.cuda.synchronize()
+            times = _event_times(call, reps, flush)
+            oc.set_timing(True)
+            call()
+            torch.cuda.synchronize()
+            sx = oc.stats()
+            oc.set_timing(False)
+            v, s_ = vel.cpu().numpy(), st.cpu().numpy()
+            r = {"ms": round(float(np.mean(times)), 3), "ms_min": round(min(times), 3),
+                 "error_vs_direct_fp64": {"vel": rel(v[:n_truth], tv),
+                                          "stretch": rel(s_[:n_truth], ts)},
+                 "phases_ms": {k: round(sx[k], 3) for k in
+                               ("ms_tree", "ms_upward", "ms_m2l", "ms_p2p", "ms_total",
+                                "ms_m2l_kernel")},
+                 "n_leaves": sx["n_leaves"], "n_m2l_pairs": sx["n_m2l_pairs"],
+                 "n_p2p_pairs": sx["n_p2p_pairs"]}
+            if full64 is None:
+                full64 = (v.copy(), s_.copy())
+            else:
+                r["error_vs_fmm_fp64"] = {"vel": rel(v, full64[0]),
+                                          "stretch": rel(s_, full64[1])}
+            w = 8 if prec == 0 else 4
+            m2l_ms = sx["ms_m2l"]
+            byts = 27 * nmon(p) * w * sx["n_m2l_pairs"]
+            flo = 12 * nmon(p + 1) * nmon(p) * sx["n_m2l_pairs"]
+            p2p_peak = pk["fp64"] if prec == 0 else pk["fp32"]
+            p2p_ach = FLOP_P2P_PAIR * sx["n_p2p_pairs"] / (sx["ms_p2p"] * 1e-3) / 1e12
+            r["roofline"] = {
+                "m2l": {"bound": "hbm", "achieved": round(byts / (m2l_ms * 1e-3) / 1e9, 1),
+                        "peak": pk["hbm_gbs"], "unit": "GB/s",
+                        "frac": round(byts / (m2l_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 3),
+                        "tflops": round(flo / (m2l_ms * 1e-3) / 1e12, 2),
+                        "algorithmic_bytes": int(byts), "ms": round(m2l_ms, 3),
+                        "peak_source": "HBM copy " + pk["src"]},
+                "p2p": {"bound": "fp64" if prec == 0 else "fp32", "achieved": round(p2p_ach, 2),
+                        "peak": round(p2p_peak, 1), "unit": "TFLOP/s",
+                        "frac": round(p2p_ach / p2p_peak, 3), "flop_per_pair": FLOP_P2P_PAIR,
+                        "ms": round(sx["ms_p2p"], 3),
+                        "peak_source": "nominal %s SIMT (148 SMs x %d lanes x 2 x %g MHz)"
+                                       % ("FP64" if prec == 0 else "FP32",
+                                          64 if prec == 0 else 128, pk["mhz"])}}
+            out["p%d_%s" % (p, name)] = r
+            oc.close()
+    return {"workload": "standalone wake FMM: 1,000,000 ring + 100,000 background particles, "
+                        "core 0.02, %d levels (leaves <= 64), vel + stretching + div-filter "
+                        "curl + PSE" % case.levels,
+            "unit": "ms per FMM evaluation", "reps": reps, "warmup": warm,
+            "truth": "FP64 direct sum (GPU) at %d seeded targets over all %d sources, %.1f s"
+                     % (n_truth, n, t_direct),
+            "l2": "256 MB flush between timed calls", "results": out}
+
+
+def run_dense_workload(reps, warm, n_target=16384, nrhs=64, flush=None):
+    """Mixed-precision dense solve: 16,384-panel ellipsoid, Dirichlet AIC, 64
+    right-hand sides; plain FP64 LU against the FP32 LU with tensor-core
+    (tcgen05 TF32) trailing updates + FP64 refinement to 1e-12."""
+    import torch
+    from dust_b200 import abi, linsys, synth
+    pk = _peaks()
+    case = synth.EllipsoidCase(n_target=n_target, nrhs=nrhs)
+    n = case.n
+    prm = case.fmm_params()
+    body = case.body
+    body.uvort = np.zeros((n, 3))
+    ls = linsys.Linsys(prm, n, 0, body)
+    G = np.empty((n, 3))
+    t_asm = []
+    for d in range(3):
+        body.ub = case.unit_ub(d)
+        t0 = time.perf_counter()
+        ls.assemble_linsys(body)
+        ls.sync()
+        t_asm.append((time.perf_counter() - t0) * 1e3)
+        A, b = ls.get_system()
+        G[:, d] = b
+    ls.close()
+    B = -G @ case.U
+    dev = torch.device("cuda")
+    Ad = torch.as_tensor(np.ascontiguousarray(A.T), device=dev)  # column-major A
+    del A
+    Bd = torch.as_tensor(np.ascontiguousarray(B.T), device=dev)
+    X64 = torch.empty_like(Bd)
+    X32 = torch.empty_like(Bd)
+    if flush is None:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for name, mode, X in (("lu64", abi.DUST_SOLVE_LU64, X64), ("mixed", abi.DUST_SOLVE_MIXED, X32)):
+        reps_ = []
+        call = lambda: reps_.append(linsys.dense_solve_device(Ad, Bd, X, mode, 1e-12, stream))
+        for _ in range(warm):
+            call()
+        times = _event_times(call, reps, flush)
+        rep = reps_[-1]
+        res[name] = {"ms": round(float(np.mean(times)), 3), "ms_min": round(min(times), 3),
+                     "report": rep}
+    # backward errors ||B - A X||_inf / (||A||_inf ||X||_inf) per column (FP64 on the GPU)
+    Anorm = float(Ad.abs().sum(dim=0).max())  # rows of A are columns of Ad
+    def berr(X):
+        R = Bd - X @ Ad  # (nrhs, n): row c = (A x_c)^T
+        return float((R.abs().amax(dim=1) / (Anorm * X.abs().amax(dim=1))).max())
+    for name, X in (("lu64", X64), ("mixed", X32)):
+        res[name]["backward_error"] = berr(X)
+    res["mixed"]["rel_error_vs_lu64"] = float(torch.linalg.norm(X32 - X64) / torch.linalg.norm(X64))
+    flops_lu = 2.0 / 3.0 * n ** 3
+    flops_tot = flops_lu + 2.0 * n * n * nrhs
+    tf32 = pk["bf16"] / 2
+    f = res["mixed"]["report"]["ms_factor"]
+    res["mixed"]["roofline"] = {
+        "bound": "tensor", "achieved": round(flops_lu / (f * 1e-3) / 1e12, 1), "peak": tf32,
+        "unit": "TFLOP/s", "frac": round(flops_lu / (f * 1e-3) / 1e12 / tf32, 3),
+        "what": "FP32 LU (TF32 tcgen05 trailing updates), (2/3) n^3 over ms_factor",
+        "peak_source": "TF32 = bf16 %s / 2" % pk["src"]}
+    f64 = res["lu64"]["report"]["ms_factor"]
+    res["lu64"]["roofline"] = {
+        "bound": "fp64", "achieved": round(flops_lu / (f64 * 1e-3) / 1e12, 2),
+        "peak": round(pk["fp64"], 1), "unit": "TFLOP/s",
+        "frac": round(flops_lu / (f64 * 1e-3) / 1e12 / pk["fp64"], 3),
+        "peak_source": "nominal FP64 (148 SMs x 64 x 2 x %g MHz)" % pk["mhz"]}
+    del Ad
+    torch.cuda.empty_cache()
+    return {"workload": "dense solve: closed ellipsoid (4, 1, 0.5) of %d surface panels "
+                        "(%d quads + %d cap triangles), Dirichlet AIC, %d freestream RHS"
+                        % (n, int(np.sum(body.n_ver == 4)), int(np.sum(body.n_ver == 3)), nrhs),
+            "unit": "ms per solve (factor + all RHS)", "reps": reps, "warmup": warm,
+            "assembly_ms_wall": [round(t, 2) for t in t_asm],
+            "flops_factor": flops_lu, "flops_total": flops_tot,
+            "speedup_mixed_vs_lu64": round(res["lu64"]["ms"] / res["mixed"]["ms"], 3),
+            "l2": "256 MB flush between timed calls; A is %.2f GB" % (n * n * 8 / 1e9),
+            "results": res}
+
+
+def workload_line(args, ws, name):
+    """--workload fmm / dense: that workload as the bench line."""
+    import torch
+    torch.cuda.set_stream(torch.cuda.Stream())
+    warm = max(args.warmup, 3)
+    if name == "fmm":
+        degs = tuple(int(x) for x in args.degrees.split(","))
+        with Clocks(0) as clk:
+            w = run_fmm_workload(args.steps, warm, degs)
+        best = w["results"]["p%d_fp32c" % degs[0]]
+        plain = w["results"]["p%d_fp64" % degs[0]]
+        metric = "ms per FMM evaluation (1.1M ring particles, p=%d, FP32C vs FP64)" % degs[0]
+        rf = dict(best["roofline"]["m2l"])
+        rf["kernel"] = "M2L phase"
+        rf["traffic"] = None
+        rf["others"] = [dict(best["roofline"]["p2p"], kernel="P2P phase")]
+        dtype = "f32/tf32 (FP32C)"
+    else:
+        with Clocks(0) as clk:
+            w = run_dense_workload(args.steps, warm)
+        best = w["results"]["mixed"]
+        plain = w["results"]["lu64"]
+        metric = "ms per dense solve (16,384-panel ellipsoid, 64 RHS), MIXED vs LU64"
+        rf = dict(best["roofline"])
+        rf["kernel"] = "FP32 LU with tcgen05 TF32 trailing updates"
+        rf["traffic"] = None
+        dtype = "f32/tf32 with f64 refinement"
+    ms = max_over_ranks(best["ms"], ws)
+    line = {"metric": metric, "value": round(ms, 3), "unit": "ms", "n_gpus": ws,
+            "steps": args.steps, "warmup": warm, "ms_per_step": round(ms, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded)", "config": {"workload": w["workload"],
+                                                     "l2": w["l2"]},
+            "plain_fp64_ms": plain["ms"], "detail": w, "roofline": rf,
+            "clocks": clk.summary(), "cpu_baseline": None, "e2e": None}
+    return line
 
 
 def phase_breakdown(st, case, params):

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "dust_common.cuh"
@@ -139,6 +140,94 @@ int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w
   return worst <= tol ? DUST_OK : DUST_ERR_NOT_CONVERGED;
 }
 
+// LU64 on device arrays: A copied into the work matrix F unless it already
+// is F's storage, F = P L U (lu_getrf), X = U^-1 L^-1 P B (lu_getrs).
+static int dense_lu64_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &F,
+                             DevBuf &piv, int n, int nrhs, const double *A, const double *B,
+                             double *X, dust_solve_report *r) {
+  const size_t nn = (size_t)n * n, nr = (size_t)n * nrhs;
+  if (A != F.p) DUST_TRY(devbuf_grow(F, nn * 8));
+  DUST_TRY(devbuf_grow(piv, (size_t)n * 4 + 64));
+  int *ipiv = (int *)piv.p;
+  int *info = ipiv + n;
+  cudaEvent_t e0, e1, e2;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventCreate(&e2);
+  int s = DUST_OK;
+  cudaEventRecord(e0, st);
+  if (A != F.p && cudaMemcpyAsync(F.p, A, nn * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    s = DUST_ERR_CUDA;
+  if (s == DUST_OK) s = lu_getrf<double>(cb, st, lu, n, (double *)F.p, n, ipiv, info, 0);
+  cudaEventRecord(e1, st);
+  int hinfo = 0;
+  if (s == DUST_OK) {
+    cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) s = DUST_ERR_CUDA;
+    else if (hinfo) s = DUST_ERR_SINGULAR;
+  }
+  if (s == DUST_OK) {
+    if (X != B && cudaMemcpyAsync(X, B, nr * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      s = DUST_ERR_CUDA;
+    if (s == DUST_OK)
+      s = lu_getrs<double>(cb, st, n, nrhs, (const double *)F.p, n, ipiv, X, n);
+    cudaEventRecord(e2, st);
+  }
+  if (s == DUST_OK && cudaStreamSynchronize(st) == cudaSuccess && r) {
+    cudaEventElapsedTime(&r->ms_factor, e0, e1);
+    cudaEventElapsedTime(&r->ms_solve, e1, e2);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  if (r) r->mode_used = DUST_SOLVE_LU64;
+  return s;
+}
+
+// Work areas of the device-array dense solve, kept between calls (grown,
+// never shrunk) so that repeated solves of one size allocate nothing after
+// the first; one set per process, guarded by a mutex.
+namespace {
+struct DenseWork {
+  std::mutex mu;
+  cublasHandle_t cb = nullptr;
+  DevBuf F, piv, w32, wrk;
+  LuWork lu;
+};
+DenseWork &dense_work() {
+  static DenseWork *w = new DenseWork();  // never destroyed: no teardown at exit
+  return *w;
+}
+}  // namespace
+
+extern "C" int dust_dense_solve_device(int n, int nrhs, const double *A, const double *B,
+                                       double *X, int mode, double tol,
+                                       dust_solve_report *rep, void *stream) {
+  if (n <= 0 || nrhs <= 0 || !A || !B || !X) return DUST_ERR_BAD_ARG;
+  if (mode != DUST_SOLVE_LU64 && mode != DUST_SOLVE_MIXED) return DUST_ERR_BAD_ARG;
+  if (X == A) return DUST_ERR_BAD_ARG;
+  DenseWork &w = dense_work();
+  std::lock_guard<std::mutex> g(w.mu);
+  if (!w.cb && cublasCreate(&w.cb) != CUBLAS_STATUS_SUCCESS) {
+    w.cb = nullptr;
+    return DUST_ERR_CUDA;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  cublasSetStream(w.cb, st);
+  dust_solve_report r;
+  memset(&r, 0, sizeof(r));
+  int s;
+  if (mode == DUST_SOLVE_LU64) {
+    s = dense_lu64_device(w.cb, st, w.lu, w.F, w.piv, n, nrhs, A, B, X, &r);
+  } else {
+    if (X == B) return DUST_ERR_BAD_ARG;
+    s = mixed_solve_device(w.cb, st, w.lu, w.w32, w.wrk, n, nrhs, A, B, X,
+                           tol > 0 ? tol : 1e-12, 30, 1, &r);
+  }
+  if (rep) *rep = r;
+  return s;
+}
+
 extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *B, double *X,
                                 int mode, double tol, dust_solve_report *rep) {
   if (n <= 0 || nrhs <= 0 || !A || !B || !X) return DUST_ERR_BAD_ARG;
@@ -151,7 +240,7 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
     return DUST_ERR_CUDA;
   }
   cublasSetStream(cb, st);
-  DevBuf dA, dB, dX, w32, wrk;
+  DevBuf dA, dB, dX, piv, w32, wrk;
   LuWork lu;
   dust_solve_report r;
   memset(&r, 0, sizeof(r));
@@ -162,40 +251,9 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
     cudaMemcpyAsync(dA.p, A, nn * 8, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(dB.p, B, nr * 8, cudaMemcpyHostToDevice, st);
     if (mode == DUST_SOLVE_LU64) {
-      cudaEvent_t e0, e1, e2;
-      cudaEventCreate(&e0);
-      cudaEventCreate(&e1);
-      cudaEventCreate(&e2);
-      int *ipiv = nullptr, *info = nullptr;
-      DevBuf piv;
-      s = devbuf_grow(piv, (size_t)n * 4 + 64);
-      if (s == DUST_OK) {
-        ipiv = (int *)piv.p;
-        info = ipiv + n;
-        cudaEventRecord(e0, st);
-        s = lu_getrf<double>(cb, st, lu, n, (double *)dA.p, n, ipiv, info, 0);
-        cudaEventRecord(e1, st);
-        int hinfo = 0;
-        if (s == DUST_OK) {
-          cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st);
-          cudaStreamSynchronize(st);
-          if (hinfo) s = DUST_ERR_SINGULAR;
-        }
-        if (s == DUST_OK) {
-          cudaMemcpyAsync(dX.p, dB.p, nr * 8, cudaMemcpyDeviceToDevice, st);
-          s = lu_getrs<double>(cb, st, n, nrhs, (const double *)dA.p, n, ipiv, (double *)dX.p, n);
-          cudaEventRecord(e2, st);
-        }
-        if (s == DUST_OK && cudaStreamSynchronize(st) == cudaSuccess) {
-          cudaEventElapsedTime(&r.ms_factor, e0, e1);
-          cudaEventElapsedTime(&r.ms_solve, e1, e2);
-        }
-      }
-      devbuf_free(piv);
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      cudaEventDestroy(e2);
-      r.mode_used = DUST_SOLVE_LU64;
+      // factored in place in the device copy (the host array is the caller's)
+      s = dense_lu64_device(cb, st, lu, dA, piv, n, nrhs, (const double *)dA.p,
+                            (const double *)dB.p, (double *)dX.p, &r);
     } else {
       s = mixed_solve_device(cb, st, lu, w32, wrk, n, nrhs, (const double *)dA.p,
                              (const double *)dB.p, (double *)dX.p, tol > 0 ? tol : 1e-12, 30,
@@ -210,6 +268,7 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
   devbuf_free(dA);
   devbuf_free(dB);
   devbuf_free(dX);
+  devbuf_free(piv);
   devbuf_free(w32);
   devbuf_free(wrk);
   devbuf_free(lu.sync);

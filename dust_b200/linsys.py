@@ -92,3 +92,17 @@ def dense_solve(A, B, mode=abi.DUST_SOLVE_LU64, tol=1e-12):
                                  C.c_double(tol), C.byref(rep)), "dust_dense_solve")
     out = X[:, 0].copy() if vec else np.ascontiguousarray(X)
     return out, {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+
+
+def dense_solve_device(A, B, X, mode=abi.DUST_SOLVE_LU64, tol=1e-12, stream=None):
+    """A X = B on device arrays (torch CUDA float64 tensors; A (n, n) and B, X
+    (n, nrhs) in column-major storage, i.e. the transposes of C-contiguous
+    (n, n) / (nrhs, n) tensors).  A is not modified.  Returns the report."""
+    n = A.shape[0]
+    nrhs = B.numel() // n
+    rep = abi.SolveReport()
+    vp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))
+    check(lib().dust_dense_solve_device(int(n), int(nrhs), vp(A), vp(B), vp(X), int(mode),
+                                        C.c_double(tol), C.byref(rep),
+                                        C.c_void_p(stream or 0)), "dust_dense_solve_device")
+    return {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}

@@ -76,20 +76,23 @@ def flat_wing(span=10.0, chord=1.0, n_span=40, n_chord=10, alpha_deg=0.0):
     return abi.PanelSet(ver, kind=np.full(n, abi.DUST_ELEM_VORTLATT)), te
 
 
-def ellipsoid(n_target=16384, axes=(4.0, 1.0, 0.5), seed=0):
+def ellipsoid(n_target=16384, axes=(4.0, 1.0, 0.5), seed=0, n_u=None, n_lat=None):
     """Closed ellipsoid of quadrilateral surface panels (outward normals),
-    n_u x n_v ~ n_target panels, with a seeded random rigid rotation.
+    n_u x n_v ~ n_target panels (exactly n_u x n_lat when both are given),
+    with a seeded random rigid rotation.
     The poles are closed by triangles folded into quads with a repeated
     vertex avoided: the grid is built in a parameter range that excludes the
     poles and the two polar caps are closed by triangle fans."""
     rng = np.random.default_rng(seed)
-    n_v = int(round(np.sqrt(n_target / 2.0)))
-    # even azimuthal count: with an odd one, a cap triangle's centroid lies on
-    # the extension of the opposite fan edge, where the solid-angle formula of
-    # potential_calc_doublet divides by zero
-    n_u = (n_target // n_v) // 2 * 2
-    # quads: n_u (azimuth) x (n_v - 2) latitude bands; caps: 2 * n_u triangles
-    n_lat = n_v
+    if n_u is None or n_lat is None:
+        n_v = int(round(np.sqrt(n_target / 2.0)))
+        # even azimuthal count: with an odd one, a cap triangle's centroid lies
+        # on the extension of the opposite fan edge, where the solid-angle
+        # formula of potential_calc_doublet divides by zero
+        n_u = (n_target // n_v) // 2 * 2
+        n_lat = n_v
+    assert n_u % 2 == 0, "the azimuthal count must be even"
+    # quads: n_u (azimuth) x (n_lat - 2) latitude bands; caps: 2 * n_u triangles
     th = np.linspace(0.0, np.pi, n_lat + 1)  # polar angle
     ph = np.linspace(0.0, 2.0 * np.pi, n_u + 1)
     ax = np.asarray(axes, dtype=np.float64)
@@ -443,3 +446,78 @@ class FullStepCase:
             f = rho * np.cross(urel, e1) * (g - gup)[:, None]
             out.append(f.sum(axis=0)[2])
         return np.asarray(out)
+
+
+class RingCase:
+    """Standalone wake FMM workload: ``n_ring`` particles on a vortex ring
+    (radius 1, Gaussian cross-section 0.1) plus ``n_bg`` uniform background
+    particles in [-2, 2]^3, tangential circulation vectors of Gaussian
+    magnitude (mean 1e-3, sd 1e-4), core radius 0.02 (1M + 100k at the named
+    size).  The octree box is [-2, 2]^3 with one level-1 box; the number of
+    levels is the smallest that keeps every finest cell at <= ``max_leaf``
+    particles."""
+
+    def __init__(self, n_ring=1_000_000, n_bg=100_000, seed=0, core=0.02, max_leaf=64):
+        self.cen, self.dir, self.mag = ring_particles(n_ring, n_bg, seed=seed)
+        self.n = self.mag.shape[0]
+        self.r_vortex = np.full(self.n, core)
+        self.core = core
+        self.levels = choose_levels(self.cen, 4.0, (1, 1, 1), (-2.0, -2.0, -2.0), max_leaf)
+
+    def fmm_params(self, degree=4, precision=abi.DUST_PREC_FP64, min_part=8):
+        from .params import FmmParams
+        return FmmParams(box_length=4.0, origin=(-2.0, -2.0, -2.0),
+                         n_octree_levels=self.levels, min_octree_part=min_part,
+                         multipole_degree=degree, rankine_rad=self.core, precision=precision)
+
+    def truth_order(self, n_tgt, seed=1):
+        """A permutation that puts a seeded random subset of ``n_tgt``
+        particles first (the direct-sum targets); the FMM result does not
+        depend on the particle order."""
+        rng = np.random.default_rng(seed)
+        sub = rng.choice(self.n, n_tgt, replace=False)
+        rest = np.setdiff1d(np.arange(self.n), sub, assume_unique=False)
+        return np.concatenate([sub, rest])
+
+    def permuted(self, order):
+        c = RingCase.__new__(RingCase)
+        c.__dict__.update(self.__dict__)
+        c.cen = np.ascontiguousarray(self.cen[order])
+        c.dir = np.ascontiguousarray(self.dir[order])
+        c.mag = np.ascontiguousarray(self.mag[order])
+        c.r_vortex = np.ascontiguousarray(self.r_vortex[order])
+        return c
+
+
+class EllipsoidCase:
+    """Mixed-precision dense-solve workload: closed ellipsoid (semi-axes 4, 1,
+    0.5) of ``n_target`` surface panels (source + doublet, Dirichlet rows) in
+    a seeded random rigid rotation, with ``nrhs`` right-hand sides from
+    seeded random unit freestream directions.
+
+    The Dirichlet right-hand side is linear in the freestream u
+    (b_i = sum_j sou_ij n_j . (ub_j - u - uvort_j), mod_surfpan.f90:448-481),
+    so the three assemblies with a unit body velocity along x, y, z (u = 0)
+    give the columns G = [b_x b_y b_z] and the right-hand side of a
+    freestream u is -G u."""
+
+    def __init__(self, n_target=16384, nrhs=64, seed=0):
+        # n_u x n_lat = n_target panels when n_target is 2 * a square
+        # (16,384 = 128 x 128: 16,128 quads and 256 cap triangles)
+        side = int(round(np.sqrt(n_target)))
+        kw = dict(n_u=side, n_lat=side) if side * side == n_target and side % 2 == 0 else {}
+        self.body = ellipsoid(n_target=n_target, axes=(4.0, 1.0, 0.5), seed=seed, **kw)
+        self.n = self.body.n
+        rng = np.random.default_rng(seed + 1000)
+        U = rng.standard_normal((3, nrhs))
+        self.U = U / np.linalg.norm(U, axis=0)[None, :]
+        self.nrhs = nrhs
+
+    def fmm_params(self):
+        from .params import FmmParams
+        return FmmParams(u_inf=(0.0, 0.0, 0.0))
+
+    def unit_ub(self, d):
+        ub = np.zeros((self.n, 3))
+        ub[:, d] = 1.0
+        return ub

@@ -313,6 +313,19 @@ DUST_API int dust_linsys_get_system(dust_linsys *ls, double *A, double *b);
 DUST_API int dust_dense_solve(int n, int nrhs, const double *A, const double *B,
                      double *X, int mode, double tol, dust_solve_report *rep);
 
+/* dust_dense_solve on device arrays (A n x n, B and X n x nrhs, column-major,
+ * leading dimension n), queued on `stream` (cudaStream_t, NULL = the legacy
+ * default stream) and synchronised before return.  A is not modified: the
+ * LU64 mode factors a copy, the MIXED mode only reads it (FP32 copy for the
+ * factorisation, FP64 A for the residuals).  LU64 allows X == B (solved in
+ * place); MIXED needs X != B.  The work areas (the factor copy, the FP32
+ * matrix, pivots, refinement vectors) are kept between calls and grow with
+ * the largest size seen, so repeated solves of one size allocate nothing
+ * after the first; calls are serialised by a process-wide lock. */
+DUST_API int dust_dense_solve_device(int n, int nrhs, const double *A, const double *B,
+                                     double *X, int mode, double tol,
+                                     dust_solve_report *rep, void *stream);
+
 /* Tensor-core (tcgen05, kind::tf32) update C -= A B on device arrays
  * (column-major FP32, read as TF32, FP32 accumulation): the trailing update
  * of the mixed-precision LU (the dgemm of mod_linsys.f90:428-438 in its

@@ -95,6 +95,29 @@ int or_linsys_run(const dust_fmm_params *prm, int rank, int nstatic,
                   const dust_wake_rows *wake_step,
                   double *A_out, double *b_out, double *res);
 
+/* The two assembly halves of or_linsys_run on caller arrays (A rank x rank
+ * column-major, bst nst x nst, b rank, all zero-initialised by the caller):
+ * initialize_linsys's static rows and static wake, and one assemble_linsys
+ * (uvort from elems->uvort).  The static LU between them is the caller's. */
+void or_linsys_init(const dust_fmm_params *prm, int rank, int nst,
+                    const dust_panels *elems, const dust_wake_rows *wake, double *A,
+                    double *bst, double *b);
+void or_linsys_step(const dust_fmm_params *prm, int rank, int nst,
+                    const dust_panels *elems, const dust_wake_rows *wake, double *A,
+                    const double *bst, double *b);
+
+/* Work sampling of or_fmm_apply for the timed CPU baseline (stride 1 =
+ * full evaluation) and the phase times / sampled work of the last call. */
+void or_set_sample_stride(int s);
+void or_set_threads(int n);
+void or_last_fmm_times(double *t4, int64_t *sampled);
+
+/* Rows `rows[0..nrows)` of the all-moving system (nstatic = 0) as
+ * assemble_linsys builds them; A_rows nrows x rank row-major. */
+int or_linsys_rows(const dust_fmm_params *prm, int rank, const dust_panels *elems,
+                   const dust_wake_rows *wake, int nrows, const int *rows,
+                   double *A_rows, double *b_rows);
+
 /* LAPACK-equivalent dense kernels (column-major). */
 int  or_dgetrf(int m, int n, double *A, int lda, int *ipiv);
 void or_dgetrs(int n, int nrhs, const double *A, int lda, const int *ipiv,

@@ -23,6 +23,8 @@
 #include "dust_oracle.h"
 #include "or_internal.h"
 
+#include <omp.h>
+
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -33,6 +35,27 @@
 
 static int g_fact_wrap = 0;
 void or_set_factorial_wrap(int on) { g_fact_wrap = on; }
+
+/* Work sampling for the timed CPU baseline: with stride s > 1, M2L runs for
+ * every s-th target cell only and the apply loop (L2P, P2P, elements) for
+ * every s-th leaf; the tree, P2M, M2M and L2L run in full.  The results of
+ * a sampled run are incomplete and serve timing only. */
+static int g_stride = 1;
+static double g_times[4];
+static int64_t g_sampled[2];
+void or_set_sample_stride(int s) { g_stride = s > 1 ? s : 1; }
+/* OpenMP threads of every oracle loop */
+void or_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+}
+/* times (s) of the last or_fmm_apply: tree (init + sort), upward (P2M +
+ * M2M), M2L + L2L, apply; sampled[0] = M2L pairs evaluated, sampled[1] =
+ * particles evaluated in the apply loop */
+void or_last_fmm_times(double *t4, int64_t *sampled) {
+  for (int i = 0; i < 4; ++i) t4[i] = g_times[i];
+  sampled[0] = g_sampled[0];
+  sampled[1] = g_sampled[1];
+}
 
 /* ---------------------------------------------------------------- polyexp */
 typedef struct {
@@ -619,6 +642,7 @@ static int64_t tree_multipole(tree_t *T, const double *cen, const double *dir,
                               const double *mag) {
   int ll = T->ll;
   int64_t npairs = 0;
+  double t0 = omp_get_wtime();
 #pragma omp parallel for schedule(guided)
   for (int64_t lv = 0; lv < T->nleaves; ++lv) {
     int l = T->leaf_lev[lv];
@@ -644,10 +668,13 @@ static int64_t tree_multipole(tree_t *T, const double *cen, const double *dir,
       }
     }
   }
+  g_times[1] = omp_get_wtime() - t0;
+  t0 = omp_get_wtime();
   for (int l = 1; l <= ll; ++l) {
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : npairs)
     for (int64_t c = 0; c < T->ncell[l]; ++c) {
       if (!(T->fl[l][c] & FL_ACTIVE)) continue;
+      if (g_stride > 1 && c % g_stride != 0) continue;
       int i, j, k;
       cart_of(T, l, c, &i, &j, &k);
       int cap = (l == 1) ? (int)T->ncell[1] : 216;
@@ -678,6 +705,8 @@ static int64_t tree_multipole(tree_t *T, const double *cen, const double *dir,
       }
     }
   }
+  g_times[2] = omp_get_wtime() - t0;
+  g_sampled[0] = npairs;
   return npairs;
 }
 
@@ -745,10 +774,11 @@ static int64_t tree_apply(tree_t *T, int n, const double *cen, const double *dir
                           double *vel_o, double *str_o, double *rot_o) {
   const pexp_t *P = &T->pe;
   int nmon = P->n_mon;
-  int64_t npairs = 0;
+  int64_t npairs = 0, nsampled = 0;
   (void)n;
-#pragma omp parallel for schedule(dynamic) reduction(+ : npairs)
+#pragma omp parallel for schedule(dynamic) reduction(+ : npairs, nsampled)
   for (int64_t lv = 0; lv < T->nleaves; ++lv) {
+    if (g_stride > 1 && lv % g_stride != 0) continue;
     int l = T->leaf_lev[lv];
     int64_t c = T->leaf_lin[lv];
     int i, j, k;
@@ -756,6 +786,7 @@ static int64_t tree_apply(tree_t *T, int n, const double *cen, const double *dir
     int64_t lo, hi;
     cell_range(T, l, i, j, k, &lo, &hi);
     int64_t np = hi - lo;
+    nsampled += np;
     const mp_t *m = &T->mp[l][c];
     const double *cc = T->cen[l] + 3 * c;
     double *velv = (double *)calloc(3 * (np > 0 ? np : 1), sizeof(double));
@@ -858,6 +889,7 @@ static int64_t tree_apply(tree_t *T, int n, const double *cen, const double *dir
     free(strv);
     free(rotv);
   }
+  g_sampled[1] = nsampled;
   return npairs;
 }
 
@@ -868,17 +900,21 @@ int or_fmm_apply(const dust_fmm_params *prm, int n, const double *cen,
   if (!prm || n < 0 || prm->n_octree_levels < 1 ||
       prm->n_octree_levels > MAXLEV || prm->multipole_degree < 0)
     return DUST_ERR_BAD_ARG;
+  double t0 = omp_get_wtime();
   tree_t *T = tree_init(prm);
   int st = tree_sort(T, n, cen);
   if (st != DUST_OK) {
     tree_free(T);
     return st;
   }
+  g_times[0] = omp_get_wtime() - t0;
   int64_t m2lp = tree_multipole(T, cen, dir, mag);
+  t0 = omp_get_wtime();
   or_elemctx *ectx = or_elemctx_build(elems, prm->u_inf);
   int64_t p2pp = tree_apply(T, n, cen, dir, mag, r_vortex, prm, ectx, vel,
                             stretch, rotu);
   or_elemctx_free(ectx);
+  g_times[3] = omp_get_wtime() - t0;
   if (counters) {
     int64_t act = 0;
     for (int l = 1; l <= T->ll; ++l)

@@ -187,49 +187,51 @@ static void build_row_static(const rowctx *c, double *A, int lda, double *bst,
   }
 }
 
+/* Row ie of A (element (ie, j) at A[j * lda + ie - roff]) and b[ie - roff]:
+ * roff = 0 for the full system, roff = ie with lda = 1 for a single row. */
 static void build_row(const rowctx *c, double *A, int lda, const double *bst,
                       int nst, const double *uvort, double *b, int ie, int ista,
-                      int iend) {
+                      int iend, int roff) {
   const or_pan_t *r = &c->el[ie];
   const double *u = c->prm->u_inf;
-  b[ie] = 0.0;
+  b[ie - roff] = 0.0;
   for (int j = 0; j < ista; ++j)
-    b[ie] = b[ie] + bst[(size_t)j * nst + ie] * nor_static(&c->el[j], u, uvort + 3 * j);
+    b[ie - roff] = b[ie - roff] + bst[(size_t)j * nst + ie] * nor_static(&c->el[j], u, uvort + 3 * j);
   for (int j = ista; j <= iend; ++j) {
     double b1;
     if (r->kind == DUST_ELEM_SURFPAN) {
-      compute_pot(c, j, r->cen, ie, &A_(ie, j), &b1);
-      b[ie] = b[ie] + b1 * nor_rel(&c->el[j]);
+      compute_pot(c, j, r->cen, ie, &A[(size_t)j * lda + (size_t)(ie - roff)], &b1);
+      b[ie - roff] = b[ie - roff] + b1 * nor_rel(&c->el[j]);
     } else {
-      compute_psi(c, j, r->cen, r->nor, ie, &A_(ie, j), &b1);
+      compute_psi(c, j, r->cen, r->nor, ie, &A[(size_t)j * lda + (size_t)(ie - roff)], &b1);
       if (ie == j) {
         /* nor_ie . (ub_ie - wind - uvort_j) with j == ie */
-        b[ie] = b[ie] + b1 * nor_rel(&c->el[ie]);
+        b[ie - roff] = b[ie - roff] + b1 * nor_rel(&c->el[ie]);
       } else {
-        b[ie] = b[ie] + b1 * nor_rel(&c->el[j]);
+        b[ie - roff] = b[ie - roff] + b1 * nor_rel(&c->el[j]);
       }
     }
   }
 }
 
 static void add_wake(const rowctx *c, double *A, int lda, double *b, int ie,
-                     int ista, int iend) {
+                     int ista, int iend, int roff) {
   const or_pan_t *r = &c->el[ie];
   for (int j = 0; j < c->n_impl; ++j) {
     int i1 = c->impl[2 * j] - 1, i2 = c->impl[2 * j + 1] - 1;
     if (r->kind == DUST_ELEM_SURFPAN) {
       if (i1 >= ista && i1 <= iend && i2 >= ista && i2 <= iend) {
         double a = -or_pot_dou(c->prm, &c->wk[j], r->cen);
-        A_(ie, i1) = A_(ie, i1) + a;
-        A_(ie, i2) = A_(ie, i2) - a;
+        A[(size_t)i1 * lda + (size_t)(ie - roff)] = A[(size_t)i1 * lda + (size_t)(ie - roff)] + a;
+        A[(size_t)i2 * lda + (size_t)(ie - roff)] = A[(size_t)i2 * lda + (size_t)(ie - roff)] - a;
       }
     } else {
       if (i1 >= ista && i1 <= iend) {
         double vd[3];
         or_vel_dou(c->prm, &c->wk[j], r->cen, vd);
         double a = vd[0] * r->nor[0] + vd[1] * r->nor[1] + vd[2] * r->nor[2];
-        A_(ie, i1) = A_(ie, i1) + a;
-        if (i2 >= 0) A_(ie, i2) = A_(ie, i2) - a;
+        A[(size_t)i1 * lda + (size_t)(ie - roff)] = A[(size_t)i1 * lda + (size_t)(ie - roff)] + a;
+        if (i2 >= 0) A[(size_t)i2 * lda + (size_t)(ie - roff)] = A[(size_t)i2 * lda + (size_t)(ie - roff)] - a;
       }
     }
   }
@@ -242,7 +244,7 @@ static void add_wake(const rowctx *c, double *A, int lda, double *b, int ie,
       or_vel_dou(c->prm, &c->wk[j], r->cen, vd);
       a = vd[0] * r->nor[0] + vd[1] * r->nor[1] + vd[2] * r->nor[2];
     }
-    b[ie] = b[ie] - a * c->wk[j].mag;
+    b[ie - roff] = b[ie - roff] - a * c->wk[j].mag;
   }
 }
 
@@ -262,6 +264,51 @@ static void ctx_free(rowctx *c) {
   free(c->wk);
 }
 
+/* initialize_linsys without the LU (mod_linsys.f90:109-229): the static
+ * rows (columns 0..nst-1) and the static wake into A (rank x rank,
+ * column-major), bst (nst x nst) and b. */
+void or_linsys_init(const dust_fmm_params *prm, int rank, int nst,
+                    const dust_panels *elems, const dust_wake_rows *wake, double *A,
+                    double *bst, double *b) {
+  int lda = rank;
+  rowctx c;
+  ctx_load(&c, prm, rank, elems, wake);
+#pragma omp parallel for schedule(dynamic)
+  for (int ie = 0; ie < nst; ++ie) build_row_static(&c, A, lda, bst, nst, ie, 0, nst - 1);
+#pragma omp parallel for schedule(dynamic)
+  for (int ie = 0; ie < nst; ++ie) add_wake(&c, A, lda, b, ie, 0, nst - 1, 0);
+  ctx_free(&c);
+}
+
+/* assemble_linsys with uvort given (mod_linsys.f90:279-344): moving columns
+ * of the static rows, all columns of the moving rows, the right-hand side
+ * and the wake terms; the static block of A (its LU) is not touched. */
+void or_linsys_step(const dust_fmm_params *prm, int rank, int nst,
+                    const dust_panels *elems, const dust_wake_rows *wake, double *A,
+                    const double *bst, double *b) {
+  int n = rank, lda = rank;
+  rowctx c;
+  ctx_load(&c, prm, rank, elems, wake);
+  double *uv = (double *)calloc(3 * (size_t)n, sizeof(double));
+  if (elems->uvort) memcpy(uv, elems->uvort, sizeof(double) * 3 * n);
+#pragma omp parallel for schedule(dynamic)
+  for (int ie = 0; ie < n; ++ie) {
+    if (ie < nst)
+      build_row(&c, A, lda, bst, nst, uv, b, ie, nst, n - 1, 0);
+    else
+      build_row(&c, A, lda, bst, nst, uv, b, ie, 0, n - 1, 0);
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int ie = 0; ie < n; ++ie) {
+    if (ie < nst)
+      add_wake(&c, A, lda, b, ie, nst, n - 1, 0);
+    else
+      add_wake(&c, A, lda, b, ie, 0, n - 1, 0);
+  }
+  free(uv);
+  ctx_free(&c);
+}
+
 int or_linsys_run(const dust_fmm_params *prm, int rank, int nstatic,
                   const dust_panels *elems_init, const dust_panels *elems_step,
                   const dust_wake_rows *wake_init, const dust_wake_rows *wake_step,
@@ -273,40 +320,12 @@ int or_linsys_run(const dust_fmm_params *prm, int rank, int nstatic,
                                  sizeof(double));
   int *P = (int *)calloc(n, sizeof(int));
   int info = 0;
-  rowctx c;
-  /* initialize_linsys */
-  ctx_load(&c, prm, rank, elems_init, wake_init);
-#pragma omp parallel for schedule(dynamic)
-  for (int ie = 0; ie < nst; ++ie) build_row_static(&c, A, lda, bst, nst, ie, 0, nst - 1);
-#pragma omp parallel for schedule(dynamic)
-  for (int ie = 0; ie < nst; ++ie) add_wake(&c, A, lda, b, ie, 0, nst - 1);
-  ctx_free(&c);
+  or_linsys_init(prm, rank, nst, elems_init, wake_init, A, bst, b);
   if (nst > 0) {
     info = or_dgetrf(nst, nst, A, lda, P);
     if (info) goto done;
   }
-  /* assemble_linsys (uvort given) */
-  ctx_load(&c, prm, rank, elems_step, wake_step);
-  {
-    double *uv = (double *)calloc(3 * (size_t)n, sizeof(double));
-    if (elems_step->uvort) memcpy(uv, elems_step->uvort, sizeof(double) * 3 * n);
-#pragma omp parallel for schedule(dynamic)
-    for (int ie = 0; ie < n; ++ie) {
-      if (ie < nst)
-        build_row(&c, A, lda, bst, nst, uv, b, ie, nst, n - 1);
-      else
-        build_row(&c, A, lda, bst, nst, uv, b, ie, 0, n - 1);
-    }
-#pragma omp parallel for schedule(dynamic)
-    for (int ie = 0; ie < n; ++ie) {
-      if (ie < nst)
-        add_wake(&c, A, lda, b, ie, nst, n - 1);
-      else
-        add_wake(&c, A, lda, b, ie, 0, n - 1);
-    }
-    free(uv);
-  }
-  ctx_free(&c);
+  or_linsys_step(prm, rank, nst, elems_step, wake_step, A, bst, b);
   if (A_out) memcpy(A_out, A, sizeof(double) * (size_t)n * n);
   if (b_out) memcpy(b_out, b, sizeof(double) * n);
   /* solve_linsys */
@@ -353,4 +372,35 @@ done:
   free(bst);
   free(P);
   return info ? DUST_ERR_SINGULAR : DUST_OK;
+}
+
+/* Selected rows of the system as assemble_linsys builds them when every
+ * element is moving (nstatic = 0: build_row over all columns, then
+ * add_wake; mod_linsys.f90:279-344): row r of the output is element
+ * rows[r]; A_rows is nrows x rank row-major, b_rows nrows. */
+int or_linsys_rows(const dust_fmm_params *prm, int rank, const dust_panels *elems,
+                   const dust_wake_rows *wake, int nrows, const int *rows,
+                   double *A_rows, double *b_rows) {
+  rowctx c;
+  ctx_load(&c, prm, rank, elems, wake);
+  double *uv = (double *)calloc(3 * (size_t)rank, sizeof(double));
+  if (elems->uvort) memcpy(uv, elems->uvort, sizeof(double) * 3 * rank);
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic)
+  for (int r = 0; r < nrows; ++r) {
+    int ie = rows[r];
+    if (ie < 0 || ie >= rank) {
+      bad = 1;
+      continue;
+    }
+    double *Ar = A_rows + (size_t)r * rank;
+    double *br = b_rows + r;
+    for (int j = 0; j < rank; ++j) Ar[j] = 0.0;
+    *br = 0.0;
+    build_row(&c, Ar, 1, NULL, 1, uv, br, ie, 0, rank - 1, ie);
+    add_wake(&c, Ar, 1, br, ie, 0, rank - 1, ie);
+  }
+  free(uv);
+  ctx_free(&c);
+  return bad ? 6 : 0;
 }

@@ -37,6 +37,7 @@ def lib():
         L.or_potential_source.restype = C.c_double
         L.or_dgetrf.restype = C.c_int
         L.or_linsys_run.restype = C.c_int
+        L.or_linsys_rows.restype = C.c_int
         L.or_last_tree_flags.restype = C.c_int
         L.or_particles_update.restype = C.c_int
     return _lib
@@ -48,6 +49,20 @@ def set_factorial_wrap(on):
 
 def _out(n, on=True):
     return np.zeros((n, 3)) if on else None
+
+
+def set_sample_stride(stride):
+    """Work sampling of fmm_apply for timing (1 = full evaluation)."""
+    lib().or_set_sample_stride(C.c_int(int(stride)))
+
+
+def last_fmm_times():
+    """Phase times (s) of the last fmm_apply -- tree, upward, M2L + L2L,
+    apply -- and the sampled work (M2L pairs, particles evaluated)."""
+    t = np.zeros(4)
+    n = np.zeros(2, dtype=np.int64)
+    lib().or_last_fmm_times(abi.dptr(t), n.ctypes.data_as(C.POINTER(C.c_int64)))
+    return t, n
 
 
 def fmm_apply(prm, cen, dir_, mag, rvort, elems=None):
@@ -179,6 +194,51 @@ def linsys_run(prm, rank, nstatic, elems_init, elems_step, wake_init, wake_step)
     if rc != 0:
         raise RuntimeError(f"oracle linsys status {rc}")
     return A.reshape(rank, rank).T.copy(), b, res
+
+
+def linsys_init(prm, rank, nstatic, elems, wake):
+    """initialize_linsys's static rows and wake (no LU): returns (A, bst, b)
+    with A as a Fortran-ordered (rank, rank) array."""
+    es = elems.struct()
+    ws, kk = abi.wake_rows_struct(*wake)
+    A = np.zeros((rank, rank), order="F")
+    nb = max(int(nstatic), 1)
+    bst = np.zeros((nb, nb), order="F")
+    b = np.zeros(rank)
+    p = prm.struct()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    lib().or_linsys_init(C.byref(p), int(rank), int(nstatic), C.byref(es), C.byref(ws), dp(A),
+                         dp(bst), dp(b))
+    return A, bst, b
+
+
+def linsys_step(prm, rank, nstatic, elems, wake, A, bst, b):
+    """assemble_linsys into A (Fortran-ordered, static block untouched) and b."""
+    assert A.flags.f_contiguous and bst.flags.f_contiguous
+    es = elems.struct()
+    ws, kk = abi.wake_rows_struct(*wake)
+    p = prm.struct()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    lib().or_linsys_step(C.byref(p), int(rank), int(nstatic), C.byref(es), C.byref(ws), dp(A),
+                         dp(bst), dp(b))
+
+
+def linsys_rows(prm, elems, rows, wake=None):
+    """Rows of the all-moving system (A rows (len(rows), rank), b rows)."""
+    rank = elems.n
+    es = elems.struct()
+    wk = wake if wake is not None else (abi.empty_panels(), 0, None)
+    ws, kk = abi.wake_rows_struct(*wk)
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    A = np.zeros((len(rows), rank))
+    b = np.zeros(len(rows))
+    p = prm.struct()
+    rc = lib().or_linsys_rows(C.byref(p), int(rank), C.byref(es), C.byref(ws), len(rows),
+                              rows.ctypes.data_as(C.POINTER(C.c_int)), abi.dptr(A),
+                              abi.dptr(b))
+    if rc != 0:
+        raise RuntimeError(f"oracle linsys rows status {rc}")
+    return A, b
 
 
 def particles_update(u, cen, dir_, mag, vel, stretch, rotu, free):

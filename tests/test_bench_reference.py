@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_reference_arm_json_line():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--quick", "--steps", "1", "--warmup", "0"],
+                          "--quick", "--particles", "20000", "--steps", "1", "--warmup", "0"],
                          capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
@@ -20,6 +20,8 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["unit"] == "ms" and d["higher_is_better"] is False
     assert d["value"] > 0 and d["ms_per_step"] == d["value"]
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    # whole steps timed in full: the reported time fits the run
+    assert d["steps"] >= 1 and "whole step" in d["cpu_baseline"]["sample"]
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "ms", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
@@ -31,8 +33,8 @@ def test_reference_arm_two_ranks():
     rank exits 0 without work (gloo here, no GPU needed)."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", "29617",
-           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--quick", "--steps", "1",
-           "--warmup", "0", "--gpus", "2"]
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--quick", "--particles", "20000",
+           "--steps", "1", "--warmup", "0", "--gpus", "2"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]

@@ -384,3 +384,26 @@ def test_vortex_particle_pair_curl_and_diffusion():
         diff = (vol * al[q] - vol * al[p]) / rv[q] ** 2 * eta
         assert rel(ro[p], rot) < 1e-12
         assert rel(st[p], s + diff * nu) < 1e-12
+
+
+def test_oracle_row_sample_equals_full_assembly():
+    """or_linsys_rows (the row sample the configuration-size tests compare
+    against) builds exactly the rows of the full all-moving assembly."""
+    from dust_b200 import synth
+    rng = np.random.default_rng(0)
+    prm = FmmParams(u_inf=(1.0, 0.2, 0.0))
+    body = synth.ellipsoid(n_target=600, seed=3)
+    body.uvort = rng.standard_normal((body.n, 3)) * 0.1
+    body.ub = rng.standard_normal((body.n, 3)) * 0.1
+    e = abi.empty_panels()
+    A, b, _ = O.linsys_run(prm, body.n, 0, body, body, (e, 0, None), (e, 0, None))
+    rows = np.array([0, 5, 17, body.n - 1])
+    Ar, br = O.linsys_rows(prm, body, rows)
+    assert np.array_equal(Ar, A[rows]) and np.array_equal(br, b[rows])
+    wing, te = synth.flat_wing(span=4.0, chord=1.0, n_span=12, n_chord=5, alpha_deg=5.0)
+    wake, ind = synth.te_wake(wing, te, (0.3, 0.0, 0.02))
+    wing.uvort = rng.standard_normal((wing.n, 3)) * 0.05
+    A, b, _ = O.linsys_run(prm, wing.n, 0, wing, wing, (wake, wake.n, ind), (wake, wake.n, ind))
+    rows = np.arange(0, wing.n, 7)
+    Ar, br = O.linsys_rows(prm, wing, rows, (wake, wake.n, ind))
+    assert np.array_equal(Ar, A[rows]) and np.array_equal(br, b[rows])
