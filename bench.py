@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-workloads", action="store_true",
                     help="full step only, without the fmm / dense sub-objects")
     ap.add_argument("--degrees", default="4,6,8", help="FMM degrees of the fmm workload")
+    ap.add_argument("--no-advect", action="store_true",
+                    help="leave the particles in place (no complete_wake particle update)")
     return ap.parse_args()
 
 
@@ -355,7 +357,7 @@ def main():
     steppers = {}
     for name, mode in modes:
         prm = params if name == "plain" else params.replace(precision=abi.DUST_PREC_FP32C)
-        st = step.DeviceStepper(case, prm, mode)
+        st = step.DeviceStepper(case, prm, mode, advect=not args.no_advect)
         if name == "learned":
             learned["precond"].attach(st.ls)
         steppers[name] = st
@@ -370,9 +372,11 @@ def main():
         barrier(ws)
         ms = max_over_ranks(float(np.mean(times)), ws)
         res = st.res.cpu().numpy()
-        results[name] = {"ms": ms, "times": times, "loads": case.loads(res),
+        results[name] = {"ms": ms, "times": times,
+                         "loads": case.loads(res, st.euv.cpu().numpy()),
                          "report": st.last_report, "clocks": clk.summary(), "res": res,
-                         "fmm": [t.cpu().numpy() for t in (st.vel, st.str, st.rot)]}
+                         "fmm": [t.cpu().numpy() for t in (st.vel, st.str, st.rot)],
+                         "cen": st.cen.cpu().numpy(), "n_freed": int(st.free.sum())}
     if args.profile_step:
         return
     # phase breakdown (plain and mixed share the FMM): one timed step with events
@@ -389,6 +393,10 @@ def main():
         return {"vel_induced": rel(a[0] - uinf, b[0] - uinf), "stretch": rel(a[1], b[1]),
                 "rot": rel(a[2], b[2])}
     fmm_errs = {k: fmm_err(k) for k in results}
+    # the particles after all advected steps against the FP64 run's
+    cp = results["plain"]["cen"]
+    for k in results:
+        fmm_errs[k]["position_max_abs"] = float(np.max(np.abs(results[k]["cen"] - cp)))
     # the headline mode: the fastest whose loads are within 1e-6 of FP64
     best = min((k for k in results if load_err[k] <= 1e-6), key=lambda k: results[k]["ms"])
     # end to end through the host API (pinned buffers)
@@ -423,6 +431,11 @@ def main():
             "plain_fp64_ms": round(results["plain"]["ms"], 3),
             "speedup_vs_plain_fp64": round(results["plain"]["ms"] / r["ms"], 3),
             "load_error_vs_fp64": load_err[best],
+            "steps_advected": 0 if args.no_advect else max(args.warmup, 3) + args.steps,
+            "load_error_note": "loads (wing lift, two rotor thrusts) of the last timed step; "
+                               "every mode advects its own particles from the same initial "
+                               "wake for all warm-up + timed steps, so the FMM error of each "
+                               "step reaches the loads of the next",
             "modes": {k: {"ms": round(v["ms"], 3), "load_error_vs_fp64": load_err[k],
                           "particle_error_vs_fp64": fmm_errs[k], "solve": v["report"]}
                       for k, v in results.items()},
@@ -703,8 +716,8 @@ def phase_breakdown(st, case, params):
     st.oc.set_timing(False)
     st.phase_events = False
     t = lambda a, b: round(ev[a].elapsed_time(ev[b]), 3)
-    return {"total": t(0, 4), "uvort": t(0, 1), "assemble": t(1, 2), "solve": t(2, 3),
-            "fmm_total": t(3, 4), "fmm_tree": round(s["ms_tree"], 3),
+    return {"total": t(0, 5), "uvort": t(0, 1), "assemble": t(1, 2), "solve": t(2, 3),
+            "fmm_total": t(3, 4), "particles_update": t(4, 5), "fmm_tree": round(s["ms_tree"], 3),
             "fmm_upward": round(s["ms_upward"], 3), "fmm_m2l": round(s["ms_m2l"], 3),
             "fmm_p2p": round(s["ms_p2p"], 3), "fmm_elements": round(s["ms_elems"], 3),
             "n_leaves": s["n_leaves"], "n_active_cells": s["n_active_cells"],
@@ -787,6 +800,30 @@ def count_launches(st):
         return None
 
 
+def e2e_bytes(case, n, advect):
+    """Bytes the host entry points copy per step (each call copies its own
+    inputs and outputs): dust_points_uvort (points, particles, end vortices ->
+    uvort), dust_linsys_assemble (panels, wake rows), dust_linsys_solve (->
+    strengths), dust_fmm_apply (particles, panels, wake panels, end vortices
+    -> vel, stretch, rotu) and, when advecting, dust_particles_update
+    (cen, dir, mag, vel, stretch, rotu, free flags -> cen, dir, stretch, free
+    flags, count)."""
+    d, i = 8, 4
+    nr, nw, nl = case.rank, case.wake.n, case.end_vort.n
+    panels = nr * (12 * d + 2 * i + 7 * d)        # ver, n_ver, kind, mag, ub, uvort
+    wakep = nw * (12 * d + 2 * i + d)             # ver, n_ver, kind, mag
+    lines = nl * 7 * d
+    parts = n * 8 * d                             # cen, dir, mag, r_vortex
+    h2d = (nr * 3 * d + parts + lines)            # uvort
+    h2d += panels + wakep + nw * 2 * i            # assemble (+ implicit indices)
+    h2d += parts + panels + wakep + lines         # FMM
+    d2h = nr * 3 * d + nr * d + n * 9 * d         # uvort, strengths, vel/stretch/rotu
+    if advect:
+        h2d += n * (16 * d + i)
+        d2h += n * (9 * d + i) + i
+    return h2d, d2h
+
+
 def run_e2e(case, params, mode, args, ws, pc=None):
     """Same step through the host API with pinned host buffers: every step
     copies particles and panels in and velocities/strengths out."""
@@ -797,7 +834,7 @@ def run_e2e(case, params, mode, args, ws, pc=None):
                                                   pin(case.mag), pin(case.r_vortex))
     n = case.mag.shape[0]
     out = tuple(pin(np.empty((n, 3))) for _ in range(3))  # page-locked outputs
-    hs = step.HostStepper(case, params, mode, out=out)
+    hs = step.HostStepper(case, params, mode, out=out, advect=not args.no_advect)
     if pc is not None:
         pc.attach(hs.ls)
     for _ in range(3):
@@ -815,8 +852,7 @@ def run_e2e(case, params, mode, args, ws, pc=None):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     ms = max_over_ranks(float(np.mean(times)), ws)
-    h2d = n * 8 * 8 + case.rank * 8 * (12 + 3 + 3 + 1) + case.wake.n * 8 * 13 + case.end_vort.n * 56
-    d2h = n * 9 * 8 + case.rank * 8
+    h2d, d2h = e2e_bytes(case, n, not args.no_advect)
     return {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "step_ms": [round(t, 2) for t in times]}
 

@@ -830,7 +830,6 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
 // and the radix-sort work space) lives in the fixed array below, reserved
 // when the library is loaded.
 static __device__ __align__(256) unsigned char g_uv_noalloc[DUST_UVORT_NOALLOC_SCRATCH];
-static void *g_uv_noalloc_ptr[64];  // per device, looked up on the first call there
 
 __global__ void k_line_build(int n, const double *ver, const double *mag, LineGeo *out);
 
@@ -842,10 +841,10 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
                                                 const double *r_vortex,
                                                 const dust_lines *end_vort, double *uvort,
                                                 void *stream) {
-  if (!prm || n_pts < 0 || n < 0) return DUST_ERR_BAD_ARG;
+  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
+    return DUST_ERR_BAD_ARG;
   if (n_pts == 0) return DUST_OK;
   const int nl = end_vort ? end_vort->n : 0;
-  if (nl < 0) return DUST_ERR_BAD_ARG;
   const bool f32 = prm->precision == DUST_PREC_FP32C && n > 0;
   const size_t N = (size_t)n;
   // scratch layout: [LineGeo x nl][keys/vals 16N][F 16N][X 24N][sort work]
@@ -873,15 +872,11 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
     dust_set_last_error(msg, __FILE__, __LINE__);
     return DUST_ERR_CAPACITY;
   }
-  int dev = 0;
-  DUST_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return DUST_ERR_NO_DEVICE;
-  if (!g_uv_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    DUST_CUDA(cudaGetSymbolAddress(&p, g_uv_noalloc));
-    g_uv_noalloc_ptr[dev] = p;
-  }
-  char *b = (char *)g_uv_noalloc_ptr[dev];
+  // the array's device address in the current device's context, looked up on
+  // every call (nothing cached: a context reset reloads the module)
+  void *sym = nullptr;
+  DUST_CUDA(cudaGetSymbolAddress(&sym, g_uv_noalloc));
+  char *b = (char *)sym;
   cudaStream_t st = (cudaStream_t)stream;
   ElemDev e;
   memset(&e, 0, sizeof(e));

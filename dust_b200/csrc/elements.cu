@@ -291,11 +291,24 @@ int points_uvort_device(const dust_fmm_params *prm, int n_pts, const double *pts
   return points_uvort_run(prm, n_pts, pts, n, cen, dir, mag, rv, lines, g_uv_scratch, uv, st);
 }
 
+bool uvort_args_ok(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                   const double *cen, const double *dir, const double *mag,
+                   const double *r_vortex, const dust_lines *end_vort, const double *uvort) {
+  if (!prm || n_pts < 0 || n < 0) return false;
+  if (end_vort && (end_vort->n < 0 || (end_vort->n > 0 && (!end_vort->ver || !end_vort->mag))))
+    return false;
+  if (n_pts == 0) return true;
+  if (!pts || !uvort) return false;
+  if (n > 0 && (!cen || !dir || !mag || !r_vortex)) return false;
+  return true;
+}
+
 extern "C" int dust_points_uvort(const dust_fmm_params *prm, int n_pts, const double *pts,
                                  int n, const double *cen, const double *dir,
                                  const double *mag, const double *r_vortex,
                                  const dust_lines *end_vort, double *uvort) {
-  if (!prm || n_pts < 0 || n < 0) return DUST_ERR_BAD_ARG;
+  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
+    return DUST_ERR_BAD_ARG;
   if (n_pts == 0) return DUST_OK;
   Scratch s;
   cudaStream_t st = 0;
@@ -384,7 +397,8 @@ extern "C" int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts, c
                                         int n, const double *cen, const double *dir,
                                         const double *mag, const double *r_vortex,
                                         const dust_lines *end_vort, double *uvort, void *stream) {
-  if (!prm || n_pts < 0 || n < 0) return DUST_ERR_BAD_ARG;
+  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
+    return DUST_ERR_BAD_ARG;
   if (n_pts == 0) return DUST_OK;
   cudaStream_t st = (cudaStream_t)stream;
   static thread_local Scratch s;

@@ -217,6 +217,7 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
   devbuf_free(o->shift);
   devbuf_free(o->ffbuf);
   devbuf_free(o->elem_work);
+  devbuf_free(o->p2p_grp);
   DevBuf *bufs[] = {&o->idxsum, &o->keys,   &o->keys_s, &o->vals,   &o->perm,
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
                     &o->cidx,   &o->lidx,   &o->act_key, &o->act_lev, &o->leaf_ci,
@@ -1454,6 +1455,349 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
   }
 }
 
+// --------------------------------- L2P + P2P, FP32C (CTA per sibling group)
+// The leaves of one parent share their near field: the 26 same-level
+// neighbours of any child lie in the 4 x 4 x 4 block of level-l cells around
+// the parent, and the coarser leaf neighbours (leaf_neigh, which the
+// reference derives from the parent, mod_octree.f90:964-988) are the same
+// for every child.  One CTA takes such a group (the consecutive leaves of
+// one level with one parent key; a level-1 leaf is a group of its own),
+// lists the block's active cells and the coarse leaves as particle ranges
+// once, stages the sources in tiles of PG_TILE (FP32, relative to the
+// parent's centre, tagged with their block cell or 255 for coarse ones) and
+// lets every target take the sources of its own 27 cells and all coarse
+// ones, skipping itself -- the reference's pair set exactly.  Threads per
+// target: G = 128 / (targets of the chunk) groups split the sources; FP32
+// partial sums of one tile (<= 128 terms) are folded into FP64; L2P stays
+// FP64.  Groups are taken from an atomic work counter (they differ in
+// size).
+#define PG_T 128
+#define PG_TILE 128
+#define PG_MAXR 480  // 64 block cells + 26 coarse leaves per coarser level (<= 15)
+#define PG_MAXL 8
+
+__global__ void k_p2p_groups_flag(FmmDev d, uint32_t *flag) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > d.n_leaves) return;
+  if (i == d.n_leaves) {
+    flag[i] = 0;
+    return;
+  }
+  bool start = i == 0;
+  if (!start) {
+    const uint32_t a = d.leaf_ci[i], b = d.leaf_ci[i - 1];
+    const int la = d.act_lev[a], lb = d.act_lev[b];
+    start = la != lb || la == 1 || (d.act_key[a] >> 3) != (d.act_key[b] >> 3);
+  }
+  flag[i] = start ? 1u : 0u;
+}
+
+__global__ void k_p2p_groups_scatter(uint32_t nleaves, const uint32_t *flag, const uint32_t *gid,
+                                     uint32_t *gstart, uint32_t *ngroups) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nleaves) return;
+  if (i == nleaves) {
+    gstart[gid[i]] = nleaves;
+    *ngroups = gid[i];
+  } else if (flag[i]) {
+    gstart[gid[i]] = i;
+  }
+}
+
+template <bool VS, bool DF, bool VD, bool TV>
+__global__ void __launch_bounds__(PG_T) k_p2p_g(FmmDev d, const uint32_t *gstart,
+                                                const uint32_t *ngroups_p, uint32_t *work) {
+  __shared__ float s_src[7][PG_TILE];
+  __shared__ uint32_t s_sid[PG_TILE];
+  __shared__ uint8_t s_tag[PG_TILE];
+  __shared__ uint32_t s_rlo[PG_MAXR], s_rcum[PG_MAXR + 1];
+  __shared__ uint8_t s_rtag[PG_MAXR];
+  __shared__ double s_red[12][PG_T];
+  __shared__ uint32_t s_lci[PG_MAXL], s_llo[PG_MAXL], s_tcum[PG_MAXL + 1];
+  __shared__ uint8_t s_ltag[PG_MAXL];
+  __shared__ double s_lcc[PG_MAXL][3], s_ros[PG_MAXL];
+  __shared__ int s_nr, s_wcnt[2];
+  __shared__ uint32_t s_g;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t n = d.n;
+  const uint32_t ngroups = *ngroups_p;
+  const int nm = d.nm, nm1 = d.nm1;
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  while (true) {
+    __syncthreads();
+    if (tid == 0) s_g = atomicAdd(work, 1u);
+    __syncthreads();
+    const uint32_t g = s_g;
+    if (g >= ngroups) break;
+    const uint32_t L0 = gstart[g], L1 = gstart[g + 1];
+    const int nleaf = (int)min(L1 - L0, (uint32_t)PG_MAXL);
+    const uint32_t ci0 = d.leaf_ci[L0];
+    const int l = d.act_lev[ci0];
+    int c0i, c0j, c0k;
+    cart_of_key(d.G, l, d.act_key[ci0], c0i, c0j, c0k);
+    // block origin and centre: the parent's 4^3 block (level >= 2), the
+    // leaf's own 3^3 neighbourhood at level 1
+    int bo[3], pc[3] = {c0i >> 1, c0j >> 1, c0k >> 1};
+    double bc[3];
+    const int ext = l >= 2 ? 4 : 3;
+    if (l >= 2) {
+      for (int q = 0; q < 3; ++q) bo[q] = 2 * pc[q] - 1;
+      cell_center(d.G, l - 1, pc[0], pc[1], pc[2], bc);
+    } else {
+      bo[0] = c0i - 1, bo[1] = c0j - 1, bo[2] = c0k - 1;
+      cell_center(d.G, 1, c0i, c0j, c0k, bc);
+    }
+    if (tid < nleaf) {
+      const uint32_t ci = d.leaf_ci[L0 + tid];
+      const uint32_t key = d.act_key[ci];
+      int a, b, c;
+      cart_of_key(d.G, l, key, a, b, c);
+      s_lci[tid] = ci;
+      s_llo[tid] = cell_lo(d.G, d.cstart, l, key);
+      s_ltag[tid] = (uint8_t)((a - bo[0]) + 4 * (b - bo[1]) + 16 * (c - bo[2]));
+      cell_center(d.G, l, a, b, c, s_lcc[tid]);
+      s_ros[tid] = 0.0;
+      s_tcum[tid + 1] = cell_hi(d.G, d.cstart, l, key) - s_llo[tid];
+    }
+    // the group's source ranges: block cells (warps 0-1), then the coarse
+    // leaves level by level (warp 0), in a fixed order
+    uint32_t a0 = 0, a1 = 0;
+    bool pred = false;
+    if (tid < 64) {
+      const int i = tid & 3, j = (tid >> 2) & 3, k = tid >> 4;
+      if (i < ext && j < ext && k < ext) {
+        const int ci_ = bo[0] + i, cj = bo[1] + j, ck = bo[2] + k;
+        if (cart_in(d.G, l, ci_, cj, ck)) {
+          const uint32_t nk = key_of(d.G, l, ci_, cj, ck);
+          if (d.flags[d.G.lev_off[l] + nk] & FL_ACTIVE) {
+            a0 = cell_lo(d.G, d.cstart, l, nk);
+            a1 = cell_hi(d.G, d.cstart, l, nk);
+            pred = a1 > a0;
+          }
+        }
+      }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, pred);
+    if (lane == 0 && warp < 2) s_wcnt[warp] = __popc(bal);
+    __syncthreads();
+    if (tid == 0) {
+      s_tcum[0] = 0;
+      for (int q = 0; q < nleaf; ++q) s_tcum[q + 1] += s_tcum[q];
+    }
+    if (tid < 64 && pred) {
+      const int pos = (warp == 1 ? s_wcnt[0] : 0) + __popc(bal & ((1u << lane) - 1u));
+      s_rlo[pos] = a0;
+      s_rcum[pos] = a1 - a0;
+      s_rtag[pos] = (uint8_t)tid;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int nr = s_wcnt[0] + s_wcnt[1];
+      for (int lev = l - 1; lev >= 1; --lev) {
+        const int sh = l - lev;
+        const int ai = c0i >> sh, aj = c0j >> sh, ak = c0k >> sh;
+        bool pr = false;
+        uint32_t b0 = 0, b1 = 0;
+        if (lane < 27 && lane != 13) {
+          const int di = lane % 3 - 1, dj = (lane / 3) % 3 - 1, dk = lane / 9 - 1;
+          if (cart_in(d.G, lev, ai + di, aj + dj, ak + dk)) {
+            const uint32_t nk = key_of(d.G, lev, ai + di, aj + dj, ak + dk);
+            if (d.flags[d.G.lev_off[lev] + nk] & FL_LEAF) {
+              b0 = cell_lo(d.G, d.cstart, lev, nk);
+              b1 = cell_hi(d.G, d.cstart, lev, nk);
+              pr = b1 > b0;
+            }
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, pr);
+        if (pr && nr + __popc(m) <= PG_MAXR) {
+          const int pos = nr + __popc(m & ((1u << lane) - 1u));
+          s_rlo[pos] = b0;
+          s_rcum[pos] = b1 - b0;
+          s_rtag[pos] = 255;
+        }
+        nr = min(nr + __popc(m), PG_MAXR);
+      }
+      // exclusive prefix of the range lengths (32 at a time)
+      uint32_t run = 0;
+      for (int r0 = 0; r0 < nr; r0 += 32) {
+        const int r = r0 + lane;
+        const uint32_t len = r < nr ? s_rcum[r] : 0u;
+        uint32_t x = len;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (r < nr) s_rcum[r] = run + x - len;
+        run += __shfl_sync(0xffffffffu, x, 31);
+      }
+      if (lane == 0) {
+        s_rcum[nr] = run;
+        s_nr = nr;
+      }
+    }
+    __syncthreads();
+    const int nr = s_nr;
+    const uint32_t S = s_rcum[nr];
+    const int NT = (int)s_tcum[nleaf];
+    // pair counts of the reference's near field (per leaf: its targets x the
+    // sources of its 27 cells and the coarse leaves, minus itself)
+    if (tid < nleaf && d.counters) {
+      const int lt = s_ltag[tid], lx = lt & 3, ly = (lt >> 2) & 3, lz = lt >> 4;
+      uint64_t ns = 0;
+      for (int r = 0; r < nr; ++r) {
+        const int tg = s_rtag[r];
+        if (tg != 255) {
+          const int dx = (tg & 3) - lx, dy = ((tg >> 2) & 3) - ly, dz = (tg >> 4) - lz;
+          if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+        }
+        ns += s_rcum[r + 1] - s_rcum[r];
+      }
+      const uint64_t nt = s_tcum[tid + 1] - s_tcum[tid];
+      atomicAdd((unsigned long long *)d.counters + 1, (unsigned long long)(nt * (ns - 1)));
+    }
+    // L2P of one target (FP64) with its leaf's local expansion
+    auto l2p = [&](int lf, uint32_t ti, double *lv, double *gg) {
+      const uint32_t ci = s_lci[lf];
+      const double *bl = d.B + (size_t)ci * 3 * nm, *gl = d.Gx + (size_t)ci * 3 * nm1;
+      const double x = d.P[ti] - s_lcc[lf][0], y = d.P[n + ti] - s_lcc[lf][1],
+                   z = d.P[2 * n + ti] - s_lcc[lf][2];
+      double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
+      px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+      for (int e = 1; e <= DUST_MAXP; ++e) {
+        px[e] = px[e - 1] * x;
+        py[e] = py[e - 1] * y;
+        pz[e] = pz[e - 1] * z;
+      }
+      for (int e = 0; e < 3; ++e) lv[e] = 0.0;
+      for (int e = 0; e < 9; ++e) gg[e] = 0.0;
+      for (int m = 0; m < nm; ++m) {
+        int mi, mj, mk;
+        mono_exp(m, mi, mj, mk);
+        const double pr = px[mi] * py[mj] * pz[mk];
+        for (int e = 0; e < 3; ++e) lv[e] += __ldg(bl + 3 * m + e) * pr;
+        if (VS) {
+          const double *g0 = gl + 3 * mono_idx(mi + 1, mj, mk),
+                       *g1 = gl + 3 * mono_idx(mi, mj + 1, mk),
+                       *g2 = gl + 3 * mono_idx(mi, mj, mk + 1);
+          const double f0 = (mi + 1) * pr, f1 = (mj + 1) * pr, f2 = (mk + 1) * pr;
+          for (int e = 0; e < 3; ++e) {
+            gg[0 + 3 * e] += f0 * __ldg(g0 + e);
+            gg[1 + 3 * e] += f1 * __ldg(g1 + e);
+            gg[2 + 3 * e] += f2 * __ldg(g2 + e);
+          }
+        }
+      }
+    };
+    auto leaf_of = [&](int t) {
+      int lf = 0;
+      while (lf + 1 < nleaf && (int)s_tcum[lf + 1] <= t) ++lf;
+      return lf;
+    };
+    if (TV) {
+      // leaf average of |sym(grad)|^2 from the local expansion (:1214-1230)
+      for (int t = tid; t < NT; t += PG_T) {
+        const int lf = leaf_of(t);
+        double lv[3], gg[9];
+        l2p(lf, s_llo[lf] + (t - s_tcum[lf]), lv, gg);
+        double part = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) {
+            const double sy = 0.5 * (gg[a + 3 * b] + gg[b + 3 * a]);
+            part += sy * sy;
+          }
+        atomicAdd(&s_ros[lf], part);
+      }
+      __syncthreads();
+    }
+    for (int tc0 = 0; tc0 < NT; tc0 += PG_T) {
+      const int cnt = min(PG_T, NT - tc0);
+      const int G = PG_T / cnt, tl = tid % cnt, grp = tid / cnt;
+      const bool act = grp < G;
+      const int t = tc0 + tl;
+      const int lf = leaf_of(t);
+      const uint32_t ti = s_llo[lf] + (uint32_t)(t - (int)s_tcum[lf]);
+      const int lt = s_ltag[lf], tx = lt & 3, ty = (lt >> 2) & 3, tz = lt >> 4;
+      const float ftp[3] = {(float)(d.P[ti] - bc[0]), (float)(d.P[n + ti] - bc[1]),
+                            (float)(d.P[2 * n + ti] - bc[2])};
+      const float fta[3] = {(float)d.P[3 * n + ti], (float)d.P[4 * n + ti],
+                            (float)d.P[5 * n + ti]};
+      double A[12];
+      for (int e = 0; e < 12; ++e) A[e] = 0.0;
+      for (uint32_t s0 = 0; s0 < S; s0 += PG_TILE) {
+        __syncthreads();
+        const uint32_t v = s0 + tid;
+        if (v < S) {
+          int a = 0, b = nr - 1;
+          while (a < b) {  // last r with s_rcum[r] <= v
+            const int mid = (a + b + 1) >> 1;
+            if (s_rcum[mid] <= v) a = mid; else b = mid - 1;
+          }
+          const uint32_t sidx = s_rlo[a] + (v - s_rcum[a]);
+          s_sid[tid] = sidx;
+          s_tag[tid] = s_rtag[a];
+          for (int q = 0; q < 3; ++q) s_src[q][tid] = (float)(d.P[(size_t)q * n + sidx] - bc[q]);
+          for (int q = 3; q < 7; ++q) s_src[q][tid] = (float)d.P[(size_t)q * n + sidx];
+        }
+        __syncthreads();
+        const int m = (int)min((uint32_t)PG_TILE, S - s0);
+        if (act) {
+          P2PAccF B;
+          for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+          for (int u = grp; u < m; u += G) {
+            const int tg = s_tag[u];
+            if (tg != 255) {
+              const int dx = (tg & 3) - tx, dy = ((tg >> 2) & 3) - ty, dz = (tg >> 4) - tz;
+              if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+            }
+            if (s_sid[u] == ti) continue;
+            p2p_pair_f<VS, DF, VD>(ftp, fta, s_src[0][u], s_src[1][u], s_src[2][u], s_src[3][u],
+                                   s_src[4][u], s_src[5][u], s_src[6][u], B);
+          }
+          for (int e = 0; e < 3; ++e) {
+            A[e] += (double)B.v[e];
+            A[3 + e] += (double)B.s[e];
+            A[6 + e] += (double)B.r[e];
+            A[9 + e] += (double)B.f[e];
+          }
+        }
+      }
+      // combine the groups of each target: group 0 adds the others' sums
+      __syncthreads();
+      if (act && grp > 0)
+        for (int e = 0; e < 12; ++e) s_red[e][tid] = A[e];
+      __syncthreads();
+      if (act && grp == 0) {
+        for (int g2 = 1; g2 < G; ++g2)
+          for (int e = 0; e < 12; ++e) A[e] += s_red[e][g2 * cnt + tl];
+        const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
+        double lv[3], gg[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
+        l2p(lf, ti, lv, gg);
+        if (VS) {
+          for (int e = 0; e < 3; ++e) ls[e] = ta[0] * gg[e] + ta[1] * gg[e + 3] + ta[2] * gg[e + 6];
+          if (DF) {
+            lr[0] = gg[1 + 6] - gg[2 + 3];
+            lr[1] = gg[2 + 0] - gg[0 + 6];
+            lr[2] = gg[0 + 3] - gg[1 + 0];
+          }
+        }
+        double nu = d.nu_inf;
+        if (TV) {
+          const double rv = d.P[6 * n + ti];
+          const double ave = s_ros[lf] / (double)(s_tcum[lf + 1] - s_tcum[lf]);
+          nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave);
+        }
+        for (int e = 0; e < 3; ++e) {
+          d.out[(size_t)e * n + ti] = lv[e] + A[e] * k4pi;
+          d.out[(size_t)(3 + e) * n + ti] = ls[e] + A[3 + e] * k4pi + (VD ? A[9 + e] * nu : 0.0);
+          d.out[(size_t)(6 + e) * n + ti] = lr[e] + A[6 + e] * k4pi;
+        }
+      }
+    }
+  }
+}
+
 // ======================================================== host orchestration
 static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -1647,11 +1991,36 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
     size_t shl = (size_t)3 * (o->nm + o->nm1) * 8 + (size_t)4 * o->nm * 4;
     bool vs = d.use_vs, df = d.use_df, vd = d.use_vd, tv = o->prm.turbulent_viscosity != 0;
     const bool f32 = o->prm.precision == DUST_PREC_FP32C;
+    uint32_t *gstart = nullptr, *ngroups = nullptr, *work = nullptr;
+    unsigned pg_grid = 0;
+    if (f32) {
+      // sibling groups of the leaf list (consecutive leaves of one level
+      // and one parent): flags, exclusive scan, starts
+      const size_t nl1 = (size_t)o->n_leaves + 1;
+      DUST_TRY(grow(o->p2p_grp, 3 * nl1 * 4 + 256));
+      uint32_t *flag = (uint32_t *)o->p2p_grp.p, *gid = flag + nl1;
+      gstart = gid + nl1;
+      ngroups = gstart + nl1;
+      work = ngroups + 1;
+      k_p2p_groups_flag<<<nblk(nl1, 256), 256, 0, st>>>(d, flag);
+      size_t tbg = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tbg, flag, gid, (int)nl1, st);
+      DUST_TRY(grow(o->cub_tmp, tbg));
+      DUST_CUDA(cub::DeviceScan::ExclusiveSum(o->cub_tmp.p, tbg, flag, gid, (int)nl1, st));
+      k_p2p_groups_scatter<<<nblk(nl1, 256), 256, 0, st>>>((uint32_t)o->n_leaves, flag, gid,
+                                                           gstart, ngroups);
+      DUST_CUDA(cudaMemsetAsync(work, 0, 4, st));
+      int dev = 0, nsm = 148, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2p_g<true, true, true, false>,
+                                                    PG_T, 0);
+      pg_grid = (unsigned)std::min<int64_t>((int64_t)nsm * std::max(per, 1), o->n_leaves);
+    }
 #define LAUNCH_P2P(A, B, C, D)                                                   \
   do {                                                                         \
     if (f32)                                                                   \
-      k_p2p_w<A, B, C, D><<<(unsigned)((o->n_leaves + P2W_WARPS - 1) / P2W_WARPS), \
-                            P2W_WARPS * 32, 0, st>>>(d);                        \
+      k_p2p_g<A, B, C, D><<<pg_grid, PG_T, 0, st>>>(d, gstart, ngroups, work);  \
     else                                                                       \
       k_p2p<A, B, C, D, false><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);   \
   } while (0)

@@ -66,6 +66,7 @@ struct dust_octree {
   DevBuf h_in, h_out, el_geo, el_raw;  // staging of host-API calls
   DevBuf ffbuf;                        // far-field panel records
   DevBuf elem_work;                    // FP32C element sums: far sums, near-pair list
+  DevBuf p2p_grp;                      // FP32C P2P sibling groups: flags, ids, starts, counters
   size_t near_cap = 0;                 // capacity of the near-pair list
   DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless M2L tables (FP64)
   DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless M2L tables (FP32)
@@ -99,6 +100,12 @@ int elem_build_device(const dust_panels *body, const dust_panels *wake,
                       bool host_arrays, DevBuf &raw, DevBuf &geo, ElemDev &out,
                       cudaStream_t st);
 RegParams reg_params(const dust_fmm_params *prm);
+// Argument check shared by the uvort entry points: the points and the
+// output when there are points, the four particle arrays when there are
+// particles, the end vortices' vertices and strengths when there are any.
+bool uvort_args_ok(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                   const double *cen, const double *dir, const double *mag,
+                   const double *r_vortex, const dust_lines *end_vort, const double *uvort);
 
 // m2l.cu
 int m2l_batch_tables(dust_octree *o);

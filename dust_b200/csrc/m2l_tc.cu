@@ -17,23 +17,23 @@
 // the FP32 remainder, and a product is Ah Bh + Ah Bl + Al Bh, which keeps
 // about FP32 accuracy; the tables are split from their FP64 values.
 //
-// Roles (320 threads):
+// Roles (448 threads):
 //  warps 0-7  producers: per offset look up the 128 source cells (empty,
-//             inactive or missing ones give zero rows), then per component
-//             gather their coefficients into shared memory as TF32 high/low
-//             parts in the canonical no-swizzle K-major layout.  They also
-//             drain the TMEM accumulators to FP64 (one row = one target per
-//             thread, half the columns per warp) every MT_GROUP offsets and
-//             at the end add the rescaled locals to the FP64 b and g;
-//  warp 8     lane 0 issues the 90 tcgen05.mma of an offset and commits;
-//  warp 9     lane 0 streams the offset's table image (61,440 B, prepared
+//             inactive or missing ones give zero rows) and copy their
+//             pre-split coefficients (TF32 high part, FP32 remainder) with
+//             cp.async into the canonical no-swizzle K-major layout, one
+//             (component, split) per stage, four stages in rotation;
+//  warps 8-11 drain the TMEM accumulators to FP64 (one TMEM lane quarter =
+//             32 targets per warp, all columns per thread) every MT_GROUP
+//             offsets while the tensor core runs the next group, and at the
+//             end add the rescaled locals to the FP64 b and g;
+//  warp 12    lane 0 issues the 90 tcgen05.mma of an offset and commits;
+//  warp 13    lane 0 streams the offset's table image (61,440 B, prepared
 //             once per level in the operand layout) with one bulk copy.
-// Two A buffers (one component each) and two B buffers overlap gathering,
-// copying and the tensor core.  Offsets where no target of the CTA has a
-// source are skipped altogether.  Every mbarrier wait is bounded: a role
-// that gives up raises a CTA flag that stops the others; the kernel then
-// reports through `err`, waits (bounded) for its copies and MMAs, frees TMEM
-// and returns.
+// Offsets where no target of the CTA has a source are skipped altogether.
+// Every mbarrier wait is bounded: a role that gives up raises a CTA flag
+// that stops the others; the kernel then reports through `err`, waits
+// (bounded) for its copies and MMAs, frees TMEM and returns.
 #include <cstring>
 #include <vector>
 
@@ -46,11 +46,10 @@
 #define MT_N 64
 #define MT_KCH (MT_K / 4)
 #define MT_ASPLIT (MT_KCH * 2048)  // one split of an A buffer: 128 rows x 40
-#define MT_ABUF (2 * MT_ASPLIT)
 #define MT_BSPLIT (MT_KCH * 1024)  // one split of one component table: 64 rows
 #define MT_BCOMP (2 * MT_BSPLIT)
 #define MT_BIMG (3 * MT_BCOMP)  // one offset: 3 components x (high, low)
-#define MT_SMEM (2 * MT_BIMG + 2 * MT_ABUF + 1024)
+#define MT_SMEM (2 * MT_BIMG + 4 * MT_ASPLIT + 1024)  // 2 table images, 4 A stages
 #define MT_NCAND 216
 
 // byte offsets in the canonical K-major no-swizzle layouts (core matrices of
@@ -81,7 +80,8 @@ __global__ void k_m2l_tc_image(const double *dtab, const uint16_t *isum, int nD,
 }
 
 // scaled source coefficients ahat(n, c) = a(n, c) / (n! h^|n|) of the active
-// cells of levels >= 2, as [cell][c][40] (zero beyond nm)
+// cells of levels >= 2 in FP32, split for 3xTF32 into the TF32 rounding and
+// the FP32 remainder: [cell][c][hi, lo][40] (zero beyond nm)
 __global__ void k_scale_a_tc(FmmDev d, uint32_t c0, uint32_t nact, float *out) {
   size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)(nact - c0) * 3 * MT_K;
@@ -97,7 +97,10 @@ __global__ void k_scale_a_tc(FmmDev d, uint32_t c0, uint32_t nact, float *out) {
     for (int q = 0; q < ni + nj + nk; ++q) hp *= hi;
     v = (float)(d.A[(size_t)ci * 3 * d.nm + 3 * nn + c] * d.inv_fact[nn] * hp);
   }
-  out[e] = v;
+  const float hv = tf32_rna(v);
+  float *o = out + (size_t)(ci - c0) * 6 * MT_K + 2 * c * MT_K + nn;
+  o[0] = hv;
+  o[MT_K] = v - hv;
 }
 
 struct MtCand {
@@ -162,64 +165,51 @@ __global__ void k_m2l_tc_lists(FmmDev d, const int4 *batches, const uint32_t *li
   if (r < 7) mask[(size_t)blockIdx.x * 8 + r] = s_mask[r];
 }
 
-#define MT_HALF 28  // output columns per drain thread (two threads per target)
+#define MT_NOUT 56  // output monomials of the drain and epilogue (nout <= 56)
 
-// Drain of one accumulator set (the FP32 sums of a group of offsets): this
-// warp's TMEM lanes are its 32 targets, the thread's columns m' are
-// [28 h, 28 h + 28) of each component.  The sums are added in FP64 to the
-// CTA's scratch scr[e][m'][r] (stored, not added, for the first group), a
-// layout in which a warp's 32 targets are contiguous.
-__device__ __forceinline__ void mt_drain(uint32_t tmem, int warp, int h, int set, int r, int nout,
+// Drain of one accumulator set (the FP32 sums of a group of offsets): the
+// drain warp's TMEM lane quarter holds its 32 targets, the thread is target
+// row r; all 3 x nout sums are added in FP64 to the CTA's scratch
+// scr[e][m'][r] (stored, not added, for the first group), a layout in which
+// a warp's 32 targets are contiguous.  16 columns per tcgen05.ld, their 16
+// FP64 partial sums loaded together.
+__device__ __forceinline__ void mt_drain(uint32_t tmem, int quarter, int set, int r, int nout,
                                          bool first, double *__restrict__ scr) {
-  const uint32_t base =
-      tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(set * 256 + MT_HALF * h);
+  const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(set * 256);
 #pragma unroll 1
   for (int e = 0; e < 3; ++e) {
-    uint32_t v[MT_HALF];
-    const uint32_t a = base + (uint32_t)(e * MT_N);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-        "%10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-          "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(a));
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-          "=r"(v[22]), "=r"(v[23])
-        : "r"(a + 16));
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27])
-                 : "r"(a + 24));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    double *sc = scr + ((size_t)e * nout + MT_HALF * h) * MT_M + r;
+#pragma unroll 1
+    for (int j0 = 0; j0 < nout; j0 += 16) {
+      uint32_t v[16];
+      const uint32_t a = base + (uint32_t)(e * MT_N + j0);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+          "%10, %11, %12, %13, %14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(a));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double *sc = scr + ((size_t)e * nout + j0) * MT_M + r;
+      double o[16];
 #pragma unroll
-    for (int j0 = 0; j0 < MT_HALF; j0 += MT_HALF / 2) {
-      double o[MT_HALF / 2];
+      for (int j = 0; j < 16; ++j)
+        o[j] = (!first && j0 + j < nout) ? sc[(size_t)j * MT_M] : 0.0;
 #pragma unroll
-      for (int j = 0; j < MT_HALF / 2; ++j)
-        o[j] = (!first && MT_HALF * h + j0 + j < nout) ? sc[(size_t)(j0 + j) * MT_M] : 0.0;
-#pragma unroll
-      for (int j = 0; j < MT_HALF / 2; ++j)
-        if (MT_HALF * h + j0 + j < nout)
-          sc[(size_t)(j0 + j) * MT_M] = o[j] + (double)__uint_as_float(v[j0 + j]);
+      for (int j = 0; j < 16; ++j)
+        if (j0 + j < nout) sc[(size_t)j * MT_M] = o[j] + (double)__uint_as_float(v[j]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
 }
 
-// adds the CTA's scratch sums, rescaled, to the targets' b and g (once)
-__device__ __forceinline__ void mt_epilogue(const FmmDev &d, int h, int r, bool valid,
-                                            uint32_t ci, int nout, const double *s_sc,
-                                            const double *__restrict__ scr) {
-  if (!valid) return;
+// adds the CTA's scratch sums, rescaled, to target row r's b and g (once)
+__device__ __forceinline__ void mt_epilogue(const FmmDev &d, int r, uint32_t ci, int nout,
+                                            const double *s_sc, const double *__restrict__ scr) {
   const int nm = d.nm, nm1 = d.nm1;
   double *__restrict__ gx = d.Gx + (size_t)ci * 3 * nm1;
   double *__restrict__ bb = d.B + (size_t)ci * 3 * nm;
-  for (int j = 0; j < MT_HALF; ++j) {
-    const int mo = MT_HALF * h + j;
-    if (mo >= nout) break;
+  for (int mo = 0; mo < nout; ++mo) {
     for (int e = 0; e < 3; ++e) {
       const double val = s_sc[mo] * scr[((size_t)e * nout + mo) * MT_M + r];
       if (d.use_vs) gx[3 * mo + e] += val;
@@ -228,28 +218,47 @@ __device__ __forceinline__ void mt_epilogue(const FmmDev &d, int h, int r, bool 
   }
 }
 
-// producers (MT_PW warps, MT_DW of them also drainers); the MMA issuer and
-// the table loader: one warp each
-#ifndef MT_PW
-#define MT_PW 8  // producer warps (gathers); 10 and 20 measured slower
-#endif
-#define MT_DW 8  // of which drain the TMEM accumulators (4 lane quarters x 2 column halves)
+// Roles: MT_PW producer warps, 4 drain warps (warps MT_PW .. MT_PW + 3, one
+// TMEM lane quarter each: MT_PW is a multiple of 4), the MMA issuer and the
+// table loader.
+#define MT_PW 8
 #define MT_P (MT_PW * 32)
-#define MT_D (MT_DW * 32)
-#define MT_THREADS2 (MT_P + 64)
-static_assert((MT_M * MT_KCH) % MT_P == 0 && MT_PW >= MT_DW, "producer layout");
+#define MT_DRAIN0 MT_PW
+#define MT_MMAW (MT_PW + 4)
+#define MT_TMAW (MT_PW + 5)
+#define MT_THREADS2 ((MT_PW + 6) * 32)
+// A stages: one (component, split) of 128 rows x 40 monomials each; a
+// producer keeps MT_LAG stages of copies in flight before it publishes one
+#define MT_NS 4
+#define MT_LAG 2
+#define MT_ITEMS ((MT_M * MT_KCH) / MT_P)  // 16-byte chunks per producer and stage
+static_assert((MT_M * MT_KCH) % MT_P == 0 && MT_PW % 4 == 0 && MT_LAG < MT_NS, "layout");
 // offsets accumulated in one TMEM set before it is drained to FP64 (the
 // tensor core's FP32 accumulation truncates, so its runs are kept short)
 #ifndef MT_GROUP
 #define MT_GROUP 4
 #endif
 
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"((uint64_t)src)
+               : "memory");
+}
+
+// One CTA = up to 128 targets of one level and octant class.  Sources are
+// the pre-split coefficients ahat2[cell][c][hi, lo][40] (TF32-rounded high
+// part and FP32 remainder of the FP32 scaled coefficient), copied with
+// cp.async into MT_NS rotating stages of one (component, split) each; per
+// offset the six stages feed 90 tcgen05.mma (for source component c: the
+// high part with the table's high and low parts, the low part with the
+// table's high part, for the two output components its cross product
+// reaches).  The accumulators of MT_GROUP offsets are drained to FP64 by
+// dedicated warps while the next group runs.
 __global__ void __launch_bounds__(MT_THREADS2, 1)
     k_m2l_tc(FmmDev d, const int4 *batches, const uint32_t *list, const int *srcl,
-             const uint32_t *maskl, const float *img, const float *ahat, uint32_t c0, int nout,
+             const uint32_t *maskl, const float *img, const float *ahat2, uint32_t c0, int nout,
              double *scratch, unsigned long long *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
-  __shared__ __align__(8) uint64_t s_bfull[2], s_bempty[2], s_afull[2], s_aempty[2];
+  __shared__ __align__(8) uint64_t s_bfull[2], s_bempty[2], s_afull[MT_NS], s_aempty[MT_NS];
   __shared__ __align__(8) uint64_t s_cfull[2], s_cempty[2], s_done;
   __shared__ uint32_t s_tmem;
   __shared__ int s_fail, s_bissued, s_bconsumed;
@@ -265,20 +274,22 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
   double *scr = scratch + (size_t)blockIdx.x * 3 * nout * MT_M;
   volatile int *fail = &s_fail;
 
-  if (warp == MT_PW) {
+  if (warp == MT_MMAW) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&s_tmem)),
                  "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == MT_P + 32) {
+  if (tid == MT_TMAW * 32) {
     for (int b = 0; b < 2; ++b) {
       mbar_init(&s_bfull[b], 1);
       mbar_init(&s_bempty[b], 1);
+      mbar_init(&s_cfull[b], 1);
+      mbar_init(&s_cempty[b], 128);
+    }
+    for (int b = 0; b < MT_NS; ++b) {
       mbar_init(&s_afull[b], MT_P);
       mbar_init(&s_aempty[b], 1);
-      mbar_init(&s_cfull[b], 1);
-      mbar_init(&s_cempty[b], MT_D);
     }
     mbar_init(&s_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;");
@@ -303,16 +314,11 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
+  int ntot = 0;  // offsets with a source for some target of the CTA
+  for (int w = 0; w < 7; ++w) ntot += __popc(s_mask[w]);
 
   if (warp < MT_PW) {
-    // ------------------------------------------------ producers / drainers
-    // drain role: target row r (TMEM lane), columns m' in [28 h, 28 h + 28)
-    const bool drainer = warp < MT_DW;
-    const int r = (warp & 3) * 32 + lane, h = warp >> 2;
-    const bool valid = drainer && r < cnt;
-    const uint32_t ci = valid ? list[t0 + r] : 0u;
-    int ntot = 0;  // present offsets
-    for (int w = 0; w < 7; ++w) ntot += __popc(s_mask[w]);
+    // ------------------------------------------------------------ producers
     // next candidate offset after `c` with a source for some target (216 = none)
     auto next_cand = [&](int c) {
       for (int w = (c + 1) >> 5; w < 7; ++w) {
@@ -322,87 +328,80 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
       }
       return MT_NCAND;
     };
-    constexpr int NI = (MT_M * MT_KCH) / MT_P;  // gather items per thread
-    int u = 0, oi = 0;
+    int u = 0;
     bool ok = true;
     int cand = next_cand(-1);
-    int sidx_next[NI];
+    int sidx_next[MT_ITEMS];
 #pragma unroll
-    for (int i = 0; i < NI; ++i)
-      sidx_next[i] = cand < MT_NCAND ? __ldg(src + (size_t)cand * MT_M + (tid + MT_P * i) / MT_KCH) : -1;
+    for (int i = 0; i < MT_ITEMS; ++i)
+      sidx_next[i] =
+          cand < MT_NCAND ? __ldg(src + (size_t)cand * MT_M + (tid + MT_P * i) / MT_KCH) : -1;
     while (cand < MT_NCAND && ok) {
-      int sidx[NI];
+      int sidx[MT_ITEMS];
 #pragma unroll
-      for (int i = 0; i < NI; ++i) sidx[i] = sidx_next[i];
+      for (int i = 0; i < MT_ITEMS; ++i) sidx[i] = sidx_next[i];
       const int ncand = next_cand(cand);
-      // the next offset's sources are fetched while this one is gathered
 #pragma unroll
-      for (int i = 0; i < NI; ++i)
+      for (int i = 0; i < MT_ITEMS; ++i)
         sidx_next[i] =
             ncand < MT_NCAND ? __ldg(src + (size_t)ncand * MT_M + (tid + MT_P * i) / MT_KCH) : -1;
-      // all three components' loads in flight at once
-      float4 v[3][NI];
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int i = 0; i < NI; ++i) {
-          const int kc = (tid + MT_P * i) % MT_KCH;
-          v[c][i] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (sidx[i] >= 0)
-            v[c][i] = __ldg((const float4 *)(ahat + (size_t)(sidx[i] - (int)c0) * 3 * MT_K +
-                                             c * MT_K + 4 * kc));
-        }
-#pragma unroll
-      for (int c = 0; c < 3; ++c, ++u) {
-        const int sa = u & 1;
-        if (u >= 2 && !mbar_wait_f(smem_u32(&s_aempty[sa]), (uint32_t)(((u >> 1) - 1) & 1), fail)) {
+      for (int cs = 0; cs < 6 && ok; ++cs, ++u) {
+        const int buf = u % MT_NS;
+        if (u >= MT_NS &&
+            !mbar_wait_f(smem_u32(&s_aempty[buf]), (uint32_t)((u / MT_NS - 1) & 1), fail)) {
           ok = false;
           break;
         }
-        unsigned char *A = sA + sa * MT_ABUF;
+        const uint32_t abase = smem_u32(sA + buf * MT_ASPLIT);
+        const int c = cs >> 1, sp = cs & 1;
 #pragma unroll
-        for (int i = 0; i < NI; ++i) {
+        for (int i = 0; i < MT_ITEMS; ++i) {
           const int item = tid + MT_P * i, rr = item / MT_KCH, kc = item % MT_KCH;
-          const float4 x = v[c][i];
-          const float4 hv = make_float4(tf32_rna(x.x), tf32_rna(x.y), tf32_rna(x.z), tf32_rna(x.w));
-          const float4 lv = make_float4(x.x - hv.x, x.y - hv.y, x.z - hv.z, x.w - hv.w);
-          *(float4 *)(A + mt_aoff(rr, 4 * kc)) = hv;
-          *(float4 *)(A + MT_ASPLIT + mt_aoff(rr, 4 * kc)) = lv;
+          const uint32_t dst = abase + mt_aoff(rr, 4 * kc);
+          if (sidx[i] >= 0) {
+            cp_async16(dst, ahat2 + (size_t)(sidx[i] - (int)c0) * 6 * MT_K + (2 * c + sp) * MT_K +
+                                4 * kc);
+          } else {
+            asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(dst), "r"(0u)
+                         : "memory");
+          }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&s_afull[sa]);
-      }
-      if (!ok) break;
-      // a group's set is drained once the next group has started (its MMAs
-      // then overlap the drain), the last group after the loop
-      if (drainer && oi % MT_GROUP == 0 && oi >= MT_GROUP) {
-        const int g = oi / MT_GROUP - 1;
-        if (!mbar_wait_f(smem_u32(&s_cfull[g & 1]), (uint32_t)((g >> 1) & 1), fail)) {
-          ok = false;
-          break;
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        if (u >= MT_LAG) {
+          // the copies of stage u - MT_LAG have landed: publish it
+          asm volatile("cp.async.wait_group %0;" ::"n"(MT_LAG) : "memory");
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(&s_afull[(u - MT_LAG) % MT_NS]);
         }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        mt_drain(tmem, warp, h, g & 1, r, nout, g == 0, scr);
-        mbar_arrive(&s_cempty[g & 1]);
       }
-      ++oi;
       cand = ncand;
     }
-    if (drainer && ok && ntot > 0) {
-      const int g = (ntot - 1) / MT_GROUP;
-      if (mbar_wait_f(smem_u32(&s_cfull[g & 1]), (uint32_t)((g >> 1) & 1), fail)) {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        mt_drain(tmem, warp, h, g & 1, r, nout, g == 0, scr);
-        mbar_arrive(&s_cempty[g & 1]);
-        mt_epilogue(d, h, r, valid, ci, nout, s_sc, scr);
+    // publish the stages still in flight (on every path: the copies land
+    // whether or not a consumer is left)
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (ok)
+      for (int v = (u > MT_LAG ? u - MT_LAG : 0); v < u; ++v) mbar_arrive(&s_afull[v % MT_NS]);
+  } else if (warp < MT_DRAIN0 + 4) {
+    // --------------------------------------------------------------- drains
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
+    const int ngroups = (ntot + MT_GROUP - 1) / MT_GROUP;
+    bool ok = true;
+    for (int g = 0; g < ngroups && ok; ++g) {
+      if (!mbar_wait_f(smem_u32(&s_cfull[g & 1]), (uint32_t)((g >> 1) & 1), fail)) {
+        ok = false;
+        break;
       }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      mt_drain(tmem, quarter, g & 1, r, nout, g == 0, scr);
+      mbar_arrive(&s_cempty[g & 1]);
     }
-  } else if (warp == MT_PW && lane == 0) {
+    if (ok && ngroups > 0 && r < cnt) mt_epilogue(d, r, list[t0 + r], nout, s_sc, scr);
+  } else if (warp == MT_MMAW && lane == 0) {
     // ---------------------------------------------------------- MMA issuer
     const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(MT_N >> 3) << 17) |
                            ((uint32_t)(MT_M >> 4) << 24);
-    int ntot = 0;
-    for (int w = 0; w < 7; ++w) ntot += __popc(s_mask[w]);
     int u = 0, oi = 0;
     bool ok = true;
     uint32_t started = 0;  // bit e: accumulator e written in this group
@@ -419,14 +418,15 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
         started = 0;
       }
       const uint32_t bbase = smem_u32(sB + sb * MT_BIMG);
-      for (int c = 0; c < 3; ++c, ++u) {
-        const int sa = u & 1;
-        if (!mbar_wait_f(smem_u32(&s_afull[sa]), (uint32_t)((u >> 1) & 1), fail)) {
+      for (int cs = 0; cs < 6; ++cs, ++u) {
+        const int buf = u % MT_NS;
+        if (!mbar_wait_f(smem_u32(&s_afull[buf]), (uint32_t)((u / MT_NS) & 1), fail)) {
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t abase = smem_u32(sA + sa * MT_ABUF);
+        const uint32_t as = smem_u32(sA + buf * MT_ASPLIT);
+        const int c = cs >> 1, sp = cs & 1;
         for (int pp = 0; pp < 2; ++pp) {
           // source component c feeds two accumulators e with table component
           // dd and sign:  c = x: (y, D_z, +) (z, D_y, -);  c = y: (x, D_z, -)
@@ -436,19 +436,20 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
           const uint32_t neg = pp == 0 ? (c == 1 ? 1u : 0u) : (c == 1 ? 0u : 1u);
           const uint32_t id = idesc | (neg << 13);
           const uint32_t bcomp = bbase + dd * MT_BCOMP;
-          // 3xTF32: (A hi, B hi), (A hi, B lo), (A lo, B hi)
-          for (int sp = 0; sp < 3; ++sp) {
-            const uint32_t as = abase + (sp == 2 ? MT_ASPLIT : 0);
-            const uint32_t bs = bcomp + (sp == 1 ? MT_BSPLIT : 0);
+          // 3xTF32: the high stage meets the table's high and low parts,
+          // the low stage the table's high part
+          for (int tb = 0; tb < (sp == 0 ? 2 : 1); ++tb) {
+            const uint32_t bs = bcomp + (tb == 1 ? MT_BSPLIT : 0);
 #pragma unroll
             for (int j = 0; j < MT_K / 8; ++j) {
-              umma_tf32(tmem + (uint32_t)(set * 256 + e * MT_N), make_sdesc(as + j * 4096, 2048, 128),
+              umma_tf32(tmem + (uint32_t)(set * 256 + e * MT_N),
+                        make_sdesc(as + j * 4096, 2048, 128),
                         make_sdesc(bs + j * 2048, 1024, 128), id, (started >> e) & 1u);
               started |= 1u << e;
             }
           }
         }
-        umma_commit(&s_aempty[sa]);
+        umma_commit(&s_aempty[buf]);
       }
       if (!ok) break;
       umma_commit(&s_bempty[sb]);
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
       ++oi;
     }
     umma_commit(&s_done);
-  } else if (warp == MT_PW + 1 && lane == 0) {
+  } else if (warp == MT_TMAW && lane == 0) {
     // ---------------------------------------------------------- table loader
     const char *limg = (const char *)img + (size_t)(l - 2) * 343 * MT_BIMG;
     int oi = 0;
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(MT_THREADS2, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  if (warp == MT_PW)
+  if (warp == MT_MMAW)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
@@ -495,7 +496,7 @@ static inline unsigned nblk_tc(size_t n, int t) { return (unsigned)((n + t - 1) 
 
 bool m2l_tc_usable(const dust_octree *o) {
   const int nout = o->prm.vortstretch ? o->nm1 : o->nm;
-  return o->prm.precision == DUST_PREC_FP32C && o->nm <= MT_K && nout <= 2 * MT_HALF &&
+  return o->prm.precision == DUST_PREC_FP32C && o->nm <= MT_K && nout <= MT_NOUT &&
          o->G.ll >= 2;
 }
 
@@ -516,7 +517,7 @@ int m2l_tc_tables(dust_octree *o) {
   return DUST_OK;
 }
 
-size_t m2l_tc_ahat_bytes(size_t ncells) { return ncells * 3 * MT_K * 4; }
+size_t m2l_tc_ahat_bytes(size_t ncells) { return ncells * 6 * MT_K * 4; }
 
 int m2l_tc_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
   uint32_t c0 = o->ahat_c0, nact = (uint32_t)o->n_active;

@@ -4,7 +4,12 @@
 // particle direction.  One thread per particle; the arithmetic follows the
 // reference's expressions operation by operation with explicitly rounded
 // intrinsics (no fused multiply-adds), so the result equals a plain FP64
-// evaluation of the same expressions.
+// evaluation of the same expressions, as the CPU oracle writes them.  The
+// reference takes vector lengths with Fortran's norm2, which gfortran may
+// evaluate as a scaled sum of squares; here (and in the oracle) the length
+// is sqrt(x*x + y*y + z*z), which can differ from that in the last unit of
+// the result.  Penetration avoidance (use_pa, :1312-1317) is not part of
+// this step.
 #include <cstring>
 
 #include "dust_common.cuh"

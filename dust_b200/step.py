@@ -15,6 +15,10 @@ the same sequence on the GPU through the C ABI:
   5. dust_fmm_apply[_device]                 (particle velocity, stretching,
                                               div-filter curl: tree build,
                                               multipoles, L2P, P2P, elements)
+  6. dust_particles_update[_device]          (complete_wake's particle loop:
+                                              explicit Euler move, box culling,
+                                              direction renewal; mod_wake.f90:
+                                              1309-1355), when ``advect``
 
 Two drivers: ``HostStepper`` takes host (pinned) arrays and lets the library
 copy them every step (end-to-end); ``DeviceStepper`` keeps everything in HBM
@@ -30,15 +34,30 @@ from .linsys import Linsys
 from .octree import Octree
 
 
+def update_params_for(case, params):
+    """The particles' Euler step of the case: dt, a particle box that holds
+    the whole octree box (no particle is freed by the move), the model
+    switches of the FMM; divergence filtering off, as the reference runs it
+    (sim_param%use_divfilt is never assigned, mod_sim_param.f90:450-451)."""
+    lo = np.asarray(params.origin, dtype=np.float64)
+    hi = lo + np.asarray(params.n_box, dtype=np.float64) * params.box_length
+    return abi.update_params(case.dt, lo, hi, 1, params.vortstretch, params.diffusion, False,
+                             0.0)
+
+
 class HostStepper:
-    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None):
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None, advect=False):
         """``out``: optional (vel, stretch, rotu) host arrays the particle
-        outputs are written to every step (e.g. page-locked buffers)."""
+        outputs are written to every step (e.g. page-locked buffers);
+        ``advect``: move the particles at the end of each step."""
         self.case = case
         self.params = params
         self.mode = mode
         self.out = out
+        self.advect = advect
+        self.upd = update_params_for(case, params)
         c = case
+        self.free = np.zeros(c.mag.shape[0], dtype=np.int32)
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
         self.oc = Octree(params)
         self.ind = c.impl_ind.astype(np.int64) - 1
@@ -68,18 +87,27 @@ class HostStepper:
         c.wake.mag = res[self.ind[:, 0]] - m2
         els = abi.elements_struct(c.elems, c.wake, c.end_vort)
         vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els, out=self.out)
+        if self.advect:
+            nf = C.c_int(0)
+            check(lib().dust_particles_update(C.byref(self.upd), c.mag.shape[0], abi.dptr(c.cen),
+                                              abi.dptr(c.dir), abi.dptr(c.mag), abi.dptr(vel),
+                                              abi.dptr(st), abi.dptr(ro),
+                                              self.free.ctypes.data_as(C.POINTER(C.c_int)),
+                                              C.byref(nf)), "dust_particles_update")
         return res, vel, st, ro
 
 
 class DeviceStepper:
     """All per-step inputs resident in HBM; library calls on device pointers."""
 
-    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda"):
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda", advect=False):
         import torch
         self.torch = torch
         self.case = case
         self.params = params
         self.mode = mode
+        self.advect = advect
+        self.upd = update_params_for(case, params)
         c = case
         dev = torch.device(device)
         T = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt,
@@ -111,6 +139,8 @@ class DeviceStepper:
         self.str = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
         self.rot = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
         self.res = torch.empty(c.rank, dtype=torch.float64, device=dev)
+        self.free = torch.zeros(self.n, dtype=torch.int32, device=dev)
+        self.n_freed = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
         self.oc = Octree(params)
         self._ps = params.struct()
@@ -170,5 +200,11 @@ class DeviceStepper:
                                           P(self.mag), P(self.rv), C.byref(els), P(self.vel),
                                           P(self.str), P(self.rot), C.c_void_p(stream), 0),
               "dust_fmm_apply_device")
+        self._mark()
+        if self.advect:
+            check(lib().dust_particles_update_device(
+                C.byref(self.upd), self.n, P(self.cen), P(self.dir), P(self.mag), P(self.vel),
+                P(self.str), P(self.rot), P(self.free, C.c_int), P(self.n_freed, C.c_int),
+                C.c_void_p(stream)), "dust_particles_update_device")
         self._mark()
         return self.res

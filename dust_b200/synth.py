@@ -423,12 +423,15 @@ class FullStepCase:
                          multipole_degree=degree, rankine_rad=0.1, cutoff_rad=0.001,
                          u_inf=tuple(self.u_inf))
 
-    def loads(self, res, rho=1.225):
+    def loads(self, res, uvort=None, rho=1.225):
         """Integrated loads from the doublet strengths: wing lift from the
         trailing-edge doublet jump (rho |U| sum (mu_up - mu_lo) dy) and rotor
         thrust by Kutta-Joukowski on the bound vortices with the panel-centre
-        relative velocity (restating compute_dforce_jukowski_vortlatt,
-        src/aeroel/mod_vortlatt.f90:502-545, without the unsteady term)."""
+        relative velocity u_inf - ub + uvort (restating
+        compute_dforce_jukowski_vortlatt, src/aeroel/mod_vortlatt.f90:502-545,
+        without the unsteady term); ``uvort`` (rank, 3) is the step's
+        wake-induced velocity at the panel centres (default: the case's)."""
+        uv = self.elems.uvort if uvort is None else uvort
         te_up, te_lo, dy = self.wing_te
         lift = rho * np.linalg.norm(self.u_inf) * np.sum((res[te_up] - res[te_lo]) * dy)
         out = [lift]
@@ -442,7 +445,7 @@ class FullStepCase:
             gb = g.reshape(3, nch, nsb)
             gup = np.concatenate([np.zeros((3, 1, nsb)), gb[:, :-1, :]], axis=1).reshape(-1)
             e1 = (ver[idx, 3] - ver[idx, 0])  # spanwise (bound-vortex) edge
-            urel = self.u_inf - self.elems.ub[idx] + self.elems.uvort[idx]
+            urel = self.u_inf - self.elems.ub[idx] + uv[idx]
             f = rho * np.cross(urel, e1) * (g - gup)[:, None]
             out.append(f.sum(axis=0)[2])
         return np.asarray(out)

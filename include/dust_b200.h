@@ -213,10 +213,14 @@ DUST_API int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts,
  *   - The scratch is one array per device, shared by every call: calls that
  *     overlap in time (two streams, or two host threads) race on it and give
  *     wrong results.  Serialise them.
- *   - The first call on each device looks the array up
- *     (cudaGetSymbolAddress, which also loads the library's device code); a
- *     caller that records its stream into a graph should make that first
- *     call before it starts capturing. */
+ *   - Every call looks the array's address up in the current device's
+ *     context (cudaGetSymbolAddress; nothing is cached, so a context reset
+ *     is harmless); the first call on a device also loads the library's
+ *     device code there, so a caller that records its stream into a graph
+ *     should make one call before it starts capturing.
+ *   - Null pointers where data is needed (points and output with n_pts > 0,
+ *     particle arrays with n > 0, end-vortex arrays with end_vort->n > 0)
+ *     return DUST_ERR_BAD_ARG before anything is launched. */
 #define DUST_UVORT_NOALLOC_SCRATCH (4u << 20)
 DUST_API int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int n_pts,
                                               const double *pts, int n,

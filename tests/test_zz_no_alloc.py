@@ -87,3 +87,48 @@ def test_noalloc_refuses_oversize():
     assert _call(lib().dust_points_uvort_device_noalloc, prm64, c, out, stream) == abi.DUST_OK
     torch.cuda.synchronize()
     assert rel(out.cpu().numpy(), ref.cpu().numpy()) < TOL
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After one warm-up call, a call at a new, larger size that still fits
+    the scratch leaves the device's free memory exactly as it was."""
+    prm = FmmParams(box_length=4.0, origin=(-2.0, -2.0, -2.0), n_octree_levels=5,
+                    min_octree_part=5, multipole_degree=4, rankine_rad=0.02,
+                    precision=abi.DUST_PREC_FP32C)
+    stream = torch.cuda.current_stream().cuda_stream
+    small = _case(5000, 100, seed=5)
+    big = _case(60000, 300, seed=6)  # about 3.4 MB of the 4 MiB scratch in FP32C
+    out_s = torch.empty(small["n_pts"] * 3, dtype=torch.float64, device="cuda")
+    out_b = torch.empty(big["n_pts"] * 3, dtype=torch.float64, device="cuda")
+    assert _call(lib().dust_points_uvort_device_noalloc, prm, small, out_s, stream) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    st = _call(lib().dust_points_uvort_device_noalloc, prm, big, out_b, stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert st == abi.DUST_OK, lib().dust_last_error().decode()
+    assert free1 == free0
+
+
+def test_noalloc_rejects_null_arrays():
+    prm = FmmParams(box_length=4.0, origin=(-2.0, -2.0, -2.0), rankine_rad=0.02)
+    c = _case(1000, 10, seed=7)
+    out = torch.empty(c["n_pts"] * 3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    null = C.POINTER(C.c_double)()
+    lines = abi.Lines(2, _p(c["lver"]), _p(c["lmag"]))
+    bad_lines = abi.Lines(2, null, _p(c["lmag"]))
+    ps = prm.struct()
+    for fn in (lib().dust_points_uvort_device_noalloc, lib().dust_points_uvort_device):
+        # particles missing
+        assert fn(C.byref(ps), c["n_pts"], _p(c["pts"]), c["n"], null, _p(c["dir"]),
+                  _p(c["mag"]), _p(c["rv"]), C.byref(lines), _p(out),
+                  C.c_void_p(stream)) == abi.DUST_ERR_BAD_ARG
+        # output missing
+        assert fn(C.byref(ps), c["n_pts"], _p(c["pts"]), c["n"], _p(c["cen"]), _p(c["dir"]),
+                  _p(c["mag"]), _p(c["rv"]), C.byref(lines), null,
+                  C.c_void_p(stream)) == abi.DUST_ERR_BAD_ARG
+        # end-vortex vertices missing
+        assert fn(C.byref(ps), c["n_pts"], _p(c["pts"]), c["n"], _p(c["cen"]), _p(c["dir"]),
+                  _p(c["mag"]), _p(c["rv"]), C.byref(bad_lines), _p(out),
+                  C.c_void_p(stream)) == abi.DUST_ERR_BAD_ARG
