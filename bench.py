@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--train-iters", type=int, default=400)
     ap.add_argument("--profile-step", action="store_true",
                     help="run warm-up + one step only (for ncu launch lists)")
-    ap.add_argument("--workload", default="full", choices=["full", "fmm", "dense"],
+    ap.add_argument("--workload", default="full", choices=["full", "fmm", "dense", "learned"],
                     help="full: the full-step line (with the fmm and dense workloads as "
                          "sub-objects); fmm / dense: that workload's own line")
     ap.add_argument("--no-workloads", action="store_true",
@@ -417,7 +417,9 @@ def main():
         # the other named workloads at their full sizes, 5 timed calls each
         # after 3 warm-ups (time per call, not per step)
         subs = {"fmm": run_fmm_workload(5, 3, flush=flush),
-                "dense": run_dense_workload(5, 3, flush=flush)}
+                "dense": run_dense_workload(5, 3, flush=flush),
+                "learned": run_learned_workload(n_train=500, n_test=6, train_iters=2000,
+                                                flush=flush)}
     if rank == 0:
         r = results[best]
         line = {
@@ -663,6 +665,79 @@ def run_dense_workload(reps, warm, n_target=16384, nrhs=64, flush=None):
             "results": res}
 
 
+def run_learned_workload(n_train=500, n_test=8, train_iters=2000, flush=None):
+    """Learned preconditioner on the moving-body system: rotor over a
+    fuselage (about 7k unknowns, 960 moving), systems drawn from plain-method
+    steps with seeded rpm (+-20 %), azimuth and inflow angle.  The network is
+    trained on n_train systems the plain LU solved; on n_test held-out draws
+    the plain per-step solve (LU64: static LU reused, Schur update of the
+    moving block) is timed against the learned-preconditioned GMRES
+    (iterations, fallback, error against LU)."""
+    import torch
+    from dust_b200 import abi, linsys, precond, synth
+    case = synth.RotorFuselageCase()
+    prm = case.fmm_params()
+    t0 = time.perf_counter()
+    els0 = case.system(10 ** 6)
+    ls = linsys.Linsys(prm, case.rank, case.nstatic, els0)
+    pc = precond.Precond(precond._centres(els0), k=8, seed=0)
+    for q in range(n_train):
+        els = case.system(q)
+        ls.assemble_linsys(els)
+        x, _ = ls.solve_linsys(abi.DUST_SOLVE_LU64)
+        ls.assemble_linsys(els)
+        pc.add_sample(ls, x, seed=q)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    l0 = float(np.mean([pc.loss_grad(i, with_grad=False)[0] for i in range(min(64, n_train))]))
+    l1 = pc.train(train_iters, 2e-3)
+    t_train = time.perf_counter() - t0
+    untrained = precond.Precond(precond._centres(els0), k=8, seed=0)
+    stream = torch.cuda.current_stream()
+    rows = []
+    for q in range(n_test):
+        els = case.system(10 ** 6 + q)
+        rec = {}
+        for name, mode, p in (("lu64", abi.DUST_SOLVE_LU64, None),
+                              ("gmres_untrained", abi.DUST_SOLVE_GMRES_NN, untrained),
+                              ("gmres_nn", abi.DUST_SOLVE_GMRES_NN, pc)):
+            if p is not None:
+                p.attach(ls)
+            ls.assemble_linsys(els)
+            ls.sync()
+            if flush is not None:
+                flush.zero_()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            x, rep = ls.solve_linsys(mode)
+            ms = (time.perf_counter() - t1) * 1e3
+            rec[name] = {"ms": ms, "x": x, "rep": rep}
+            if p is not None:
+                precond.Precond.detach(ls)
+        xl = rec["lu64"]["x"]
+        rows.append({k: {"ms": round(v["ms"], 3), "iterations": int(v["rep"]["iterations"]),
+                         "fell_back": int(v["rep"]["fell_back"]),
+                         "rel_error_vs_lu64": float(np.linalg.norm(v["x"] - xl)
+                                                    / np.linalg.norm(xl))}
+                     for k, v in rec.items()})
+    ls.close()
+    summ = {}
+    for k in ("lu64", "gmres_untrained", "gmres_nn"):
+        r = [row[k] for row in rows[1:]]  # the first draw warms the handles up
+        summ[k] = {"ms_mean": round(float(np.mean([x["ms"] for x in r])), 3),
+                   "iterations_mean": round(float(np.mean([x["iterations"] for x in r])), 2),
+                   "fallbacks": int(sum(x["fell_back"] for x in r)),
+                   "max_rel_error_vs_lu64": max(x["rel_error_vs_lu64"] for x in r)}
+    return {"workload": "learned preconditioner: 4-blade rotor (30 x 8 VLM per blade, 960 "
+                        "moving unknowns) over a %d-panel fuselage, %d unknowns"
+                        % (case.nstatic, case.rank),
+            "unit": "ms per solve (host wall clock around the synchronous solve call)",
+            "train": {"systems": n_train, "adam_iters": train_iters, "loss_untrained": l0,
+                      "loss_trained": l1, "s_data": round(t_data, 1),
+                      "s_train": round(t_train, 1)},
+            "test_draws": n_test - 1, "results": summ}
+
+
 def workload_line(args, ws, name):
     """--workload fmm / dense: that workload as the bench line."""
     import torch
@@ -680,6 +755,17 @@ def workload_line(args, ws, name):
         rf["traffic"] = None
         rf["others"] = [dict(best["roofline"]["p2p"], kernel="P2P phase")]
         dtype = "f32/tf32 (FP32C)"
+    elif name == "learned":
+        with Clocks(0) as clk:
+            w = run_learned_workload(n_train=2000, n_test=max(args.steps, 3) + 1,
+                                     train_iters=6000)
+        best = dict(w["results"]["gmres_nn"], ms=w["results"]["gmres_nn"]["ms_mean"])
+        plain = dict(w["results"]["lu64"], ms=w["results"]["lu64"]["ms_mean"])
+        metric = "ms per moving-body solve (~7k unknowns), learned GMRES vs per-step LU"
+        rf = {"kernel": "GMRES_NN solve", "bound": "hbm", "achieved": None, "peak": None,
+              "unit": "GB/s", "frac": None, "traffic": None,
+              "note": "latency-bound iterative solve; no roofline claimed"}
+        dtype = "f64 GMRES with f32 preconditioner"
     else:
         with Clocks(0) as clk:
             w = run_dense_workload(args.steps, warm)
