@@ -116,3 +116,114 @@ extern "C" int dust_fmm_apply_device(dust_octree *o, int n, const double *cen,
   if (o->timing || sync) return fmm_collect_stats(o, n, n_elem_of(elems));
   return DUST_OK;
 }
+
+// ------------------------------------------------ the FMM in two halves
+// prepare_wake's octree part (sort_particles + calculate_multipole,
+// mod_wake.f90:797-800) and apply_multipole_panels (:801), then
+// update_wake's apply_multipole (:1115-1118): the particles enter the tree
+// once per step and serve both the panels' uvort and the particles' own
+// velocities.
+
+extern "C" int dust_fmm_prepare(dust_octree *o, int n, const double *cen, const double *dir,
+                                const double *mag, const double *r_vortex) {
+  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex))) return DUST_ERR_BAD_ARG;
+  cudaStream_t st = o->stream;
+  size_t N = (size_t)(n > 0 ? n : 1);
+  DUST_TRY(devbuf_grow(o->h_in, N * 8 * 8));
+  double *dc = (double *)o->h_in.p, *dd = dc + 3 * N, *dm = dd + 3 * N, *dr = dm + N;
+  if (n > 0) {
+    DUST_CUDA(cudaMemcpyAsync(dc, cen, (size_t)n * 24, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dd, dir, (size_t)n * 24, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dm, mag, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dr, r_vortex, (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  }
+  o->prepared_n = -1;
+  const int s = fmm_prepare_device(o, n, dc, dd, dm, dr, st);
+  if (s != DUST_OK) o->prepared_n = -1;
+  return s;
+}
+
+extern "C" int dust_fmm_prepare_device(dust_octree *o, int n, const double *cen,
+                                       const double *dir, const double *mag,
+                                       const double *r_vortex, void *stream) {
+  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex))) return DUST_ERR_BAD_ARG;
+  cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
+  o->prepared_n = -1;
+  const int s = fmm_prepare_device(o, n, cen, dir, mag, r_vortex, st);
+  if (s != DUST_OK) o->prepared_n = -1;
+  return s;
+}
+
+extern "C" int dust_fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts,
+                                            const dust_lines *end_vort, double *uvort,
+                                            void *stream) {
+  if (!o || n_pts < 0 || (n_pts > 0 && (!pts || !uvort))) return DUST_ERR_BAD_ARG;
+  if (end_vort && (end_vort->n < 0 || (end_vort->n > 0 && (!end_vort->ver || !end_vort->mag))))
+    return DUST_ERR_BAD_ARG;
+  if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
+  cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, o->prm.u_inf, reg_params(&o->prm),
+                             false, o->el_raw, o->el_geo, e, st));
+  return fmm_points_uvort_device(o, n_pts, pts, e, uvort, st);
+}
+
+extern "C" int dust_fmm_points_uvort(dust_octree *o, int n_pts, const double *pts,
+                                     const dust_lines *end_vort, double *uvort) {
+  if (!o || n_pts < 0 || (n_pts > 0 && (!pts || !uvort))) return DUST_ERR_BAD_ARG;
+  if (end_vort && (end_vort->n < 0 || (end_vort->n > 0 && (!end_vort->ver || !end_vort->mag))))
+    return DUST_ERR_BAD_ARG;
+  if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  cudaStream_t st = o->stream;
+  DUST_TRY(devbuf_grow(o->h_pts, (size_t)n_pts * 48));
+  double *dp = (double *)o->h_pts.p, *du = dp + 3 * (size_t)n_pts;
+  DUST_CUDA(cudaMemcpyAsync(dp, pts, (size_t)n_pts * 24, cudaMemcpyHostToDevice, st));
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, o->prm.u_inf, reg_params(&o->prm),
+                             true, o->el_raw, o->el_geo, e, st));
+  DUST_TRY(fmm_points_uvort_device(o, n_pts, dp, e, du, st));
+  DUST_CUDA(cudaMemcpyAsync(uvort, du, (size_t)n_pts * 24, cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  return DUST_OK;
+}
+
+extern "C" int dust_fmm_finish_device(dust_octree *o, const dust_elements *elems, double *vel,
+                                      double *stretch, double *rotu, void *stream, int sync) {
+  if (!o || o->prepared_n < 0 || (o->prepared_n > 0 && !vel)) return DUST_ERR_BAD_ARG;
+  const int n = o->prepared_n;
+  cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
+  ElemDev e;
+  DUST_TRY(elem_build_device(elems ? &elems->body : nullptr, elems ? &elems->wake : nullptr,
+                             elems ? &elems->end_vort : nullptr, o->prm.u_inf,
+                             reg_params(&o->prm), false, o->el_raw, o->el_geo, e, st));
+  DUST_TRY(fmm_near_device(o, st));
+  DUST_TRY(fmm_finish_device(o, n, e, vel, stretch, rotu, st));
+  if (sync) DUST_CUDA(cudaStreamSynchronize(st));
+  if (o->timing || sync) return fmm_collect_stats(o, n, n_elem_of(elems));
+  return DUST_OK;
+}
+
+extern "C" int dust_fmm_finish(dust_octree *o, const dust_elements *elems, double *vel,
+                               double *stretch, double *rotu) {
+  if (!o || o->prepared_n < 0 || (o->prepared_n > 0 && !vel)) return DUST_ERR_BAD_ARG;
+  const int n = o->prepared_n;
+  cudaStream_t st = o->stream;
+  size_t N = (size_t)(n > 0 ? n : 1);
+  DUST_TRY(devbuf_grow(o->h_out, N * 9 * 8));
+  double *ov = (double *)o->h_out.p, *os = ov + 3 * N, *orr = os + 3 * N;
+  ElemDev e;
+  DUST_TRY(elem_build_device(elems ? &elems->body : nullptr, elems ? &elems->wake : nullptr,
+                             elems ? &elems->end_vort : nullptr, o->prm.u_inf,
+                             reg_params(&o->prm), true, o->el_raw, o->el_geo, e, st));
+  DUST_TRY(fmm_near_device(o, st));
+  DUST_TRY(fmm_finish_device(o, n, e, ov, stretch ? os : nullptr, rotu ? orr : nullptr, st));
+  if (n > 0) {
+    DUST_CUDA(cudaMemcpyAsync(vel, ov, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+    if (stretch)
+      DUST_CUDA(cudaMemcpyAsync(stretch, os, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+    if (rotu) DUST_CUDA(cudaMemcpyAsync(rotu, orr, (size_t)n * 24, cudaMemcpyDeviceToHost, st));
+  }
+  DUST_CUDA(cudaStreamSynchronize(st));
+  return fmm_collect_stats(o, n, n_elem_of(elems));
+}

@@ -776,6 +776,12 @@ __global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv
   for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
 }
 
+void points_lines_add(int npts, const double *pts, const ElemDev &lines, double *uv,
+                      cudaStream_t st) {
+  if (npts > 0 && lines.nline > 0)
+    k_uvort_lines<<<nblk(npts, 128), 128, 0, st>>>(npts, pts, lines, uv);
+}
+
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st) {

@@ -189,7 +189,7 @@ extern "C" int dust_octree_create(const dust_fmm_params *prm, dust_octree **out)
     delete o;
     return DUST_ERR_CUDA;
   }
-  for (int e = 0; e < 10; ++e) cudaEventCreate(&o->ev[e]);
+  for (int e = 0; e < 12; ++e) cudaEventCreate(&o->ev[e]);
   st = build_tables(o);
   if (st == DUST_OK) st = build_shift_tables(o);
   if (st == DUST_OK) st = m2l_batch_tables(o);
@@ -222,9 +222,9 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
                     &o->cidx,   &o->lidx,   &o->act_key, &o->act_lev, &o->leaf_ci,
                     &o->mp,     &o->outs,   &o->cub_tmp, &o->small,  &o->h_in,
-                    &o->h_out,  &o->el_geo, &o->el_raw};
+                    &o->h_out,  &o->h_pts,  &o->el_geo, &o->el_raw};
   for (DevBuf *b : bufs) devbuf_free(*b);
-  for (int e = 0; e < 10; ++e) cudaEventDestroy(o->ev[e]);
+  for (int e = 0; e < 12; ++e) cudaEventDestroy(o->ev[e]);
   cudaStreamDestroy(o->stream);
   delete o;
   return DUST_OK;
@@ -1833,8 +1833,8 @@ static void fill_dev(dust_octree *o, FmmDev &d, int n) {
 
 // Builds the tree of n device-resident particles and evaluates the FMM; the
 // outputs stay in o->outs (sorted order) for the element pass.
-int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
-                   const double *mag, const double *rv, cudaStream_t st) {
+int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *dir,
+                       const double *mag, const double *rv, cudaStream_t st) {
   TreeGeom &G = o->G;
   o->last_stream = st;
   const int ll = G.ll;
@@ -1986,7 +1986,17 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
         (const int *)o->shift_o[l][2], ntg);
   }
   if (o->timing) cudaEventRecord(o->ev[3], st);
-  // leaves: L2P + P2P
+  o->dev = d;
+  o->prepared_n = n;
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+// leaves: L2P + P2P of the particles with the prepared tree and expansions
+int fmm_near_device(dust_octree *o, cudaStream_t st) {
+  FmmDev &d = o->dev;
+  o->last_stream = st;
+  if (o->timing) cudaEventRecord(o->ev[10], st);
   if (o->n_leaves > 0) {
     size_t shl = (size_t)3 * (o->nm + o->nm1) * 8 + (size_t)4 * o->nm * 4;
     bool vs = d.use_vs, df = d.use_df, vd = d.use_vd, tv = o->prm.turbulent_viscosity != 0;
@@ -2040,6 +2050,120 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
   return DUST_OK;
 }
 
+int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
+                   const double *mag, const double *rv, cudaStream_t st) {
+  DUST_TRY(fmm_prepare_device(o, n, cen, dir, mag, rv, st));
+  return fmm_near_device(o, st);
+}
+
+// ----------------------------------------------- particles -> points (FMM)
+// apply_multipole_panels (mod_octree.f90:1433-1508) on the GPU: one thread
+// per point.  The point is binned into the finest cell as sort_particles
+// bins panel centres (:776-799) and takes the leaf above that cell (the
+// leaves partition the box); its velocity is the leaf's local expansion
+// (FP64 L2P of b) plus the particles of the leaf's 26 active same-level
+// neighbours, of its coarser leaf neighbours (leaf_neigh) and of the leaf
+// itself, summed in FP64 with the particle kernel of compute_vel
+// (mod_vortpart.f90:139-155).  A point outside the octree box sets the
+// error word (the reference stops there).
+__global__ void k_points_fmm(FmmDev d, int npts, const double *__restrict__ pts,
+                             double *__restrict__ uv, int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const TreeGeom &G = d.G;
+  const int ll = G.ll;
+  const size_t n = d.n;
+  const double pos[3] = {pts[3 * (size_t)q], pts[3 * (size_t)q + 1], pts[3 * (size_t)q + 2]};
+  int idx[3];
+  for (int c = 0; c < 3; ++c) {
+    idx[c] = (int)ceil((pos[c] - G.xmin[c]) / G.csize[ll]) - 1;
+    if (idx[c] < 0 || idx[c] >= G.ncl[ll][c]) {
+      atomicMin(err, q);
+      for (int e = 0; e < 3; ++e) uv[3 * (size_t)q + e] = 0.0;
+      return;
+    }
+  }
+  int l = 0, ci = 0, cj = 0, ck = 0;
+  uint32_t key = 0;
+  for (int lv = 1; lv <= ll; ++lv) {
+    const int sh = ll - lv;
+    const int a = idx[0] >> sh, b = idx[1] >> sh, c = idx[2] >> sh;
+    const uint32_t k = key_of(G, lv, a, b, c);
+    if (d.flags[G.lev_off[lv] + k] & FL_LEAF) {
+      l = lv, ci = a, cj = b, ck = c, key = k;
+      break;
+    }
+  }
+  double v[3] = {0.0, 0.0, 0.0};
+  if (l > 0) {
+    const uint32_t cell = d.cidx[G.lev_off[l] + key];
+    double cc[3];
+    cell_center(G, l, ci, cj, ck, cc);
+    const double x = pos[0] - cc[0], y = pos[1] - cc[1], z = pos[2] - cc[2];
+    const double *bl = d.B + (size_t)cell * 3 * d.nm;
+    for (int m = 0; m < d.nm; ++m) {
+      int mi, mj, mk;
+      mono_exp(m, mi, mj, mk);
+      double pr = 1.0;
+      for (int e = 0; e < mi; ++e) pr *= x;
+      for (int e = 0; e < mj; ++e) pr *= y;
+      for (int e = 0; e < mk; ++e) pr *= z;
+      for (int e = 0; e < 3; ++e) v[e] += bl[3 * m + e] * pr;
+    }
+    const double k4pi = 1.0 / (4.0 * DUST_PI);
+    auto range = [&](uint32_t lo, uint32_t hi) {
+      for (uint32_t t = lo; t < hi; ++t) {
+        const double dx = pos[0] - d.P[t], dy = pos[1] - d.P[n + t], dz = pos[2] - d.P[2 * n + t];
+        const double ax = d.P[3 * n + t], ay = d.P[4 * n + t], az = d.P[5 * n + t],
+                     s = d.P[6 * n + t];
+        const double dn = sqrt(dx * dx + dy * dy + dz * dz + s * s);
+        const double c = -1.0 / (dn * dn * dn) * k4pi;
+        v[0] += c * (dy * az - dz * ay);
+        v[1] += c * (dz * ax - dx * az);
+        v[2] += c * (dx * ay - dy * ax);
+      }
+    };
+    for (int lev = l; lev >= 1; --lev) {
+      const int sh = l - lev;
+      const int ai = ci >> sh, aj = cj >> sh, ak = ck >> sh;
+      for (int kk = -1; kk <= 1; ++kk)
+        for (int jj = -1; jj <= 1; ++jj)
+          for (int ii = -1; ii <= 1; ++ii) {
+            if (ii == 0 && jj == 0 && kk == 0) continue;
+            if (!cart_in(G, lev, ai + ii, aj + jj, ak + kk)) continue;
+            const uint32_t nk = key_of(G, lev, ai + ii, aj + jj, ak + kk);
+            const uint8_t f = d.flags[G.lev_off[lev] + nk];
+            if (lev == l ? !(f & FL_ACTIVE) : !(f & FL_LEAF)) continue;
+            range(cell_lo(G, d.cstart, lev, nk), cell_hi(G, d.cstart, lev, nk));
+          }
+    }
+    range(cell_lo(G, d.cstart, l, key), cell_hi(G, d.cstart, l, key));
+  }
+  for (int e = 0; e < 3; ++e) uv[3 * (size_t)q + e] = v[e];
+}
+
+void points_lines_add(int npts, const double *pts, const ElemDev &lines, double *uv,
+                      cudaStream_t st);
+
+int fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts, const ElemDev &lines,
+                            double *uv, cudaStream_t st) {
+  if (n_pts <= 0) return DUST_OK;
+  if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
+  int *err = (int *)((int64_t *)o->small.p + 41);
+  const int big = 0x7fffffff;
+  DUST_CUDA(cudaMemcpyAsync(err, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+  k_points_fmm<<<nblk(n_pts, 128), 128, 0, st>>>(o->dev, n_pts, pts, uv, err);
+  if (lines.nline > 0) points_lines_add(n_pts, pts, lines, uv, st);
+  int herr = big;
+  DUST_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  if (herr != big) {
+    dust_set_last_error("a point lies outside the octree box", __FILE__, __LINE__);
+    return DUST_ERR_OUT_OF_BOX;
+  }
+  return DUST_OK;
+}
+
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st) {
   if (n > 0)
@@ -2072,9 +2196,12 @@ int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem) {
     cudaEventElapsedTime(&s.ms_tree, o->ev[0], o->ev[1]);
     cudaEventElapsedTime(&s.ms_upward, o->ev[1], o->ev[2]);
     cudaEventElapsedTime(&s.ms_m2l, o->ev[2], o->ev[3]);
-    cudaEventElapsedTime(&s.ms_p2p, o->ev[3], o->ev[4]);
+    cudaEventElapsedTime(&s.ms_p2p, o->ev[10], o->ev[4]);
     cudaEventElapsedTime(&s.ms_elems, o->ev[4], o->ev[5]);
-    cudaEventElapsedTime(&s.ms_total, o->ev[0], o->ev[5]);
+    float t_pre = 0.f, t_post = 0.f;
+    cudaEventElapsedTime(&t_pre, o->ev[0], o->ev[3]);
+    cudaEventElapsedTime(&t_post, o->ev[10], o->ev[5]);
+    s.ms_total = t_pre + t_post;
     if (o->kev_m2l) cudaEventElapsedTime(&s.ms_m2l_kernel, o->ev[6], o->ev[7]);
     if (o->kev_far) cudaEventElapsedTime(&s.ms_elem_far, o->ev[8], o->ev[9]);
   }

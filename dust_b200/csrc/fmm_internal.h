@@ -54,7 +54,8 @@ struct dust_octree {
   uint64_t ncell_tot = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t last_stream = nullptr;  // stream of the last evaluation
-  cudaEvent_t ev[10];  // phases [0..5], M2L kernel [6, 7], far element kernel [8, 9]
+  cudaEvent_t ev[12];  // phases [0..5], M2L kernel [6, 7], far element kernel [8, 9],
+                       // start of the particles' near field [10]
   bool kev_m2l = false, kev_far = false;  // whether [6, 7] / [8, 9] were recorded
   bool timing = false;
   DevBuf dtab[DUST_MAXLEV + 1];
@@ -63,7 +64,7 @@ struct dust_octree {
   // per-call buffers (grown on demand, kept across calls)
   DevBuf keys, keys_s, vals, perm, cnt, cstart, part, flags, ind, cidx, lidx;
   DevBuf act_key, act_lev, leaf_ci, mp, outs, cub_tmp, small;
-  DevBuf h_in, h_out, el_geo, el_raw;  // staging of host-API calls
+  DevBuf h_in, h_out, h_pts, el_geo, el_raw;  // staging of host-API calls
   DevBuf ffbuf;                        // far-field panel records
   DevBuf elem_work;                    // FP32C element sums: far sums, near-pair list
   DevBuf p2p_grp;                      // FP32C P2P sibling groups: flags, ids, starts, counters
@@ -84,12 +85,21 @@ struct dust_octree {
   int64_t n_active = 0, n_leaves = 0;
   int64_t act_off[DUST_MAXLEV + 3];
   int bad_particle = -1;
+  int prepared_n = -1;  // particles of the last prepared tree (-1: none)
   FmmDev dev;
   dust_fmm_stats stats;
 };
 
 int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
                    const double *mag, const double *rv, cudaStream_t st);
+// the two halves of fmm_run_device: tree, multipoles and locals; then the
+// particles' L2P + P2P
+int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *dir,
+                       const double *mag, const double *rv, cudaStream_t st);
+int fmm_near_device(dust_octree *o, cudaStream_t st);
+// particles -> points through the prepared tree, plus the lines directly
+int fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts, const ElemDev &lines,
+                            double *uv, cudaStream_t st);
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st);
 int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem);

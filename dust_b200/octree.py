@@ -69,6 +69,39 @@ class Octree:
                                    abi.dptr(ro)), "dust_fmm_apply")
         return vel, st, ro
 
+    # --- the two halves (prepare_wake's octree part / update_wake's apply)
+    def prepare(self, cen, dir_, mag, r_vortex):
+        """sort_particles + calculate_multipole (host arrays)."""
+        cen, dir_, mag, rv = (abi.f64(cen), abi.f64(dir_), abi.f64(mag), abi.f64(r_vortex))
+        self._n = mag.shape[0]
+        check(lib().dust_fmm_prepare(self._h, self._n, abi.dptr(cen), abi.dptr(dir_),
+                                     abi.dptr(mag), abi.dptr(rv)), "dust_fmm_prepare")
+
+    def points_uvort(self, pts, end_vort=None):
+        """apply_multipole_panels: the prepared particles' velocity at the
+        points plus the end vortices (host arrays)."""
+        pts = abi.f64(pts).reshape(-1, 3)
+        ev = end_vort if end_vort is not None else abi.empty_lines()
+        evs = ev.struct()
+        out = np.empty_like(pts)
+        check(lib().dust_fmm_points_uvort(self._h, pts.shape[0], abi.dptr(pts), C.byref(evs),
+                                          abi.dptr(out)), "dust_fmm_points_uvort")
+        return out
+
+    def finish(self, elements=None, want_stretch=True, want_rotu=True, out=None):
+        """apply_multipole at the prepared particles (host outputs)."""
+        n = self._n
+        est, keep = elements if elements is not None else abi.elements_struct()
+        if out is not None:
+            vel, st, ro = out
+        else:
+            vel = np.empty((n, 3))
+            st = np.empty((n, 3)) if want_stretch else None
+            ro = np.empty((n, 3)) if want_rotu else None
+        check(lib().dust_fmm_finish(self._h, C.byref(est), abi.dptr(vel), abi.dptr(st),
+                                    abi.dptr(ro)), "dust_fmm_finish")
+        return vel, st, ro
+
     def apply_multipole_device(self, cen, dir_, mag, r_vortex, vel, stretch=None, rotu=None,
                                elements=None, stream=0, sync=True):
         """Device-resident variant: arguments are torch CUDA tensors (float64,

@@ -46,10 +46,15 @@ def update_params_for(case, params):
 
 
 class HostStepper:
-    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None, advect=False):
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None, advect=False,
+                 fmm_uvort=False):
         """``out``: optional (vel, stretch, rotu) host arrays the particle
         outputs are written to every step (e.g. page-locked buffers);
-        ``advect``: move the particles at the end of each step."""
+        ``advect``: move the particles at the end of each step;
+        ``fmm_uvort``: uvort through the particles' FMM (prepare, points,
+        finish: the particles are uploaded once per step) instead of the
+        direct sum."""
+        self.fmm_uvort = fmm_uvort
         self.case = case
         self.params = params
         self.mode = mode
@@ -74,10 +79,14 @@ class HostStepper:
         evs = c.end_vort.struct()
         uv = np.empty((c.rank, 3))
         cen_el = np.ascontiguousarray(cen_el)
-        check(lib().dust_points_uvort(C.byref(ps), c.rank, abi.dptr(cen_el), c.mag.shape[0],
-                                      abi.dptr(c.cen), abi.dptr(c.dir), abi.dptr(c.mag),
-                                      abi.dptr(c.r_vortex), C.byref(evs), abi.dptr(uv)),
-              "dust_points_uvort")
+        if self.fmm_uvort:
+            self.oc.prepare(c.cen, c.dir, c.mag, c.r_vortex)
+            uv = self.oc.points_uvort(cen_el, c.end_vort)
+        else:
+            check(lib().dust_points_uvort(C.byref(ps), c.rank, abi.dptr(cen_el),
+                                          c.mag.shape[0], abi.dptr(c.cen), abi.dptr(c.dir),
+                                          abi.dptr(c.mag), abi.dptr(c.r_vortex), C.byref(evs),
+                                          abi.dptr(uv)), "dust_points_uvort")
         c.elems.uvort = uv
         self.ls.assemble_linsys(c.elems, c.wake, c.n_impl, c.impl_ind)
         res, rep = self.ls.solve_linsys(self.mode)
@@ -86,7 +95,11 @@ class HostStepper:
         m2 = np.where(self.ind[:, 1] >= 0, res[np.maximum(self.ind[:, 1], 0)], 0.0)
         c.wake.mag = res[self.ind[:, 0]] - m2
         els = abi.elements_struct(c.elems, c.wake, c.end_vort)
-        vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els, out=self.out)
+        if self.fmm_uvort:
+            vel, st, ro = self.oc.finish(els, out=self.out)
+        else:
+            vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els,
+                                                  out=self.out)
         if self.advect:
             nf = C.c_int(0)
             check(lib().dust_particles_update(C.byref(self.upd), c.mag.shape[0], abi.dptr(c.cen),
@@ -100,13 +113,15 @@ class HostStepper:
 class DeviceStepper:
     """All per-step inputs resident in HBM; library calls on device pointers."""
 
-    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda", advect=False):
+    def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda", advect=False,
+                 fmm_uvort=False):
         import torch
         self.torch = torch
         self.case = case
         self.params = params
         self.mode = mode
         self.advect = advect
+        self.fmm_uvort = fmm_uvort
         self.upd = update_params_for(case, params)
         c = case
         dev = torch.device(device)
@@ -169,10 +184,20 @@ class DeviceStepper:
         check(lib().dust_panels_centres_device(C.byref(el), P(self.ecen), C.c_void_p(stream)),
               "dust_panels_centres_device")
         lines = abi.Lines(c.end_vort.n, P(self.lver), P(self.lmag))
-        check(lib().dust_points_uvort_device(C.byref(self._ps), c.rank, P(self.ecen), self.n,
-                                             P(self.cen), P(self.dir), P(self.mag), P(self.rv),
-                                             C.byref(lines), P(self.euv), C.c_void_p(stream)),
-              "dust_points_uvort_device")
+        if self.fmm_uvort:
+            # prepare_wake: the particles enter the tree once per step
+            check(lib().dust_fmm_prepare_device(self.oc._h, self.n, P(self.cen), P(self.dir),
+                                                P(self.mag), P(self.rv), C.c_void_p(stream)),
+                  "dust_fmm_prepare_device")
+            check(lib().dust_fmm_points_uvort_device(self.oc._h, c.rank, P(self.ecen),
+                                                     C.byref(lines), P(self.euv),
+                                                     C.c_void_p(stream)),
+                  "dust_fmm_points_uvort_device")
+        else:
+            check(lib().dust_points_uvort_device(C.byref(self._ps), c.rank, P(self.ecen),
+                                                 self.n, P(self.cen), P(self.dir), P(self.mag),
+                                                 P(self.rv), C.byref(lines), P(self.euv),
+                                                 C.c_void_p(stream)), "dust_points_uvort_device")
         self._mark()
         torch.cuda.current_stream().synchronize()
         wk = abi.WakeRows(abi.Panels(c.wake.n, P(self.wnv, C.c_int), P(self.wkind, C.c_int),
@@ -196,10 +221,15 @@ class DeviceStepper:
         wake = abi.Panels(c.wake.n, P(self.wnv, C.c_int), P(self.wkind, C.c_int),
                           P(self.wver), P(self.wmag), abi._dp(), abi._dp())
         els = abi.Elements(body, wake, lines)
-        check(lib().dust_fmm_apply_device(self.oc._h, self.n, P(self.cen), P(self.dir),
-                                          P(self.mag), P(self.rv), C.byref(els), P(self.vel),
-                                          P(self.str), P(self.rot), C.c_void_p(stream), 0),
-              "dust_fmm_apply_device")
+        if self.fmm_uvort:
+            check(lib().dust_fmm_finish_device(self.oc._h, C.byref(els), P(self.vel),
+                                               P(self.str), P(self.rot), C.c_void_p(stream), 0),
+                  "dust_fmm_finish_device")
+        else:
+            check(lib().dust_fmm_apply_device(self.oc._h, self.n, P(self.cen), P(self.dir),
+                                              P(self.mag), P(self.rv), C.byref(els), P(self.vel),
+                                              P(self.str), P(self.rot), C.c_void_p(stream), 0),
+                  "dust_fmm_apply_device")
         self._mark()
         if self.advect:
             check(lib().dust_particles_update_device(

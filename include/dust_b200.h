@@ -160,6 +160,49 @@ DUST_API int dust_fmm_apply_device(dust_octree *oct, int n,
                           double *vel, double *stretch, double *rotu,
                           void *stream, int sync);
 
+/* The same evaluation in the reference's two halves, so that the particles
+ * enter the tree once per step and serve both the panels and themselves:
+ *   dust_fmm_prepare[_device]      sort_particles + calculate_multipole of
+ *                                  prepare_wake (mod_wake.f90:797-800): tree,
+ *                                  multipoles, local expansions;
+ *   dust_fmm_points_uvort[_device] apply_multipole_panels (:801,
+ *                                  mod_octree.f90:1433-1508): the particles'
+ *                                  velocity at n_pts points (panel centres,
+ *                                  each taking the local expansion of the
+ *                                  leaf that holds it plus the particles of
+ *                                  that leaf's near field) plus the end
+ *                                  vortices by direct sum, into uvort(3,n_pts)
+ *                                  (overwritten).  The reference adds this to
+ *                                  uvort and then discards it in get_vort_vel
+ *                                  (mod_surfpan.f90:970); here it is the
+ *                                  result, an approximation of
+ *                                  dust_points_uvort to the FMM's accuracy.
+ *                                  A point outside the octree box is
+ *                                  DUST_ERR_OUT_OF_BOX;
+ *   dust_fmm_finish[_device]       apply_multipole (mod_wake.f90:1115-1118):
+ *                                  L2P + P2P at the prepared particles and
+ *                                  the element sums, outputs as
+ *                                  dust_fmm_apply (caller order).
+ * points_uvort and finish need a prepared tree (DUST_ERR_BAD_ARG otherwise);
+ * the tree stays valid until the next prepare or apply on the handle.  The
+ * device variants run on `stream` (NULL = the handle's stream); finish
+ * synchronises when `sync` != 0, points_uvort always (it reads its error
+ * word). */
+DUST_API int dust_fmm_prepare(dust_octree *oct, int n, const double *cen, const double *dir,
+                              const double *mag, const double *r_vortex);
+DUST_API int dust_fmm_prepare_device(dust_octree *oct, int n, const double *cen,
+                                     const double *dir, const double *mag,
+                                     const double *r_vortex, void *stream);
+DUST_API int dust_fmm_points_uvort(dust_octree *oct, int n_pts, const double *pts,
+                                   const dust_lines *end_vort, double *uvort);
+DUST_API int dust_fmm_points_uvort_device(dust_octree *oct, int n_pts, const double *pts,
+                                          const dust_lines *end_vort, double *uvort,
+                                          void *stream);
+DUST_API int dust_fmm_finish(dust_octree *oct, const dust_elements *elems, double *vel,
+                             double *stretch, double *rotu);
+DUST_API int dust_fmm_finish_device(dust_octree *oct, const dust_elements *elems, double *vel,
+                                    double *stretch, double *rotu, void *stream, int sync);
+
 /* Counters of the last dust_fmm_apply*.  Timings are filled only when
  * `timing` was enabled with dust_octree_set_timing. */
 DUST_API int dust_octree_get_stats(const dust_octree *oct, dust_fmm_stats *st);

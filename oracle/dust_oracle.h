@@ -57,6 +57,13 @@ int or_fmm_apply(const dust_fmm_params *prm, int n, const double *cen,
  * sum_l prod(nbox)*8^(l-1) bytes. */
 int or_last_tree_flags(unsigned char *flags, int64_t cap);
 
+/* apply_multipole_panels: particle velocity at points from the FMM (leaf
+ * local expansion + near-field particles) plus end vortices by direct sum. */
+int or_fmm_points_uvort(const dust_fmm_params *prm, int n, const double *cen,
+                        const double *dir, const double *mag, const double *r_vortex,
+                        int n_pts, const double *pts, const dust_lines *end_vort,
+                        double *uvort);
+
 /* Direct sum of the particle kernels over all pairs (targets = first n_tgt). */
 int or_direct_particles(const dust_fmm_params *prm, int n, const double *cen,
                         const double *dir, const double *mag,

@@ -929,6 +929,121 @@ int or_fmm_apply(const dust_fmm_params *prm, int n, const double *cen,
   return DUST_OK;
 }
 
+/* Velocity of one vortex particle q at pos (compute_vel of t_vortpart,
+ * mod_vortpart.f90:139-155, divided by 4 pi as the callers do). */
+static inline void part_vel(const double *pos, int64_t q, const double *cen, const double *dir,
+                            const double *mag, const double *rv, double *u) {
+  double dist[3] = {pos[0] - cen[3 * q], pos[1] - cen[3 * q + 1], pos[2] - cen[3 * q + 2]};
+  double distn = norm3(dist);
+  double dn = sqrt(distn * distn + rv[q] * rv[q]);
+  double c = -1.0 / (dn * dn * dn), cr[3];
+  cross3(dist, dir + 3 * q, cr);
+  for (int d = 0; d < 3; ++d) u[d] = u[d] + (c * cr[d] * mag[q]) / (4.0 * OR_PI);
+}
+
+/* apply_multipole_panels (mod_octree.f90:1433-1508): the particles' velocity
+ * at points (panel centres) from the FMM -- each point is sorted into the
+ * finest cell that holds it (sort_particles, :776-799) and takes the local
+ * expansion of the leaf above it, then the particles of that leaf's 26
+ * active same-level neighbours, of its leaf_neigh and of the leaf itself --
+ * plus the end vortices by direct sum (the vortical elements get_vort_vel
+ * keeps in vort_p when the particles go through the FMM, mod_wake.f90:
+ * 819-845).  The reference adds the FMM part to uvort and then resets uvort
+ * in get_vort_vel (mod_surfpan.f90:970); here the sum is returned. */
+int or_fmm_points_uvort(const dust_fmm_params *prm, int n, const double *cen,
+                        const double *dir, const double *mag, const double *r_vortex,
+                        int n_pts, const double *pts, const dust_lines *end_vort,
+                        double *uvort) {
+  if (!prm || n < 0 || n_pts < 0 || prm->n_octree_levels < 1 ||
+      prm->n_octree_levels > MAXLEV || prm->multipole_degree < 0)
+    return DUST_ERR_BAD_ARG;
+  tree_t *T = tree_init(prm);
+  int st = tree_sort(T, n, cen);
+  if (st != DUST_OK) {
+    tree_free(T);
+    return st;
+  }
+  tree_multipole(T, cen, dir, mag);
+  const int ll = T->ll;
+  const pexp_t *P = &T->pe;
+  int nl = end_vort ? end_vort->n : 0;
+  or_line_t *ls = (or_line_t *)malloc(sizeof(or_line_t) * (nl + 1));
+  for (int j = 0; j < nl; ++j) or_line_build(end_vort, j, &ls[j]);
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int ip = 0; ip < n_pts; ++ip) {
+    const double *pos = pts + 3 * ip;
+    int idx[3];
+    for (int d = 0; d < 3; ++d) idx[d] = (int)ceil((pos[d] - T->xmin[d]) / T->csize[ll]);
+    int out = 0;
+    for (int d = 0; d < 3; ++d) out |= idx[d] <= 0 || idx[d] > T->ncl[ll][d];
+    if (out) {
+      bad = 1;
+      continue;
+    }
+    /* the leaf above the finest cell */
+    int l = 1, i = 0, j = 0, k = 0;
+    int64_t c = -1;
+    for (int lv = 1; lv <= ll; ++lv) {
+      int sh = ll - lv;
+      i = (idx[0] - 1) >> sh, j = (idx[1] - 1) >> sh, k = (idx[2] - 1) >> sh;
+      int64_t cc = lin_of(T, lv, i, j, k);
+      if (T->fl[lv][cc] & FL_LEAF) {
+        l = lv;
+        c = cc;
+        break;
+      }
+    }
+    double v[3] = {0, 0, 0};
+    if (c >= 0) {
+      const mp_t *m = &T->mp[l][c];
+      const double *cc = T->cen[l] + 3 * c;
+      for (int mm = 0; mm < P->n_mon; ++mm) {
+        const int *pw = P->pwr + 3 * mm;
+        double pr = ipow(pos[0] - cc[0], pw[0]) * ipow(pos[1] - cc[1], pw[1]) *
+                    ipow(pos[2] - cc[2], pw[2]);
+        for (int e = 0; e < 3; ++e) v[e] = v[e] + m->b[3 * mm + e] * pr;
+      }
+      for (int kk = -1; kk <= 1; ++kk)
+        for (int jj = -1; jj <= 1; ++jj)
+          for (int ii = -1; ii <= 1; ++ii) {
+            if (ii == 0 && jj == 0 && kk == 0) continue;
+            if (!tree_in(T, l, i + ii, j + jj, k + kk)) continue;
+            int64_t nc = lin_of(T, l, i + ii, j + jj, k + kk);
+            if (!(T->fl[l][nc] & FL_ACTIVE)) continue;
+            int64_t nlo, nhi;
+            cell_range(T, l, i + ii, j + jj, k + kk, &nlo, &nhi);
+            for (int64_t t = nlo; t < nhi; ++t)
+              part_vel(pos, T->perm[t], cen, dir, mag, r_vortex, v);
+          }
+      int64_t nln = (l >= 2) ? T->ln_cnt[l][c] : 0;
+      for (int64_t q = 0; q < nln; ++q) {
+        int64_t e = T->ln[l][c][q];
+        int el_ = (int)(e >> 40);
+        int64_t elin = e & ((1ll << 40) - 1);
+        int ei, ej, ek;
+        cart_of(T, el_, elin, &ei, &ej, &ek);
+        int64_t nlo, nhi;
+        cell_range(T, el_, ei, ej, ek, &nlo, &nhi);
+        for (int64_t t = nlo; t < nhi; ++t)
+          part_vel(pos, T->perm[t], cen, dir, mag, r_vortex, v);
+      }
+      int64_t lo, hi;
+      cell_range(T, l, i, j, k, &lo, &hi);
+      for (int64_t t = lo; t < hi; ++t) part_vel(pos, T->perm[t], cen, dir, mag, r_vortex, v);
+    }
+    for (int q = 0; q < nl; ++q) {
+      double w[3];
+      or_vel_line(prm, &ls[q], pos, w);
+      for (int d = 0; d < 3; ++d) v[d] = v[d] + w[d] / (4.0 * OR_PI);
+    }
+    for (int d = 0; d < 3; ++d) uvort[3 * ip + d] = v[d];
+  }
+  free(ls);
+  tree_free(T);
+  return bad ? DUST_ERR_OUT_OF_BOX : DUST_OK;
+}
+
 int or_last_tree_flags(unsigned char *flags, int64_t cap) {
   if (!g_last) return DUST_ERR_BAD_ARG;
   tree_t *T = g_last;

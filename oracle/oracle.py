@@ -33,6 +33,7 @@ def lib():
         L.or_direct_particles.restype = C.c_int
         L.or_elements_vel.restype = C.c_int
         L.or_points_uvort.restype = C.c_int
+        L.or_fmm_points_uvort.restype = C.c_int
         L.or_potential_doublet.restype = C.c_double
         L.or_potential_source.restype = C.c_double
         L.or_dgetrf.restype = C.c_int
@@ -129,6 +130,23 @@ def points_uvort(prm, pts, cen, dir_, mag, rvort, end_vort=None):
                                abi.dptr(rvort), C.byref(evs), abi.dptr(out))
     if rc != 0:
         raise RuntimeError(f"oracle uvort status {rc}")
+    return out
+
+
+def fmm_points_uvort(prm, pts, cen, dir_, mag, rvort, end_vort=None):
+    """apply_multipole_panels: uvort at points from the particles' FMM plus
+    the end vortices by direct sum."""
+    pts = abi.f64(pts).reshape(-1, 3)
+    cen, dir_, mag, rvort = (abi.f64(cen), abi.f64(dir_), abi.f64(mag), abi.f64(rvort))
+    ev = end_vort if end_vort is not None else abi.empty_lines()
+    evs = ev.struct()
+    out = np.zeros_like(pts)
+    p = prm.struct()
+    rc = lib().or_fmm_points_uvort(C.byref(p), mag.shape[0], abi.dptr(cen), abi.dptr(dir_),
+                                   abi.dptr(mag), abi.dptr(rvort), pts.shape[0], abi.dptr(pts),
+                                   C.byref(evs), abi.dptr(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle FMM uvort status {rc}")
     return out
 
 

@@ -254,3 +254,43 @@ def test_fmm_degree8_matches_oracle():
     ov, os_, orr, _ = O.fmm_apply(prm, cen, dir_, mag, rv)
     v, s, r = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
     assert rel(v, ov) < TOL64 and rel(s, os_) < TOL64 and rel(r, orr) < TOL64
+
+
+@pytest.mark.parametrize("prec", [abi.DUST_PREC_FP64, abi.DUST_PREC_FP32C])
+def test_fmm_points_uvort_matches_oracle(prec):
+    """apply_multipole_panels: the panels' uvort through the particles' FMM
+    (leaf local expansion + near-field particles) plus the end vortices,
+    against the oracle's restatement; the split evaluation (prepare, points,
+    finish) gives the particles the same outputs as dust_fmm_apply."""
+    cen, dir_, mag, rv = ring(4000, seed=14)
+    pts = np.random.default_rng(3).uniform(-1.6, 1.6, (500, 3))
+    ev = abi.LineSet(np.array([[[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]]]), np.array([0.7]))
+    prm = prm_ring(precision=prec)
+    ref = O.fmm_points_uvort(prm.replace(precision=abi.DUST_PREC_FP64), pts, cen, dir_, mag,
+                             rv, ev)
+    oc = octree.initialize_octree(prm)
+    oc.prepare(cen, dir_, mag, rv)
+    u = oc.points_uvort(pts, ev)
+    tol = TOL64 if prec == abi.DUST_PREC_FP64 else TOL32
+    assert rel(u, ref) < tol
+    v1, s1, r1 = oc.finish()
+    v0, s0, r0 = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
+    assert np.array_equal(v1, v0) and np.array_equal(s1, s0) and np.array_equal(r1, r0)
+    # the FMM result approximates the direct sum to the FMM's accuracy
+    direct = O.points_uvort(prm, pts, cen, dir_, mag, rv, ev)
+    assert rel(u, direct) < 5e-3
+
+
+def test_fmm_points_uvort_errors():
+    prm = prm_ring()
+    oc = octree.initialize_octree(prm)
+    with pytest.raises(Exception) as ei:
+        oc.points_uvort(np.zeros((3, 3)))
+    assert "status 6" in str(ei.value)  # no prepared tree
+    cen, dir_, mag, rv = ring(500, seed=1)
+    oc.prepare(cen, dir_, mag, rv)
+    with pytest.raises(Exception) as ei:
+        oc.points_uvort(np.array([[5.0, 0.0, 0.0]]))
+    assert "status 2" in str(ei.value)  # outside the octree box
+    u = oc.points_uvort(np.array([[0.1, 0.2, 0.3]]))  # the handle stays usable
+    assert np.all(np.isfinite(u))

@@ -407,3 +407,19 @@ def test_oracle_row_sample_equals_full_assembly():
     rows = np.arange(0, wing.n, 7)
     Ar, br = O.linsys_rows(prm, wing, rows, (wake, wake.n, ind))
     assert np.array_equal(Ar, A[rows]) and np.array_equal(br, b[rows])
+
+
+def test_oracle_fmm_panel_uvort_converges_to_direct_sum():
+    """apply_multipole_panels (leaf local expansion + near-field particles)
+    approaches the direct particle sum as the multipole degree grows; the
+    end vortices enter both by direct sum."""
+    cen, dir_, mag = synth.ring_particles(3600, 400, seed=2)
+    rv = np.full(len(mag), 0.02)
+    pts = np.random.default_rng(0).uniform(-1.6, 1.6, (300, 3))
+    ev = abi.LineSet(np.array([[[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]]]), np.array([0.7]))
+    base = dict(box_length=4.0, origin=(-2.0, -2.0, -2.0), n_octree_levels=5,
+                min_octree_part=5, rankine_rad=0.02)
+    ref = O.points_uvort(FmmParams(**base), pts, cen, dir_, mag, rv, ev)
+    errs = [rel(O.fmm_points_uvort(FmmParams(multipole_degree=p, **base), pts, cen, dir_, mag,
+                                   rv, ev), ref) for p in (2, 4, 6)]
+    assert errs[2] < errs[1] < errs[0] and errs[2] < 5e-4
