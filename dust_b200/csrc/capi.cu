@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points of the FMM path and library utilities.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -125,11 +126,15 @@ extern "C" int dust_fmm_apply_device(dust_octree *o, int n, const double *cen,
 // velocities.
 
 extern "C" int dust_fmm_prepare(dust_octree *o, int n, const double *cen, const double *dir,
-                                const double *mag, const double *r_vortex) {
-  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex))) return DUST_ERR_BAD_ARG;
+                                const double *mag, const double *r_vortex, int n_pts,
+                                const double *pts) {
+  if (!o || n < 0 || n_pts < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex)) ||
+      (n_pts > 0 && !pts))
+    return DUST_ERR_BAD_ARG;
   cudaStream_t st = o->stream;
   size_t N = (size_t)(n > 0 ? n : 1);
   DUST_TRY(devbuf_grow(o->h_in, N * 8 * 8));
+  DUST_TRY(devbuf_grow(o->h_pts, (size_t)std::max(n_pts, 1) * 24));
   double *dc = (double *)o->h_in.p, *dd = dc + 3 * N, *dm = dd + 3 * N, *dr = dm + N;
   if (n > 0) {
     DUST_CUDA(cudaMemcpyAsync(dc, cen, (size_t)n * 24, cudaMemcpyHostToDevice, st));
@@ -137,52 +142,57 @@ extern "C" int dust_fmm_prepare(dust_octree *o, int n, const double *cen, const 
     DUST_CUDA(cudaMemcpyAsync(dm, mag, (size_t)n * 8, cudaMemcpyHostToDevice, st));
     DUST_CUDA(cudaMemcpyAsync(dr, r_vortex, (size_t)n * 8, cudaMemcpyHostToDevice, st));
   }
+  if (n_pts > 0)
+    DUST_CUDA(cudaMemcpyAsync(o->h_pts.p, pts, (size_t)n_pts * 24, cudaMemcpyHostToDevice, st));
   o->prepared_n = -1;
-  const int s = fmm_prepare_device(o, n, dc, dd, dm, dr, st);
+  const int s = fmm_prepare_device(o, n, dc, dd, dm, dr, n_pts, (const double *)o->h_pts.p, st);
   if (s != DUST_OK) o->prepared_n = -1;
   return s;
 }
 
 extern "C" int dust_fmm_prepare_device(dust_octree *o, int n, const double *cen,
                                        const double *dir, const double *mag,
-                                       const double *r_vortex, void *stream) {
-  if (!o || n < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex))) return DUST_ERR_BAD_ARG;
+                                       const double *r_vortex, int n_pts, const double *pts,
+                                       void *stream) {
+  if (!o || n < 0 || n_pts < 0 || (n > 0 && (!cen || !dir || !mag || !r_vortex)) ||
+      (n_pts > 0 && !pts))
+    return DUST_ERR_BAD_ARG;
   cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
+  DUST_TRY(devbuf_grow(o->h_pts, (size_t)std::max(n_pts, 1) * 24));
+  if (n_pts > 0)
+    DUST_CUDA(cudaMemcpyAsync(o->h_pts.p, pts, (size_t)n_pts * 24, cudaMemcpyDeviceToDevice, st));
   o->prepared_n = -1;
-  const int s = fmm_prepare_device(o, n, cen, dir, mag, r_vortex, st);
+  const int s =
+      fmm_prepare_device(o, n, cen, dir, mag, r_vortex, n_pts, (const double *)o->h_pts.p, st);
   if (s != DUST_OK) o->prepared_n = -1;
   return s;
 }
 
-extern "C" int dust_fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts,
-                                            const dust_lines *end_vort, double *uvort,
-                                            void *stream) {
-  if (!o || n_pts < 0 || (n_pts > 0 && (!pts || !uvort))) return DUST_ERR_BAD_ARG;
+extern "C" int dust_fmm_points_uvort_device(dust_octree *o, const dust_lines *end_vort,
+                                            double *uvort, void *stream) {
+  if (!o || o->prepared_n < 0 || (o->prepared_pts > 0 && !uvort)) return DUST_ERR_BAD_ARG;
   if (end_vort && (end_vort->n < 0 || (end_vort->n > 0 && (!end_vort->ver || !end_vort->mag))))
     return DUST_ERR_BAD_ARG;
-  if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
   cudaStream_t st = stream ? (cudaStream_t)stream : o->stream;
   ElemDev e;
   DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, o->prm.u_inf, reg_params(&o->prm),
                              false, o->el_raw, o->el_geo, e, st));
-  return fmm_points_uvort_device(o, n_pts, pts, e, uvort, st);
+  return fmm_points_uvort_device(o, e, uvort, st);
 }
 
-extern "C" int dust_fmm_points_uvort(dust_octree *o, int n_pts, const double *pts,
-                                     const dust_lines *end_vort, double *uvort) {
-  if (!o || n_pts < 0 || (n_pts > 0 && (!pts || !uvort))) return DUST_ERR_BAD_ARG;
+extern "C" int dust_fmm_points_uvort(dust_octree *o, const dust_lines *end_vort, double *uvort) {
+  if (!o || o->prepared_n < 0 || (o->prepared_pts > 0 && !uvort)) return DUST_ERR_BAD_ARG;
   if (end_vort && (end_vort->n < 0 || (end_vort->n > 0 && (!end_vort->ver || !end_vort->mag))))
     return DUST_ERR_BAD_ARG;
-  if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
+  const int n_pts = o->prepared_pts;
   if (n_pts == 0) return DUST_OK;
   cudaStream_t st = o->stream;
-  DUST_TRY(devbuf_grow(o->h_pts, (size_t)n_pts * 48));
-  double *dp = (double *)o->h_pts.p, *du = dp + 3 * (size_t)n_pts;
-  DUST_CUDA(cudaMemcpyAsync(dp, pts, (size_t)n_pts * 24, cudaMemcpyHostToDevice, st));
+  DUST_TRY(devbuf_grow(o->h_out, (size_t)n_pts * 24));
+  double *du = (double *)o->h_out.p;
   ElemDev e;
   DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, o->prm.u_inf, reg_params(&o->prm),
                              true, o->el_raw, o->el_geo, e, st));
-  DUST_TRY(fmm_points_uvort_device(o, n_pts, dp, e, du, st));
+  DUST_TRY(fmm_points_uvort_device(o, e, du, st));
   DUST_CUDA(cudaMemcpyAsync(uvort, du, (size_t)n_pts * 24, cudaMemcpyDeviceToHost, st));
   DUST_CUDA(cudaStreamSynchronize(st));
   return DUST_OK;

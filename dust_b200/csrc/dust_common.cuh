@@ -128,4 +128,5 @@ __host__ __device__ inline bool cart_in(const TreeGeom &G, int l, int i, int j, 
 #define FL_LEAF 1
 #define FL_BRANCH 2
 #define FL_ACTIVE 4
+#define FL_PTS 8  // an empty leaf that holds evaluation points (its locals are needed)
 

@@ -330,6 +330,34 @@ __global__ void k_flags_up(TreeGeom G, int l, const uint32_t *__restrict__ cstar
   }
 }
 
+// Evaluation points (panel centres) sorted into the tree as sort_particles
+// sorts the panels (mod_octree.f90:776-799): the leaf above each point's
+// finest cell gets FL_PTS, so that an empty leaf that holds a point still
+// gets its local expansion (the particles' own M2L skips empty targets).  A
+// point outside the box records its index in *err.
+__global__ void k_mark_points(TreeGeom G, int npts, const double *__restrict__ pts,
+                              uint8_t *__restrict__ flags, int *err) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int ll = G.ll;
+  int idx[3];
+  for (int c = 0; c < 3; ++c) {
+    idx[c] = (int)ceil((pts[3 * (size_t)q + c] - G.xmin[c]) / G.csize[ll]) - 1;
+    if (idx[c] < 0 || idx[c] >= G.ncl[ll][c]) {
+      atomicMin(err, q);
+      return;
+    }
+  }
+  for (int lv = 1; lv <= ll; ++lv) {
+    const int sh = ll - lv;
+    uint8_t *f = flags + G.lev_off[lv] + key_of(G, lv, idx[0] >> sh, idx[1] >> sh, idx[2] >> sh);
+    if (*f & FL_LEAF) {
+      *f = *f | FL_PTS;  // every writer stores the same value
+      return;
+    }
+  }
+}
+
 __global__ void k_indicators(uint32_t ntot, const uint8_t *__restrict__ flags,
                              uint32_t *__restrict__ ia, uint32_t *__restrict__ il) {
   uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -741,8 +769,11 @@ __global__ void k_m2l(FmmDev d, int l, uint32_t act_lo) {
   uint32_t ci = act_lo + blockIdx.x;
   uint32_t key = d.act_key[ci];
   // an empty target cell is a leaf without particles: its local expansion
-  // is never evaluated (and it has no children to pass it to)
-  if (cell_hi(d.G, d.cstart, l, key) == cell_lo(d.G, d.cstart, l, key)) return;
+  // is evaluated only when points were sorted into it (and it has no
+  // children to pass it to)
+  if (cell_hi(d.G, d.cstart, l, key) == cell_lo(d.G, d.cstart, l, key) &&
+      !(d.flags[d.G.lev_off[l] + key] & FL_PTS))
+    return;
   int i, j, k;
   cart_of_key(d.G, l, key, i, j, k);
   const int nm = d.nm;
@@ -1834,7 +1865,8 @@ static void fill_dev(dust_octree *o, FmmDev &d, int n) {
 // Builds the tree of n device-resident particles and evaluates the FMM; the
 // outputs stay in o->outs (sorted order) for the element pass.
 int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *dir,
-                       const double *mag, const double *rv, cudaStream_t st) {
+                       const double *mag, const double *rv, int n_pts, const double *pts,
+                       cudaStream_t st) {
   TreeGeom &G = o->G;
   o->last_stream = st;
   const int ll = G.ll;
@@ -1890,18 +1922,26 @@ int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *d
   for (int l = ll - 1; l >= 1; --l)
     k_flags_up<<<nblk(G.ncell[l], 256), 256, 0, st>>>(G, l, cstart, o->prm.min_octree_part,
                                                       flags);
+  int *perr = (int *)(small + 41);
+  DUST_CUDA(cudaMemcpyAsync(perr, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+  if (n_pts > 0) k_mark_points<<<nblk(n_pts, 128), 128, 0, st>>>(G, n_pts, pts, flags, perr);
   k_indicators<<<nblk(ntot + 1, 256), 256, 0, st>>>(ntot, flags, ia, il);
   DUST_CUDA(cub::DeviceScan::ExclusiveSum(o->cub_tmp.p, tb, ia, cidx, (int)ntot + 1, st));
   DUST_CUDA(cub::DeviceScan::ExclusiveSum(o->cub_tmp.p, tb, il, lidx, (int)ntot + 1, st));
   k_level_counts<<<1, 32, 0, st>>>(G, cidx, lidx, small);
   int64_t hsmall[DUST_MAXLEV + 3];
-  int herr = 0;
+  int herr = 0, hperr = 0;
   DUST_CUDA(cudaMemcpyAsync(hsmall, small, sizeof(int64_t) * (ll + 2), cudaMemcpyDeviceToHost,
                             st));
   DUST_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaMemcpyAsync(&hperr, perr, sizeof(int), cudaMemcpyDeviceToHost, st));
   DUST_CUDA(cudaStreamSynchronize(st));
   if (herr != 0x7fffffff) {
     o->bad_particle = herr;
+    return DUST_ERR_OUT_OF_BOX;
+  }
+  if (hperr != 0x7fffffff) {
+    dust_set_last_error("an evaluation point lies outside the octree box", __FILE__, __LINE__);
     return DUST_ERR_OUT_OF_BOX;
   }
   o->n_leaves = hsmall[0];
@@ -1988,6 +2028,7 @@ int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *d
   if (o->timing) cudaEventRecord(o->ev[3], st);
   o->dev = d;
   o->prepared_n = n;
+  o->prepared_pts = n_pts;
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }
@@ -2052,7 +2093,7 @@ int fmm_near_device(dust_octree *o, cudaStream_t st) {
 
 int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
                    const double *mag, const double *rv, cudaStream_t st) {
-  DUST_TRY(fmm_prepare_device(o, n, cen, dir, mag, rv, st));
+  DUST_TRY(fmm_prepare_device(o, n, cen, dir, mag, rv, 0, nullptr, st));
   return fmm_near_device(o, st);
 }
 
@@ -2145,11 +2186,12 @@ __global__ void k_points_fmm(FmmDev d, int npts, const double *__restrict__ pts,
 void points_lines_add(int npts, const double *pts, const ElemDev &lines, double *uv,
                       cudaStream_t st);
 
-int fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts, const ElemDev &lines,
-                            double *uv, cudaStream_t st) {
-  if (n_pts <= 0) return DUST_OK;
+int fmm_points_uvort_device(dust_octree *o, const ElemDev &lines, double *uv, cudaStream_t st) {
+  const int n_pts = o->prepared_pts;
   if (o->prepared_n < 0) return DUST_ERR_BAD_ARG;
-  int *err = (int *)((int64_t *)o->small.p + 41);
+  if (n_pts <= 0) return DUST_OK;
+  const double *pts = (const double *)o->h_pts.p;
+  int *err = (int *)((int64_t *)o->small.p + 42);
   const int big = 0x7fffffff;
   DUST_CUDA(cudaMemcpyAsync(err, &big, sizeof(int), cudaMemcpyHostToDevice, st));
   k_points_fmm<<<nblk(n_pts, 128), 128, 0, st>>>(o->dev, n_pts, pts, uv, err);

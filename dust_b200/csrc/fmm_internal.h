@@ -85,7 +85,8 @@ struct dust_octree {
   int64_t n_active = 0, n_leaves = 0;
   int64_t act_off[DUST_MAXLEV + 3];
   int bad_particle = -1;
-  int prepared_n = -1;  // particles of the last prepared tree (-1: none)
+  int prepared_n = -1;    // particles of the last prepared tree (-1: none)
+  int prepared_pts = 0;   // evaluation points sorted into it (kept in h_pts)
   FmmDev dev;
   dust_fmm_stats stats;
 };
@@ -95,11 +96,11 @@ int fmm_run_device(dust_octree *o, int n, const double *cen, const double *dir,
 // the two halves of fmm_run_device: tree, multipoles and locals; then the
 // particles' L2P + P2P
 int fmm_prepare_device(dust_octree *o, int n, const double *cen, const double *dir,
-                       const double *mag, const double *rv, cudaStream_t st);
+                       const double *mag, const double *rv, int n_pts, const double *pts,
+                       cudaStream_t st);
 int fmm_near_device(dust_octree *o, cudaStream_t st);
-// particles -> points through the prepared tree, plus the lines directly
-int fmm_points_uvort_device(dust_octree *o, int n_pts, const double *pts, const ElemDev &lines,
-                            double *uv, cudaStream_t st);
+// particles -> the prepared points through the tree, plus the lines directly
+int fmm_points_uvort_device(dust_octree *o, const ElemDev &lines, double *uv, cudaStream_t st);
 int fmm_finish_device(dust_octree *o, int n, const ElemDev &e, double *vel, double *str,
                       double *rot, cudaStream_t st);
 int fmm_collect_stats(dust_octree *o, int n, int64_t n_elem);

@@ -193,7 +193,8 @@ __global__ void k_scale_a(FmmDev d, uint32_t c0, uint32_t nact, T *out) {
 }
 
 // class keys of the active cells of levels >= 2: (level << 3 | key & 7) for
-// non-empty cells, 0xff for empty ones (dropped)
+// non-empty cells and for empty leaves that hold evaluation points, 0xff for
+// the other empty ones (dropped)
 __global__ void k_m2l_keys(FmmDev d, uint32_t c0, uint32_t nact, uint32_t *keys,
                            uint32_t *vals, int *hist) {
   uint32_t ci = c0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -201,7 +202,8 @@ __global__ void k_m2l_keys(FmmDev d, uint32_t c0, uint32_t nact, uint32_t *keys,
   int l = d.act_lev[ci];
   uint32_t key = d.act_key[ci];
   int sh = 3 * (d.G.ll - l);
-  bool ne = d.cstart[(key + 1u) << sh] > d.cstart[key << sh];
+  bool ne = d.cstart[(key + 1u) << sh] > d.cstart[key << sh] ||
+            (d.flags[d.G.lev_off[l] + key] & FL_PTS);
   uint32_t k = ne ? (uint32_t)((l << 3) | (key & 7)) : 0xffu;
   keys[ci - c0] = k;
   vals[ci - c0] = ci;

@@ -70,22 +70,25 @@ class Octree:
         return vel, st, ro
 
     # --- the two halves (prepare_wake's octree part / update_wake's apply)
-    def prepare(self, cen, dir_, mag, r_vortex):
-        """sort_particles + calculate_multipole (host arrays)."""
+    def prepare(self, cen, dir_, mag, r_vortex, pts=None):
+        """sort_particles + calculate_multipole (host arrays); ``pts`` are the
+        evaluation points (panel centres) sorted into the tree with them."""
         cen, dir_, mag, rv = (abi.f64(cen), abi.f64(dir_), abi.f64(mag), abi.f64(r_vortex))
+        pts = None if pts is None else abi.f64(pts).reshape(-1, 3)
         self._n = mag.shape[0]
+        self._npts = 0 if pts is None else pts.shape[0]
         check(lib().dust_fmm_prepare(self._h, self._n, abi.dptr(cen), abi.dptr(dir_),
-                                     abi.dptr(mag), abi.dptr(rv)), "dust_fmm_prepare")
+                                     abi.dptr(mag), abi.dptr(rv), self._npts, abi.dptr(pts)),
+              "dust_fmm_prepare")
 
-    def points_uvort(self, pts, end_vort=None):
+    def points_uvort(self, end_vort=None):
         """apply_multipole_panels: the prepared particles' velocity at the
-        points plus the end vortices (host arrays)."""
-        pts = abi.f64(pts).reshape(-1, 3)
+        prepared points plus the end vortices (host arrays)."""
         ev = end_vort if end_vort is not None else abi.empty_lines()
         evs = ev.struct()
-        out = np.empty_like(pts)
-        check(lib().dust_fmm_points_uvort(self._h, pts.shape[0], abi.dptr(pts), C.byref(evs),
-                                          abi.dptr(out)), "dust_fmm_points_uvort")
+        out = np.empty((getattr(self, "_npts", 0), 3))
+        check(lib().dust_fmm_points_uvort(self._h, C.byref(evs), abi.dptr(out)),
+              "dust_fmm_points_uvort")
         return out
 
     def finish(self, elements=None, want_stretch=True, want_rotu=True, out=None):

@@ -80,8 +80,8 @@ class HostStepper:
         uv = np.empty((c.rank, 3))
         cen_el = np.ascontiguousarray(cen_el)
         if self.fmm_uvort:
-            self.oc.prepare(c.cen, c.dir, c.mag, c.r_vortex)
-            uv = self.oc.points_uvort(cen_el, c.end_vort)
+            self.oc.prepare(c.cen, c.dir, c.mag, c.r_vortex, cen_el)
+            uv = self.oc.points_uvort(c.end_vort)
         else:
             check(lib().dust_points_uvort(C.byref(ps), c.rank, abi.dptr(cen_el),
                                           c.mag.shape[0], abi.dptr(c.cen), abi.dptr(c.dir),
@@ -187,10 +187,9 @@ class DeviceStepper:
         if self.fmm_uvort:
             # prepare_wake: the particles enter the tree once per step
             check(lib().dust_fmm_prepare_device(self.oc._h, self.n, P(self.cen), P(self.dir),
-                                                P(self.mag), P(self.rv), C.c_void_p(stream)),
-                  "dust_fmm_prepare_device")
-            check(lib().dust_fmm_points_uvort_device(self.oc._h, c.rank, P(self.ecen),
-                                                     C.byref(lines), P(self.euv),
+                                                P(self.mag), P(self.rv), c.rank, P(self.ecen),
+                                                C.c_void_p(stream)), "dust_fmm_prepare_device")
+            check(lib().dust_fmm_points_uvort_device(self.oc._h, C.byref(lines), P(self.euv),
                                                      C.c_void_p(stream)),
                   "dust_fmm_points_uvort_device")
         else:

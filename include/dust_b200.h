@@ -163,22 +163,28 @@ DUST_API int dust_fmm_apply_device(dust_octree *oct, int n,
 /* The same evaluation in the reference's two halves, so that the particles
  * enter the tree once per step and serve both the panels and themselves:
  *   dust_fmm_prepare[_device]      sort_particles + calculate_multipole of
- *                                  prepare_wake (mod_wake.f90:797-800): tree,
- *                                  multipoles, local expansions;
+ *                                  prepare_wake (mod_wake.f90:797-800): the
+ *                                  particles and the n_pts evaluation points
+ *                                  (panel centres, pts(3,n_pts), copied) are
+ *                                  sorted into the tree as sort_particles
+ *                                  sorts particles and panels
+ *                                  (mod_octree.f90:703-799); multipoles and
+ *                                  local expansions, including those of the
+ *                                  empty leaves that hold points.  A particle
+ *                                  or point outside the box is
+ *                                  DUST_ERR_OUT_OF_BOX;
  *   dust_fmm_points_uvort[_device] apply_multipole_panels (:801,
  *                                  mod_octree.f90:1433-1508): the particles'
- *                                  velocity at n_pts points (panel centres,
- *                                  each taking the local expansion of the
- *                                  leaf that holds it plus the particles of
- *                                  that leaf's near field) plus the end
- *                                  vortices by direct sum, into uvort(3,n_pts)
- *                                  (overwritten).  The reference adds this to
- *                                  uvort and then discards it in get_vort_vel
+ *                                  velocity at the prepared points (each takes
+ *                                  the local expansion of the leaf that holds
+ *                                  it plus the particles of that leaf's near
+ *                                  field) plus the end vortices by direct
+ *                                  sum, into uvort(3,n_pts) (overwritten).
+ *                                  The reference adds this to uvort and then
+ *                                  discards it in get_vort_vel
  *                                  (mod_surfpan.f90:970); here it is the
  *                                  result, an approximation of
- *                                  dust_points_uvort to the FMM's accuracy.
- *                                  A point outside the octree box is
- *                                  DUST_ERR_OUT_OF_BOX;
+ *                                  dust_points_uvort to the FMM's accuracy;
  *   dust_fmm_finish[_device]       apply_multipole (mod_wake.f90:1115-1118):
  *                                  L2P + P2P at the prepared particles and
  *                                  the element sums, outputs as
@@ -186,18 +192,17 @@ DUST_API int dust_fmm_apply_device(dust_octree *oct, int n,
  * points_uvort and finish need a prepared tree (DUST_ERR_BAD_ARG otherwise);
  * the tree stays valid until the next prepare or apply on the handle.  The
  * device variants run on `stream` (NULL = the handle's stream); finish
- * synchronises when `sync` != 0, points_uvort always (it reads its error
- * word). */
+ * synchronises when `sync` != 0, points_uvort always. */
 DUST_API int dust_fmm_prepare(dust_octree *oct, int n, const double *cen, const double *dir,
-                              const double *mag, const double *r_vortex);
+                              const double *mag, const double *r_vortex, int n_pts,
+                              const double *pts);
 DUST_API int dust_fmm_prepare_device(dust_octree *oct, int n, const double *cen,
                                      const double *dir, const double *mag,
-                                     const double *r_vortex, void *stream);
-DUST_API int dust_fmm_points_uvort(dust_octree *oct, int n_pts, const double *pts,
-                                   const dust_lines *end_vort, double *uvort);
-DUST_API int dust_fmm_points_uvort_device(dust_octree *oct, int n_pts, const double *pts,
-                                          const dust_lines *end_vort, double *uvort,
-                                          void *stream);
+                                     const double *r_vortex, int n_pts, const double *pts,
+                                     void *stream);
+DUST_API int dust_fmm_points_uvort(dust_octree *oct, const dust_lines *end_vort, double *uvort);
+DUST_API int dust_fmm_points_uvort_device(dust_octree *oct, const dust_lines *end_vort,
+                                          double *uvort, void *stream);
 DUST_API int dust_fmm_finish(dust_octree *oct, const dust_elements *elems, double *vel,
                              double *stretch, double *rotu);
 DUST_API int dust_fmm_finish_device(dust_octree *oct, const dust_elements *elems, double *vel,

@@ -269,8 +269,8 @@ def test_fmm_points_uvort_matches_oracle(prec):
     ref = O.fmm_points_uvort(prm.replace(precision=abi.DUST_PREC_FP64), pts, cen, dir_, mag,
                              rv, ev)
     oc = octree.initialize_octree(prm)
-    oc.prepare(cen, dir_, mag, rv)
-    u = oc.points_uvort(pts, ev)
+    oc.prepare(cen, dir_, mag, rv, pts)
+    u = oc.points_uvort(ev)
     tol = TOL64 if prec == abi.DUST_PREC_FP64 else TOL32
     assert rel(u, ref) < tol
     v1, s1, r1 = oc.finish()
@@ -285,12 +285,15 @@ def test_fmm_points_uvort_errors():
     prm = prm_ring()
     oc = octree.initialize_octree(prm)
     with pytest.raises(Exception) as ei:
-        oc.points_uvort(np.zeros((3, 3)))
+        oc.points_uvort()
     assert "status 6" in str(ei.value)  # no prepared tree
     cen, dir_, mag, rv = ring(500, seed=1)
-    oc.prepare(cen, dir_, mag, rv)
     with pytest.raises(Exception) as ei:
-        oc.points_uvort(np.array([[5.0, 0.0, 0.0]]))
-    assert "status 2" in str(ei.value)  # outside the octree box
-    u = oc.points_uvort(np.array([[0.1, 0.2, 0.3]]))  # the handle stays usable
-    assert np.all(np.isfinite(u))
+        oc.prepare(cen, dir_, mag, rv, np.array([[5.0, 0.0, 0.0]]))
+    assert "status 2" in str(ei.value)  # a point outside the octree box
+    with pytest.raises(Exception) as ei:
+        oc.points_uvort()
+    assert "status 6" in str(ei.value)  # the failed prepare left no tree
+    oc.prepare(cen, dir_, mag, rv, np.array([[0.1, 0.2, 0.3]]))  # the handle stays usable
+    u = oc.points_uvort()
+    assert u.shape == (1, 3) and np.all(np.isfinite(u))
