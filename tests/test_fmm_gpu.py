@@ -261,7 +261,7 @@ def test_fmm_points_uvort_matches_oracle(prec):
     """apply_multipole_panels: the panels' uvort through the particles' FMM
     (leaf local expansion + near-field particles) plus the end vortices,
     against the oracle's restatement; the split evaluation (prepare, points,
-    finish) gives the particles the same outputs as dust_fmm_apply."""
+    finish) gives the particles the outputs of dust_fmm_apply."""
     cen, dir_, mag, rv = ring(4000, seed=14)
     pts = np.random.default_rng(3).uniform(-1.6, 1.6, (500, 3))
     ev = abi.LineSet(np.array([[[0.0, 0.0, 0.0], [0.5, 0.5, 0.0]]]), np.array([0.7]))
@@ -275,7 +275,9 @@ def test_fmm_points_uvort_matches_oracle(prec):
     assert rel(u, ref) < tol
     v1, s1, r1 = oc.finish()
     v0, s0, r0 = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
-    assert np.array_equal(v1, v0) and np.array_equal(s1, s0) and np.array_equal(r1, r0)
+    # the same sums; the extra targets (empty leaves holding points) change
+    # only the M2L batching, so rounding order may differ
+    assert rel(v1, v0) < 1e-13 and rel(s1, s0) < 1e-13 and rel(r1, r0) < 1e-13
     # the FMM result approximates the direct sum to the FMM's accuracy
     direct = O.points_uvort(prm, pts, cen, dir_, mag, rv, ev)
     assert rel(u, direct) < 5e-3
