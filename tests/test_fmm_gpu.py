@@ -276,8 +276,10 @@ def test_fmm_points_uvort_matches_oracle(prec):
     v1, s1, r1 = oc.finish()
     v0, s0, r0 = octree.initialize_octree(prm).apply_multipole(cen, dir_, mag, rv)
     # the same sums; the extra targets (empty leaves holding points) change
-    # only the M2L batching, so rounding order may differ
-    assert rel(v1, v0) < 1e-13 and rel(s1, s0) < 1e-13 and rel(r1, r0) < 1e-13
+    # only the M2L batching, so the rounding (FP64) or the FP32 partial sums
+    # of the tensor-core M2L (FP32C) may differ
+    tsplit = 1e-13 if prec == abi.DUST_PREC_FP64 else TOL32
+    assert rel(v1, v0) < tsplit and rel(s1, s0) < tsplit and rel(r1, r0) < tsplit
     # the FMM result approximates the direct sum to the FMM's accuracy
     direct = O.points_uvort(prm, pts, cen, dir_, mag, rv, ev)
     assert rel(u, direct) < 5e-3
