@@ -2044,7 +2044,13 @@ int fmm_near_device(dust_octree *o, cudaStream_t st) {
     const bool f32 = o->prm.precision == DUST_PREC_FP32C;
     uint32_t *gstart = nullptr, *ngroups = nullptr, *work = nullptr;
     unsigned pg_grid = 0;
-    if (f32) {
+    // FP32C near-field kernel: 0 = warp per leaf, 1 = CTA per leaf (FP32
+    // pairs), 2 = CTA per sibling group
+#ifndef DUST_P2P32
+#define DUST_P2P32 0
+#endif
+    const int p32 = DUST_P2P32;
+    if (f32 && p32 == 2) {
       // sibling groups of the leaf list (consecutive leaves of one level
       // and one parent): flags, exclusive scan, starts
       const size_t nl1 = (size_t)o->n_leaves + 1;
@@ -2070,8 +2076,13 @@ int fmm_near_device(dust_octree *o, cudaStream_t st) {
     }
 #define LAUNCH_P2P(A, B, C, D)                                                   \
   do {                                                                         \
-    if (f32)                                                                   \
+    if (f32 && p32 == 2)                                                       \
       k_p2p_g<A, B, C, D><<<pg_grid, PG_T, 0, st>>>(d, gstart, ngroups, work);  \
+    else if (f32 && p32 == 0)                                                  \
+      k_p2p_w<A, B, C, D><<<(unsigned)((o->n_leaves + P2W_WARPS - 1) / P2W_WARPS), \
+                            P2W_WARPS * 32, 0, st>>>(d);                        \
+    else if (f32)                                                              \
+      k_p2p<A, B, C, D, true><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);    \
     else                                                                       \
       k_p2p<A, B, C, D, false><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);   \
   } while (0)
