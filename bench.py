@@ -9,16 +9,20 @@ vortices, and a particle wake of 2,000,000 particles; FMM degree 4, leaves
 public dataset exists for this path.
 
 A step = uvort at the 13,920 collocation points (direct sum over particles
-and end vortices) + AIC assembly + solve + FMM evaluation of the particle
-velocities/stretching (tree, multipoles, L2P, P2P, element sums).
+and end vortices; --uvort fmm takes it from the particles' FMM instead) +
+AIC assembly + solve + FMM evaluation of the particle velocities/stretching
+(tree, multipoles, L2P, P2P, element sums) + the particle update of
+complete_wake (explicit Euler advection and stretching, so the next step's
+tree is built on moved particles; --no-advect leaves them in place).
 
 Arms:
   default            this library; ``value`` = device-resident step time of
                      the fastest solve mode, ``e2e`` = host-API step time
                      with pinned host buffers (copies inside the timed region)
   --impl reference   the reference's algorithm on the host cores (the C/OpenMP
-                     oracle; the Fortran reference cannot be built here),
-                     timed on a bounded sample and scaled to one step
+                     oracle + LAPACK/BLAS; the Fortran reference cannot be
+                     built here): one whole step timed in full, after the
+                     untimed initialize_linsys
 
 One process per GPU under torchrun; the path does not shard (replicas only):
 every rank runs its own replica, timing is the max over ranks.
@@ -852,7 +856,8 @@ def phase_breakdown(st, case, params):
             "n_leaves": s["n_leaves"], "n_active_cells": s["n_active_cells"],
             "n_m2l_pairs": s["n_m2l_pairs"], "n_p2p_pairs": s["n_p2p_pairs"],
             "n_elem_pairs": s["n_elem_pairs"],
-            "k_m2l_tc_ms": round(s["ms_m2l_kernel"], 3), "k_elem_far_ms": round(s["ms_elem_far"], 3)}
+            "k_m2l_batch_ms": round(s["ms_m2l_kernel"], 3),
+            "k_elem_far_ms": round(s["ms_elem_far"], 3)}
 
 
 # Algorithmic work per unit (FMA = 2 flops), from the kernels' formulas:
@@ -864,6 +869,12 @@ FLOP_UVORT_PAIR = 24
 #  M2L pair at p = 4 with stretching: 56 outputs x 35 inputs x 3 components x
 #  2 cross-product terms, one FMA each
 FLOP_M2L_PAIR = 56 * 35 * 6 * 2
+#  M2L pair, algorithmic bytes at p = 4 (35 monomials, w bytes a word): source
+#  a (3 x 35 w) + target b read and write (2 x 3 x 35 w) + stretching c read
+#  and write (2 x 9 x 35 w)
+BYTES_M2L_PAIR_WORDS = 3 * 35 + 2 * 3 * 35 + 2 * 9 * 35
+#  P2P pair with stretching, div-filter rotu and PSE diffusion: 27 + 30 + 18 + 20
+FLOP_P2P_PAIR = 95
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) on the 300k-particle case and scaled by the particle
 # count to 2M (profiles/traffic_mixed_step_300k.txt)
@@ -871,45 +882,73 @@ TRAFFIC_ELEM_FAR_PER_PARTICLE = 381.5
 
 
 def roofline(ph, case, params, best):
-    """Roofline of the dominant kernel of the headline mode, plus the other
-    large kernels.  Peaks: MEASURED_PEAKS.json (HBM copy GB/s, cuBLAS bf16
-    TFLOP/s); the FP32 SIMT peak is not measured there and is the nominal
-    148 SMs x 128 lanes x 2 flops x sm_max_mhz; the TF32 dense peak is half
-    the measured bf16 figure (the nominal ratio)."""
+    """Roofline of the dominant kernel of the headline mode (``best``), with
+    the step's other large kernels in ``others``.  Peaks: MEASURED_PEAKS.json
+    (HBM copy GB/s); the FP32 and FP64 SIMT peaks are not measured there and
+    are the nominal 148 SMs x 128 (FP32) or 64 (FP64) lanes x 2 flops x
+    sm_max_mhz."""
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
         peaks = json.load(open(pk))
     mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    src = "of measured" if peaks else "of fallback"
-    bf16 = peaks.get("bf16_tflops", 1590.0)
+    fp64_peak = fp32_peak / 2
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
     p = ph.get(best, {})
+    f64 = best.startswith("plain")
+    w = 8 if f64 else 4
+    simt = fp64_peak if f64 else fp32_peak
+    simt_name = "nominal %s SIMT (148 SMs x %d x 2 x %g MHz)" % ("FP64" if f64 else "FP32",
+                                                                  64 if f64 else 128, mhz)
     n = case.mag.shape[0]
-    out = {}
+    ks = []
     if p.get("k_elem_far_ms"):
         a = FLOP_ELEM_PAIR * p["n_elem_pairs"] / (p["k_elem_far_ms"] * 1e-3) / 1e12
         tr = None if TRAFFIC_ELEM_FAR_PER_PARTICLE is None else int(TRAFFIC_ELEM_FAR_PER_PARTICLE * n)
-        out = {"kernel": "k_elem_far", "bound": "fp32", "achieved": round(a, 2),
-               "peak": round(fp32_peak, 1), "unit": "TFLOP/s", "frac": round(a / fp32_peak, 3),
-               "traffic": tr, "peak_source": "nominal FP32 SIMT (148 SMs x 128 x 2 x %g MHz)" % mhz,
-               "flop_per_pair": FLOP_ELEM_PAIR, "pairs": p["n_elem_pairs"],
-               "ms": p["k_elem_far_ms"]}
-    others = []
-    if p.get("k_m2l_tc_ms"):
-        a = FLOP_M2L_PAIR * p["n_m2l_pairs"] / (p["k_m2l_tc_ms"] * 1e-3) / 1e12
-        others.append({"kernel": "k_m2l_tc", "bound": "tensor", "achieved": round(a, 2),
-                       "peak": round(bf16 / 2, 1), "unit": "TFLOP/s",
-                       "frac": round(a / (bf16 / 2), 4), "ms": p["k_m2l_tc_ms"],
-                       "peak_source": "TF32 = bf16 %s / 2" % src,
-                       "note": "useful FP32-equivalent flops; 3xTF32 issues 3x on the tensor pipe"})
+        ks.append({"kernel": "k_elem_far", "bound": "fp32", "achieved": round(a, 2),
+                   "peak": round(fp32_peak, 1), "unit": "TFLOP/s", "frac": round(a / fp32_peak, 3),
+                   "traffic": tr, "peak_source": simt_name, "flop_per_pair": FLOP_ELEM_PAIR,
+                   "pairs": p["n_elem_pairs"], "ms": p["k_elem_far_ms"]})
+    elif p.get("fmm_elements"):
+        a = FLOP_ELEM_PAIR * p["n_elem_pairs"] / (p["fmm_elements"] * 1e-3) / 1e12
+        ks.append({"kernel": "k_elem_out (elements, end vortices, outputs)",
+                   "bound": "fp64" if f64 else "fp32", "achieved": round(a, 2),
+                   "peak": round(simt, 1), "unit": "TFLOP/s", "frac": round(a / simt, 3),
+                   "traffic": None, "peak_source": simt_name, "flop_per_pair": FLOP_ELEM_PAIR,
+                   "pairs": p["n_elem_pairs"], "ms": p["fmm_elements"]})
+    if p.get("k_m2l_batch_ms"):
+        t = p["k_m2l_batch_ms"] * 1e-3
+        gbs = BYTES_M2L_PAIR_WORDS * w * p["n_m2l_pairs"] / t / 1e9
+        fl = FLOP_M2L_PAIR * p["n_m2l_pairs"] / t / 1e12
+        ks.append({"kernel": "k_m2l_batch", "bound": "hbm", "achieved": round(gbs, 1),
+                   "peak": round(hbm, 1), "unit": "GB/s", "frac": round(gbs / hbm, 3),
+                   "traffic": None, "peak_source": "HBM copy %s" % hbm_src,
+                   "bytes_per_pair": BYTES_M2L_PAIR_WORDS * w, "pairs": p["n_m2l_pairs"],
+                   "ms": p["k_m2l_batch_ms"],
+                   "flops": {"achieved": round(fl, 2), "peak": round(simt, 1),
+                             "unit": "TFLOP/s", "frac": round(fl / simt, 3),
+                             "flop_per_pair": FLOP_M2L_PAIR, "peak_source": simt_name}})
+    if p.get("fmm_p2p"):
+        a = FLOP_P2P_PAIR * p["n_p2p_pairs"] / (p["fmm_p2p"] * 1e-3) / 1e12
+        ks.append({"kernel": "k_p2p_w (L2P + P2P)", "bound": "fp64" if f64 else "fp32",
+                   "achieved": round(a, 2), "peak": round(simt, 1), "unit": "TFLOP/s",
+                   "frac": round(a / simt, 3), "traffic": None, "peak_source": simt_name,
+                   "flop_per_pair": FLOP_P2P_PAIR, "pairs": p["n_p2p_pairs"], "ms": p["fmm_p2p"]})
     if p.get("uvort"):
         pairs = case.rank * n
         a = FLOP_UVORT_PAIR * pairs / (p["uvort"] * 1e-3) / 1e12
-        others.append({"kernel": "uvort phase (k_uvort_sorted + sort)", "bound": "fp32",
-                       "achieved": round(a, 2), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
-                       "frac": round(a / fp32_peak, 3), "ms": p["uvort"]})
-    out["others"] = others
+        ks.append({"kernel": "uvort phase (%s)" % ("k_uvort" if f64 else "k_uvort_sorted + sort"),
+                   "bound": "fp64" if f64 else "fp32", "achieved": round(a, 2),
+                   "peak": round(simt, 1), "unit": "TFLOP/s", "frac": round(a / simt, 3),
+                   "traffic": None, "peak_source": simt_name, "flop_per_pair": FLOP_UVORT_PAIR,
+                   "pairs": pairs, "ms": p["uvort"]})
+    if not ks:
+        return {"others": [], "peaks_file": bool(peaks)}
+    ks.sort(key=lambda k: -k["ms"])
+    out = dict(ks[0])
+    out["others"] = ks[1:]
     out["peaks_file"] = bool(peaks)
     return out
 

@@ -129,6 +129,7 @@ class SolveReport(C.Structure):
         ("residual", C.c_double),
         ("ms_factor", C.c_float),
         ("ms_solve", C.c_float),
+        ("pivoted", C.c_int),
     ]
 
 

@@ -65,73 +65,178 @@ __device__ inline void near_pan(const RegParams &rp, const PanelGeo *pg, int j,
   vel_pan_near(rp, pg[j], pos, v);
 }
 
-#define EF_T 128
-#define EF_TILE 64
-
 // FP64 element sums (plain mode): far field by the closed form above, near
 // pairs by the reference's formulas; then end vortices, wind and the scatter
 // of all outputs to the caller's order.
-__global__ void __launch_bounds__(EF_T) k_elem_out(FmmDev d, ElemDev e, const FFRec *ff,
+//
+// EO_PPT particles per thread against shared-memory tiles of EO_LOAD panels
+// (far-field records, FP64).  The loader threads test each panel against the
+// bounding box of the CTA's particles: a sub-tile of EO_TILE panels that
+// lies beyond the far-field radius of the whole box runs the far formula
+// without a per-pair test (the box distance is formed with the per-pair
+// test's own operation order, so rounding, being monotone, cannot make the
+// box call far a pair the per-pair test calls near).  In the other sub-tiles
+// each pair is tested; the near pairs of a particle are marked in a bit mask
+// and evaluated after the sub-tile's far loop, in panel order, so the sums
+// are deterministic.  The reciprocal square root of the far formula is the
+// FP32 approximation refined by one second-order Newton-Raphson
+// (Householder) step in FP64: with y0 = x^-1/2 (1 + d) and e = 1 - x y0^2,
+// y = y0 (1 + e/2 + 3 e^2/8) has relative error O(d^3), below the FP64
+// rounding for |d| < 2^-21.
+#define EO_PPT 2
+#define EO_T 128
+#define EO_NP (EO_T * EO_PPT)
+#define EO_TILE 16
+#define EO_SUB 4
+#define EO_LOAD (EO_TILE * EO_SUB)
+#define EO_PK 12  // nm x/y/z, mn x/y/z, -c x/y/z, as, ff2, pad
+static_assert(EO_LOAD <= EO_T && EO_LOAD % 32 == 0 && EO_TILE <= 32, "staging layout");
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// x^-1/2 for a normal FP32-range x > 0
+__device__ __forceinline__ double rsqrt_hh(double x) {
+  const double y = (double)rsqrt_approx((float)x);
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
+__global__ void __launch_bounds__(EO_T) k_elem_out(FmmDev d, ElemDev e, const FFRec *ff,
                                                    double *vel, double *str, double *rot) {
-  __shared__ double s_c[EF_TILE][3], s_n[EF_TILE][3];
-  __shared__ double s_amu[EF_TILE], s_asig[EF_TILE], s_ff2[EF_TILE];
-  const uint32_t t = blockIdx.x * EF_T + threadIdx.x;
+  __shared__ __align__(16) double s_pk[EO_LOAD][EO_PK];
+  __shared__ unsigned s_nearw[EO_LOAD / 32];
+  __shared__ double s_box[EO_T / 32][6];
   const size_t n = d.n;
-  const bool act = t < n;
-  double pos[3] = {0.0, 0.0, 0.0};
-  if (act)
-    for (int c = 0; c < 3; ++c) pos[c] = d.P[(size_t)c * n + t];
-  double v[3] = {0, 0, 0};
+  const uint32_t t0 = blockIdx.x * EO_NP;
+  const int tid = threadIdx.x;
+  double pos[EO_PPT][3], v[EO_PPT][3];
+  bool act[EO_PPT];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+  for (int i = 0; i < EO_PPT; ++i) {
+    const uint32_t t = t0 + tid + i * EO_T;
+    act[i] = t < n;
+    const uint32_t tt = act[i] ? t : t0;
+    for (int c = 0; c < 3; ++c) {
+      pos[i][c] = d.P[(size_t)c * n + tt];
+      lo[c] = fmin(lo[c], pos[i][c]);
+      hi[c] = fmax(hi[c], pos[i][c]);
+      v[i][c] = 0.0;
+    }
+  }
+  // bounding box of the CTA's particles
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+  if ((tid & 31) == 0)
+    for (int c = 0; c < 3; ++c) s_box[tid >> 5][c] = lo[c], s_box[tid >> 5][3 + c] = hi[c];
+  __syncthreads();
+  for (int w = 0; w < EO_T / 32; ++w)
+    for (int c = 0; c < 3; ++c) lo[c] = fmin(lo[c], s_box[w][c]), hi[c] = fmax(hi[c], s_box[w][3 + c]);
   const int ntot = e.nbody + e.nwake;
-  for (int p0 = 0; p0 < ntot; p0 += EF_TILE) {
+  for (int p0 = 0; p0 < ntot; p0 += EO_LOAD) {
     __syncthreads();
-    const int m = min(EF_TILE, ntot - p0);
-    for (int q = threadIdx.x; q < m; q += EF_T) {
-      const FFRec &r = ff[p0 + q];
-      for (int c = 0; c < 3; ++c) {
-        s_c[q][c] = r.c[c];
-        s_n[q][c] = r.n[c];
-      }
-      s_amu[q] = r.amu;
-      s_asig[q] = r.asig;
-      s_ff2[q] = r.ff2;
-    }
-    __syncthreads();
-    if (!act) continue;
-    for (int q = 0; q < m; ++q) {
-      double rx = pos[0] - s_c[q][0], ry = pos[1] - s_c[q][1], rz = pos[2] - s_c[q][2];
-      double r2 = rx * rx + ry * ry + rz * rz;
-      if (r2 > s_ff2[q]) {
-        double ir = rsqrt(r2);
-        double ir2 = ir * ir;
-        double rn = rx * s_n[q][0] + ry * s_n[q][1] + rz * s_n[q][2];
-        double k3 = ir2 * ir;
-        double coef = 3.0 * s_amu[q] * rn * ir2 + s_asig[q];
-        v[0] += k3 * (coef * rx - s_amu[q] * s_n[q][0]);
-        v[1] += k3 * (coef * ry - s_amu[q] * s_n[q][1]);
-        v[2] += k3 * (coef * rz - s_amu[q] * s_n[q][2]);
+    bool near_box = false;
+    if (tid < EO_LOAD) {
+      double *pk = s_pk[tid];
+      if (p0 + tid < ntot) {
+        const FFRec &r = ff[p0 + tid];
+        for (int c = 0; c < 3; ++c) {
+          pk[c] = 3.0 * r.amu * r.n[c];
+          pk[3 + c] = -r.amu * r.n[c];
+          pk[6 + c] = -r.c[c];
+        }
+        pk[9] = r.asig;
+        pk[10] = r.ff2;
+        // box distance in the per-pair test's operation order
+        double q[3];
+        for (int c = 0; c < 3; ++c) {
+          const double a = lo[c] - r.c[c], b = hi[c] - r.c[c];
+          q[c] = a > 0.0 ? a : (b < 0.0 ? b : 0.0);
+        }
+        const double d2 = fma(q[0], q[0], fma(q[1], q[1], q[2] * q[2]));
+        near_box = !(d2 > r.ff2);
       } else {
-        int j = p0 + q;
-        const PanelGeo *pg = j < e.nbody ? e.body : e.wake;
-        int jj = j < e.nbody ? j : j - e.nbody;
-        double u[3];
-        near_pan(e.rp, pg, jj, pos, u);
-        for (int c = 0; c < 3; ++c) v[c] += u[c];
+        // padding: no strength, far away
+        for (int c = 0; c < 11; ++c) pk[c] = 0.0;
+        pk[6] = -1.0e6;
+      }
+      pk[11] = 0.0;
+    }
+    const unsigned nb = __ballot_sync(0xffffffffu, near_box);
+    if ((tid & 31) == 0 && tid < EO_LOAD) s_nearw[tid >> 5] = nb;
+    __syncthreads();
+    const int nsub = min(EO_SUB, (ntot - p0 + EO_TILE - 1) / EO_TILE);
+    for (int sb = 0; sb < nsub; ++sb) {
+      const int qs = sb * EO_TILE;
+      const bool near_sub = (s_nearw[qs >> 5] >> (qs & 31)) & ((1u << EO_TILE) - 1u);
+      unsigned nmask[EO_PPT];
+#pragma unroll
+      for (int i = 0; i < EO_PPT; ++i) nmask[i] = 0u;
+#pragma unroll 4
+      for (int q = 0; q < EO_TILE; ++q) {
+        const double2 *pk = (const double2 *)s_pk[qs + q];
+        const double2 A = pk[0], B = pk[1], C = pk[2], D = pk[3], E = pk[4], F = pk[5];
+        // A = (nmx, nmy), B = (nmz, mnx), C = (mny, mnz), D = (-cx, -cy), E = (-cz, as), F = (ff2, 0)
+#pragma unroll
+        for (int i = 0; i < EO_PPT; ++i) {
+          const double rx = pos[i][0] + D.x, ry = pos[i][1] + D.y, rz = pos[i][2] + E.x;
+          const double r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+          const bool far = !near_sub || r2 > F.x;
+          if (far) {
+            const double ir = rsqrt_hh(r2);
+            const double ir2 = ir * ir;
+            const double k3 = ir2 * ir;
+            const double rn = fma(rx, A.x, fma(ry, A.y, rz * B.x));
+            const double coef = fma(rn, ir2, E.y);
+            v[i][0] = fma(k3, fma(coef, rx, B.y), v[i][0]);
+            v[i][1] = fma(k3, fma(coef, ry, C.x), v[i][1]);
+            v[i][2] = fma(k3, fma(coef, rz, C.y), v[i][2]);
+          } else {
+            nmask[i] |= 1u << q;
+          }
+        }
+      }
+      if (near_sub) {
+#pragma unroll
+        for (int i = 0; i < EO_PPT; ++i) {
+          unsigned m = act[i] ? nmask[i] : 0u;
+          while (m) {
+            const int q = __ffs(m) - 1;
+            m &= m - 1u;
+            const int j = p0 + qs + q;
+            const PanelGeo *pg = j < e.nbody ? e.body + j : e.wake + (j - e.nbody);
+            double u[3];
+            vel_pan_near(e.rp, *pg, pos[i], u);
+            for (int c = 0; c < 3; ++c) v[i][c] += u[c];
+          }
+        }
       }
     }
   }
-  if (!act) return;
-  for (int q = 0; q < e.nline; ++q) {
-    double u[3];
-    vel_line(e.rp, e.lines[q], pos, u);
-    for (int c = 0; c < 3; ++c) v[c] += u[c];
-  }
-  const uint32_t ip = d.perm[t];
   const double k4pi = 1.0 / (4.0 * DUST_PI);
-  for (int c = 0; c < 3; ++c) {
-    vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + v[c] * k4pi + d.u_inf[c];
-    if (str) str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
-    if (rot) rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
+#pragma unroll
+  for (int i = 0; i < EO_PPT; ++i) {
+    if (!act[i]) continue;
+    for (int q = 0; q < e.nline; ++q) {
+      double u[3];
+      vel_line(e.rp, e.lines[q], pos[i], u);
+      for (int c = 0; c < 3; ++c) v[i][c] += u[c];
+    }
+    const uint32_t t = t0 + tid + i * EO_T;
+    const uint32_t ip = d.perm[t];
+    for (int c = 0; c < 3; ++c) {
+      vel[3 * (size_t)ip + c] = d.out[(size_t)c * n + t] + v[i][c] * k4pi + d.u_inf[c];
+      if (str) str[3 * (size_t)ip + c] = (d.use_vs || d.use_vd) ? d.out[(size_t)(3 + c) * n + t] : 0.0;
+      if (rot) rot[3 * (size_t)ip + c] = (d.use_vs && d.use_df) ? d.out[(size_t)(6 + c) * n + t] : 0.0;
+    }
   }
 }
 
@@ -171,12 +276,6 @@ static_assert(EF2_NP <= 1024, "local particle index is packed in 10 bits");
 struct NearPair {
   uint32_t t, j;  // particle (sorted order), panel
 };
-
-__device__ __forceinline__ float rsqrt_approx(float x) {
-  float r;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
 
 __device__ __forceinline__ void ef2_flush(const uint32_t *s_q, int qn, uint32_t t0,
                                           unsigned long long *count, NearPair *list,
@@ -574,7 +673,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
     if (precision == DUST_PREC_FP32C && ntot < (1 << 22))
       return elem_output_split(d, e, ff, work, near_cap, vel, str, rot, st, kev, kev_done);
     else
-      k_elem_out<<<nblk(d.n, EF_T), EF_T, 0, st>>>(d, e, ff, vel, str, rot);
+      k_elem_out<<<nblk(d.n, EO_NP), EO_T, 0, st>>>(d, e, ff, vel, str, rot);
   }
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
@@ -586,44 +685,64 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
 #define UV2_T 128
 #define UV2_TILE 128
 
-// FP64 uvort (plain mode): particles in the caller's order
+// FP64 uvort (plain mode): particles in the caller's order, UVD_PPT points
+// per thread (consecutive CTA slices of UV2_T points) against a shared tile
+// of (x, y, z, r_v^2, alpha) records; the reciprocal square root as in
+// k_elem_out (FP32 seed, one Householder step in FP64).
+#define UVD_PPT 2
 __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, int n,
                                                  const double *cen, const double *dir,
                                                  const double *mag, const double *rv,
                                                  int chunk, double *uv) {
-  __shared__ double s_x[UV2_TILE][3], s_a[UV2_TILE][3], s_s[UV2_TILE];
-  const int t = blockIdx.x * UV2_T + threadIdx.x;
-  const bool act = t < npts;
+  __shared__ __align__(16) double s_q[UV2_TILE][8];
+  const int t0 = blockIdx.x * UV2_T * UVD_PPT + threadIdx.x;
   const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
-  double pos[3] = {0, 0, 0};
-  if (act)
-    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
-  double v[3] = {0, 0, 0};
+  double pos[UVD_PPT][3], v[UVD_PPT][3];
+#pragma unroll
+  for (int i = 0; i < UVD_PPT; ++i) {
+    const int t = t0 + i * UV2_T;
+    for (int c = 0; c < 3; ++c) {
+      pos[i][c] = t < npts ? pts[3 * (size_t)t + c] : 0.0;
+      v[i][c] = 0.0;
+    }
+  }
   for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
     __syncthreads();
     const int q = q0 + threadIdx.x;
     const int m = min(UV2_TILE, q_hi - q0);
     if (threadIdx.x < m) {
-      double mg = mag[q];
-      for (int c = 0; c < 3; ++c) s_x[threadIdx.x][c] = cen[3 * (size_t)q + c];
-      for (int c = 0; c < 3; ++c) s_a[threadIdx.x][c] = mg * dir[3 * (size_t)q + c];
-      s_s[threadIdx.x] = rv[q];
+      const double mg = mag[q], r = rv[q];
+      double *w = s_q[threadIdx.x];
+      for (int c = 0; c < 3; ++c) w[c] = cen[3 * (size_t)q + c];
+      w[3] = r * r;
+      for (int c = 0; c < 3; ++c) w[4 + c] = mg * dir[3 * (size_t)q + c];
+      w[7] = 0.0;
     }
     __syncthreads();
-    if (!act) continue;
+#pragma unroll 2
     for (int u = 0; u < m; ++u) {
-      double dx = pos[0] - s_x[u][0], dy = pos[1] - s_x[u][1], dz = pos[2] - s_x[u][2];
-      double r2 = dx * dx + dy * dy + dz * dz + s_s[u] * s_s[u];
-      double ir = rsqrt(r2);
-      double c = -ir * ir * ir;
-      v[0] += c * (dy * s_a[u][2] - dz * s_a[u][1]);
-      v[1] += c * (dz * s_a[u][0] - dx * s_a[u][2]);
-      v[2] += c * (dx * s_a[u][1] - dy * s_a[u][0]);
+      const double2 *w = (const double2 *)s_q[u];
+      const double2 X = w[0], Y = w[1], Z = w[2], W = w[3];
+      // X = (x, y), Y = (z, r_v^2), Z = (ax, ay), W = (az, -)
+#pragma unroll
+      for (int i = 0; i < UVD_PPT; ++i) {
+        const double dx = pos[i][0] - X.x, dy = pos[i][1] - X.y, dz = pos[i][2] - Y.x;
+        const double r2 = dx * dx + dy * dy + dz * dz + Y.y;
+        const double ir = rsqrt_hh(r2);
+        const double c = -ir * ir * ir;
+        v[i][0] = fma(c, dy * W.x - dz * Z.y, v[i][0]);
+        v[i][1] = fma(c, dz * Z.x - dx * W.x, v[i][1]);
+        v[i][2] = fma(c, dx * Z.y - dy * Z.x, v[i][2]);
+      }
     }
   }
-  if (!act) return;
   const double k4pi = 1.0 / (4.0 * DUST_PI);
-  for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[c] * k4pi);
+#pragma unroll
+  for (int i = 0; i < UVD_PPT; ++i) {
+    const int t = t0 + i * UV2_T;
+    if (t < npts)
+      for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[i][c] * k4pi);
+  }
 }
 
 // FP32C uvort on particles sorted along a Morton curve: a tile of 128
@@ -790,7 +909,7 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
   if (n > 0) {
     // point blocks: UV2_T points (UV2_T * UV2_PPT for the sorted FP32 kernel)
     const bool srt = prm->precision == DUST_PREC_FP32C;
-    int pb = (int)nblk(n_pts, srt ? UV2_T * UV2_PPT : UV2_T);
+    int pb = (int)nblk(n_pts, UV2_T * (srt ? UV2_PPT : UVD_PPT));
     // enough CTAs for every SM several times over; chunks of whole tiles
     int want = std::max(1, (148 * 8 + pb - 1) / pb);
     int chunk = (n + want - 1) / want;
@@ -893,7 +1012,7 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
                                                           (LineGeo *)b);
   DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
   if (n > 0) {
-    int pb = (int)nblk(n_pts, f32 ? UV2_T * UV2_PPT : UV2_T);
+    int pb = (int)nblk(n_pts, UV2_T * (f32 ? UV2_PPT : UVD_PPT));
     int want = std::max(1, (148 * 8 + pb - 1) / pb);
     int chunk = (n + want - 1) / want;
     chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);

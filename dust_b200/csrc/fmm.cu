@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dust_common.cuh"
@@ -217,7 +218,6 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
   devbuf_free(o->shift);
   devbuf_free(o->ffbuf);
   devbuf_free(o->elem_work);
-  devbuf_free(o->p2p_grp);
   DevBuf *bufs[] = {&o->idxsum, &o->keys,   &o->keys_s, &o->vals,   &o->perm,
                     &o->cnt,    &o->cstart, &o->part,   &o->flags,  &o->ind,
                     &o->cidx,   &o->lidx,   &o->act_key, &o->act_lev, &o->leaf_ci,
@@ -912,26 +912,34 @@ __global__ void k_l2l(FmmDev d, int l, uint32_t act_lo) {
   }
 }
 
-// ------------------------------------------------------- L2P + P2P (FP64)
-#define P2P_T 128
-#define P2P_TILE 128
-#define P2P_MAXR 480
-
+// ------------------------------------------------------------- L2P + P2P
 struct P2PAcc {
   double v[3], s[3], r[3], f[3];
 };
 
+// x^-1/2 for a normal FP32-range x > 0: the FP32 approximation refined by
+// one second-order Newton-Raphson (Householder) step in FP64.  With
+// y0 = x^-1/2 (1 + d) and e = 1 - x y0^2, y = y0 (1 + e/2 + 3 e^2/8) has
+// relative error O(d^3), below the FP64 rounding for |d| < 2^-21.
+__device__ __forceinline__ double p2p_rsqrt(double x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"((float)x));
+  const double y = (double)r;
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
 // One source q acting on target p: the reference's compute_vel,
 // compute_stretch, compute_rotu and compute_diffusion of source q
-// (mod_vortpart.f90:139-336), 4*pi factors applied by the caller.
+// (mod_vortpart.f90:139-336), 4*pi factors applied by the caller.  s2 and
+// is2 are the source's r_v^2 and 1 / r_v^2.
 template <bool VS, bool DF, bool VD>
 __device__ __forceinline__ void p2p_pair(const double *tp, const double *ta, double qx,
                                          double qy, double qz, double qax, double qay,
-                                         double qaz, double sq, P2PAcc &A) {
+                                         double qaz, double s2, double is2, P2PAcc &A) {
   double dx = tp[0] - qx, dy = tp[1] - qy, dz = tp[2] - qz;
   double r2 = dx * dx + dy * dy + dz * dz;
-  double s2 = sq * sq;
-  double inv = rsqrt(r2 + s2);
+  double inv = p2p_rsqrt(r2 + s2);
   double inv2 = inv * inv;
   double c = -inv2 * inv;        // -1/rho^3
   double dd = -3.0 * c * inv2;   // 3/rho^5
@@ -956,9 +964,8 @@ __device__ __forceinline__ void p2p_pair(const double *tp, const double *ta, dou
   }
   if (VD) {
     // (1/s^2) vol (aq - ap) eta, vol = 4/3 pi s^3, eta = 105/(8 pi)/s^3/(1+r^2/s^2)^4.5
-    double is2 = 1.0 / s2;
     double t = r2 * is2 + 1.0;
-    double rt = rsqrt(t);
+    double rt = p2p_rsqrt(t);
     double rt2 = rt * rt, rt4 = rt2 * rt2;
     double w = 17.5 * is2 * (rt4 * rt4 * rt);
     A.f[0] += w * (qax - ta[0]);
@@ -974,11 +981,10 @@ struct P2PAccF {
 // FP32 form of p2p_pair on coordinates relative to the leaf centre
 template <bool VS, bool DF, bool VD>
 __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, float qx, float qy,
-                                           float qz, float qax, float qay, float qaz, float sq,
-                                           P2PAccF &A) {
+                                           float qz, float qax, float qay, float qaz, float s2,
+                                           float is2, P2PAccF &A) {
   float dx = tp[0] - qx, dy = tp[1] - qy, dz = tp[2] - qz;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  float s2 = sq * sq;
   float inv = rsqrtf(r2 + s2);
   float inv2 = inv * inv;
   float c = -inv2 * inv;
@@ -1002,7 +1008,6 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
     }
   }
   if (VD) {
-    float is2 = 1.0f / s2;
     float t = fmaf(r2, is2, 1.0f);
     float rt = rsqrtf(t);
     float rt2 = rt * rt, rt4 = rt2 * rt2;
@@ -1013,279 +1018,32 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
   }
 }
 
-template <bool VS, bool DF, bool VD, bool TV, bool F32 = false>
-__global__ void __launch_bounds__(P2P_T) k_p2p(FmmDev d) {
-  __shared__ double s_src[7][P2P_TILE];
-  __shared__ uint32_t s_sid[P2P_TILE];
-  __shared__ uint32_t s_rlo[P2P_MAXR];
-  __shared__ uint32_t s_rcum[P2P_MAXR + 1];
-  __shared__ int s_nr;
-  __shared__ double s_red[P2P_T * 12];
-  __shared__ double s_ros;
-  extern __shared__ double s_loc[];  // b (3 nm) then g (3 nm1)
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t ci = d.leaf_ci[blockIdx.x];
-  const int l = d.act_lev[ci];
-  const uint32_t key = d.act_key[ci];
-  int ci_, cj, ck;
-  cart_of_key(d.G, l, key, ci_, cj, ck);
-  double cc[3];
-  cell_center(d.G, l, ci_, cj, ck, cc);
-  const uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
-  if (hi == lo) return;
-  const int nm = d.nm, nm1 = d.nm1;
-  for (int t = tid; t < 3 * nm; t += P2P_T) s_loc[t] = d.B[(size_t)ci * 3 * nm + t];
-  if (VS)
-    for (int t = tid; t < 3 * nm1; t += P2P_T) s_loc[3 * nm + t] = d.Gx[(size_t)ci * 3 * nm1 + t];
-  // monomial tables: exponents (packed) and, for the gradient, the indices
-  // of m + e_r in the degree-(p+1) ordering
-  int *s_mexp = (int *)(s_loc + 3 * (nm + nm1));
-  int *s_mgr = s_mexp + nm;
-  for (int m = tid; m < nm; m += P2P_T) {
-    int mi, mj, mk;
-    mono_exp(m, mi, mj, mk);
-    s_mexp[m] = mi | (mj << 8) | (mk << 16);
-    s_mgr[3 * m + 0] = mono_idx(mi + 1, mj, mk);
-    s_mgr[3 * m + 1] = mono_idx(mi, mj + 1, mk);
-    s_mgr[3 * m + 2] = mono_idx(mi, mj, mk + 1);
-  }
-  // near-field source ranges: 26 same-level neighbours (active), the leaf
-  // neighbours (leaves among the neighbours of every ancestor), own leaf.
-  if (warp == 0) {
-    int nr = 0;
-    for (int lev = l; lev >= 1; --lev) {
-      int sh = l - lev;
-      int ai = ci_ >> sh, aj = cj >> sh, ak = ck >> sh;
-      bool pred = false;
-      uint32_t rlo = 0, rhi = 0;
-      if (lane < 27 && lane != 13) {
-        int di = lane % 3 - 1, dj = (lane / 3) % 3 - 1, dk = lane / 9 - 1;
-        if (cart_in(d.G, lev, ai + di, aj + dj, ak + dk)) {
-          uint32_t nk = key_of(d.G, lev, ai + di, aj + dj, ak + dk);
-          uint8_t f = d.flags[d.G.lev_off[lev] + nk];
-          bool want = (lev == l) ? (f & FL_ACTIVE) != 0 : (f & FL_LEAF) != 0;
-          if (want) {
-            rlo = cell_lo(d.G, d.cstart, lev, nk);
-            rhi = cell_hi(d.G, d.cstart, lev, nk);
-            pred = rhi > rlo;
-          }
-        }
-      }
-      unsigned msk = __ballot_sync(0xffffffffu, pred);
-      if (pred) {
-        int pos = nr + __popc(msk & ((1u << lane) - 1u));
-        s_rlo[pos] = rlo;
-        s_rcum[pos] = rhi - rlo;  // length, prefix-summed below
-      }
-      nr += __popc(msk);
-    }
-    if (lane == 0) {
-      s_rlo[nr] = lo;
-      s_rcum[nr] = hi - lo;
-      ++nr;
-      uint32_t run = 0;
-      for (int r = 0; r < nr; ++r) {
-        uint32_t len = s_rcum[r];
-        s_rcum[r] = run;
-        run += len;
-      }
-      s_rcum[nr] = run;
-      s_nr = nr;
-    }
-  }
-  __syncthreads();
-  const int nr = s_nr;
-  const uint32_t S = s_rcum[nr];
-  const size_t n = d.n;
-  const int nt = (int)(hi - lo);
-  if (tid == 0 && d.counters)
-    atomicAdd((unsigned long long *)d.counters + 1, (unsigned long long)nt * (S - 1));
-  const double k4pi = 1.0 / (4.0 * DUST_PI);
-
-  double ave_ros = 0.0;
-  if (TV) {
-    // leaf average of |sym(grad)|^2 from the local expansion (:1214-1230)
-    if (tid == 0) s_ros = 0.0;
-    __syncthreads();
-    double part = 0.0;
-    for (int t = tid; t < nt; t += P2P_T) {
-      uint32_t ti = lo + t;
-      double x = d.P[ti] - cc[0], y = d.P[n + ti] - cc[1], z = d.P[2 * n + ti] - cc[2];
-      double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int m = 0; m < nm; ++m) {
-        int mi, mj, mk;
-        mono_exp(m, mi, mj, mk);
-        double pr = ipow_d(x, mi) * ipow_d(y, mj) * ipow_d(z, mk);
-        int mr[3] = {mono_idx(mi + 1, mj, mk), mono_idx(mi, mj + 1, mk), mono_idx(mi, mj, mk + 1)};
-        int fr[3] = {mi + 1, mj + 1, mk + 1};
-        for (int r = 0; r < 3; ++r)
-          for (int e = 0; e < 3; ++e) g[r + 3 * e] += fr[r] * s_loc[3 * nm + 3 * mr[r] + e] * pr;
-      }
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) {
-          double sy = 0.5 * (g[a + 3 * b] + g[b + 3 * a]);
-          part += sy * sy;
-        }
-    }
-    atomicAdd(&s_ros, part);
-    __syncthreads();
-    ave_ros = nt > 0 ? s_ros / (double)nt : 0.0;
-  }
-
-  for (int t0 = 0; t0 < nt; t0 += P2P_T) {
-    const int cnt = min(P2P_T, nt - t0);
-    const int TPR = (cnt + 31) & ~31;
-    const int G = P2P_T / TPR;
-    const int tl = tid % TPR, grp = tid / TPR;
-    const bool act = (tl < cnt) && (grp < G);
-    const uint32_t ti = lo + t0 + (act ? tl : 0);
-    double tp[3] = {d.P[ti], d.P[n + ti], d.P[2 * n + ti]};
-    double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
-    P2PAcc A;
-    for (int e = 0; e < 3; ++e) A.v[e] = A.s[e] = A.r[e] = A.f[e] = 0.0;
-    double lv[3] = {0, 0, 0}, ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
-    if (act && grp == 0) {
-      // L2P (mod_octree.f90:1171-1212): vel from b (degree p), grad(r,:)
-      // = sum_m (m_r+1) g(m+e_r) (x-c)^m
-      double x = tp[0] - cc[0], y = tp[1] - cc[1], z = tp[2] - cc[2];
-      double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
-      px[0] = py[0] = pz[0] = 1.0;
-#pragma unroll
-      for (int e = 1; e <= DUST_MAXP; ++e) {
-        px[e] = px[e - 1] * x;
-        py[e] = py[e - 1] * y;
-        pz[e] = pz[e - 1] * z;
-      }
-      double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int m = 0; m < nm; ++m) {
-        int ex = s_mexp[m];
-        int mi = ex & 255, mj = (ex >> 8) & 255, mk = ex >> 16;
-        double pr = px[mi] * py[mj] * pz[mk];
-        for (int e = 0; e < 3; ++e) lv[e] += s_loc[3 * m + e] * pr;
-        if (VS) {
-          const double *gl = s_loc + 3 * nm;
-          double f0 = (double)(mi + 1) * pr, f1 = (double)(mj + 1) * pr,
-                 f2 = (double)(mk + 1) * pr;
-          const double *g0 = gl + 3 * s_mgr[3 * m], *g1 = gl + 3 * s_mgr[3 * m + 1],
-                       *g2 = gl + 3 * s_mgr[3 * m + 2];
-          for (int e = 0; e < 3; ++e) {
-            g[0 + 3 * e] += f0 * g0[e];
-            g[1 + 3 * e] += f1 * g1[e];
-            g[2 + 3 * e] += f2 * g2[e];
-          }
-        }
-      }
-      if (VS) {
-        for (int e = 0; e < 3; ++e) ls[e] = ta[0] * g[e] + ta[1] * g[e + 3] + ta[2] * g[e + 6];
-        if (DF) {
-          lr[0] = g[1 + 6] - g[2 + 3];
-          lr[1] = g[2 + 0] - g[0 + 6];
-          lr[2] = g[0 + 3] - g[1 + 0];
-        }
-      }
-    }
-    for (uint32_t s0 = 0; s0 < S; s0 += P2P_TILE) {
-      __syncthreads();
-      uint32_t v = s0 + tid;
-      if (tid < P2P_TILE && v < S) {
-        int a = 0, b = nr - 1;
-        while (a < b) {  // last r with s_rcum[r] <= v
-          int mid = (a + b + 1) >> 1;
-          if (s_rcum[mid] <= v) a = mid; else b = mid - 1;
-        }
-        uint32_t sidx = s_rlo[a] + (v - s_rcum[a]);
-        s_sid[tid] = sidx;
-        if (F32) {
-          float *fs = (float *)&s_src[0][0];  // 7 x TILE floats in the double tile
-          for (int q = 0; q < 3; ++q) fs[q * P2P_TILE + tid] = (float)(d.P[(size_t)q * n + sidx] - cc[q]);
-          for (int q = 3; q < 7; ++q) fs[q * P2P_TILE + tid] = (float)d.P[(size_t)q * n + sidx];
-        } else {
-          for (int q = 0; q < 7; ++q) s_src[q][tid] = d.P[(size_t)q * n + sidx];
-        }
-      }
-      __syncthreads();
-      const int m = (int)min((uint32_t)P2P_TILE, S - s0);
-      if (act) {
-        if (F32) {
-          const float *fs = (const float *)&s_src[0][0];
-          float ftp[3] = {(float)(tp[0] - cc[0]), (float)(tp[1] - cc[1]), (float)(tp[2] - cc[2])};
-          float fta[3] = {(float)ta[0], (float)ta[1], (float)ta[2]};
-          P2PAccF B;
-          for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
-          for (int u = grp; u < m; u += G) {
-            if (s_sid[u] == ti) continue;
-            p2p_pair_f<VS, DF, VD>(ftp, fta, fs[u], fs[P2P_TILE + u], fs[2 * P2P_TILE + u],
-                                   fs[3 * P2P_TILE + u], fs[4 * P2P_TILE + u],
-                                   fs[5 * P2P_TILE + u], fs[6 * P2P_TILE + u], B);
-          }
-          // FP32 partial sums of one tile (at most 128/G terms) folded into FP64
-          for (int e = 0; e < 3; ++e) {
-            A.v[e] += (double)B.v[e];
-            A.s[e] += (double)B.s[e];
-            A.r[e] += (double)B.r[e];
-            A.f[e] += (double)B.f[e];
-          }
-        } else {
-          for (int u = grp; u < m; u += G) {
-            if (s_sid[u] == ti) continue;
-            p2p_pair<VS, DF, VD>(tp, ta, s_src[0][u], s_src[1][u], s_src[2][u], s_src[3][u],
-                                 s_src[4][u], s_src[5][u], s_src[6][u], A);
-          }
-        }
-      }
-    }
-    // reduce the groups
-    __syncthreads();
-    if (act && grp > 0) {
-      double *r = s_red + 12 * ((grp - 1) * TPR + tl);
-      for (int e = 0; e < 3; ++e) {
-        r[e] = A.v[e];
-        r[3 + e] = A.s[e];
-        r[6 + e] = A.r[e];
-        r[9 + e] = A.f[e];
-      }
-    }
-    __syncthreads();
-    if (act && grp == 0) {
-      for (int g2 = 1; g2 < G; ++g2) {
-        const double *r = s_red + 12 * ((g2 - 1) * TPR + tl);
-        for (int e = 0; e < 3; ++e) {
-          A.v[e] += r[e];
-          A.s[e] += r[3 + e];
-          A.r[e] += r[6 + e];
-          A.f[e] += r[9 + e];
-        }
-      }
-      double nu = d.nu_inf;
-      if (TV) {
-        double rv = d.P[6 * n + ti];
-        nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave_ros);
-      }
-      for (int e = 0; e < 3; ++e) {
-        d.out[(size_t)e * n + ti] = lv[e] + A.v[e] * k4pi;
-        d.out[(size_t)(3 + e) * n + ti] = ls[e] + A.s[e] * k4pi + (VD ? A.f[e] * nu : 0.0);
-        d.out[(size_t)(6 + e) * n + ti] = lr[e] + A.r[e] * k4pi;
-      }
-    }
-  }
-}
-
-// ------------------------------------------- L2P + P2P, FP32C (warp per leaf)
-// Leaves hold a few particles (6 on average in the full-step case), so a
-// CTA per leaf leaves most lanes idle.  Here one warp owns one leaf: lanes
-// are split into G = 32 / cnt groups of cnt lanes (cnt targets, at most 32
-// at a time), lane (tl, grp) accumulates target tl over the sources
-// u = grp mod G of each 32-source tile staged in the warp's own shared
-// memory, and group 0 adds the other groups' sums from shared memory.  Pair arithmetic is p2p_pair_f (FP32 on
-// coordinates relative to the leaf centre) with the FP32 partial sums folded
-// into FP64 after every 128 sources; L2P stays FP64.
+// L2P + P2P, one warp per leaf.  Leaves hold a few particles (6 on average
+// in the 2M-particle full step), so a CTA per leaf would leave most lanes
+// idle.  The warp lists the leaf's near field as particle ranges (the 26
+// active same-level neighbours, the coarser leaf neighbours of every level
+// above -- leaf_neigh, mod_octree.f90:964-988 -- and the leaf itself, at most
+// 26 * DUST_MAXLEV + 1 ranges), then takes its targets 32 at a time: lanes
+// are split into G = 32 / cnt groups of cnt lanes (one lane per target),
+// lane (tl, grp) accumulates target tl over the sources u = grp mod G of
+// each 32-source tile staged in the warp's own shared memory, and group 0
+// adds the other groups' sums from shared memory.  A source is found from
+// its position in the concatenated ranges by a binary search over the
+// range prefix sums.
+//   FP64: pairs by p2p_pair on absolute coordinates, summed in FP64.
+//   FP32C (F32): pairs by p2p_pair_f on coordinates relative to the leaf
+//   centre (differences formed in FP64, rounded once), FP32 partial sums of
+//   up to 128 sources folded into FP64.
+// L2P (mod_octree.f90:1171-1212) is FP64 in both.
 #define P2W_WARPS 4
 #define P2W_TILE 32
-#define P2W_MAXR 320
+#define P2W_MAXR (26 * DUST_MAXLEV + 4)
+#define P2W_NV 8  // staged per source: x y z, alpha x y z, r_v^2, 1 / r_v^2
 
-template <bool VS, bool DF, bool VD, bool TV>
-__global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
-  __shared__ float s_src[P2W_WARPS][7][P2W_TILE];
+template <bool VS, bool DF, bool VD, bool TV, bool F32>
+__global__ void __launch_bounds__(P2W_WARPS * 32, F32 ? 6 : 5) k_p2p_w(FmmDev d) {
+  using R = typename std::conditional<F32, float, double>::type;
+  __shared__ R s_src[P2W_WARPS][P2W_NV][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
   __shared__ uint32_t s_rlo[P2W_WARPS][P2W_MAXR];
   __shared__ uint32_t s_rcum[P2W_WARPS][P2W_MAXR + 1];
@@ -1303,7 +1061,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
   const uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
   if (hi == lo) return;
   uint32_t *rlo = s_rlo[w], *rcum = s_rcum[w];
-  // near-field source ranges, in the order of k_p2p
+  // near-field source ranges: same level first, then coarser levels
   int nr = 0;
   for (int lev = l; lev >= 1; --lev) {
     const int sh = l - lev;
@@ -1324,6 +1082,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
       }
     }
     const unsigned msk = __ballot_sync(0xffffffffu, pred);
+    // 26 per level and l <= DUST_MAXLEV levels: the list cannot overflow
     if (pred && nr + __popc(msk) < P2W_MAXR) {
       const int pos = nr + __popc(msk & ((1u << lane) - 1u));
       rlo[pos] = a0;
@@ -1399,7 +1158,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
     ave_ros = part / (double)nt;
   }
-  float *fs = &s_src[w][0][0];
+  R *fs = &s_src[w][0][0];
   double *acc = &s_acc[w][0][lane];  // this lane's 12 FP64 sums, stride 32
   for (int t0 = 0; t0 < nt; t0 += 32) {
     // G groups of cnt lanes (one lane per target) split the sources; lanes
@@ -1408,12 +1167,21 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
     const int TPR = cnt, G = 32 / TPR, tl = lane % TPR, grp = lane / TPR;
     const bool act = grp < G;
     const uint32_t ti = lo + t0 + (act ? tl : 0);
-    const float ftp[3] = {(float)(d.P[ti] - cc[0]), (float)(d.P[n + ti] - cc[1]),
-                          (float)(d.P[2 * n + ti] - cc[2])};
-    const float fta[3] = {(float)d.P[3 * n + ti], (float)d.P[4 * n + ti], (float)d.P[5 * n + ti]};
-    for (int e = 0; e < 12; ++e) acc[32 * e] = 0.0;
+    R tp[3], ta[3];
+    for (int q = 0; q < 3; ++q) {
+      tp[q] = F32 ? (R)(d.P[(size_t)q * n + ti] - cc[q]) : (R)d.P[(size_t)q * n + ti];
+      ta[q] = (R)d.P[(size_t)(3 + q) * n + ti];
+    }
+    // FP64 sums: in registers (FP64 pairs) or in shared memory (FP32C,
+    // which keeps its registers for the FP32 partial sums)
+    P2PAcc A;
     P2PAccF B;
-    for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+    for (int e = 0; e < 3; ++e) {
+      A.v[e] = A.s[e] = A.r[e] = A.f[e] = 0.0;
+      B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
+    }
+    if (F32)
+      for (int e = 0; e < 12; ++e) acc[32 * e] = 0.0;
     int since = 0;
     for (uint32_t s0 = 0; s0 < S; s0 += P2W_TILE) {
       __syncwarp();
@@ -1426,19 +1194,38 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
         }
         const uint32_t sidx = rlo[a] + (v - rcum[a]);
         s_sid[w][lane] = sidx;
-        for (int q = 0; q < 3; ++q) fs[q * P2W_TILE + lane] = (float)(d.P[(size_t)q * n + sidx] - cc[q]);
-        for (int q = 3; q < 7; ++q) fs[q * P2W_TILE + lane] = (float)d.P[(size_t)q * n + sidx];
+        for (int q = 0; q < 3; ++q)
+          fs[q * P2W_TILE + lane] =
+              F32 ? (R)(d.P[(size_t)q * n + sidx] - cc[q]) : (R)d.P[(size_t)q * n + sidx];
+        for (int q = 3; q < 6; ++q) fs[q * P2W_TILE + lane] = (R)d.P[(size_t)q * n + sidx];
+        const double rv = d.P[(size_t)6 * n + sidx];
+        if constexpr (F32) {
+          const float s2 = (float)rv * (float)rv;
+          fs[6 * P2W_TILE + lane] = s2;
+          fs[7 * P2W_TILE + lane] = VD ? __frcp_rn(s2) : 0.f;
+        } else {
+          const double s2 = rv * rv;
+          fs[6 * P2W_TILE + lane] = s2;
+          fs[7 * P2W_TILE + lane] = VD ? __drcp_rn(s2) : 0.0;
+        }
       }
       __syncwarp();
       const int m = (int)min((uint32_t)P2W_TILE, S - s0);
       if (act)
         for (int u = grp; u < m; u += G) {
           if (s_sid[w][u] == ti) continue;
-          p2p_pair_f<VS, DF, VD>(ftp, fta, fs[u], fs[P2W_TILE + u], fs[2 * P2W_TILE + u],
-                                 fs[3 * P2W_TILE + u], fs[4 * P2W_TILE + u], fs[5 * P2W_TILE + u],
-                                 fs[6 * P2W_TILE + u], B);
+          if constexpr (F32)
+            p2p_pair_f<VS, DF, VD>(tp, ta, fs[u], fs[P2W_TILE + u], fs[2 * P2W_TILE + u],
+                                   fs[3 * P2W_TILE + u], fs[4 * P2W_TILE + u],
+                                   fs[5 * P2W_TILE + u], fs[6 * P2W_TILE + u],
+                                   fs[7 * P2W_TILE + u], B);
+          else
+            p2p_pair<VS, DF, VD>(tp, ta, fs[u], fs[P2W_TILE + u], fs[2 * P2W_TILE + u],
+                                 fs[3 * P2W_TILE + u], fs[4 * P2W_TILE + u],
+                                 fs[5 * P2W_TILE + u], fs[6 * P2W_TILE + u],
+                                 fs[7 * P2W_TILE + u], A);
         }
-      if (++since == 4 || s0 + P2W_TILE >= S) {
+      if (F32 && (++since == 4 || s0 + P2W_TILE >= S)) {
         // FP32 partial sums of up to 128 sources folded into FP64
         since = 0;
         for (int e = 0; e < 3; ++e) {
@@ -1452,20 +1239,27 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
     }
     // combine the groups of each target (group 0's lane sums the others'
     // shared-memory sums)
+    if (!F32)
+      for (int e = 0; e < 3; ++e) {
+        acc[32 * e] = A.v[e];
+        acc[32 * (3 + e)] = A.s[e];
+        acc[32 * (6 + e)] = A.r[e];
+        acc[32 * (9 + e)] = A.f[e];
+      }
     __syncwarp();
-    double A[12];
+    double Q[12];
     for (int e = 0; e < 12; ++e) {
-      A[e] = acc[32 * e];
+      Q[e] = acc[32 * e];
       if (grp == 0)
-        for (int g = 1; g < G; ++g) A[e] += acc[32 * e + g * TPR];
+        for (int g = 1; g < G; ++g) Q[e] += acc[32 * e + g * TPR];
     }
     __syncwarp();
     if (act && grp == 0) {
-      const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
+      const double tad[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
       double lv[3], g[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
       l2p(ti, lv, g);
       if (VS) {
-        for (int e = 0; e < 3; ++e) ls[e] = ta[0] * g[e] + ta[1] * g[e + 3] + ta[2] * g[e + 6];
+        for (int e = 0; e < 3; ++e) ls[e] = tad[0] * g[e] + tad[1] * g[e + 3] + tad[2] * g[e + 6];
         if (DF) {
           lr[0] = g[1 + 6] - g[2 + 3];
           lr[1] = g[2 + 0] - g[0 + 6];
@@ -1478,352 +1272,9 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 6) k_p2p_w(FmmDev d) {
         nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave_ros);
       }
       for (int e = 0; e < 3; ++e) {
-        d.out[(size_t)e * n + ti] = lv[e] + A[e] * k4pi;
-        d.out[(size_t)(3 + e) * n + ti] = ls[e] + A[3 + e] * k4pi + (VD ? A[9 + e] * nu : 0.0);
-        d.out[(size_t)(6 + e) * n + ti] = lr[e] + A[6 + e] * k4pi;
-      }
-    }
-  }
-}
-
-// --------------------------------- L2P + P2P, FP32C (CTA per sibling group)
-// The leaves of one parent share their near field: the 26 same-level
-// neighbours of any child lie in the 4 x 4 x 4 block of level-l cells around
-// the parent, and the coarser leaf neighbours (leaf_neigh, which the
-// reference derives from the parent, mod_octree.f90:964-988) are the same
-// for every child.  One CTA takes such a group (the consecutive leaves of
-// one level with one parent key; a level-1 leaf is a group of its own),
-// lists the block's active cells and the coarse leaves as particle ranges
-// once, stages the sources in tiles of PG_TILE (FP32, relative to the
-// parent's centre, tagged with their block cell or 255 for coarse ones) and
-// lets every target take the sources of its own 27 cells and all coarse
-// ones, skipping itself -- the reference's pair set exactly.  Threads per
-// target: G = 128 / (targets of the chunk) groups split the sources; FP32
-// partial sums of one tile (<= 128 terms) are folded into FP64; L2P stays
-// FP64.  Groups are taken from an atomic work counter (they differ in
-// size).
-#define PG_T 128
-#define PG_TILE 128
-#define PG_MAXR 480  // 64 block cells + 26 coarse leaves per coarser level (<= 15)
-#define PG_MAXL 8
-
-__global__ void k_p2p_groups_flag(FmmDev d, uint32_t *flag) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > d.n_leaves) return;
-  if (i == d.n_leaves) {
-    flag[i] = 0;
-    return;
-  }
-  bool start = i == 0;
-  if (!start) {
-    const uint32_t a = d.leaf_ci[i], b = d.leaf_ci[i - 1];
-    const int la = d.act_lev[a], lb = d.act_lev[b];
-    start = la != lb || la == 1 || (d.act_key[a] >> 3) != (d.act_key[b] >> 3);
-  }
-  flag[i] = start ? 1u : 0u;
-}
-
-__global__ void k_p2p_groups_scatter(uint32_t nleaves, const uint32_t *flag, const uint32_t *gid,
-                                     uint32_t *gstart, uint32_t *ngroups) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > nleaves) return;
-  if (i == nleaves) {
-    gstart[gid[i]] = nleaves;
-    *ngroups = gid[i];
-  } else if (flag[i]) {
-    gstart[gid[i]] = i;
-  }
-}
-
-template <bool VS, bool DF, bool VD, bool TV>
-__global__ void __launch_bounds__(PG_T) k_p2p_g(FmmDev d, const uint32_t *gstart,
-                                                const uint32_t *ngroups_p, uint32_t *work) {
-  __shared__ float s_src[7][PG_TILE];
-  __shared__ uint32_t s_sid[PG_TILE];
-  __shared__ uint8_t s_tag[PG_TILE];
-  __shared__ uint32_t s_rlo[PG_MAXR], s_rcum[PG_MAXR + 1];
-  __shared__ uint8_t s_rtag[PG_MAXR];
-  __shared__ double s_red[12][PG_T];
-  __shared__ uint32_t s_lci[PG_MAXL], s_llo[PG_MAXL], s_tcum[PG_MAXL + 1];
-  __shared__ uint8_t s_ltag[PG_MAXL];
-  __shared__ double s_lcc[PG_MAXL][3], s_ros[PG_MAXL];
-  __shared__ int s_nr, s_wcnt[2];
-  __shared__ uint32_t s_g;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const size_t n = d.n;
-  const uint32_t ngroups = *ngroups_p;
-  const int nm = d.nm, nm1 = d.nm1;
-  const double k4pi = 1.0 / (4.0 * DUST_PI);
-  while (true) {
-    __syncthreads();
-    if (tid == 0) s_g = atomicAdd(work, 1u);
-    __syncthreads();
-    const uint32_t g = s_g;
-    if (g >= ngroups) break;
-    const uint32_t L0 = gstart[g], L1 = gstart[g + 1];
-    const int nleaf = (int)min(L1 - L0, (uint32_t)PG_MAXL);
-    const uint32_t ci0 = d.leaf_ci[L0];
-    const int l = d.act_lev[ci0];
-    int c0i, c0j, c0k;
-    cart_of_key(d.G, l, d.act_key[ci0], c0i, c0j, c0k);
-    // block origin and centre: the parent's 4^3 block (level >= 2), the
-    // leaf's own 3^3 neighbourhood at level 1
-    int bo[3], pc[3] = {c0i >> 1, c0j >> 1, c0k >> 1};
-    double bc[3];
-    const int ext = l >= 2 ? 4 : 3;
-    if (l >= 2) {
-      for (int q = 0; q < 3; ++q) bo[q] = 2 * pc[q] - 1;
-      cell_center(d.G, l - 1, pc[0], pc[1], pc[2], bc);
-    } else {
-      bo[0] = c0i - 1, bo[1] = c0j - 1, bo[2] = c0k - 1;
-      cell_center(d.G, 1, c0i, c0j, c0k, bc);
-    }
-    if (tid < nleaf) {
-      const uint32_t ci = d.leaf_ci[L0 + tid];
-      const uint32_t key = d.act_key[ci];
-      int a, b, c;
-      cart_of_key(d.G, l, key, a, b, c);
-      s_lci[tid] = ci;
-      s_llo[tid] = cell_lo(d.G, d.cstart, l, key);
-      s_ltag[tid] = (uint8_t)((a - bo[0]) + 4 * (b - bo[1]) + 16 * (c - bo[2]));
-      cell_center(d.G, l, a, b, c, s_lcc[tid]);
-      s_ros[tid] = 0.0;
-      s_tcum[tid + 1] = cell_hi(d.G, d.cstart, l, key) - s_llo[tid];
-    }
-    // the group's source ranges: block cells (warps 0-1), then the coarse
-    // leaves level by level (warp 0), in a fixed order
-    uint32_t a0 = 0, a1 = 0;
-    bool pred = false;
-    if (tid < 64) {
-      const int i = tid & 3, j = (tid >> 2) & 3, k = tid >> 4;
-      if (i < ext && j < ext && k < ext) {
-        const int ci_ = bo[0] + i, cj = bo[1] + j, ck = bo[2] + k;
-        if (cart_in(d.G, l, ci_, cj, ck)) {
-          const uint32_t nk = key_of(d.G, l, ci_, cj, ck);
-          if (d.flags[d.G.lev_off[l] + nk] & FL_ACTIVE) {
-            a0 = cell_lo(d.G, d.cstart, l, nk);
-            a1 = cell_hi(d.G, d.cstart, l, nk);
-            pred = a1 > a0;
-          }
-        }
-      }
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, pred);
-    if (lane == 0 && warp < 2) s_wcnt[warp] = __popc(bal);
-    __syncthreads();
-    if (tid == 0) {
-      s_tcum[0] = 0;
-      for (int q = 0; q < nleaf; ++q) s_tcum[q + 1] += s_tcum[q];
-    }
-    if (tid < 64 && pred) {
-      const int pos = (warp == 1 ? s_wcnt[0] : 0) + __popc(bal & ((1u << lane) - 1u));
-      s_rlo[pos] = a0;
-      s_rcum[pos] = a1 - a0;
-      s_rtag[pos] = (uint8_t)tid;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      int nr = s_wcnt[0] + s_wcnt[1];
-      for (int lev = l - 1; lev >= 1; --lev) {
-        const int sh = l - lev;
-        const int ai = c0i >> sh, aj = c0j >> sh, ak = c0k >> sh;
-        bool pr = false;
-        uint32_t b0 = 0, b1 = 0;
-        if (lane < 27 && lane != 13) {
-          const int di = lane % 3 - 1, dj = (lane / 3) % 3 - 1, dk = lane / 9 - 1;
-          if (cart_in(d.G, lev, ai + di, aj + dj, ak + dk)) {
-            const uint32_t nk = key_of(d.G, lev, ai + di, aj + dj, ak + dk);
-            if (d.flags[d.G.lev_off[lev] + nk] & FL_LEAF) {
-              b0 = cell_lo(d.G, d.cstart, lev, nk);
-              b1 = cell_hi(d.G, d.cstart, lev, nk);
-              pr = b1 > b0;
-            }
-          }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, pr);
-        if (pr && nr + __popc(m) <= PG_MAXR) {
-          const int pos = nr + __popc(m & ((1u << lane) - 1u));
-          s_rlo[pos] = b0;
-          s_rcum[pos] = b1 - b0;
-          s_rtag[pos] = 255;
-        }
-        nr = min(nr + __popc(m), PG_MAXR);
-      }
-      // exclusive prefix of the range lengths (32 at a time)
-      uint32_t run = 0;
-      for (int r0 = 0; r0 < nr; r0 += 32) {
-        const int r = r0 + lane;
-        const uint32_t len = r < nr ? s_rcum[r] : 0u;
-        uint32_t x = len;
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-          if (lane >= o) x += y;
-        }
-        if (r < nr) s_rcum[r] = run + x - len;
-        run += __shfl_sync(0xffffffffu, x, 31);
-      }
-      if (lane == 0) {
-        s_rcum[nr] = run;
-        s_nr = nr;
-      }
-    }
-    __syncthreads();
-    const int nr = s_nr;
-    const uint32_t S = s_rcum[nr];
-    const int NT = (int)s_tcum[nleaf];
-    // pair counts of the reference's near field (per leaf: its targets x the
-    // sources of its 27 cells and the coarse leaves, minus itself)
-    if (tid < nleaf && d.counters) {
-      const int lt = s_ltag[tid], lx = lt & 3, ly = (lt >> 2) & 3, lz = lt >> 4;
-      uint64_t ns = 0;
-      for (int r = 0; r < nr; ++r) {
-        const int tg = s_rtag[r];
-        if (tg != 255) {
-          const int dx = (tg & 3) - lx, dy = ((tg >> 2) & 3) - ly, dz = (tg >> 4) - lz;
-          if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
-        }
-        ns += s_rcum[r + 1] - s_rcum[r];
-      }
-      const uint64_t nt = s_tcum[tid + 1] - s_tcum[tid];
-      atomicAdd((unsigned long long *)d.counters + 1, (unsigned long long)(nt * (ns - 1)));
-    }
-    // L2P of one target (FP64) with its leaf's local expansion
-    auto l2p = [&](int lf, uint32_t ti, double *lv, double *gg) {
-      const uint32_t ci = s_lci[lf];
-      const double *bl = d.B + (size_t)ci * 3 * nm, *gl = d.Gx + (size_t)ci * 3 * nm1;
-      const double x = d.P[ti] - s_lcc[lf][0], y = d.P[n + ti] - s_lcc[lf][1],
-                   z = d.P[2 * n + ti] - s_lcc[lf][2];
-      double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
-      px[0] = py[0] = pz[0] = 1.0;
-#pragma unroll
-      for (int e = 1; e <= DUST_MAXP; ++e) {
-        px[e] = px[e - 1] * x;
-        py[e] = py[e - 1] * y;
-        pz[e] = pz[e - 1] * z;
-      }
-      for (int e = 0; e < 3; ++e) lv[e] = 0.0;
-      for (int e = 0; e < 9; ++e) gg[e] = 0.0;
-      for (int m = 0; m < nm; ++m) {
-        int mi, mj, mk;
-        mono_exp(m, mi, mj, mk);
-        const double pr = px[mi] * py[mj] * pz[mk];
-        for (int e = 0; e < 3; ++e) lv[e] += __ldg(bl + 3 * m + e) * pr;
-        if (VS) {
-          const double *g0 = gl + 3 * mono_idx(mi + 1, mj, mk),
-                       *g1 = gl + 3 * mono_idx(mi, mj + 1, mk),
-                       *g2 = gl + 3 * mono_idx(mi, mj, mk + 1);
-          const double f0 = (mi + 1) * pr, f1 = (mj + 1) * pr, f2 = (mk + 1) * pr;
-          for (int e = 0; e < 3; ++e) {
-            gg[0 + 3 * e] += f0 * __ldg(g0 + e);
-            gg[1 + 3 * e] += f1 * __ldg(g1 + e);
-            gg[2 + 3 * e] += f2 * __ldg(g2 + e);
-          }
-        }
-      }
-    };
-    auto leaf_of = [&](int t) {
-      int lf = 0;
-      while (lf + 1 < nleaf && (int)s_tcum[lf + 1] <= t) ++lf;
-      return lf;
-    };
-    if (TV) {
-      // leaf average of |sym(grad)|^2 from the local expansion (:1214-1230)
-      for (int t = tid; t < NT; t += PG_T) {
-        const int lf = leaf_of(t);
-        double lv[3], gg[9];
-        l2p(lf, s_llo[lf] + (t - s_tcum[lf]), lv, gg);
-        double part = 0.0;
-        for (int a = 0; a < 3; ++a)
-          for (int b = 0; b < 3; ++b) {
-            const double sy = 0.5 * (gg[a + 3 * b] + gg[b + 3 * a]);
-            part += sy * sy;
-          }
-        atomicAdd(&s_ros[lf], part);
-      }
-      __syncthreads();
-    }
-    for (int tc0 = 0; tc0 < NT; tc0 += PG_T) {
-      const int cnt = min(PG_T, NT - tc0);
-      const int G = PG_T / cnt, tl = tid % cnt, grp = tid / cnt;
-      const bool act = grp < G;
-      const int t = tc0 + tl;
-      const int lf = leaf_of(t);
-      const uint32_t ti = s_llo[lf] + (uint32_t)(t - (int)s_tcum[lf]);
-      const int lt = s_ltag[lf], tx = lt & 3, ty = (lt >> 2) & 3, tz = lt >> 4;
-      const float ftp[3] = {(float)(d.P[ti] - bc[0]), (float)(d.P[n + ti] - bc[1]),
-                            (float)(d.P[2 * n + ti] - bc[2])};
-      const float fta[3] = {(float)d.P[3 * n + ti], (float)d.P[4 * n + ti],
-                            (float)d.P[5 * n + ti]};
-      double A[12];
-      for (int e = 0; e < 12; ++e) A[e] = 0.0;
-      for (uint32_t s0 = 0; s0 < S; s0 += PG_TILE) {
-        __syncthreads();
-        const uint32_t v = s0 + tid;
-        if (v < S) {
-          int a = 0, b = nr - 1;
-          while (a < b) {  // last r with s_rcum[r] <= v
-            const int mid = (a + b + 1) >> 1;
-            if (s_rcum[mid] <= v) a = mid; else b = mid - 1;
-          }
-          const uint32_t sidx = s_rlo[a] + (v - s_rcum[a]);
-          s_sid[tid] = sidx;
-          s_tag[tid] = s_rtag[a];
-          for (int q = 0; q < 3; ++q) s_src[q][tid] = (float)(d.P[(size_t)q * n + sidx] - bc[q]);
-          for (int q = 3; q < 7; ++q) s_src[q][tid] = (float)d.P[(size_t)q * n + sidx];
-        }
-        __syncthreads();
-        const int m = (int)min((uint32_t)PG_TILE, S - s0);
-        if (act) {
-          P2PAccF B;
-          for (int e = 0; e < 3; ++e) B.v[e] = B.s[e] = B.r[e] = B.f[e] = 0.0f;
-          for (int u = grp; u < m; u += G) {
-            const int tg = s_tag[u];
-            if (tg != 255) {
-              const int dx = (tg & 3) - tx, dy = ((tg >> 2) & 3) - ty, dz = (tg >> 4) - tz;
-              if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
-            }
-            if (s_sid[u] == ti) continue;
-            p2p_pair_f<VS, DF, VD>(ftp, fta, s_src[0][u], s_src[1][u], s_src[2][u], s_src[3][u],
-                                   s_src[4][u], s_src[5][u], s_src[6][u], B);
-          }
-          for (int e = 0; e < 3; ++e) {
-            A[e] += (double)B.v[e];
-            A[3 + e] += (double)B.s[e];
-            A[6 + e] += (double)B.r[e];
-            A[9 + e] += (double)B.f[e];
-          }
-        }
-      }
-      // combine the groups of each target: group 0 adds the others' sums
-      __syncthreads();
-      if (act && grp > 0)
-        for (int e = 0; e < 12; ++e) s_red[e][tid] = A[e];
-      __syncthreads();
-      if (act && grp == 0) {
-        for (int g2 = 1; g2 < G; ++g2)
-          for (int e = 0; e < 12; ++e) A[e] += s_red[e][g2 * cnt + tl];
-        const double ta[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
-        double lv[3], gg[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
-        l2p(lf, ti, lv, gg);
-        if (VS) {
-          for (int e = 0; e < 3; ++e) ls[e] = ta[0] * gg[e] + ta[1] * gg[e + 3] + ta[2] * gg[e + 6];
-          if (DF) {
-            lr[0] = gg[1 + 6] - gg[2 + 3];
-            lr[1] = gg[2 + 0] - gg[0 + 6];
-            lr[2] = gg[0 + 3] - gg[1 + 0];
-          }
-        }
-        double nu = d.nu_inf;
-        if (TV) {
-          const double rv = d.P[6 * n + ti];
-          const double ave = s_ros[lf] / (double)(s_tcum[lf + 1] - s_tcum[lf]);
-          nu += (0.11 * rv) * (0.11 * rv) * sqrt(2.0 * ave);
-        }
-        for (int e = 0; e < 3; ++e) {
-          d.out[(size_t)e * n + ti] = lv[e] + A[e] * k4pi;
-          d.out[(size_t)(3 + e) * n + ti] = ls[e] + A[3 + e] * k4pi + (VD ? A[9 + e] * nu : 0.0);
-          d.out[(size_t)(6 + e) * n + ti] = lr[e] + A[6 + e] * k4pi;
-        }
+        d.out[(size_t)e * n + ti] = lv[e] + Q[e] * k4pi;
+        d.out[(size_t)(3 + e) * n + ti] = ls[e] + Q[3 + e] * k4pi + (VD ? Q[9 + e] * nu : 0.0);
+        d.out[(size_t)(6 + e) * n + ti] = lr[e] + Q[6 + e] * k4pi;
       }
     }
   }
@@ -2039,52 +1490,15 @@ int fmm_near_device(dust_octree *o, cudaStream_t st) {
   o->last_stream = st;
   if (o->timing) cudaEventRecord(o->ev[10], st);
   if (o->n_leaves > 0) {
-    size_t shl = (size_t)3 * (o->nm + o->nm1) * 8 + (size_t)4 * o->nm * 4;
     bool vs = d.use_vs, df = d.use_df, vd = d.use_vd, tv = o->prm.turbulent_viscosity != 0;
     const bool f32 = o->prm.precision == DUST_PREC_FP32C;
-    uint32_t *gstart = nullptr, *ngroups = nullptr, *work = nullptr;
-    unsigned pg_grid = 0;
-    // FP32C near-field kernel: 0 = warp per leaf, 1 = CTA per leaf (FP32
-    // pairs), 2 = CTA per sibling group
-#ifndef DUST_P2P32
-#define DUST_P2P32 0
-#endif
-    const int p32 = DUST_P2P32;
-    if (f32 && p32 == 2) {
-      // sibling groups of the leaf list (consecutive leaves of one level
-      // and one parent): flags, exclusive scan, starts
-      const size_t nl1 = (size_t)o->n_leaves + 1;
-      DUST_TRY(grow(o->p2p_grp, 3 * nl1 * 4 + 256));
-      uint32_t *flag = (uint32_t *)o->p2p_grp.p, *gid = flag + nl1;
-      gstart = gid + nl1;
-      ngroups = gstart + nl1;
-      work = ngroups + 1;
-      k_p2p_groups_flag<<<nblk(nl1, 256), 256, 0, st>>>(d, flag);
-      size_t tbg = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, tbg, flag, gid, (int)nl1, st);
-      DUST_TRY(grow(o->cub_tmp, tbg));
-      DUST_CUDA(cub::DeviceScan::ExclusiveSum(o->cub_tmp.p, tbg, flag, gid, (int)nl1, st));
-      k_p2p_groups_scatter<<<nblk(nl1, 256), 256, 0, st>>>((uint32_t)o->n_leaves, flag, gid,
-                                                           gstart, ngroups);
-      DUST_CUDA(cudaMemsetAsync(work, 0, 4, st));
-      int dev = 0, nsm = 148, per = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2p_g<true, true, true, false>,
-                                                    PG_T, 0);
-      pg_grid = (unsigned)std::min<int64_t>((int64_t)nsm * std::max(per, 1), o->n_leaves);
-    }
+    const unsigned grid = (unsigned)((o->n_leaves + P2W_WARPS - 1) / P2W_WARPS);
 #define LAUNCH_P2P(A, B, C, D)                                                   \
   do {                                                                         \
-    if (f32 && p32 == 2)                                                       \
-      k_p2p_g<A, B, C, D><<<pg_grid, PG_T, 0, st>>>(d, gstart, ngroups, work);  \
-    else if (f32 && p32 == 0)                                                  \
-      k_p2p_w<A, B, C, D><<<(unsigned)((o->n_leaves + P2W_WARPS - 1) / P2W_WARPS), \
-                            P2W_WARPS * 32, 0, st>>>(d);                        \
-    else if (f32)                                                              \
-      k_p2p<A, B, C, D, true><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);    \
+    if (f32)                                                                   \
+      k_p2p_w<A, B, C, D, true><<<grid, P2W_WARPS * 32, 0, st>>>(d);           \
     else                                                                       \
-      k_p2p<A, B, C, D, false><<<(unsigned)o->n_leaves, P2P_T, shl, st>>>(d);   \
+      k_p2p_w<A, B, C, D, false><<<grid, P2W_WARPS * 32, 0, st>>>(d);          \
   } while (0)
     if (vs && df && vd && !tv) LAUNCH_P2P(true, true, true, false);
     else if (vs && df && vd && tv) LAUNCH_P2P(true, true, true, true);

@@ -67,7 +67,6 @@ struct dust_octree {
   DevBuf h_in, h_out, h_pts, el_geo, el_raw;  // staging of host-API calls
   DevBuf ffbuf;                        // far-field panel records
   DevBuf elem_work;                    // FP32C element sums: far sums, near-pair list
-  DevBuf p2p_grp;                      // FP32C P2P sibling groups: flags, ids, starts, counters
   size_t near_cap = 0;                 // capacity of the near-pair list
   DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless M2L tables (FP64)
   DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless M2L tables (FP32)
@@ -124,12 +123,6 @@ int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st);
 int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st);
 int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
 
-// m2l_tc.cu: tensor-core M2L of levels >= 2 (FP32C mode, degree <= 4)
-bool m2l_tc_usable(const dust_octree *o);
-int m2l_tc_tables(dust_octree *o);
-size_t m2l_tc_ahat_bytes(size_t ncells);
-int m2l_tc_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
-int m2l_tc_run(dust_octree *o, FmmDev &d, cudaStream_t st);
 
 // direct.cu
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,

@@ -236,8 +236,16 @@ extern "C" int dust_linsys_create(int rank, int nstatic, const dust_fmm_params *
       if ((st = devbuf_grow(As, (size_t)nstatic * nstatic * 8)) == DUST_OK) {
         cudaMemcpy2DAsync(As.p, (size_t)nstatic * 8, L->A.p, n * 8, (size_t)nstatic * 8, nstatic,
                           cudaMemcpyDeviceToDevice, L->st);
-        st = lu_getrf<double>(L->cb, L->st, L->lu, nstatic, (double *)L->A.p, rank,
-                              (int *)L->piv.p, (int *)L->info.p, 0);
+        st = lu_getrf_auto<double>(
+            L->cb, L->st, L->lu, nstatic, (double *)L->A.p, rank, (int *)L->piv.p,
+            (int *)L->info.p, 0, nullptr, 1e-8,
+            [&]() -> int {
+              DUST_CUDA(cudaMemcpy2DAsync(L->A.p, n * 8, As.p, (size_t)nstatic * 8,
+                                          (size_t)nstatic * 8, nstatic, cudaMemcpyDeviceToDevice,
+                                          L->st));
+              return DUST_OK;
+            },
+            &L->static_pivoted);
         if (st == DUST_OK) {
           int info = 0;
           cudaMemcpy(&info, L->info.p, sizeof(int), cudaMemcpyDeviceToHost);
@@ -259,7 +267,8 @@ extern "C" int dust_linsys_destroy(dust_linsys *L) {
   if (!L) return DUST_OK;
   if (L->st) cudaStreamSynchronize(L->st);
   DevBuf *bufs[] = {&L->A,  &L->As, &L->b,    &L->bst,  &L->piv, &L->info, &L->geo,
-                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->A32, &L->gm, &L->ainv32, &L->mx, &L->kr};
+                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->lu.np, &L->A32, &L->gm, &L->ainv32, &L->mx, &L->kr,
+                    &L->mvb};
   for (DevBuf *b : bufs) devbuf_free(*b);
   if (L->cb) cublasDestroy(L->cb);
   if (L->st) cudaStreamDestroy(L->st);
@@ -331,8 +340,20 @@ int linsys_solve_lu64(dust_linsys *L, double *res_dev) {
       return DUST_ERR_CUDA;
   }
   if (nmv > 0) {
-    DUST_TRY(lu_getrf<double>(L->cb, L->st, L->lu, nmv, A + nst + (size_t)nst * n, n, P + nst,
-                              (int *)L->info.p, 0));
+    // the moving block (Schur complement) is kept unfactored in mvb until the
+    // certified unpivoted LU has been accepted
+    double *Amm = A + nst + (size_t)nst * n;
+    DUST_TRY(devbuf_grow(L->mvb, (size_t)nmv * nmv * 8));
+    DUST_CUDA(cudaMemcpy2DAsync(L->mvb.p, (size_t)nmv * 8, Amm, n * 8, (size_t)nmv * 8, nmv,
+                                cudaMemcpyDeviceToDevice, L->st));
+    DUST_TRY(lu_getrf_auto<double>(
+        L->cb, L->st, L->lu, nmv, Amm, n, P + nst, (int *)L->info.p, 0, nullptr, 1e-8,
+        [&]() -> int {
+          DUST_CUDA(cudaMemcpy2DAsync(Amm, n * 8, L->mvb.p, (size_t)nmv * 8, (size_t)nmv * 8,
+                                      nmv, cudaMemcpyDeviceToDevice, L->st));
+          return DUST_OK;
+        },
+        &L->last_pivoted));
     int info = 0;
     DUST_CUDA(cudaMemcpy(&info, L->info.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (info) return DUST_ERR_SINGULAR;
@@ -369,11 +390,14 @@ static int solve(dust_linsys *L, int mode, double *res, dust_solve_report *rep, 
   int st = DUST_OK;
   dust_solve_report r;
   memset(&r, 0, sizeof(r));
+  L->last_pivoted = 0;
   if (mode == DUST_SOLVE_LU64) {
     st = linsys_solve_lu64(L, x);
     r.mode_used = DUST_SOLVE_LU64;
+    r.pivoted = L->static_pivoted | L->last_pivoted;
   } else if (mode == DUST_SOLVE_MIXED || mode == DUST_SOLVE_GMRES_NN) {
     st = linsys_solve_iterative(L, mode, x, &r);
+    r.pivoted = L->static_pivoted | L->last_pivoted;
   } else {
     st = DUST_ERR_BAD_ARG;
   }

@@ -20,6 +20,9 @@ struct dust_linsys {
   DevBuf b, bst, piv, info, geo, raw, impl, work, A32, gm;
   DevBuf ainv32;  // FP32 inverse of the static block (mixed solve)
   DevBuf mx;      // mixed-solve work: Schur complement, coupling blocks, vectors
+  DevBuf mvb;     // unfactored moving block (LU64 step), restored if the
+                  // unpivoted LU is not certified
+  int static_pivoted = 0, last_pivoted = 0;  // which LU ran (lu_getrf_auto)
   bool ainv_ready = false;
   struct dust_precond *pc = nullptr;  // learned preconditioner (GMRES_NN)
   DevBuf kr;                          // GMRES Krylov basis and vectors

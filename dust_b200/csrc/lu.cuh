@@ -14,6 +14,7 @@
 
 struct LuWork {
   DevBuf sync;   // barrier counters, error flag, partials, candidate rows
+  DevBuf np;     // unpivoted LU: max |l| word, inverse diagonal triangles
   int nsm = 0;
 };
 
@@ -39,3 +40,33 @@ void lu_laswp(cudaStream_t st, T *A, int lda, int c0, int c1, int k1, int k2,
 template <typename T>
 int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, int lda,
              const int *ipiv, T *B, int ldb, const int *perm = nullptr);
+
+// Unpivoted blocked LU of the n x n column-major A (lu_np.cu): L unit lower
+// and U upper in place, ipiv (when given) the identity, perm (when given)
+// the identity permutation, *lmax the largest |l(i,j)| (infinity after a
+// zero diagonal).  The factors are partial pivoting's own when *lmax < 1 (no
+// interchange would have been made).  `gemm_update` as for lu_getrf.
+template <typename T>
+int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
+                   int *ipiv, int gemm_update, int *perm, float *lmax);
+
+// lu_getrf through the unpivoted factorisation when its multipliers certify
+// it (max |l| < 1 - margin: partial pivoting would interchange no row), else
+// restore() puts the unfactored matrix back into A and lu_getrf factors it
+// with pivoting.  *pivoted tells which ran.  A zero diagonal always takes
+// the pivoted path (which reports it in info as dgetrf does).
+template <typename T, typename Restore>
+int lu_getrf_auto(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
+                  int *ipiv, int *info_dev, int gemm_update, int *perm, double margin,
+                  Restore restore, int *pivoted) {
+  float lmax = INFINITY;
+  DUST_TRY(lu_getrf_nopiv<T>(cb, st, w, n, A, lda, ipiv, gemm_update, perm, &lmax));
+  if ((double)lmax < 1.0 - margin) {
+    DUST_CUDA(cudaMemsetAsync(info_dev, 0, sizeof(int), st));
+    if (pivoted) *pivoted = 0;
+    return DUST_OK;
+  }
+  DUST_TRY(restore());
+  if (pivoted) *pivoted = 1;
+  return lu_getrf<T>(cb, st, w, n, A, lda, ipiv, info_dev, gemm_update, perm);
+}

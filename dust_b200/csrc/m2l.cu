@@ -44,17 +44,78 @@ struct M2LTabs {
 // Inside a CTA the warps are independent: warp w takes offsets w, w+W, ...;
 // lane i looks up the source of target i at that offset, the present ones
 // are compacted with a ballot, the warp stages the offset's table and (in
-// chunks of M2L_TC) the present sources in its own shared-memory slice and
-// evaluates them with __syncwarp only.  Results go to the CTA's shared
-// accumulators with shared-memory atomics (a few per lane per offset, against
-// thousands of FMAs).
-#define M2L_W 8
+// chunks of up to TCX <= M2L_TC) the present sources in its own shared-memory slice
+// and evaluates them with __syncwarp only.  A chunk of kc targets runs the
+// register tile of the largest power of two <= kc (8, 4, 2, 1), so no lane
+// computes for an absent target.  In the tile a lane owns the outputs
+// m' = mb + lane and mb + 32 + lane for every target of the chunk: per
+// source monomial n it reads two table entries (Dx, Dy, Dz) at m' + n and,
+// per target, the source's (ax, ay, az), each as one vector load, for
+// 6 FMAs per (target, output).  The chunk's sums (over the nm source
+// monomials of one offset, in T) go to the CTA's FP64 accumulators with
+// shared-memory atomics.
 #define M2L_TC 8
 template <typename T>
-__global__ void __launch_bounds__(M2L_W * 32) k_m2l_batch(FmmDev d, const int4 *batches,
-                                                          const uint32_t *list, int NB, int NW,
-                                                          int TC, M2LTabs tabs, const T *ahat,
-                                                          uint32_t c0, int isum_smem) {
+struct M2LVec {
+  T x, y, z;
+};
+template <typename T>
+__device__ __forceinline__ M2LVec<T> m2l_ld(const T *p);
+template <>
+__device__ __forceinline__ M2LVec<float> m2l_ld<float>(const float *p) {
+  const float4 v = *(const float4 *)p;
+  return {v.x, v.y, v.z};
+}
+template <>
+__device__ __forceinline__ M2LVec<double> m2l_ld<double>(const double *p) {
+  const double2 a = *(const double2 *)p;
+  return {a.x, a.y, p[2]};
+}
+
+template <typename T, int TCc>
+__device__ __forceinline__ void m2l_tile(const T *__restrict__ sD, const T *__restrict__ sA,
+                                         const uint16_t *__restrict__ isum, int nm, int nm1,
+                                         int nout, int lane, const int *tl,
+                                         double *__restrict__ s_acc) {
+  for (int mb = 0; mb < nout; mb += 64) {
+    const int m0 = mb + lane, m1 = m0 + 32;
+    const int c0 = m0 < nout ? m0 : 0, c1 = m1 < nout ? m1 : 0;
+    T pa[TCc][2][3];
+#pragma unroll
+    for (int c = 0; c < TCc; ++c)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) pa[c][h][0] = pa[c][h][1] = pa[c][h][2] = (T)0;
+#pragma unroll 2
+    for (int n = 0; n < nm; ++n) {
+      const M2LVec<T> D0 = m2l_ld(sD + 4 * isum[(size_t)n * nm1 + c0]);
+      const M2LVec<T> D1 = m2l_ld(sD + 4 * isum[(size_t)n * nm1 + c1]);
+#pragma unroll
+      for (int c = 0; c < TCc; ++c) {
+        const M2LVec<T> a = m2l_ld(sA + ((size_t)c * nm + n) * 4);
+        pa[c][0][0] = fma(D0.y, a.z, fma(-D0.z, a.y, pa[c][0][0]));
+        pa[c][0][1] = fma(D0.z, a.x, fma(-D0.x, a.z, pa[c][0][1]));
+        pa[c][0][2] = fma(D0.x, a.y, fma(-D0.y, a.x, pa[c][0][2]));
+        pa[c][1][0] = fma(D1.y, a.z, fma(-D1.z, a.y, pa[c][1][0]));
+        pa[c][1][1] = fma(D1.z, a.x, fma(-D1.x, a.z, pa[c][1][1]));
+        pa[c][1][2] = fma(D1.x, a.y, fma(-D1.y, a.x, pa[c][1][2]));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < TCc; ++c) {
+      double *acc = s_acc + (size_t)tl[c] * nout * 3;
+      if (m0 < nout)
+        for (int e = 0; e < 3; ++e) atomicAdd(acc + 3 * m0 + e, (double)pa[c][0][e]);
+      if (m1 < nout)
+        for (int e = 0; e < 3; ++e) atomicAdd(acc + 3 * m1 + e, (double)pa[c][1][e]);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches,
+                                                   const uint32_t *list, int NB, int NW,
+                                                   int TCX, M2LTabs tabs, const T *ahat,
+                                                   uint32_t c0, int isum_smem) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nm = d.nm, nm1 = d.nm1, nD = d.nD;
   const int nout = d.use_vs ? nm1 : nm;
@@ -63,7 +124,7 @@ __global__ void __launch_bounds__(M2L_W * 32) k_m2l_batch(FmmDev d, const int4 *
   const T *dtab = (const T *)tabs.t[l];
   double *s_acc = (double *)smraw;                  // NB x nout x 3
   int *s_tc = (int *)(s_acc + (size_t)NB * nout * 3);  // NB x 3 target carts
-  const size_t wslice = (size_t)3 * nD + (size_t)TC * 3 * nm;  // per warp, in T
+  const size_t wslice = (size_t)4 * nD + (size_t)TCX * 4 * nm;  // per warp, in T
   uint16_t *s_isum = (uint16_t *)(s_tc + 3 * NB);  // nm x nm1 index table (optional)
   const uint16_t *isum = isum_smem ? s_isum : d.idxsum;
   const size_t isz = isum_smem ? (size_t)nm * nm1 : 0;
@@ -88,71 +149,67 @@ __global__ void __launch_bounds__(M2L_W * 32) k_m2l_batch(FmmDev d, const int4 *
   for (int e = tid; e < (int)isz; e += NW * 32) s_isum[e] = d.idxsum[e];
   __syncthreads();
   T *sD = s_w + (size_t)warp * wslice;
-  T *sA = sD + 3 * nD;
+  T *sA = sD + 4 * nD;
   unsigned long long npairs = 0;
   const int L = 3, W = 2 * L + 1;
   for (int cand = warp; cand < 216; cand += NW) {
     const int ox = cand % 6 - 2 - bx, oy = (cand / 6) % 6 - 2 - by, oz = cand / 36 - 2 - bz;
     if (abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) continue;  // adjacent: near field
-    int src = -1;
-    if (lane < cnt) {
-      int si = s_tc[3 * lane] + ox, sj = s_tc[3 * lane + 1] + oy, sk = s_tc[3 * lane + 2] + oz;
-      if (cart_in(d.G, l, si, sj, sk)) {
-        uint32_t skey = key_of(d.G, l, si, sj, sk);
-        if ((d.flags[lo_l + skey] & FL_ACTIVE) &&
-            d.cstart[(skey + 1u) << sh] > d.cstart[skey << sh])
-          src = (int)d.cidx[lo_l + skey];
+    // NB <= 64 targets: lane i looks at targets i and 32 + i
+    int src[2] = {-1, -1};
+    for (int h = 0; h < 2; ++h) {
+      const int t = lane + 32 * h;
+      if (t < cnt) {
+        int si = s_tc[3 * t] + ox, sj = s_tc[3 * t + 1] + oy, sk = s_tc[3 * t + 2] + oz;
+        if (cart_in(d.G, l, si, sj, sk)) {
+          uint32_t skey = key_of(d.G, l, si, sj, sk);
+          if ((d.flags[lo_l + skey] & FL_ACTIVE) &&
+              d.cstart[(skey + 1u) << sh] > d.cstart[skey << sh])
+            src[h] = (int)d.cidx[lo_l + skey];
+        }
       }
     }
-    unsigned msk = __ballot_sync(0xffffffffu, src >= 0);
-    if (!msk) continue;
-    npairs += __popc(msk);
+    unsigned msk[2] = {__ballot_sync(0xffffffffu, src[0] >= 0),
+                       __ballot_sync(0xffffffffu, src[1] >= 0)};
+    if (!(msk[0] | msk[1])) continue;
+    npairs += __popc(msk[0]) + __popc(msk[1]);
     const int tab = (ox + L) + W * ((oy + L) + W * (oz + L));
     const T *Dg = dtab + (size_t)tab * nD * 3;
     __syncwarp();
-    for (int e = lane; e < 3 * nD; e += 32) sD[e] = Dg[e];
-    while (msk) {
-      // next chunk of present targets
-      int tl[M2L_TC], kc = 0;
-      while (msk && kc < TC) {
-        int t = __ffs(msk) - 1;
-        msk &= msk - 1;
-        tl[kc++] = t;
-      }
-      for (int c = 0; c < kc; ++c) {
-        int sc_ = __shfl_sync(0xffffffffu, src, tl[c]);
-        const T *ag = ahat + (size_t)(sc_ - c0) * 3 * nm;
-        for (int e = lane; e < 3 * nm; e += 32) sA[c * 3 * nm + e] = ag[e];
-      }
-      __syncwarp();
-      for (int m0 = lane; m0 < nout; m0 += 32) {
-        T pa[M2L_TC][3];
-#pragma unroll
-        for (int c = 0; c < M2L_TC; ++c) pa[c][0] = pa[c][1] = pa[c][2] = (T)0;
-        for (int n = 0; n < nm; ++n) {
-          const int k0 = isum[(size_t)n * nm1 + m0];
-          const T Dx = sD[3 * k0], Dy = sD[3 * k0 + 1], Dz = sD[3 * k0 + 2];
-#pragma unroll
-          for (int c = 0; c < M2L_TC; ++c) {
-            if (c < kc) {
-              const T ax = sA[c * 3 * nm + 3 * n], ay = sA[c * 3 * nm + 3 * n + 1],
-                      az = sA[c * 3 * nm + 3 * n + 2];
-              pa[c][0] += Dy * az - Dz * ay;
-              pa[c][1] += Dz * ax - Dx * az;
-              pa[c][2] += Dx * ay - Dy * ax;
-            }
+    for (int e = lane; e < nD; e += 32) {
+      sD[4 * e] = Dg[3 * e];
+      sD[4 * e + 1] = Dg[3 * e + 1];
+      sD[4 * e + 2] = Dg[3 * e + 2];
+      sD[4 * e + 3] = (T)0;
+    }
+    for (int h = 0; h < 2; ++h) {
+      unsigned m = msk[h];
+      while (m) {
+        // next chunk of present targets: the largest tile <= what is left
+        const int left = min(__popc(m), TCX);
+        const int kc = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+        int tl[M2L_TC];
+        for (int c = 0; c < kc; ++c) {
+          const int t = __ffs(m) - 1;
+          m &= m - 1;
+          tl[c] = t + 32 * h;
+          const int sc_ = __shfl_sync(0xffffffffu, src[h], t);
+          const T *ag = ahat + (size_t)(sc_ - c0) * 3 * nm;
+          for (int e = lane; e < nm; e += 32) {
+            T *dst = sA + ((size_t)c * nm + e) * 4;
+            dst[0] = ag[3 * e];
+            dst[1] = ag[3 * e + 1];
+            dst[2] = ag[3 * e + 2];
+            dst[3] = (T)0;
           }
         }
-#pragma unroll
-        for (int c = 0; c < M2L_TC; ++c)
-          if (c < kc) {
-            double *acc = s_acc + ((size_t)tl[c] * nout + m0) * 3;
-            atomicAdd(acc, (double)pa[c][0]);
-            atomicAdd(acc + 1, (double)pa[c][1]);
-            atomicAdd(acc + 2, (double)pa[c][2]);
-          }
+        __syncwarp();
+        if (kc == 8) m2l_tile<T, 8>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
+        else if (kc == 4) m2l_tile<T, 4>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
+        else if (kc == 2) m2l_tile<T, 2>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
+        else m2l_tile<T, 1>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
+        __syncwarp();
       }
-      __syncwarp();
     }
   }
   __syncthreads();
@@ -240,7 +297,7 @@ int m2l_batch_tables(dust_octree *o) {
     DUST_CUDA(cudaMemcpy(o->dtabs[l].p, h.data(), n * 8, cudaMemcpyHostToDevice));
     DUST_CUDA(cudaMemcpy(o->dtab32[l].p, f.data(), n * 4, cudaMemcpyHostToDevice));
   }
-  return m2l_tc_tables(o);
+  return DUST_OK;
 }
 
 // Runs M2L for all levels >= 2 (level 1 is handled by the per-target kernel).
@@ -274,7 +331,6 @@ int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st) {
   bool f32 = o->prm.precision == DUST_PREC_FP32C;
   size_t w = (size_t)3 * o->nm, tot = (size_t)m * w;
   size_t ab = tot * (f32 ? 4 : 8) + 256;
-  if (m2l_tc_usable(o)) ab = std::max(ab, m2l_tc_ahat_bytes(m) + 256);
   DUST_TRY(devbuf_grow(o->ahat, ab));
   o->ahat_c0 = c0;
   return DUST_OK;
@@ -286,7 +342,6 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
   uint32_t c0 = o->ahat_c0, nact = (uint32_t)o->n_active;
   size_t tot = (size_t)(nact - c0) * 3 * o->nm;
   if (tot == 0) return DUST_OK;
-  if (m2l_tc_usable(o)) return m2l_tc_scale_sources(o, d, st);
   if (o->prm.precision == DUST_PREC_FP32C)
     k_scale_a<float><<<nblk(tot, 256), 256, 0, st>>>(d, c0, nact, (float *)o->ahat.p);
   else
@@ -297,30 +352,32 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st) {
 
 int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st) {
   if (!o->m2l_list) return DUST_OK;
-  if (m2l_tc_usable(o)) return m2l_tc_run(o, d, st);
-  // batch size, warps and chunk: the largest that fit 200 KB of shared memory
+  // batch size and warps: the largest that fit, two CTAs per SM when
+  // possible, else one
   bool f32 = o->prm.precision == DUST_PREC_FP32C;
   size_t esz = f32 ? 4 : 8;
   int nout = o->prm.vortstretch ? o->nm1 : o->nm;
-  int NB = 8, NW = 2, TC = 2;
+  int NB = 8, NW = 2, TCX = M2L_TC;
   bool found = false;
   const int isum_smem = (size_t)o->nm * o->nm1 * 2 <= 16 * 1024 ? 1 : 0;
   const size_t isb = isum_smem ? (size_t)o->nm * o->nm1 * 2 + 16 : 0;
-  const int nbs[3] = {32, 16, 8}, nws[5] = {8, 6, 4, 3, 2}, tcs[3] = {8, 4, 2};
-  // two CTAs per SM when possible, else one
-  for (size_t cap : {(size_t)110 * 1024, (size_t)200 * 1024})
-    for (int b = 0; b < 5 && !found; ++b)
-      for (int a = 0; a < 3 && !found; ++a)
-        for (int c = 0; c < 3 && !found; ++c) {
-          size_t smx = (size_t)nbs[a] * nout * 24 + (size_t)nbs[a] * 12 + 32 + isb +
-                       esz * nws[b] * ((size_t)3 * o->nD + (size_t)tcs[c] * 3 * o->nm);
-          if (smx <= cap && (tcs[c] >= 4 || cap > 110 * 1024)) {
+  auto wsl = [&](int tc) { return esz * ((size_t)4 * o->nD + (size_t)tc * 4 * o->nm); };
+  const int nbs[4] = {64, 48, 32, 16}, nws[5] = {8, 6, 4, 2, 1}, tcs[3] = {8, 4, 2};
+  auto smem_of = [&](int nb, int nw, int tc) {
+    return (size_t)nb * nout * 24 + (size_t)nb * 12 + 32 + isb + (size_t)nw * wsl(tc);
+  };
+  // two CTAs of >= 4 warps per SM when possible, else one CTA (high
+  // degrees: fewer warps, shorter chunks)
+  for (size_t cap : {(size_t)110 * 1024, (size_t)220 * 1024})
+    for (int c = 0; c < 3 && !found; ++c)
+      for (int b = 0; b < 5 && !found; ++b)
+        for (int a = 0; a < 4 && !found; ++a)
+          if (smem_of(nbs[a], nws[b], tcs[c]) <= cap && (nws[b] >= 4 || cap > 110 * 1024)) {
             NB = nbs[a];
             NW = nws[b];
-            TC = tcs[c];
+            TCX = tcs[c];
             found = true;
           }
-        }
   if (!found) return DUST_ERR_CAPACITY;
   std::vector<int4> bs;
   int start = 0;
@@ -335,27 +392,29 @@ int m2l_all_levels(dust_octree *o, FmmDev &d, cudaStream_t st) {
   DUST_TRY(devbuf_grow(o->m2l_bat, bs.size() * sizeof(int4)));
   DUST_CUDA(cudaMemcpyAsync(o->m2l_bat.p, bs.data(), bs.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, st));
-  size_t sm = (size_t)NB * nout * 24 + (size_t)NB * 12 + 32 + isb +
-              esz * NW * ((size_t)3 * o->nD + (size_t)TC * 3 * o->nm);
+  size_t sm = smem_of(NB, NW, TCX);
   M2LTabs tabs;
   for (int l = 0; l <= DUST_MAXLEV; ++l)
     tabs.t[l] = (l >= 2 && l <= o->G.ll) ? (f32 ? o->dtab32[l].p : o->dtabs[l].p) : nullptr;
   unsigned grid = (unsigned)bs.size();
+  o->kev_m2l = o->timing;
+  if (o->timing) cudaEventRecord(o->ev[6], st);
   if (f32) {
     if (sm > 48 * 1024)
       DUST_CUDA(cudaFuncSetAttribute(k_m2l_batch<float>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_m2l_batch<float><<<grid, NW * 32, sm, st>>>(d, (const int4 *)o->m2l_bat.p, o->m2l_list,
-                                                NB, NW, TC, tabs, (const float *)o->ahat.p, o->ahat_c0,
+                                                NB, NW, TCX, tabs, (const float *)o->ahat.p, o->ahat_c0,
                                                 isum_smem);
   } else {
     if (sm > 48 * 1024)
       DUST_CUDA(cudaFuncSetAttribute(k_m2l_batch<double>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_m2l_batch<double><<<grid, NW * 32, sm, st>>>(d, (const int4 *)o->m2l_bat.p, o->m2l_list,
-                                                 NB, NW, TC, tabs, (const double *)o->ahat.p,
+                                                 NB, NW, TCX, tabs, (const double *)o->ahat.p,
                                                  o->ahat_c0, isum_smem);
   }
+  if (o->timing) cudaEventRecord(o->ev[7], st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }

@@ -128,14 +128,20 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   if (nmv > 0) {
     k_blk_f32<<<2048, 256, 0, st>>>(nst, nmv, A + (size_t)nst * n, n, Asd, nst);
     k_blk_f32<<<2048, 256, 0, st>>>(nmv, nst, A + nst, n, Ads, nmv);
-    k_blk_f32<<<1024, 256, 0, st>>>(nmv, nmv, A + nst + (size_t)nst * n, n, S, nmv);
+    // S = A_mm - A_ms Ainv A_sm (Y = Ainv A_sm is kept, so S can be rebuilt)
+    auto build_s = [&]() -> int {
+      k_blk_f32<<<1024, 256, 0, st>>>(nmv, nmv, A + nst + (size_t)nst * n, n, S, nmv);
+      if (nst > 0) DUST_TRY(gemm_tf32_acc(st, nmv, nmv, nst, Ads, nmv, Y, nst, S, nmv, -1.0f));
+      DUST_CUDA(cudaGetLastError());
+      return DUST_OK;
+    };
     if (nst > 0) {
       DUST_CUDA(cudaMemsetAsync(Y, 0, (size_t)nst * nmv * 4, st));
       DUST_TRY(gemm_tf32_acc(st, nst, nmv, nst, Ainv, nst, Asd, nst, Y, nst, 1.0f));
-      DUST_TRY(gemm_tf32_acc(st, nmv, nmv, nst, Ads, nmv, Y, nst, S, nmv, -1.0f));
     }
-    DUST_TRY(lu_getrf<float>(L->cb, st, L->lu, nmv, S, nmv, piv, info, 1,
-                             use_perm ? perm : nullptr));
+    DUST_TRY(build_s());
+    DUST_TRY(lu_getrf_auto<float>(L->cb, st, L->lu, nmv, S, nmv, piv, info, 1,
+                                  use_perm ? perm : nullptr, 0.0, build_s, &L->last_pivoted));
     DUST_TRY(gemm_tf32_error(st));
     int hinfo = 0;
     DUST_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -84,7 +84,15 @@ int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
   k_to_f32<<<1184, 256, 0, st>>>(nn, A64, A32);
-  int s = lu_getrf<float>(cb, st, lu, n, A32, n, ipiv, info, use_tc);
+  int piv = 1;
+  int s = lu_getrf_auto<float>(cb, st, lu, n, A32, n, ipiv, info, use_tc, nullptr, 0.0,
+                               [&]() -> int {
+                                 k_to_f32<<<1184, 256, 0, st>>>(nn, A64, A32);
+                                 DUST_CUDA(cudaGetLastError());
+                                 return DUST_OK;
+                               },
+                               &piv);
+  if (rep) rep->pivoted = piv;
   cudaEventRecord(e1, st);
   if (s != DUST_OK) return s;
   int hinfo = 0;
@@ -158,7 +166,22 @@ static int dense_lu64_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, Dev
   cudaEventRecord(e0, st);
   if (A != F.p && cudaMemcpyAsync(F.p, A, nn * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     s = DUST_ERR_CUDA;
-  if (s == DUST_OK) s = lu_getrf<double>(cb, st, lu, n, (double *)F.p, n, ipiv, info, 0);
+  int pivd = 1;
+  if (s == DUST_OK) {
+    // A is F's storage only when the caller factors in place (then it cannot
+    // be restored, and the pivoted path runs directly)
+    if (A != F.p)
+      s = lu_getrf_auto<double>(cb, st, lu, n, (double *)F.p, n, ipiv, info, 0, nullptr, 1e-8,
+                                [&]() -> int {
+                                  DUST_CUDA(cudaMemcpyAsync(F.p, A, nn * 8,
+                                                            cudaMemcpyDeviceToDevice, st));
+                                  return DUST_OK;
+                                },
+                                &pivd);
+    else
+      s = lu_getrf<double>(cb, st, lu, n, (double *)F.p, n, ipiv, info, 0);
+  }
+  if (r) r->pivoted = pivd;
   cudaEventRecord(e1, st);
   int hinfo = 0;
   if (s == DUST_OK) {
@@ -240,7 +263,7 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
     return DUST_ERR_CUDA;
   }
   cublasSetStream(cb, st);
-  DevBuf dA, dB, dX, piv, w32, wrk;
+  DevBuf dA, dB, dX, dF, piv, w32, wrk;
   LuWork lu;
   dust_solve_report r;
   memset(&r, 0, sizeof(r));
@@ -251,8 +274,9 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
     cudaMemcpyAsync(dA.p, A, nn * 8, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(dB.p, B, nr * 8, cudaMemcpyHostToDevice, st);
     if (mode == DUST_SOLVE_LU64) {
-      // factored in place in the device copy (the host array is the caller's)
-      s = dense_lu64_device(cb, st, lu, dA, piv, n, nrhs, (const double *)dA.p,
+      // factored in a second device copy, so that the unpivoted attempt can
+      // be undone
+      s = dense_lu64_device(cb, st, lu, dF, piv, n, nrhs, (const double *)dA.p,
                             (const double *)dB.p, (double *)dX.p, &r);
     } else {
       s = mixed_solve_device(cb, st, lu, w32, wrk, n, nrhs, (const double *)dA.p,
@@ -268,10 +292,12 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
   devbuf_free(dA);
   devbuf_free(dB);
   devbuf_free(dX);
+  devbuf_free(dF);
   devbuf_free(piv);
   devbuf_free(w32);
   devbuf_free(wrk);
   devbuf_free(lu.sync);
+  devbuf_free(lu.np);
   cublasDestroy(cb);
   cudaStreamDestroy(st);
   if (rep) *rep = r;

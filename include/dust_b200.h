@@ -123,7 +123,7 @@ typedef struct dust_fmm_stats {
   int64_t n_elem_pairs;      /* particle x element evaluations               */
   int     n_levels;
   float   ms_tree, ms_upward, ms_m2l, ms_p2p, ms_elems, ms_total;
-  float   ms_m2l_kernel;     /* tensor-core M2L kernel alone (FP32C), else 0  */
+  float   ms_m2l_kernel;     /* M2L kernel of levels >= 2 alone (k_m2l_batch) */
   float   ms_elem_far;       /* FP32 far-field element kernel alone, else 0   */
 } dust_fmm_stats;
 
@@ -314,6 +314,9 @@ typedef struct dust_solve_report {
   double residual;        /* final ||b - A x||_inf / (||A||_inf ||x||_inf);
                              GMRES: ||b - A x||_2 / ||b||_2                  */
   float  ms_factor, ms_solve;
+  int    pivoted;         /* LU paths: 1 if the factorisation interchanged
+                             rows (partial pivoting ran), 0 if its unpivoted
+                             multipliers certified that dgetrf would not    */
 } dust_solve_report;
 
 /* Implicit wake panels (first n_impl wake panels) couple into A through

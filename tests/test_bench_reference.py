@@ -44,20 +44,28 @@ def test_reference_arm_two_ranks():
 
 
 def test_roofline_fields():
-    """The roofline object of the bench line (dominant kernel: the FP32C
-    element far field) from a phase breakdown: achieved = algorithmic flops /
-    kernel time, frac = achieved / peak, traffic scaled by the particles."""
+    """The roofline object of the bench line from a phase breakdown: the
+    headline mode's dominant kernel (here the FP32C element far field),
+    achieved = algorithmic flops (or bytes) / kernel time, frac = achieved /
+    peak, traffic scaled by the particles; M2L in GB/s with its flop rate."""
     sys.path.insert(0, ROOT)
     import bench
     from dust_b200 import synth
     case = synth.FullStepCase(n_particles=10_000)
     params = case.fmm_params()
-    ph = {"mixed": {"k_elem_far_ms": 2.0, "n_elem_pairs": 10_000 * 14_596, "k_m2l_tc_ms": 1.0,
-                    "n_m2l_pairs": 1000, "uvort": 1.5}}
+    ph = {"mixed": {"k_elem_far_ms": 2.0, "n_elem_pairs": 10_000 * 14_596,
+                    "k_m2l_batch_ms": 1.0, "n_m2l_pairs": 1000, "uvort": 1.5,
+                    "fmm_p2p": 0.5, "n_p2p_pairs": 4000}}
     rf = bench.roofline(ph, case, params, "mixed")
     for k in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
         assert k in rf
     ach = bench.FLOP_ELEM_PAIR * 10_000 * 14_596 / 2e-3 / 1e12
+    assert rf["kernel"] == "k_elem_far"
     assert abs(rf["achieved"] - ach) <= 0.01 and abs(rf["frac"] - ach / rf["peak"]) <= 1e-3
     assert rf["unit"] == "TFLOP/s" and rf["traffic"] > 0
-    assert [o["kernel"] for o in rf["others"]][0] == "k_m2l_tc"
+    names = [o["kernel"] for o in rf["others"]]
+    assert names[0].startswith("uvort") and "k_m2l_batch" in names
+    m2l = rf["others"][names.index("k_m2l_batch")]
+    assert m2l["unit"] == "GB/s" and m2l["bound"] == "hbm"
+    gbs = bench.BYTES_M2L_PAIR_WORDS * 4 * 1000 / 1e-3 / 1e9
+    assert abs(m2l["achieved"] - gbs) <= 0.1 and m2l["flops"]["unit"] == "TFLOP/s"

@@ -123,6 +123,8 @@ def test_ellipsoid_16k_64rhs_lu64_and_mixed(ellipsoid16k):
     r32 = linsys.dense_solve_device(Ad, Bd, X32, abi.DUST_SOLVE_MIXED, tol=1e-12)
     assert r64["mode_used"] == abi.DUST_SOLVE_LU64
     assert r32["mode_used"] == abi.DUST_SOLVE_MIXED and r32["residual"] <= 1e-12
+    # the doublet system needs no interchange, and the factors certify it
+    assert r64["pivoted"] == 0 and r32["pivoted"] == 0
     Anorm = float(Ad.abs().sum(dim=0).max())
 
     def berr(X):

@@ -135,7 +135,35 @@ def test_dense_lu64_pivoting(n):
     A = rng.standard_normal((n, n))
     B = rng.standard_normal((n, 2))
     X, rep = linsys.dense_solve(A, B, abi.DUST_SOLVE_LU64)
+    assert rep["pivoted"] == 1
     assert rel(X, np.linalg.solve(A, B)) < 1e-9
+
+
+def _col_dominant(n, seed):
+    """Columns dominated by the diagonal: elimination keeps that property, so
+    every multiplier stays below 1 and dgetrf interchanges no row."""
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n))
+    np.fill_diagonal(A, 0.0)
+    A *= 0.95 / np.maximum(np.abs(A).sum(axis=0, keepdims=True), 1e-300)
+    A += np.eye(n) * np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    return A
+
+
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (64, 2), (300, 3), (2500, 2)])
+def test_dense_unpivoted_certified(n, nrhs):
+    """Column-dominant systems take the unpivoted blocked LU, whose multipliers
+    (all |l| < 1) certify that partial pivoting makes the same (no) row
+    interchanges; the solution is LAPACK's."""
+    import scipy.linalg as sl
+    A = _col_dominant(n, n + 11)
+    B = np.random.default_rng(n).standard_normal((n, nrhs))
+    lu, piv = sl.lu_factor(A)
+    assert np.array_equal(piv, np.arange(n))  # LAPACK interchanges nothing
+    for mode in (abi.DUST_SOLVE_LU64, abi.DUST_SOLVE_MIXED):
+        X, rep = linsys.dense_solve(A, B, mode, tol=1e-13)
+        assert rep["pivoted"] == 0
+        assert rel(X, sl.lu_solve((lu, piv), B)) < 1e-11
 
 
 @pytest.mark.parametrize("n", [500, 1920])
@@ -144,7 +172,7 @@ def test_dense_mixed_pivoting(n):
     A = rng.standard_normal((n, n))
     B = rng.standard_normal((n, 3))
     X, rep = linsys.dense_solve(A, B, abi.DUST_SOLVE_MIXED, tol=1e-12)
-    assert rep["fell_back"] == 0 and rep["residual"] <= 1e-12
+    assert rep["fell_back"] == 0 and rep["residual"] <= 1e-12 and rep["pivoted"] == 1
     assert rel(X, np.linalg.solve(A, B)) < 1e-9
 
 
