@@ -71,6 +71,9 @@ def parse():
                          "FP64 step with the direct sum is timed as well)")
     ap.add_argument("--no-advect", action="store_true",
                     help="leave the particles in place (no complete_wake particle update)")
+    ap.add_argument("--accuracy-steps", type=int, default=20,
+                    help="advected steps over which every mode's loads are compared with "
+                         "the plain FP64 run (warm-up + timed + untimed steps)")
     return ap.parse_args()
 
 
@@ -176,7 +179,9 @@ def make_case(args):
     return synth.FullStepCase(n_particles=args.particles)
 
 
-def time_steps(stepper, steps, flush):
+def time_steps(stepper, steps, flush, after=None):
+    """CUDA-event time of each step; ``after()`` runs between steps, outside
+    the timed events (e.g. reading the step's loads)."""
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
@@ -187,6 +192,8 @@ def time_steps(stepper, steps, flush):
         stepper.step()
         ev[k][1].record()
         torch.cuda.synchronize()
+        if after is not None:
+            after()
     return [a.elapsed_time(b) for a, b in ev]
 
 
@@ -350,7 +357,10 @@ def main():
     case = make_case(args)
     params = case.fmm_params(degree=args.degree)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    modes = [("plain", abi.DUST_SOLVE_LU64), ("mixed", abi.DUST_SOLVE_MIXED)]
+    # mixed: FP32C FMM and uvort, mixed solve; mixed_f64uvort: the same with
+    # the direct uvort sum in FP64
+    modes = [("plain", abi.DUST_SOLVE_LU64), ("mixed", abi.DUST_SOLVE_MIXED),
+             ("mixed_f64uvort", abi.DUST_SOLVE_MIXED)]
     learned = None
     if not args.no_learned:
         # the learned preconditioner trains (untimed) on the plain solutions
@@ -372,10 +382,12 @@ def main():
     results = {}
     steppers = {}
     by_step = {}
+    n_acc = max(args.accuracy_steps, max(args.warmup, 3) + args.steps)
     for name, mode in modes:
         prm = params if name.startswith("plain") else params.replace(precision=abi.DUST_PREC_FP32C)
         st = step.DeviceStepper(case, prm, mode, advect=not args.no_advect,
-                                fmm_uvort=fmm_uv and name != "plain_direct_uvort")
+                                fmm_uvort=fmm_uv and name != "plain_direct_uvort",
+                                uvort_params=params if name == "mixed_f64uvort" else None)
         if name == "learned":
             learned["precond"].attach(st.ls)
         if name == "plain_perturbed":
@@ -384,17 +396,20 @@ def main():
                                            dtype=torch.float64)).to(st.cen.device)
         steppers[name] = st
         by_step[name] = []
+        # loads after every advected step (read between steps, untimed): how
+        # the modes drift apart
+        record = (lambda: by_step[name].append(
+            case.loads(st.res.cpu().numpy(), st.euv.cpu().numpy()))) \
+            if not args.profile_step else (lambda: None)
         for _ in range(max(args.warmup, 1 if args.profile_step else 3)):
             st.step()
-            if not args.profile_step:
-                # loads after every warm-up step (untimed): how the modes drift apart
-                by_step[name].append(case.loads(st.res.cpu().numpy(), st.euv.cpu().numpy()))
+            record()
         torch.cuda.synchronize()
         if args.profile_step:
             continue
         barrier(ws)
         with Clocks(local) as clk:
-            times = time_steps(st, args.steps, flush)
+            times = time_steps(st, args.steps, flush, after=record)
         barrier(ws)
         ms = max_over_ranks(float(np.mean(times)), ws)
         res = st.res.cpu().numpy()
@@ -403,6 +418,11 @@ def main():
                          "report": st.last_report, "clocks": clk.summary(), "res": res,
                          "fmm": [t.cpu().numpy() for t in (st.vel, st.str, st.rot)],
                          "cen": st.cen.cpu().numpy(), "n_freed": int(st.free.sum())}
+        # further untimed steps up to the accuracy horizon (phase breakdown and
+        # launch counts below run one more step each)
+        while not args.no_advect and len(by_step[name]) < n_acc:
+            st.step()
+            record()
     if args.profile_step:
         return
     # phase breakdown (plain and mixed share the FMM): one timed step with events
@@ -412,6 +432,7 @@ def main():
     load_err = {k: lerr(results[k]["loads"], lp) for k in results}
     load_err_by_step = {k: [lerr(a, b) for a, b in zip(by_step[k], by_step["plain"])]
                         for k in by_step}
+    load_err_max = {k: max(v) if v else 0.0 for k, v in load_err_by_step.items()}
     # particle outputs of the step (velocity without the wind, stretching,
     # div-filter curl) against the FP64 step: relative L2 norms
     uinf = np.asarray(params.u_inf)
@@ -426,8 +447,9 @@ def main():
     for k in results:
         fmm_errs[k]["position_max_abs"] = float(np.max(np.abs(results[k]["cen"] - cp)))
     # the headline mode: the fastest whose loads stay within 1e-6 of FP64 (the
-    # plain step of the same algorithm) after every advected step, or within
-    # twice FP64's own drift from a 1e-12 perturbation where that is larger
+    # plain step of the same algorithm) after every one of the advected steps,
+    # or within twice FP64's own drift from a 1e-12 perturbation at that step
+    # where that is larger
     floor = load_err.get("plain_perturbed", 0.0)
     floor_by_step = load_err_by_step.get("plain_perturbed", [])
     def within(k):
@@ -443,7 +465,8 @@ def main():
     if not args.no_e2e:
         prm_best = params if best == "plain" else params.replace(precision=abi.DUST_PREC_FP32C)
         e2e = run_e2e(case, prm_best, dict(modes)[best], args, ws,
-                      learned["precond"] if best == "learned" else None, fmm_uv)
+                      learned["precond"] if best == "learned" else None, fmm_uv,
+                      uvort_params=params if best == "mixed_f64uvort" else None)
     cpu = None
     if not args.no_cpu and rank == 0 and ws == 1:
         ms_cpu, cores, sample = cpu_baseline(case, params, ph[best]["n_m2l_pairs"])
@@ -465,7 +488,8 @@ def main():
             "metric": METRIC, "value": round(r["ms"] / ws, 3), "unit": "ms", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"], 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if best == "plain" else "f32/tf32 with f64 refinement",
+            "dtype": "f64" if best == "plain" else "f32 (uvort f64)/tf32 with f64 refinement"
+                     if best == "mixed_f64uvort" else "f32/tf32 with f64 refinement",
             "data": "synthetic (seeded FullStepCase)",
             "config": config_of(case, args, params),
             "mode": best,
@@ -474,17 +498,20 @@ def main():
             "plain_fp64_ms": round(results["plain"]["ms"], 3),
             "speedup_vs_plain_fp64": round(results["plain"]["ms"] / r["ms"], 3),
             "load_error_vs_fp64": load_err[best],
-            "steps_advected": 0 if args.no_advect else max(args.warmup, 3) + args.steps,
-            "load_error_by_warmup_step": load_err_by_step,
+            "steps_advected": 0 if args.no_advect else n_acc,
+            "load_error_by_step": load_err_by_step,
+            "load_error_max_over_steps": load_err_max,
             "fp64_sensitivity_floor": floor,
             "headline_rule": "fastest mode whose loads are within max(1e-6, 2 x the FP64 "
-                             "sensitivity floor) of the plain FP64 step after every warm-up "
-                             "step and after the last timed step",
-            "load_error_note": "loads (wing lift, two rotor thrusts) of the last timed step; "
-                               "every mode advects its own particles from the same initial "
-                               "wake for all warm-up + timed steps, so the FMM error of each "
-                               "step reaches the loads of the next",
+                             "sensitivity floor at that step) of the plain FP64 run after "
+                             "every one of the %d advected steps" % n_acc,
+            "load_error_note": "loads (wing lift, two rotor thrusts); every mode advects its "
+                               "own particles from the same initial wake for %d steps (warm-up, "
+                               "timed and untimed), so the FMM error of each step reaches the "
+                               "loads of the next; load_error_vs_fp64 is after the last timed "
+                               "step" % n_acc,
             "modes": {k: {"ms": round(v["ms"], 3), "load_error_vs_fp64": load_err[k],
+                          "load_error_max_over_steps": load_err_max.get(k),
                           "particle_error_vs_fp64": fmm_errs[k], "solve": v["report"]}
                       for k, v in results.items()},
             "learned_training": learned["info"] if learned else None,
@@ -864,8 +891,9 @@ def phase_breakdown(st, case, params):
 #  far element pair (k_elem_far): r (3) + r^2 (5) + rsqrt (1) + 1/r^2 (1)
 #    + r.n (5) + 1/r^3 (1) + coefficient (3) + 3 x fma(k3, fma(coef, r, -mu n)) (12)
 FLOP_ELEM_PAIR = 31
-#  uvort pair (k_uvort_sorted): d (3) + rho^2 (6) + rsqrt (1) + rho^-3 (2) + 6 fma (12)
-FLOP_UVORT_PAIR = 24
+#  uvort pair (k_uvort / k_uvort_sorted): d (3) + rho^2 (6) + rsqrt (1) + rho^-3 (2)
+#  + c d (3) + c d x alpha accumulated (6 fma, 12)
+FLOP_UVORT_PAIR = 27
 #  M2L pair at p = 4 with stretching: 56 outputs x 35 inputs x 3 components x
 #  2 cross-product terms, one FMA each
 FLOP_M2L_PAIR = 56 * 35 * 6 * 2
@@ -999,7 +1027,7 @@ def e2e_bytes(case, n, advect, fmm_uvort=False):
     return h2d, d2h
 
 
-def run_e2e(case, params, mode, args, ws, pc=None, fmm_uvort=False):
+def run_e2e(case, params, mode, args, ws, pc=None, fmm_uvort=False, uvort_params=None):
     """Same step through the host API with pinned host buffers: every step
     copies particles and panels in and velocities/strengths out."""
     import torch
@@ -1010,7 +1038,7 @@ def run_e2e(case, params, mode, args, ws, pc=None, fmm_uvort=False):
     n = case.mag.shape[0]
     out = tuple(pin(np.empty((n, 3))) for _ in range(3))  # page-locked outputs
     hs = step.HostStepper(case, params, mode, out=out, advect=not args.no_advect,
-                          fmm_uvort=fmm_uvort)
+                          fmm_uvort=fmm_uvort, uvort_params=uvort_params)
     if pc is not None:
         pc.attach(hs.ls)
     for _ in range(3):

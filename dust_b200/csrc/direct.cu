@@ -784,15 +784,13 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
                                                         const double *X, const float *F,
                                                         int chunk, double *uv) {
   // one tile of particles per pass, coordinates relative to the tile's first
-  // particle.  With d = p - x_q,  d x alpha_q = p x alpha_q - w_q where
-  // w_q = x_q x alpha_q, so the tile's sum is
-  //   sum_q c_q (d x alpha_q) = p x (sum_q c_q alpha_q) - sum_q c_q w_q,
-  // two 3-vector FMA accumulations per pair instead of a cross product
-  // (|x_q| is bounded by the tile's extent, so nothing cancels).  Pairs of
-  // particles (q, q+1) are evaluated together in packed FP32 (f32x2): their
-  // ten values (-x, -y, -z, core^2, alpha, w) are stored interleaved, value k
-  // of particle q at [q / 2][2 k + q % 2].  Partial sums over the tile in
-  // FP32, added into FP64 per tile.
+  // particle (rounded to FP32 once), d = p - x_q and the cross product
+  // d x alpha_q formed per pair, so a point close to a particle loses
+  // nothing to cancellation.  Pairs of particles (q, q+1) are evaluated
+  // together in packed FP32 (f32x2): their ten values (-x, -y, -z, core^2,
+  // alpha, -alpha) are stored interleaved, value k of particle q at
+  // [q / 2][2 k + q % 2].  Partial sums over the tile in FP32, added into
+  // FP64 per tile.
   __shared__ __align__(16) float s_pk[UV2_TILE / 2][20];
   __shared__ double s_ref[3];
   int t[UV2_PPT];
@@ -816,26 +814,25 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
       // particles beyond the chunk: far away (1e6), no strength
       float val[10] = {-1.0e6f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (threadIdx.x < m) {
-        const float x = (float)(X[q] - s_ref[0]), y = (float)(X[(size_t)n + q] - s_ref[1]),
-                    z = (float)(X[2 * (size_t)n + q] - s_ref[2]);
         const float ax = F[q], ay = F[(size_t)n + q], az = F[2 * (size_t)n + q];
-        val[0] = -x, val[1] = -y, val[2] = -z, val[3] = F[(size_t)3 * n + q];
+        val[0] = (float)(s_ref[0] - X[q]);
+        val[1] = (float)(s_ref[1] - X[(size_t)n + q]);
+        val[2] = (float)(s_ref[2] - X[2 * (size_t)n + q]);
+        val[3] = F[(size_t)3 * n + q];
         val[4] = ax, val[5] = ay, val[6] = az;
-        val[7] = fmaf(y, az, -z * ay);
-        val[8] = fmaf(z, ax, -x * az);
-        val[9] = fmaf(x, ay, -y * ax);
+        val[7] = -ax, val[8] = -ay, val[9] = -az;
       }
       for (int k = 0; k < 10; ++k) s_pk[threadIdx.x >> 1][2 * k + (threadIdx.x & 1)] = val[k];
     }
     __syncthreads();
     float px[UV2_PPT], py[UV2_PPT], pz[UV2_PPT];
-    float2 A[UV2_PPT][3], W[UV2_PPT][3];
+    float2 V[UV2_PPT][3];
 #pragma unroll
     for (int i = 0; i < UV2_PPT; ++i) {
       px[i] = (float)(pos[i][0] - s_ref[0]);
       py[i] = (float)(pos[i][1] - s_ref[1]);
       pz[i] = (float)(pos[i][2] - s_ref[2]);
-      for (int c = 0; c < 3; ++c) A[i][c] = W[i][c] = make_float2(0.f, 0.f);
+      for (int c = 0; c < 3; ++c) V[i][c] = make_float2(0.f, 0.f);
     }
     const int mp = (m + 1) >> 1;
 #pragma unroll 2
@@ -846,8 +843,8 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
       const float2 nx = make_float2(P0.x, P0.y), ny = make_float2(P0.z, P0.w),
                    nz = make_float2(P1.x, P1.y), s2 = make_float2(P1.z, P1.w),
                    ax = make_float2(P2.x, P2.y), ay = make_float2(P2.z, P2.w),
-                   az = make_float2(P3.x, P3.y), w0 = make_float2(P3.z, P3.w),
-                   w1 = make_float2(P4.x, P4.y), w2 = make_float2(P4.z, P4.w);
+                   az = make_float2(P3.x, P3.y), mx = make_float2(P3.z, P3.w),
+                   my = make_float2(P4.x, P4.y), mz = make_float2(P4.z, P4.w);
 #pragma unroll
       for (int i = 0; i < UV2_PPT; ++i) {
         const float2 dx = __fadd2_rn(make_float2(px[i], px[i]), nx),
@@ -856,23 +853,17 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
         const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
         const float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
         const float2 c = __fmul2_rn(__fmul2_rn(ir, ir), ir);
-        A[i][0] = __ffma2_rn(c, ax, A[i][0]);
-        A[i][1] = __ffma2_rn(c, ay, A[i][1]);
-        A[i][2] = __ffma2_rn(c, az, A[i][2]);
-        W[i][0] = __ffma2_rn(c, w0, W[i][0]);
-        W[i][1] = __ffma2_rn(c, w1, W[i][1]);
-        W[i][2] = __ffma2_rn(c, w2, W[i][2]);
+        const float2 cx = __fmul2_rn(c, dx), cy = __fmul2_rn(c, dy), cz = __fmul2_rn(c, dz);
+        // c (d x alpha)
+        V[i][0] = __ffma2_rn(cy, az, __ffma2_rn(cz, my, V[i][0]));
+        V[i][1] = __ffma2_rn(cz, ax, __ffma2_rn(cx, mz, V[i][1]));
+        V[i][2] = __ffma2_rn(cx, ay, __ffma2_rn(cy, mx, V[i][2]));
       }
     }
     // velocity kernel coefficient is -1/rho^3
 #pragma unroll
-    for (int i = 0; i < UV2_PPT; ++i) {
-      float a[3], w[3];
-      for (int c = 0; c < 3; ++c) a[c] = A[i][c].x + A[i][c].y, w[c] = W[i][c].x + W[i][c].y;
-      v[i][0] -= (double)(fmaf(py[i], a[2], -pz[i] * a[1]) - w[0]);
-      v[i][1] -= (double)(fmaf(pz[i], a[0], -px[i] * a[2]) - w[1]);
-      v[i][2] -= (double)(fmaf(px[i], a[1], -py[i] * a[0]) - w[2]);
-    }
+    for (int i = 0; i < UV2_PPT; ++i)
+      for (int c = 0; c < 3; ++c) v[i][c] -= (double)(V[i][c].x + V[i][c].y);
   }
   const double k4pi = 1.0 / (4.0 * DUST_PI);
 #pragma unroll

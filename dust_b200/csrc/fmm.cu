@@ -1039,9 +1039,10 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
 #define P2W_TILE 32
 #define P2W_MAXR (26 * DUST_MAXLEV + 4)
 #define P2W_NV 8  // staged per source: x y z, alpha x y z, r_v^2, 1 / r_v^2
+#define P2W_LQ 4  // levels whose near-field loads are issued together
 
 template <bool VS, bool DF, bool VD, bool TV, bool F32>
-__global__ void __launch_bounds__(P2W_WARPS * 32, F32 ? 6 : 5) k_p2p_w(FmmDev d) {
+__global__ void __launch_bounds__(P2W_WARPS * 32, 5) k_p2p_w(FmmDev d) {
   using R = typename std::conditional<F32, float, double>::type;
   __shared__ R s_src[P2W_WARPS][P2W_NV][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
@@ -1061,34 +1062,40 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, F32 ? 6 : 5) k_p2p_w(FmmDev d)
   const uint32_t lo = cell_lo(d.G, d.cstart, l, key), hi = cell_hi(d.G, d.cstart, l, key);
   if (hi == lo) return;
   uint32_t *rlo = s_rlo[w], *rcum = s_rcum[w];
-  // near-field source ranges: same level first, then coarser levels
+  // near-field source ranges: same level first, then coarser levels.  The
+  // flags and particle ranges of P2W_LQ levels are loaded without branches
+  // (predicated on the neighbour lying in the box), so those loads are in
+  // flight together rather than one dependent chain per level.
   int nr = 0;
-  for (int lev = l; lev >= 1; --lev) {
-    const int sh = l - lev;
-    const int ai = ci_ >> sh, aj = cj >> sh, ak = ck >> sh;
-    bool pred = false;
-    uint32_t a0 = 0, a1 = 0;
-    if (lane < 27 && lane != 13) {
+  for (int lev0 = l; lev0 >= 1; lev0 -= P2W_LQ) {
+    bool predq[P2W_LQ];
+    uint32_t a0q[P2W_LQ], a1q[P2W_LQ];
+#pragma unroll
+    for (int q = 0; q < P2W_LQ; ++q) {
+      const int lev = lev0 - q;
+      const int sh = l - lev;
+      const int ai = ci_ >> sh, aj = cj >> sh, ak = ck >> sh;
       const int di = lane % 3 - 1, dj = (lane / 3) % 3 - 1, dk = lane / 9 - 1;
-      if (cart_in(d.G, lev, ai + di, aj + dj, ak + dk)) {
-        const uint32_t nk = key_of(d.G, lev, ai + di, aj + dj, ak + dk);
-        const uint8_t f = d.flags[d.G.lev_off[lev] + nk];
-        const bool want = (lev == l) ? (f & FL_ACTIVE) != 0 : (f & FL_LEAF) != 0;
-        if (want) {
-          a0 = cell_lo(d.G, d.cstart, lev, nk);
-          a1 = cell_hi(d.G, d.cstart, lev, nk);
-          pred = a1 > a0;
-        }
+      const bool ok = lev >= 1 && lane < 27 && lane != 13 &&
+                      cart_in(d.G, lev, ai + di, aj + dj, ak + dk);
+      const uint32_t nk = ok ? key_of(d.G, lev, ai + di, aj + dj, ak + dk) : 0u;
+      const uint8_t f = ok ? d.flags[d.G.lev_off[lev] + nk] : (uint8_t)0;
+      a0q[q] = ok ? cell_lo(d.G, d.cstart, lev, nk) : 0u;
+      a1q[q] = ok ? cell_hi(d.G, d.cstart, lev, nk) : 0u;
+      const bool want = (lev == l) ? (f & FL_ACTIVE) != 0 : (f & FL_LEAF) != 0;
+      predq[q] = ok && want && a1q[q] > a0q[q];
+    }
+#pragma unroll
+    for (int q = 0; q < P2W_LQ; ++q) {
+      const unsigned msk = __ballot_sync(0xffffffffu, predq[q]);
+      // 26 per level and l <= DUST_MAXLEV levels: the list cannot overflow
+      if (predq[q] && nr + __popc(msk) < P2W_MAXR) {
+        const int pos = nr + __popc(msk & ((1u << lane) - 1u));
+        rlo[pos] = a0q[q];
+        rcum[pos] = a1q[q] - a0q[q];
       }
+      nr = min(nr + __popc(msk), P2W_MAXR - 1);
     }
-    const unsigned msk = __ballot_sync(0xffffffffu, pred);
-    // 26 per level and l <= DUST_MAXLEV levels: the list cannot overflow
-    if (pred && nr + __popc(msk) < P2W_MAXR) {
-      const int pos = nr + __popc(msk & ((1u << lane) - 1u));
-      rlo[pos] = a0;
-      rcum[pos] = a1 - a0;
-    }
-    nr = min(nr + __popc(msk), P2W_MAXR - 1);
   }
   __syncwarp();
   if (lane == 0) {

@@ -267,7 +267,7 @@ extern "C" int dust_linsys_destroy(dust_linsys *L) {
   if (!L) return DUST_OK;
   if (L->st) cudaStreamSynchronize(L->st);
   DevBuf *bufs[] = {&L->A,  &L->As, &L->b,    &L->bst,  &L->piv, &L->info, &L->geo,
-                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->lu.np, &L->A32, &L->gm, &L->ainv32, &L->mx, &L->kr,
+                    &L->raw, &L->impl, &L->work, &L->lu.sync, &L->lu.np, &L->lu.np_x, &L->A32, &L->gm, &L->ainv32, &L->mx, &L->kr,
                     &L->mvb};
   for (DevBuf *b : bufs) devbuf_free(*b);
   if (L->cb) cublasDestroy(L->cb);

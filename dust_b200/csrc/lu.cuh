@@ -14,7 +14,9 @@
 
 struct LuWork {
   DevBuf sync;   // barrier counters, error flag, partials, candidate rows
-  DevBuf np;     // unpivoted LU: max |l| word, inverse diagonal triangles
+  DevBuf np;     // unpivoted LU: max |l| word, inverse triangles of every
+                 // diagonal block (kept for lu_getrs_nopiv)
+  DevBuf np_x;   // lu_getrs_nopiv: the intermediate Y = L^-1 B
   int nsm = 0;
 };
 
@@ -49,6 +51,13 @@ int lu_getrs(cublasHandle_t cb, cudaStream_t st, int n, int nrhs, const T *A, in
 template <typename T>
 int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, int lda,
                    int *ipiv, int gemm_update, int *perm, float *lmax);
+
+// Solves A X = B (X over B, nrhs columns, ldb) with the factors of the last
+// lu_getrf_nopiv on this LuWork (same A, n): forward and backward block
+// substitution with the kept inverse triangles, one launch per 64-row block.
+template <typename T>
+int lu_getrs_nopiv(cudaStream_t st, LuWork &w, int n, int nrhs, const T *A, int lda, T *B,
+                   int ldb);
 
 // lu_getrf through the unpivoted factorisation when its multipliers certify
 // it (max |l| < 1 - margin: partial pivoting would interchange no row), else

@@ -213,10 +213,13 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
                    int *ipiv, int gemm_update, int *perm, float *lmax) {
   *lmax = 0.f;
   if (n <= 0) return DUST_OK;
+  // inverse triangles of every diagonal block are kept (Linv then Uinv per
+  // block) for lu_getrs_nopiv
   const size_t tri = (size_t)NP_NB * NP_NB;
-  DUST_TRY(devbuf_grow(w.np, 256 + 2 * tri * sizeof(T)));
+  const int nblk_ = (n + NP_NB - 1) / NP_NB;
+  DUST_TRY(devbuf_grow(w.np, 256 + 2 * tri * sizeof(T) * (size_t)nblk_));
   unsigned *bits = (unsigned *)w.np.p;
-  T *Linv = (T *)((char *)w.np.p + 256), *Uinv = Linv + tri;
+  T *inv0 = (T *)((char *)w.np.p + 256);
   DUST_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned), st));
   const int smd = 3 * NP_NB * NP_LD * (int)sizeof(T), smp = 2 * NP_NB * NP_LD * (int)sizeof(T);
   static bool attr = false;  // per element type
@@ -228,6 +231,7 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
   CUBLAS_CHECK(cublasSetStream(cb, st));
   for (int k = 0; k < n; k += NP_NB) {
     const int jb = std::min(NP_NB, n - k), m2 = n - k - jb;
+    T *Linv = inv0 + 2 * tri * (size_t)(k / NP_NB), *Uinv = Linv + tri;
     k_np_diag<T><<<1, NP_T, smd, st>>>(A, lda, k, jb, Linv, Uinv, bits);
     if (m2 > 0) {
       const int nrb = (m2 + NP_NB - 1) / NP_NB;
@@ -253,6 +257,110 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
   return DUST_OK;
 }
 
+// Block substitution with the kept inverse triangles: one launch per 64-row
+// block i (forward: i ascending with Linv, backward: descending with Uinv).
+// Every CTA of the launch recomputes Y_i = Inv_i B_i (64 x 64 by 64 x NP_RC,
+// from B's block i, which no CTA of the launch writes), and then updates its
+// 64 rows of the not yet solved part, B_r -= A_(r,i) Y_i; CTA 0 also stores
+// Y_i into X.  Grid: (row tiles, RHS chunks of NP_RC columns).
+#define NP_RC 32
+template <typename T, bool FWD>
+__global__ void __launch_bounds__(NP_T) k_np_subst(const T *A, int lda, int n, int nrhs,
+                                                   int i, const T *Inv, T *B, int ldb, T *X,
+                                                   int ldx) {
+  extern __shared__ __align__(16) unsigned char np_sm[];
+  T *w = (T *)np_sm;                // 64 x 64 inverse, [row][col], ld NP_LD
+  T *b = w + NP_NB * NP_LD;         // 64 x NP_RC block i of B, [row][col]
+  T *y = b + NP_NB * (NP_RC + 1);   // 64 x NP_RC Y_i
+  T *l = y + NP_NB * (NP_RC + 1);   // 64 x 64 coupling tile A_(r,i), [row][col]
+  const int tid = threadIdx.x;
+  const int k = i * NP_NB, jb = min(NP_NB, n - k);
+  const int c0 = blockIdx.y * NP_RC, nc = min(NP_RC, nrhs - c0);
+  const T *W = Inv + 2 * (size_t)NP_NB * NP_NB * i + (FWD ? 0 : (size_t)NP_NB * NP_NB);
+  for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+    const int r = e % NP_NB, c = e / NP_NB;
+    w[r * NP_LD + c] = (r < jb && c < jb) ? W[r + (size_t)c * NP_NB] : (T)0;
+  }
+  for (int e = tid; e < NP_NB * NP_RC; e += NP_T) {
+    const int r = e % NP_NB, c = e / NP_NB;
+    b[r * (NP_RC + 1) + c] = (r < jb && c < nc) ? B[(size_t)(k + r) + (size_t)(c0 + c) * ldb] : (T)0;
+  }
+  __syncthreads();
+  // Y_i = Inv_i B_i: thread (r, c-phase) computes y[r][c] for c = cp, cp + 8, ...
+  {
+    const int r = tid % NP_NB, cp = tid / NP_NB;
+    for (int c = cp; c < NP_RC; c += NP_T / NP_NB) {
+      T acc = (T)0;
+      for (int p = 0; p < NP_NB; ++p) acc = fma(w[r * NP_LD + p], b[p * (NP_RC + 1) + c], acc);
+      y[r * (NP_RC + 1) + c] = acc;
+    }
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int e = tid; e < NP_NB * NP_RC; e += NP_T) {
+      const int r = e % NP_NB, c = e / NP_NB;
+      if (r < jb && c < nc) X[(size_t)(k + r) + (size_t)(c0 + c) * ldx] = y[r * (NP_RC + 1) + c];
+    }
+  // rows still to solve: below the block (forward) or above it (backward)
+  const int nrest = FWD ? n - k - jb : k;
+  const int ntile = (nrest + NP_NB - 1) / NP_NB;
+  if ((int)blockIdx.x >= ntile) return;
+  const int r0 = FWD ? k + jb + NP_NB * blockIdx.x : NP_NB * blockIdx.x;
+  const int nr = min(NP_NB, (FWD ? n : k) - r0);
+  for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+    const int r = e % NP_NB, c = e / NP_NB;
+    l[r * NP_LD + c] = (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
+  }
+  __syncthreads();
+  {
+    const int r = tid % NP_NB, cp = tid / NP_NB;
+    if (r < nr)
+      for (int c = cp; c < nc; c += NP_T / NP_NB) {
+        T acc = (T)0;
+        for (int p = 0; p < NP_NB; ++p) acc = fma(l[r * NP_LD + p], y[p * (NP_RC + 1) + c], acc);
+        B[(size_t)(r0 + r) + (size_t)(c0 + c) * ldb] -= acc;
+      }
+  }
+}
+
+template <typename T>
+int lu_getrs_nopiv(cudaStream_t st, LuWork &w, int n, int nrhs, const T *A, int lda, T *B,
+                   int ldb) {
+  if (n <= 0 || nrhs <= 0) return DUST_OK;
+  const int nb = (n + NP_NB - 1) / NP_NB;
+  const T *inv0 = (const T *)((const char *)w.np.p + 256);
+  const size_t xb = (size_t)n * nrhs * sizeof(T);
+  DUST_TRY(devbuf_grow(w.np_x, xb));
+  T *X = (T *)w.np_x.p;
+  const int sm = (2 * NP_NB * NP_LD + 2 * NP_NB * (NP_RC + 1)) * (int)sizeof(T);
+  static bool attr = false;  // per element type
+  if (!attr) {
+    DUST_CUDA(cudaFuncSetAttribute(k_np_subst<T, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    DUST_CUDA(cudaFuncSetAttribute(k_np_subst<T, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    attr = true;
+  }
+  const unsigned gy = (unsigned)((nrhs + NP_RC - 1) / NP_RC);
+  // L Y = B: Y into X
+  for (int i = 0; i < nb; ++i) {
+    const int below = n - (i + 1) * NP_NB;
+    const unsigned gx = (unsigned)std::max(1, (below + NP_NB - 1) / NP_NB);
+    k_np_subst<T, true><<<dim3(gx, gy), NP_T, sm, st>>>(A, lda, n, nrhs, i, inv0, B, ldb, X, n);
+  }
+  // U X = Y: X back into B
+  for (int i = nb - 1; i >= 0; --i) {
+    const unsigned gx = (unsigned)std::max(1, i);
+    k_np_subst<T, false><<<dim3(gx, gy), NP_T, sm, st>>>(A, lda, n, nrhs, i, inv0, X, n, B, ldb);
+  }
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+template int lu_getrs_nopiv<double>(cudaStream_t, LuWork &, int, int, const double *, int,
+                                    double *, int);
+template int lu_getrs_nopiv<float>(cudaStream_t, LuWork &, int, int, const float *, int, float *,
+                                   int);
 template int lu_getrf_nopiv<double>(cublasHandle_t, cudaStream_t, LuWork &, int, double *, int,
                                     int *, int, int *, float *);
 template int lu_getrf_nopiv<float>(cublasHandle_t, cudaStream_t, LuWork &, int, float *, int,

@@ -55,6 +55,7 @@ struct M2LTabs {
 // monomials of one offset, in T) go to the CTA's FP64 accumulators with
 // shared-memory atomics.
 #define M2L_TC 8
+#define M2L_GQ 4
 template <typename T>
 struct M2LVec {
   T x, y, z;
@@ -70,6 +71,16 @@ template <>
 __device__ __forceinline__ M2LVec<double> m2l_ld<double>(const double *p) {
   const double2 a = *(const double2 *)p;
   return {a.x, a.y, p[2]};
+}
+
+// count padded (x y z 0) entries from global to shared memory, by the warp
+__device__ __forceinline__ void m2l_copy4(float *dst, const float *src, int count, int lane) {
+  for (int e = lane; e < count; e += 32)
+    *(float4 *)(dst + 4 * e) = __ldg((const float4 *)(src + 4 * e));
+}
+__device__ __forceinline__ void m2l_copy4(double *dst, const double *src, int count, int lane) {
+  for (int e = lane; e < 2 * count; e += 32)
+    *(double2 *)(dst + 2 * e) = __ldg((const double2 *)(src + 2 * e));
 }
 
 template <typename T, int TCc>
@@ -115,7 +126,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches,
                                                    const uint32_t *list, int NB, int NW,
                                                    int TCX, M2LTabs tabs, const T *ahat,
-                                                   uint32_t c0, int isum_smem) {
+                                                   uint32_t ahat_cell0, int isum_smem) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nm = d.nm, nm1 = d.nm1, nD = d.nD;
   const int nout = d.use_vs ? nm1 : nm;
@@ -152,36 +163,55 @@ __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches
   T *sA = sD + 4 * nD;
   unsigned long long npairs = 0;
   const int L = 3, W = 2 * L + 1;
-  for (int cand = warp; cand < 216; cand += NW) {
-    const int ox = cand % 6 - 2 - bx, oy = (cand / 6) % 6 - 2 - by, oz = cand / 36 - 2 - bz;
-    if (abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) continue;  // adjacent: near field
-    // NB <= 64 targets: lane i looks at targets i and 32 + i
-    int src[2] = {-1, -1};
-    for (int h = 0; h < 2; ++h) {
-      const int t = lane + 32 * h;
-      if (t < cnt) {
-        int si = s_tc[3 * t] + ox, sj = s_tc[3 * t + 1] + oy, sk = s_tc[3 * t + 2] + oz;
-        if (cart_in(d.G, l, si, sj, sk)) {
-          uint32_t skey = key_of(d.G, l, si, sj, sk);
-          if ((d.flags[lo_l + skey] & FL_ACTIVE) &&
-              d.cstart[(skey + 1u) << sh] > d.cstart[skey << sh])
-            src[h] = (int)d.cidx[lo_l + skey];
-        }
+  // The warp's offsets are looked up M2L_GQ at a time: for every target the
+  // source cell's flags, particle range and index are loaded without
+  // branches (predicated on the cell lying in the box), so the loads of the
+  // M2L_GQ offsets are in flight together instead of one dependent chain per
+  // offset.
+  for (int cb = warp; cb < 216; cb += NW * M2L_GQ) {
+    int srcq[M2L_GQ][2];
+#pragma unroll
+    for (int g = 0; g < M2L_GQ; ++g) {
+      const int cand = cb + g * NW;
+      const int ox = cand % 6 - 2 - bx, oy = (cand / 6) % 6 - 2 - by, oz = cand / 36 - 2 - bz;
+      const bool valid = cand < 216 && !(abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        // NB <= 64 targets: lane i looks at targets i and 32 + i
+        const int t = lane + 32 * h;
+        const int si = s_tc[3 * (t < NB ? t : 0)] + ox, sj = s_tc[3 * (t < NB ? t : 0) + 1] + oy,
+                  sk = s_tc[3 * (t < NB ? t : 0) + 2] + oz;
+        const bool ok = valid && t < cnt && cart_in(d.G, l, si, sj, sk);
+        const uint32_t skey = ok ? key_of(d.G, l, si, sj, sk) : 0u;
+        const uint8_t f = ok ? d.flags[lo_l + skey] : (uint8_t)0;
+        const uint32_t a0 = ok ? d.cstart[skey << sh] : 0u;
+        const uint32_t a1 = ok ? d.cstart[(skey + 1u) << sh] : 0u;
+        const uint32_t cx = ok ? d.cidx[lo_l + skey] : 0u;
+        srcq[g][h] = (ok && (f & FL_ACTIVE) && a1 > a0) ? (int)cx : -1;
       }
+    }
+#pragma unroll 1
+    for (int g = 0; g < M2L_GQ; ++g) {
+    const int cand = cb + g * NW;
+    if (cand >= 216) break;
+    const int ox = cand % 6 - 2 - bx, oy = (cand / 6) % 6 - 2 - by, oz = cand / 36 - 2 - bz;
+    // (selects, not a dynamically indexed array, keep srcq in registers)
+    int src[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int v = srcq[0][h];
+#pragma unroll
+      for (int q = 1; q < M2L_GQ; ++q) v = (g == q) ? srcq[q][h] : v;
+      src[h] = v;
     }
     unsigned msk[2] = {__ballot_sync(0xffffffffu, src[0] >= 0),
                        __ballot_sync(0xffffffffu, src[1] >= 0)};
     if (!(msk[0] | msk[1])) continue;
     npairs += __popc(msk[0]) + __popc(msk[1]);
     const int tab = (ox + L) + W * ((oy + L) + W * (oz + L));
-    const T *Dg = dtab + (size_t)tab * nD * 3;
+    const T *Dg = dtab + (size_t)tab * nD * 4;
     __syncwarp();
-    for (int e = lane; e < nD; e += 32) {
-      sD[4 * e] = Dg[3 * e];
-      sD[4 * e + 1] = Dg[3 * e + 1];
-      sD[4 * e + 2] = Dg[3 * e + 2];
-      sD[4 * e + 3] = (T)0;
-    }
+    m2l_copy4(sD, Dg, nD, lane);
     for (int h = 0; h < 2; ++h) {
       unsigned m = msk[h];
       while (m) {
@@ -194,14 +224,8 @@ __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches
           m &= m - 1;
           tl[c] = t + 32 * h;
           const int sc_ = __shfl_sync(0xffffffffu, src[h], t);
-          const T *ag = ahat + (size_t)(sc_ - c0) * 3 * nm;
-          for (int e = lane; e < nm; e += 32) {
-            T *dst = sA + ((size_t)c * nm + e) * 4;
-            dst[0] = ag[3 * e];
-            dst[1] = ag[3 * e + 1];
-            dst[2] = ag[3 * e + 2];
-            dst[3] = (T)0;
-          }
+          m2l_copy4(sA + (size_t)c * nm * 4, ahat + (size_t)(sc_ - ahat_cell0) * 4 * nm, nm,
+                    lane);
         }
         __syncwarp();
         if (kc == 8) m2l_tile<T, 8>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
@@ -210,6 +234,7 @@ __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches
         else m2l_tile<T, 1>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
         __syncwarp();
       }
+    }
     }
   }
   __syncthreads();
@@ -246,7 +271,10 @@ __global__ void k_scale_a(FmmDev d, uint32_t c0, uint32_t nact, T *out) {
   int l = d.act_lev[ci];
   double hi = 1.0 / d.G.csize[l], hp = 1.0;
   for (int q = 0; q < ni + nj + nk; ++q) hp *= hi;
-  out[e] = (T)(d.A[(size_t)ci * w + r] * d.inv_fact[nn] * hp);
+  // padded [cell][nm][4] (x y z 0), so a monomial is one 16- or 32-byte load
+  T *o4 = out + (size_t)(ci - c0) * 4 * d.nm + 4 * nn;
+  o4[r % 3] = (T)(d.A[(size_t)ci * w + r] * d.inv_fact[nn] * hp);
+  if (r % 3 == 2) o4[3] = (T)0;
 }
 
 // class keys of the active cells of levels >= 2: (level << 3 | key & 7) for
@@ -279,23 +307,25 @@ int m2l_batch_tables(dust_octree *o) {
     mono_exp(q, i, j, k);
     deg[q] = i + j + k;
   }
+  // padded [343 offsets][nD][4] (x y z 0): one vector load per entry
   for (int l = 2; l <= o->G.ll; ++l) {
-    size_t n = (size_t)343 * nD * 3;
-    DUST_TRY(devbuf_grow(o->dtabs[l], n * 8));
-    DUST_TRY(devbuf_grow(o->dtab32[l], n * 4));
-    std::vector<double> h(n);
+    size_t n = (size_t)343 * nD * 3, n4 = (size_t)343 * nD * 4;
+    DUST_TRY(devbuf_grow(o->dtabs[l], n4 * 8));
+    DUST_TRY(devbuf_grow(o->dtab32[l], n4 * 4));
+    std::vector<double> h(n), h4(n4, 0.0);
     DUST_CUDA(cudaMemcpy(h.data(), o->dtab[l].p, n * 8, cudaMemcpyDeviceToHost));
     double cs = o->G.csize[l];
     std::vector<double> hp(2 * DUST_MAXP + 6, 1.0);
     for (size_t e = 1; e < hp.size(); ++e) hp[e] = hp[e - 1] * cs;
-    std::vector<float> f(n);
+    std::vector<float> f(n4, 0.f);
     for (size_t i = 0; i < n; ++i) {
       size_t q = (i / 3) % nD;
-      h[i] *= hp[deg[q] + 2];
-      f[i] = (float)h[i];
+      size_t j = (i / 3) * 4 + i % 3;
+      h4[j] = h[i] * hp[deg[q] + 2];
+      f[j] = (float)h4[j];
     }
-    DUST_CUDA(cudaMemcpy(o->dtabs[l].p, h.data(), n * 8, cudaMemcpyHostToDevice));
-    DUST_CUDA(cudaMemcpy(o->dtab32[l].p, f.data(), n * 4, cudaMemcpyHostToDevice));
+    DUST_CUDA(cudaMemcpy(o->dtabs[l].p, h4.data(), n4 * 8, cudaMemcpyHostToDevice));
+    DUST_CUDA(cudaMemcpy(o->dtab32[l].p, f.data(), n4 * 4, cudaMemcpyHostToDevice));
   }
   return DUST_OK;
 }
@@ -329,8 +359,7 @@ int m2l_prepare(dust_octree *o, FmmDev &d, cudaStream_t st) {
   o->m2l_list = v_out;
   // pre-scaled source coefficients of all active cells of levels >= 2
   bool f32 = o->prm.precision == DUST_PREC_FP32C;
-  size_t w = (size_t)3 * o->nm, tot = (size_t)m * w;
-  size_t ab = tot * (f32 ? 4 : 8) + 256;
+  size_t ab = (size_t)m * 4 * o->nm * (f32 ? 4 : 8) + 256;
   DUST_TRY(devbuf_grow(o->ahat, ab));
   o->ahat_c0 = c0;
   return DUST_OK;

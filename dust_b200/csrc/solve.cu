@@ -136,7 +136,10 @@ int mixed_solve_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, DevBuf &w
       if (it == max_iter) break;
     }
     k_to_f32<<<256, 256, 0, st>>>(nr, R, D32);
-    DUST_TRY(lu_getrs<float>(cb, st, n, nrhs, A32, n, ipiv, D32, n));
+    if (piv == 0)
+      DUST_TRY(lu_getrs_nopiv<float>(st, lu, n, nrhs, A32, n, D32, n));
+    else
+      DUST_TRY(lu_getrs<float>(cb, st, n, nrhs, A32, n, ipiv, D32, n));
     k_add_f32<<<256, 256, 0, st>>>(nr, D32, X);
   }
   DUST_CUDA(cudaGetLastError());
@@ -193,7 +196,8 @@ static int dense_lu64_device(cublasHandle_t cb, cudaStream_t st, LuWork &lu, Dev
     if (X != B && cudaMemcpyAsync(X, B, nr * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
       s = DUST_ERR_CUDA;
     if (s == DUST_OK)
-      s = lu_getrs<double>(cb, st, n, nrhs, (const double *)F.p, n, ipiv, X, n);
+      s = pivd == 0 ? lu_getrs_nopiv<double>(st, lu, n, nrhs, (const double *)F.p, n, X, n)
+                    : lu_getrs<double>(cb, st, n, nrhs, (const double *)F.p, n, ipiv, X, n);
     cudaEventRecord(e2, st);
   }
   if (s == DUST_OK && cudaStreamSynchronize(st) == cudaSuccess && r) {
@@ -298,6 +302,7 @@ extern "C" int dust_dense_solve(int n, int nrhs, const double *A, const double *
   devbuf_free(wrk);
   devbuf_free(lu.sync);
   devbuf_free(lu.np);
+  devbuf_free(lu.np_x);
   cublasDestroy(cb);
   cudaStreamDestroy(st);
   if (rep) *rep = r;

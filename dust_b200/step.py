@@ -47,16 +47,18 @@ def update_params_for(case, params):
 
 class HostStepper:
     def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None, advect=False,
-                 fmm_uvort=False):
+                 fmm_uvort=False, uvort_params=None):
         """``out``: optional (vel, stretch, rotu) host arrays the particle
         outputs are written to every step (e.g. page-locked buffers);
         ``advect``: move the particles at the end of each step;
         ``fmm_uvort``: uvort through the particles' FMM (prepare, points,
         finish: the particles are uploaded once per step) instead of the
-        direct sum."""
+        direct sum; ``uvort_params``: parameters of the direct uvort sum when
+        they differ from the FMM's (e.g. an FP64 uvort beside an FP32C FMM)."""
         self.fmm_uvort = fmm_uvort
         self.case = case
         self.params = params
+        self.uvort_params = uvort_params if uvort_params is not None else params
         self.mode = mode
         self.out = out
         self.advect = advect
@@ -75,7 +77,7 @@ class HostStepper:
         tri = nv == 3
         if tri.any():
             cen_el[tri] = c.elems.ver[tri, :3].mean(axis=1)
-        ps = p.struct()
+        ps = self.uvort_params.struct()
         evs = c.end_vort.struct()
         uv = np.empty((c.rank, 3))
         cen_el = np.ascontiguousarray(cen_el)
@@ -114,11 +116,12 @@ class DeviceStepper:
     """All per-step inputs resident in HBM; library calls on device pointers."""
 
     def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda", advect=False,
-                 fmm_uvort=False):
+                 fmm_uvort=False, uvort_params=None):
         import torch
         self.torch = torch
         self.case = case
         self.params = params
+        self._ups = (uvort_params if uvort_params is not None else params).struct()
         self.mode = mode
         self.advect = advect
         self.fmm_uvort = fmm_uvort
@@ -193,7 +196,7 @@ class DeviceStepper:
                                                      C.c_void_p(stream)),
                   "dust_fmm_points_uvort_device")
         else:
-            check(lib().dust_points_uvort_device(C.byref(self._ps), c.rank, P(self.ecen),
+            check(lib().dust_points_uvort_device(C.byref(self._ups), c.rank, P(self.ecen),
                                                  self.n, P(self.cen), P(self.dir), P(self.mag),
                                                  P(self.rv), C.byref(lines), P(self.euv),
                                                  C.c_void_p(stream)), "dust_points_uvort_device")
