@@ -689,7 +689,7 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
 // per thread (consecutive CTA slices of UV2_T points) against a shared tile
 // of (x, y, z, r_v^2, alpha) records; the reciprocal square root as in
 // k_elem_out (FP32 seed, one Householder step in FP64).
-#define UVD_PPT 2
+#define UVD_PPT 4
 __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, int n,
                                                  const double *cen, const double *dir,
                                                  const double *mag, const double *rv,
@@ -780,53 +780,9 @@ __global__ void k_uv_gather(int n, const uint32_t *perm, const double *cen, cons
 #ifndef UV2_PPT
 #define UV2_PPT 4
 #endif
-// A pair is "close" when rho^2 = |d|^2 + r_v^2 < UV2_CLOSE r_v^2 (|d| below
-// sqrt(15) core radii): there the kernel is near its peak and a point's uvort
-// is most sensitive to the pair, so close pairs are evaluated in FP64.
-#define UV2_CLOSE 16.0f
-
-// FP32 sums of one tile for the thread's points; with EXCL the close pairs
-// (of points flagged near the tile) are left out, for the FP64 pass.
-template <bool EXCL>
-__device__ __forceinline__ void uv2_tile(const float (*s_pk)[20], int mp, const float *px,
-                                         const float *py, const float *pz, const bool *nearp,
-                                         float2 (*V)[3]) {
-#pragma unroll 2
-  for (int u = 0; u < mp; ++u) {
-    const float4 P0 = *(const float4 *)&s_pk[u][0], P1 = *(const float4 *)&s_pk[u][4],
-                 P2 = *(const float4 *)&s_pk[u][8], P3 = *(const float4 *)&s_pk[u][12],
-                 P4 = *(const float4 *)&s_pk[u][16];
-    const float2 nx = make_float2(P0.x, P0.y), ny = make_float2(P0.z, P0.w),
-                 nz = make_float2(P1.x, P1.y), s2 = make_float2(P1.z, P1.w),
-                 ax = make_float2(P2.x, P2.y), ay = make_float2(P2.z, P2.w),
-                 az = make_float2(P3.x, P3.y), mx = make_float2(P3.z, P3.w),
-                 my = make_float2(P4.x, P4.y), mz = make_float2(P4.z, P4.w);
-#pragma unroll
-    for (int i = 0; i < UV2_PPT; ++i) {
-      const float2 dx = __fadd2_rn(make_float2(px[i], px[i]), nx),
-                   dy = __fadd2_rn(make_float2(py[i], py[i]), ny),
-                   dz = __fadd2_rn(make_float2(pz[i], pz[i]), nz);
-      const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
-      const float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-      float2 c = __fmul2_rn(__fmul2_rn(ir, ir), ir);
-      if (EXCL && nearp[i]) {
-        if (r2.x < UV2_CLOSE * s2.x) c.x = 0.f;
-        if (r2.y < UV2_CLOSE * s2.y) c.y = 0.f;
-      }
-      const float2 cx = __fmul2_rn(c, dx), cy = __fmul2_rn(c, dy), cz = __fmul2_rn(c, dz);
-      // c (d x alpha)
-      V[i][0] = __ffma2_rn(cy, az, __ffma2_rn(cz, my, V[i][0]));
-      V[i][1] = __ffma2_rn(cz, ax, __ffma2_rn(cx, mz, V[i][1]));
-      V[i][2] = __ffma2_rn(cx, ay, __ffma2_rn(cy, mx, V[i][2]));
-    }
-  }
-}
-
 __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *pts, int n,
                                                         const double *X, const float *F,
-                                                        int chunk, double *uv,
-                                                        const uint32_t *perm, const double *dir,
-                                                        const double *mag, const double *rv) {
+                                                        int chunk, double *uv) {
   // one tile of particles per pass, coordinates relative to the tile's first
   // particle (rounded to FP32 once), d = p - x_q and the cross product
   // d x alpha_q formed per pair, so a point close to a particle loses
@@ -834,14 +790,9 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
   // together in packed FP32 (f32x2): their ten values (-x, -y, -z, core^2,
   // alpha, -alpha) are stored interleaved, value k of particle q at
   // [q / 2][2 k + q % 2].  Partial sums over the tile in FP32, added into
-  // FP64 per tile.  A thread whose points come within sqrt(15.5) of the
-  // tile's largest core radius of the tile's bounding box leaves the close
-  // pairs (UV2_CLOSE) out of the FP32 sums and evaluates them in FP64 from
-  // the caller's arrays (perm: sorted -> caller order).
-  static_assert(UV2_TILE == UV2_T, "one staged particle per thread");
+  // FP64 per tile.
   __shared__ __align__(16) float s_pk[UV2_TILE / 2][20];
   __shared__ double s_ref[3];
-  __shared__ float s_box[UV2_T / 32][7];
   int t[UV2_PPT];
   double pos[UV2_PPT][3], v[UV2_PPT][3];
 #pragma unroll
@@ -853,88 +804,60 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
     }
   }
   const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
     __syncthreads();
     const int q = q0 + threadIdx.x;
     const int m = min(UV2_TILE, q_hi - q0);
     if (threadIdx.x < 3) s_ref[threadIdx.x] = X[(size_t)threadIdx.x * n + q0];
     __syncthreads();
-    // particles beyond the chunk: far away (1e6), no strength
-    float val[10] = {-1.0e6f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY},
-          bs = 0.f;
-    if (threadIdx.x < m) {
-      const float ax = F[q], ay = F[(size_t)n + q], az = F[2 * (size_t)n + q];
-      val[0] = (float)(s_ref[0] - X[q]);
-      val[1] = (float)(s_ref[1] - X[(size_t)n + q]);
-      val[2] = (float)(s_ref[2] - X[2 * (size_t)n + q]);
-      val[3] = F[(size_t)3 * n + q];
-      val[4] = ax, val[5] = ay, val[6] = az;
-      val[7] = -ax, val[8] = -ay, val[9] = -az;
-      for (int c = 0; c < 3; ++c) bl[c] = bh[c] = -val[c];
-      bs = val[3];
-    }
-    for (int k = 0; k < 10; ++k) s_pk[threadIdx.x >> 1][2 * k + (threadIdx.x & 1)] = val[k];
-    // the tile's bounding box (relative coordinates) and largest core^2
-    for (int o = 16; o > 0; o >>= 1) {
-      for (int c = 0; c < 3; ++c) {
-        bl[c] = fminf(bl[c], __shfl_xor_sync(0xffffffffu, bl[c], o));
-        bh[c] = fmaxf(bh[c], __shfl_xor_sync(0xffffffffu, bh[c], o));
+    if (threadIdx.x < UV2_TILE) {
+      // particles beyond the chunk: far away (1e6), no strength
+      float val[10] = {-1.0e6f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (threadIdx.x < m) {
+        const float ax = F[q], ay = F[(size_t)n + q], az = F[2 * (size_t)n + q];
+        val[0] = (float)(s_ref[0] - X[q]);
+        val[1] = (float)(s_ref[1] - X[(size_t)n + q]);
+        val[2] = (float)(s_ref[2] - X[2 * (size_t)n + q]);
+        val[3] = F[(size_t)3 * n + q];
+        val[4] = ax, val[5] = ay, val[6] = az;
+        val[7] = -ax, val[8] = -ay, val[9] = -az;
       }
-      bs = fmaxf(bs, __shfl_xor_sync(0xffffffffu, bs, o));
-    }
-    if (lane == 0) {
-      for (int c = 0; c < 3; ++c) s_box[warp][c] = bl[c], s_box[warp][3 + c] = bh[c];
-      s_box[warp][6] = bs;
+      for (int k = 0; k < 10; ++k) s_pk[threadIdx.x >> 1][2 * k + (threadIdx.x & 1)] = val[k];
     }
     __syncthreads();
-    for (int w = 0; w < UV2_T / 32; ++w) {
-      for (int c = 0; c < 3; ++c) bl[c] = fminf(bl[c], s_box[w][c]), bh[c] = fmaxf(bh[c], s_box[w][3 + c]);
-      bs = fmaxf(bs, s_box[w][6]);
-    }
     float px[UV2_PPT], py[UV2_PPT], pz[UV2_PPT];
     float2 V[UV2_PPT][3];
-    bool nearp[UV2_PPT], any = false;
 #pragma unroll
     for (int i = 0; i < UV2_PPT; ++i) {
       px[i] = (float)(pos[i][0] - s_ref[0]);
       py[i] = (float)(pos[i][1] - s_ref[1]);
       pz[i] = (float)(pos[i][2] - s_ref[2]);
       for (int c = 0; c < 3; ++c) V[i][c] = make_float2(0.f, 0.f);
-      const float ex = fmaxf(fmaxf(bl[0] - px[i], px[i] - bh[0]), 0.f),
-                  ey = fmaxf(fmaxf(bl[1] - py[i], py[i] - bh[1]), 0.f),
-                  ez = fmaxf(fmaxf(bl[2] - pz[i], pz[i] - bh[2]), 0.f);
-      nearp[i] = t[i] < npts && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= 15.5f * bs;
-      any = any || nearp[i];
     }
     const int mp = (m + 1) >> 1;
-    if (!any) {
-      uv2_tile<false>(s_pk, mp, px, py, pz, nearp, V);
-    } else {
-      uv2_tile<true>(s_pk, mp, px, py, pz, nearp, V);
-      // the close pairs in FP64 (the same FP32 test picks them)
+#pragma unroll 2
+    for (int u = 0; u < mp; ++u) {
+      const float4 P0 = *(const float4 *)&s_pk[u][0], P1 = *(const float4 *)&s_pk[u][4],
+                   P2 = *(const float4 *)&s_pk[u][8], P3 = *(const float4 *)&s_pk[u][12],
+                   P4 = *(const float4 *)&s_pk[u][16];
+      const float2 nx = make_float2(P0.x, P0.y), ny = make_float2(P0.z, P0.w),
+                   nz = make_float2(P1.x, P1.y), s2 = make_float2(P1.z, P1.w),
+                   ax = make_float2(P2.x, P2.y), ay = make_float2(P2.z, P2.w),
+                   az = make_float2(P3.x, P3.y), mx = make_float2(P3.z, P3.w),
+                   my = make_float2(P4.x, P4.y), mz = make_float2(P4.z, P4.w);
+#pragma unroll
       for (int i = 0; i < UV2_PPT; ++i) {
-        if (!nearp[i]) continue;
-        for (int u = 0; u < m; ++u) {
-          const float *pk = &s_pk[u >> 1][u & 1];
-          const float dx = px[i] + pk[0], dy = py[i] + pk[2], dz = pz[i] + pk[4], s2 = pk[6];
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, s2)));
-          if (!(r2 < UV2_CLOSE * s2)) continue;
-          const size_t qq = (size_t)q0 + u;
-          const uint32_t o = perm[qq];
-          const double ddx = pos[i][0] - X[qq], ddy = pos[i][1] - X[(size_t)n + qq],
-                       ddz = pos[i][2] - X[2 * (size_t)n + qq];
-          const double r = rv[o], mg = mag[o];
-          const double rr = ddx * ddx + ddy * ddy + ddz * ddz + r * r;
-          const double ir = rsqrt_hh(rr);
-          const double cc = -ir * ir * ir;
-          const double ax = mg * dir[3 * (size_t)o], ay = mg * dir[3 * (size_t)o + 1],
-                       az = mg * dir[3 * (size_t)o + 2];
-          v[i][0] += cc * (ddy * az - ddz * ay);
-          v[i][1] += cc * (ddz * ax - ddx * az);
-          v[i][2] += cc * (ddx * ay - ddy * ax);
-        }
+        const float2 dx = __fadd2_rn(make_float2(px[i], px[i]), nx),
+                     dy = __fadd2_rn(make_float2(py[i], py[i]), ny),
+                     dz = __fadd2_rn(make_float2(pz[i], pz[i]), nz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
+        const float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+        const float2 c = __fmul2_rn(__fmul2_rn(ir, ir), ir);
+        const float2 cx = __fmul2_rn(c, dx), cy = __fmul2_rn(c, dy), cz = __fmul2_rn(c, dz);
+        // c (d x alpha)
+        V[i][0] = __ffma2_rn(cy, az, __ffma2_rn(cz, my, V[i][0]));
+        V[i][1] = __ffma2_rn(cz, ax, __ffma2_rn(cx, mz, V[i][1]));
+        V[i][2] = __ffma2_rn(cx, ay, __ffma2_rn(cy, mx, V[i][2]));
       }
     }
     // velocity kernel coefficient is -1/rho^3
@@ -1005,8 +928,7 @@ int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, i
       DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
                                                 st));
       k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, rv, X, F);
-      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uv, v_out, dir, mag,
-                                            rv);
+      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uv);
     } else {
       k_uvort<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, rv, chunk, uv);
     }
@@ -1099,8 +1021,7 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
       DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
                                                 st));
       k_uv_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, r_vortex, X, F);
-      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uvort, v_out, dir, mag,
-                                            r_vortex);
+      k_uvort_sorted<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uvort);
     } else {
       k_uvort<<<grd, UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, r_vortex, chunk, uvort);
     }

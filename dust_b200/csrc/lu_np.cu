@@ -13,14 +13,19 @@
 // needs no column-by-column barrier across the matrix and the whole
 // factorisation is blocks and GEMMs:
 //
-//   for each block column k (NP_NB wide):
+//   for each outer panel of NP_NBO columns, for each block column k (NP_NB
+//   wide) in it:
 //     k_np_diag   one CTA: unpivoted LU of the diagonal block in shared
 //                 memory, its inverse triangles Linv (unit lower) and Uinv
 //                 (upper) by substitution, max |l| of the block;
-//     k_np_panel  L21 = A21 Uinv (row tiles) and U12 = Linv A12 (column
-//                 tiles), 64 x 64 register-tiled products, max |l| of L21;
-//     trailing    A22 -= L21 U12 (tcgen05 TF32 GEMM for FP32, DGEMM for
-//                 FP64).
+//     k_np_panel  L21 = A21 Uinv (row tiles, down to n) and U12 = Linv A12
+//                 (column tiles, inside the outer panel), 64 x 64
+//                 register-tiled products, max |l| of L21;
+//     update      of the outer panel's own columns;
+//   then the outer panel's U12 right of it (forward substitution over its
+//   blocks with Linv) and the trailing update A22 -= L21 U12 of inner
+//   dimension NP_NBO (tcgen05 TF32 GEMM for FP32, DGEMM for FP64), which
+//   streams the trailing matrix a quarter as often as NP_NB-wide steps.
 //
 // The largest |l| is kept as float bits (monotone for non-negative values)
 // with atomicMax.  The caller accepts the factors when it is below
@@ -42,6 +47,7 @@
   } while (0)
 
 #define NP_NB 64
+#define NP_NBO 256  // outer panel width (a multiple of NP_NB)
 #define NP_T 256
 #define NP_LD (NP_NB + 1)
 
@@ -68,19 +74,21 @@ __global__ void __launch_bounds__(NP_T) k_np_diag(T *A, int lda, int k, int jb, 
   __syncthreads();
   float lm = 0.f;
   bool zero = false;
+  // thread (row i, column phase cp) forms its row's multiplier itself and
+  // updates its columns; the multiplier is stored into column j only after
+  // the step's barrier (no later step reads column j), so one barrier per
+  // column suffices
   const int i = tid & (NP_NB - 1), cp = tid / NP_NB;  // row, column phase (0..3)
+  T lprev = (T)0;
   for (int j = 0; j < jb; ++j) {
+    if (j > 0 && cp == 0 && i > j - 1 && i < jb) a[i * NP_LD + j - 1] = lprev;
     const T piv = a[j * NP_LD + j];
     if (piv == (T)0) zero = true;
-    if (cp == 0 && i > j && i < jb) {
-      const T l = a[i * NP_LD + j] / piv;
-      a[i * NP_LD + j] = l;
-      lm = fmaxf(lm, (float)fabs((double)l));
-    }
-    __syncthreads();
     if (i > j && i < jb) {
-      const T l = a[i * NP_LD + j];
+      const T l = a[i * NP_LD + j] / piv;
       for (int c = j + 1 + cp; c < jb; c += NP_T / NP_NB) a[i * NP_LD + c] -= l * a[j * NP_LD + c];
+      lprev = l;
+      if (cp == 0) lm = fmaxf(lm, (float)fabs((double)l));
     }
     __syncthreads();
   }
@@ -88,21 +96,29 @@ __global__ void __launch_bounds__(NP_T) k_np_diag(T *A, int lda, int k, int jb, 
   // max |l| of the block (CTA reduction through one shared word)
   for (int o = 16; o > 0; o >>= 1) lm = fmaxf(lm, __shfl_xor_sync(0xffffffffu, lm, o));
   if ((tid & 31) == 0) atomicMax((unsigned *)&s_lmax, __float_as_uint(lm));
-  // inverse triangles, one column per thread: threads [0, jb) Uinv, [64, 64 + jb) Linv
-  if (tid < jb) {
-    const int c = tid;
-    for (int r = c; r >= 0; --r) {
-      T s = (r == c) ? (T)1 : (T)0;
-      for (int p = r + 1; p <= c; ++p) s -= a[r * NP_LD + p] * inv[p * NP_LD + c];
-      inv[r * NP_LD + c] = s / a[r * NP_LD + r];
+  // inverse triangles by substitution, one column per group of 4 lanes (the
+  // dot products split over the group, summed by shuffles): Uinv column c
+  // from row c up, then Linv column c from row c down
+  {
+    const int c = tid >> 2, q = tid & 3;
+    const bool on = c < jb;
+    for (int r = NP_NB - 1; r >= 0; --r) {
+      T part = (T)0;
+      if (on && r <= c)
+        for (int p = r + 1 + q; p <= c; p += 4) part += a[r * NP_LD + p] * inv[p * NP_LD + c];
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      if (on && r <= c && q == 0) inv[r * NP_LD + c] = ((r == c ? (T)1 : (T)0) - part) / a[r * NP_LD + r];
+      __syncwarp();
     }
-  } else if (tid >= NP_NB && tid < NP_NB + jb) {
-    const int c = tid - NP_NB;
-    linv[c * NP_LD + c] = (T)1;
-    for (int r = c + 1; r < jb; ++r) {
-      T s = (T)0;
-      for (int p = c; p < r; ++p) s -= a[r * NP_LD + p] * linv[p * NP_LD + c];
-      linv[r * NP_LD + c] = s;
+    for (int r = 0; r < NP_NB; ++r) {
+      T part = (T)0;
+      if (on && r > c)
+        for (int p = c + q; p < r; p += 4) part += a[r * NP_LD + p] * linv[p * NP_LD + c];
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      if (on && r >= c && r < jb && q == 0) linv[r * NP_LD + c] = r == c ? (T)1 : -part;
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -115,14 +131,15 @@ __global__ void __launch_bounds__(NP_T) k_np_diag(T *A, int lda, int k, int jb, 
   if (tid == 0) np_note_lmax(lmax_bits, s_lmax);
 }
 
-// 64 x 64 tiles of the panel: blocks [0, nrb) take 64 rows of A21 and write
-// A21 Uinv over them; blocks [nrb, nrb + ncb) take 64 columns of A12 and
-// write Linv A12.  Each thread computes a 4 x 4 piece of the tile from the
-// two shared operands (the tile and the inverse triangle).
+// 64 x 64 tiles of the panel: blocks [0, nrb) take 64 rows of A21 (rows
+// below the block, to n) and write A21 Uinv over them; blocks [nrb, nrb + ncb)
+// take 64 columns of A12 (rows of the block, columns [cbeg, cend)) and write
+// Linv A12.  Each thread computes a 4 x 4 piece of the tile from the two
+// shared operands (the tile and the inverse triangle).
 template <typename T>
 __global__ void __launch_bounds__(NP_T) k_np_panel(T *A, int lda, int n, int k, int jb,
                                                    const T *Linv, const T *Uinv, int nrb,
-                                                   unsigned *lmax_bits) {
+                                                   int cbeg, int cend, unsigned *lmax_bits) {
   extern __shared__ __align__(16) unsigned char np_sm[];
   T *x = (T *)np_sm;            // 64 x 64 operand tile, [row][col], ld NP_LD
   T *w = x + NP_NB * NP_LD;     // 64 x 64 inverse, [row][col], ld NP_LD
@@ -130,9 +147,9 @@ __global__ void __launch_bounds__(NP_T) k_np_panel(T *A, int lda, int n, int k, 
   const bool rows = (int)blockIdx.x < nrb;
   const int b = rows ? blockIdx.x : blockIdx.x - nrb;
   const int r0 = rows ? k + jb + NP_NB * b : k;      // first row of the tile in A
-  const int c0 = rows ? k : k + jb + NP_NB * b;      // first column of the tile in A
+  const int c0 = rows ? k : cbeg + NP_NB * b;        // first column of the tile in A
   const int nr = rows ? min(NP_NB, n - r0) : jb;
-  const int nc = rows ? jb : min(NP_NB, n - c0);
+  const int nc = rows ? jb : min(NP_NB, cend - c0);
   const T *W = rows ? Uinv : Linv;
   for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
     const int r = e % NP_NB, c = e / NP_NB;
@@ -229,21 +246,41 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
     attr = true;
   }
   CUBLAS_CHECK(cublasSetStream(cb, st));
-  for (int k = 0; k < n; k += NP_NB) {
-    const int jb = std::min(NP_NB, n - k), m2 = n - k - jb;
-    T *Linv = inv0 + 2 * tri * (size_t)(k / NP_NB), *Uinv = Linv + tri;
-    k_np_diag<T><<<1, NP_T, smd, st>>>(A, lda, k, jb, Linv, Uinv, bits);
-    if (m2 > 0) {
-      const int nrb = (m2 + NP_NB - 1) / NP_NB;
-      k_np_panel<T><<<2 * nrb, NP_T, smp, st>>>(A, lda, n, k, jb, Linv, Uinv, nrb, bits);
-      T *L21 = A + (k + jb) + (size_t)k * lda, *U12 = A + k + (size_t)(k + jb) * lda,
-        *A22 = A + (k + jb) + (size_t)(k + jb) * lda;
-      if (sizeof(T) == 4 && gemm_update == 1) {
-        DUST_TRY(gemm_tf32_minus(st, m2, m2, jb, (const float *)L21, lda, (const float *)U12,
-                                 lda, (float *)A22, lda));
-      } else {
-        CUBLAS_CHECK(np_gemm_minus(cb, m2, m2, jb, L21, lda, U12, lda, A22, lda));
+  // C -= A B (m x nn, inner kk) on the tensor cores (FP32) or DGEMM
+  auto update = [&](int m, int nn, int kk, const T *Am, const T *Bm, T *Cm) -> int {
+    if (m <= 0 || nn <= 0 || kk <= 0) return DUST_OK;
+    if (sizeof(T) == 4 && gemm_update == 1)
+      return gemm_tf32_minus(st, m, nn, kk, (const float *)Am, lda, (const float *)Bm, lda,
+                             (float *)Cm, lda);
+    CUBLAS_CHECK(np_gemm_minus(cb, m, nn, kk, Am, lda, Bm, lda, Cm, lda));
+    return DUST_OK;
+  };
+  auto at = [&](int r, int c) { return A + r + (size_t)c * lda; };
+  // two levels: outer panels of NP_NBO columns factored in NP_NB steps that
+  // update only the panel's own columns; then the panel's U12 (its unit lower
+  // block's forward substitution, with the kept inverse triangles) and one
+  // trailing update of inner dimension NP_NBO
+  for (int K = 0; K < n; K += NP_NBO) {
+    const int Ke = std::min(K + NP_NBO, n);
+    for (int k = K; k < Ke; k += NP_NB) {
+      const int jb = std::min(NP_NB, n - k), m2 = n - k - jb, wc = Ke - k - jb;
+      T *Linv = inv0 + 2 * tri * (size_t)(k / NP_NB), *Uinv = Linv + tri;
+      k_np_diag<T><<<1, NP_T, smd, st>>>(A, lda, k, jb, Linv, Uinv, bits);
+      const int nrb = (m2 + NP_NB - 1) / NP_NB, ncb = (wc + NP_NB - 1) / NP_NB;
+      if (nrb + ncb > 0)
+        k_np_panel<T><<<nrb + ncb, NP_T, smp, st>>>(A, lda, n, k, jb, Linv, Uinv, nrb, k + jb,
+                                                     Ke, bits);
+      DUST_TRY(update(m2, wc, jb, at(k + jb, k), at(k, k + jb), at(k + jb, k + jb)));
+    }
+    if (Ke < n) {
+      const int ncb = (n - Ke + NP_NB - 1) / NP_NB;
+      for (int k = K; k < Ke; k += NP_NB) {
+        const T *Linv = inv0 + 2 * tri * (size_t)(k / NP_NB);
+        k_np_panel<T><<<ncb, NP_T, smp, st>>>(A, lda, n, k, NP_NB, Linv, Linv, 0, Ke, n, bits);
+        DUST_TRY(update(Ke - k - NP_NB, n - Ke, NP_NB, at(k + NP_NB, k), at(k, Ke),
+                        at(k + NP_NB, Ke)));
       }
+      DUST_TRY(update(n - Ke, n - Ke, Ke - K, at(Ke, K), at(K, Ke), at(Ke, Ke)));
     }
   }
   if (ipiv) k_np_ipiv<<<(n + 255) / 256, 256, 0, st>>>(n, ipiv);
@@ -257,69 +294,136 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
   return DUST_OK;
 }
 
-// Block substitution with the kept inverse triangles: one launch per 64-row
-// block i (forward: i ascending with Linv, backward: descending with Uinv).
-// Every CTA of the launch recomputes Y_i = Inv_i B_i (64 x 64 by 64 x NP_RC,
-// from B's block i, which no CTA of the launch writes), and then updates its
-// 64 rows of the not yet solved part, B_r -= A_(r,i) Y_i; CTA 0 also stores
-// Y_i into X.  Grid: (row tiles, RHS chunks of NP_RC columns).
-#define NP_RC 32
+// Block substitution with the kept inverse triangles, one cooperative launch
+// per triangle (forward: blocks i ascending with Linv; backward: descending
+// with Uinv).  At step i every CTA computes Y_i = Inv_i B_i for a chunk of
+// NP_NB right-hand sides (B's block i is final: every earlier step ended at a
+// grid barrier) and then updates its share of the 64-row tiles not yet
+// solved, B_r -= A_(r,i) Y_i; CTA 0 stores Y_i into X.  The grid barrier
+// spins with an iteration limit and raises the error word instead of
+// hanging; every CTA then stops at the same step.
+#define NP_SPIN_LIMIT (1ll << 24)
+
+__device__ __forceinline__ bool np_grid_barrier(unsigned *bar, unsigned G, int *err) {
+  __syncthreads();
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    volatile unsigned *vgen = bar + 1;
+    const unsigned g0 = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == G - 1u) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*vgen == g0) {
+        if (++it > NP_SPIN_LIMIT || *(volatile int *)err) {
+          atomicExch(err, 1);
+          s_fail = 1;
+          break;
+        }
+        if (it > 64) __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_fail == 0;
+}
+
+// out (64 x 64) of thread (ty, tx): rows 4 ty .., columns 4 tx .. of L R, both
+// [row][col] with ld NP_LD in shared memory
+template <typename T>
+__device__ __forceinline__ void np_mm64(const T *L, const T *R, int ty, int tx, T (&acc)[4][4]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = (T)0;
+#pragma unroll 4
+  for (int p = 0; p < NP_NB; ++p) {
+    T lv[4], rv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) lv[u] = L[(4 * ty + u) * NP_LD + p];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) rv[v] = R[p * NP_LD + 4 * tx + v];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(lv[u], rv[v], acc[u][v]);
+  }
+}
+
 template <typename T, bool FWD>
 __global__ void __launch_bounds__(NP_T) k_np_subst(const T *A, int lda, int n, int nrhs,
-                                                   int i, const T *Inv, T *B, int ldb, T *X,
-                                                   int ldx) {
+                                                   const T *Inv, T *B, int ldb, T *X, int ldx,
+                                                   unsigned *bar, int *err) {
   extern __shared__ __align__(16) unsigned char np_sm[];
-  T *w = (T *)np_sm;                // 64 x 64 inverse, [row][col], ld NP_LD
-  T *b = w + NP_NB * NP_LD;         // 64 x NP_RC block i of B, [row][col]
-  T *y = b + NP_NB * (NP_RC + 1);   // 64 x NP_RC Y_i
-  T *l = y + NP_NB * (NP_RC + 1);   // 64 x 64 coupling tile A_(r,i), [row][col]
-  const int tid = threadIdx.x;
-  const int k = i * NP_NB, jb = min(NP_NB, n - k);
-  const int c0 = blockIdx.y * NP_RC, nc = min(NP_RC, nrhs - c0);
-  const T *W = Inv + 2 * (size_t)NP_NB * NP_NB * i + (FWD ? 0 : (size_t)NP_NB * NP_NB);
-  for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
-    const int r = e % NP_NB, c = e / NP_NB;
-    w[r * NP_LD + c] = (r < jb && c < jb) ? W[r + (size_t)c * NP_NB] : (T)0;
-  }
-  for (int e = tid; e < NP_NB * NP_RC; e += NP_T) {
-    const int r = e % NP_NB, c = e / NP_NB;
-    b[r * (NP_RC + 1) + c] = (r < jb && c < nc) ? B[(size_t)(k + r) + (size_t)(c0 + c) * ldb] : (T)0;
-  }
-  __syncthreads();
-  // Y_i = Inv_i B_i: thread (r, c-phase) computes y[r][c] for c = cp, cp + 8, ...
-  {
-    const int r = tid % NP_NB, cp = tid / NP_NB;
-    for (int c = cp; c < NP_RC; c += NP_T / NP_NB) {
-      T acc = (T)0;
-      for (int p = 0; p < NP_NB; ++p) acc = fma(w[r * NP_LD + p], b[p * (NP_RC + 1) + c], acc);
-      y[r * (NP_RC + 1) + c] = acc;
-    }
-  }
-  __syncthreads();
-  if (blockIdx.x == 0)
-    for (int e = tid; e < NP_NB * NP_RC; e += NP_T) {
-      const int r = e % NP_NB, c = e / NP_NB;
-      if (r < jb && c < nc) X[(size_t)(k + r) + (size_t)(c0 + c) * ldx] = y[r * (NP_RC + 1) + c];
-    }
-  // rows still to solve: below the block (forward) or above it (backward)
-  const int nrest = FWD ? n - k - jb : k;
-  const int ntile = (nrest + NP_NB - 1) / NP_NB;
-  if ((int)blockIdx.x >= ntile) return;
-  const int r0 = FWD ? k + jb + NP_NB * blockIdx.x : NP_NB * blockIdx.x;
-  const int nr = min(NP_NB, (FWD ? n : k) - r0);
-  for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
-    const int r = e % NP_NB, c = e / NP_NB;
-    l[r * NP_LD + c] = (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
-  }
-  __syncthreads();
-  {
-    const int r = tid % NP_NB, cp = tid / NP_NB;
-    if (r < nr)
-      for (int c = cp; c < nc; c += NP_T / NP_NB) {
-        T acc = (T)0;
-        for (int p = 0; p < NP_NB; ++p) acc = fma(l[r * NP_LD + p], y[p * (NP_RC + 1) + c], acc);
-        B[(size_t)(r0 + r) + (size_t)(c0 + c) * ldb] -= acc;
+  T *w = (T *)np_sm;               // Inv_i
+  T *b = w + NP_NB * NP_LD;        // B_i (a chunk of right-hand sides)
+  T *y = b + NP_NB * NP_LD;        // Y_i
+  T *l = y + NP_NB * NP_LD;        // A_(r,i)
+  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+  const unsigned G = gridDim.x;
+  const int nb = (n + NP_NB - 1) / NP_NB;
+  for (int s = 0; s < nb; ++s) {
+    const int i = FWD ? s : nb - 1 - s;
+    const int k = i * NP_NB, jb = min(NP_NB, n - k);
+    const T *W = Inv + 2 * (size_t)NP_NB * NP_NB * i + (FWD ? 0 : (size_t)NP_NB * NP_NB);
+    const int nrest = FWD ? n - k - jb : k;
+    const int ntile = (nrest + NP_NB - 1) / NP_NB;
+    for (int c0 = 0; c0 < nrhs; c0 += NP_NB) {
+      const int nc = min(NP_NB, nrhs - c0);
+      __syncthreads();
+      for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+        const int r = e % NP_NB, c = e / NP_NB;
+        w[r * NP_LD + c] = (r < jb && c < jb) ? W[r + (size_t)c * NP_NB] : (T)0;
+        // B changes between steps on other SMs: read it past L1
+        b[r * NP_LD + c] =
+            (r < jb && c < nc) ? __ldcg(B + (size_t)(k + r) + (size_t)(c0 + c) * ldb) : (T)0;
       }
+      __syncthreads();
+      T acc[4][4];
+      np_mm64(w, b, ty, tx, acc);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) y[(4 * ty + u) * NP_LD + 4 * tx + v] = acc[u][v];
+      __syncthreads();
+      if (blockIdx.x == 0)
+        for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+          const int r = e % NP_NB, c = e / NP_NB;
+          if (r < jb && c < nc) X[(size_t)(k + r) + (size_t)(c0 + c) * ldx] = y[r * NP_LD + c];
+        }
+      for (int tile = blockIdx.x; tile < ntile; tile += G) {
+        const int r0 = FWD ? k + jb + NP_NB * tile : NP_NB * tile;
+        const int nr = min(NP_NB, (FWD ? n : k) - r0);
+        __syncthreads();
+        for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+          const int r = e % NP_NB, c = e / NP_NB;
+          l[r * NP_LD + c] = (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
+        }
+        __syncthreads();
+        np_mm64(l, y, ty, tx, acc);
+        // through shared memory, then coalesced along the columns
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) l[(4 * ty + u) * NP_LD + 4 * tx + v] = acc[u][v];
+        __syncthreads();
+        for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+          const int r = e % NP_NB, c = e / NP_NB;
+          if (r < nr && c < nc) {
+            T *bp = B + (size_t)(r0 + r) + (size_t)(c0 + c) * ldb;
+            *bp = __ldcg(bp) - l[r * NP_LD + c];
+          }
+        }
+      }
+    }
+    if (!np_grid_barrier(bar, G, err)) return;
   }
 }
 
@@ -327,34 +431,46 @@ template <typename T>
 int lu_getrs_nopiv(cudaStream_t st, LuWork &w, int n, int nrhs, const T *A, int lda, T *B,
                    int ldb) {
   if (n <= 0 || nrhs <= 0) return DUST_OK;
-  const int nb = (n + NP_NB - 1) / NP_NB;
   const T *inv0 = (const T *)((const char *)w.np.p + 256);
   const size_t xb = (size_t)n * nrhs * sizeof(T);
-  DUST_TRY(devbuf_grow(w.np_x, xb));
-  T *X = (T *)w.np_x.p;
-  const int sm = (2 * NP_NB * NP_LD + 2 * NP_NB * (NP_RC + 1)) * (int)sizeof(T);
-  static bool attr = false;  // per element type
-  if (!attr) {
+  DUST_TRY(devbuf_grow(w.np_x, xb + 256));
+  T *X = (T *)((char *)w.np_x.p + 256);
+  unsigned *bar = (unsigned *)w.np_x.p;  // arrivals, generation, error word
+  int *err = (int *)(bar + 2);
+  const int sm = 4 * NP_NB * NP_LD * (int)sizeof(T);
+  static int G = 0;  // co-resident CTAs, per element type
+  if (G == 0) {
     DUST_CUDA(cudaFuncSetAttribute(k_np_subst<T, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     DUST_CUDA(cudaFuncSetAttribute(k_np_subst<T, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    attr = true;
+    int dev = 0, nsm = 0, per = 0;
+    DUST_CUDA(cudaGetDevice(&dev));
+    DUST_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    DUST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_np_subst<T, true>, NP_T, sm));
+    G = std::max(1, nsm * std::max(per, 1));
   }
-  const unsigned gy = (unsigned)((nrhs + NP_RC - 1) / NP_RC);
-  // L Y = B: Y into X
-  for (int i = 0; i < nb; ++i) {
-    const int below = n - (i + 1) * NP_NB;
-    const unsigned gx = (unsigned)std::max(1, (below + NP_NB - 1) / NP_NB);
-    k_np_subst<T, true><<<dim3(gx, gy), NP_T, sm, st>>>(A, lda, n, nrhs, i, inv0, B, ldb, X, n);
+  const int nb = (n + NP_NB - 1) / NP_NB;
+  const int g = std::min(G, std::max(1, nb - 1));
+  DUST_CUDA(cudaMemsetAsync(bar, 0, 16, st));
+  // L Y = B: Y into X; U X = Y: X back into B
+  int ldn = n;
+  {
+    void *args[] = {(void *)&A, (void *)&lda, (void *)&n, (void *)&nrhs, (void *)&inv0,
+                    (void *)&B, (void *)&ldb, (void *)&X, (void *)&ldn, (void *)&bar, (void *)&err};
+    DUST_CUDA(cudaLaunchCooperativeKernel((void *)k_np_subst<T, true>, dim3(g), dim3(NP_T), args,
+                                          sm, st));
   }
-  // U X = Y: X back into B
-  for (int i = nb - 1; i >= 0; --i) {
-    const unsigned gx = (unsigned)std::max(1, i);
-    k_np_subst<T, false><<<dim3(gx, gy), NP_T, sm, st>>>(A, lda, n, nrhs, i, inv0, X, n, B, ldb);
+  {
+    void *args[] = {(void *)&A, (void *)&lda, (void *)&n, (void *)&nrhs, (void *)&inv0,
+                    (void *)&X, (void *)&ldn, (void *)&B, (void *)&ldb, (void *)&bar, (void *)&err};
+    DUST_CUDA(cudaLaunchCooperativeKernel((void *)k_np_subst<T, false>, dim3(g), dim3(NP_T), args,
+                                          sm, st));
   }
-  DUST_CUDA(cudaGetLastError());
-  return DUST_OK;
+  int herr = 0;
+  DUST_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
+  return herr ? DUST_ERR_TIMEOUT : DUST_OK;
 }
 
 template int lu_getrs_nopiv<double>(cudaStream_t, LuWork &, int, int, const double *, int,
