@@ -71,6 +71,9 @@ def parse():
                          "FP64 step with the direct sum is timed as well)")
     ap.add_argument("--no-advect", action="store_true",
                     help="leave the particles in place (no complete_wake particle update)")
+    ap.add_argument("--modes", default="",
+                    help="comma-separated subset of the step modes to run (plain always "
+                         "runs: it is the reference of the load errors); default all")
     ap.add_argument("--accuracy-steps", type=int, default=20,
                     help="advected steps over which every mode's loads are compared with "
                          "the plain FP64 run (warm-up + timed + untimed steps)")
@@ -362,7 +365,7 @@ def main():
     modes = [("plain", abi.DUST_SOLVE_LU64), ("mixed", abi.DUST_SOLVE_MIXED),
              ("mixed_f64uvort", abi.DUST_SOLVE_MIXED)]
     learned = None
-    if not args.no_learned:
+    if not args.no_learned and (not args.modes or "learned" in args.modes.split(",")):
         # the learned preconditioner trains (untimed) on the plain solutions
         # of the same geometry at rotor azimuths other than the benchmarked one
         from dust_b200 import precond
@@ -379,6 +382,10 @@ def main():
         # FP64's own sensitivity: the plain step from particle positions
         # moved by 1e-12 (seeded), advected like the others
         modes.append(("plain_perturbed", abi.DUST_SOLVE_LU64))
+    if args.modes:
+        # (a profiling run, --profile-step, needs no reference mode)
+        keep = set(args.modes.split(",")) | (set() if args.profile_step else {"plain"})
+        modes = [m for m in modes if m[0] in keep]
     results = {}
     steppers = {}
     by_step = {}
@@ -925,11 +932,15 @@ def roofline(ph, case, params, best):
     hbm = peaks.get("hbm_gbs", 6650.0)
     hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
     p = ph.get(best, {})
+    # FMM kernels are FP64 in the plain modes; the direct uvort sum also in
+    # mixed_f64uvort
     f64 = best.startswith("plain")
+    uv64 = f64 or best == "mixed_f64uvort"
     w = 8 if f64 else 4
     simt = fp64_peak if f64 else fp32_peak
-    simt_name = "nominal %s SIMT (148 SMs x %d x 2 x %g MHz)" % ("FP64" if f64 else "FP32",
-                                                                  64 if f64 else 128, mhz)
+    name_of = lambda d: "nominal %s SIMT (148 SMs x %d x 2 x %g MHz)" % (
+        "FP64" if d else "FP32", 64 if d else 128, mhz)
+    simt_name = name_of(f64)
     n = case.mag.shape[0]
     ks = []
     if p.get("k_elem_far_ms"):
@@ -967,11 +978,12 @@ def roofline(ph, case, params, best):
     if p.get("uvort"):
         pairs = case.rank * n
         a = FLOP_UVORT_PAIR * pairs / (p["uvort"] * 1e-3) / 1e12
-        ks.append({"kernel": "uvort phase (%s)" % ("k_uvort" if f64 else "k_uvort_sorted + sort"),
-                   "bound": "fp64" if f64 else "fp32", "achieved": round(a, 2),
-                   "peak": round(simt, 1), "unit": "TFLOP/s", "frac": round(a / simt, 3),
-                   "traffic": None, "peak_source": simt_name, "flop_per_pair": FLOP_UVORT_PAIR,
-                   "pairs": pairs, "ms": p["uvort"]})
+        pk_uv = fp64_peak if uv64 else fp32_peak
+        ks.append({"kernel": "uvort phase (%s)" % ("k_uvort" if uv64 else "k_uvort_sorted + sort"),
+                   "bound": "fp64" if uv64 else "fp32", "achieved": round(a, 2),
+                   "peak": round(pk_uv, 1), "unit": "TFLOP/s", "frac": round(a / pk_uv, 3),
+                   "traffic": None, "peak_source": name_of(uv64),
+                   "flop_per_pair": FLOP_UVORT_PAIR, "pairs": pairs, "ms": p["uvort"]})
     if not ks:
         return {"others": [], "peaks_file": bool(peaks)}
     ks.sort(key=lambda k: -k["ms"])
