@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--workload", default="full", choices=["full", "fmm", "dense", "learned"],
                     help="full: the full-step line (with the fmm and dense workloads as "
                          "sub-objects); fmm / dense: that workload's own line")
+    ap.add_argument("--dense-panels", type=int, default=16384,
+                    help="panels of the dense-solve workload's ellipsoid (smaller for "
+                         "profiling captures)")
     ap.add_argument("--no-workloads", action="store_true",
                     help="full step only, without the fmm / dense sub-objects")
     ap.add_argument("--degrees", default="4,6,8", help="FMM degrees of the fmm workload")
@@ -848,10 +851,11 @@ def workload_line(args, ws, name):
         dtype = "f64 GMRES with f32 preconditioner"
     else:
         with Clocks(0) as clk:
-            w = run_dense_workload(args.steps, warm)
+            w = run_dense_workload(args.steps, warm, n_target=args.dense_panels)
         best = w["results"]["mixed"]
         plain = w["results"]["lu64"]
-        metric = "ms per dense solve (16,384-panel ellipsoid, 64 RHS), MIXED vs LU64"
+        metric = "ms per dense solve (%s-panel ellipsoid, 64 RHS), MIXED vs LU64" % format(
+            args.dense_panels, ",")
         rf = dict(best["roofline"])
         rf["kernel"] = "FP32 LU with tcgen05 TF32 trailing updates"
         rf["traffic"] = None

@@ -687,14 +687,19 @@ int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
 
 // FP64 uvort (plain mode): particles in the caller's order, UVD_PPT points
 // per thread (consecutive CTA slices of UV2_T points) against a shared tile
-// of (x, y, z, r_v^2, alpha) records; the reciprocal square root as in
-// k_elem_out (FP32 seed, one Householder step in FP64).
+// of (x, y, z, r_v^2, alpha, w = x x alpha) records; the reciprocal square
+// root as in k_elem_out (FP32 seed, one Householder step in FP64).  With
+// c = rho^-3 the tile's sum is
+//   sum_q c_q (p - x_q) x alpha_q = p x (sum_q c_q alpha_q) - sum_q c_q w_q,
+// two 3-vector FMA accumulations per pair instead of a cross product and its
+// accumulation; in FP64 the difference of the two sums costs at most about
+// 1e-13 relative for a point very close to a particle.
 #define UVD_PPT 4
 __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, int n,
                                                  const double *cen, const double *dir,
                                                  const double *mag, const double *rv,
                                                  int chunk, double *uv) {
-  __shared__ __align__(16) double s_q[UV2_TILE][8];
+  __shared__ __align__(16) double s_q[UV2_TILE][10];
   const int t0 = blockIdx.x * UV2_T * UVD_PPT + threadIdx.x;
   const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
   double pos[UVD_PPT][3], v[UVD_PPT][3];
@@ -713,27 +718,43 @@ __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, in
     if (threadIdx.x < m) {
       const double mg = mag[q], r = rv[q];
       double *w = s_q[threadIdx.x];
-      for (int c = 0; c < 3; ++c) w[c] = cen[3 * (size_t)q + c];
-      w[3] = r * r;
-      for (int c = 0; c < 3; ++c) w[4 + c] = mg * dir[3 * (size_t)q + c];
-      w[7] = 0.0;
+      const double x = cen[3 * (size_t)q], y = cen[3 * (size_t)q + 1], z = cen[3 * (size_t)q + 2];
+      const double ax = mg * dir[3 * (size_t)q], ay = mg * dir[3 * (size_t)q + 1],
+                   az = mg * dir[3 * (size_t)q + 2];
+      w[0] = x, w[1] = y, w[2] = z, w[3] = r * r;
+      w[4] = ax, w[5] = ay, w[6] = az;
+      w[7] = y * az - z * ay, w[8] = z * ax - x * az, w[9] = x * ay - y * ax;
     }
     __syncthreads();
+    double A[UVD_PPT][3], W[UVD_PPT][3];
+#pragma unroll
+    for (int i = 0; i < UVD_PPT; ++i)
+      for (int c = 0; c < 3; ++c) A[i][c] = W[i][c] = 0.0;
 #pragma unroll 2
     for (int u = 0; u < m; ++u) {
       const double2 *w = (const double2 *)s_q[u];
-      const double2 X = w[0], Y = w[1], Z = w[2], W = w[3];
-      // X = (x, y), Y = (z, r_v^2), Z = (ax, ay), W = (az, -)
+      const double2 X = w[0], Y = w[1], Z = w[2], P = w[3], Q = w[4];
+      // X = (x, y), Y = (z, r_v^2), Z = (ax, ay), P = (az, wx), Q = (wy, wz)
 #pragma unroll
       for (int i = 0; i < UVD_PPT; ++i) {
         const double dx = pos[i][0] - X.x, dy = pos[i][1] - X.y, dz = pos[i][2] - Y.x;
-        const double r2 = dx * dx + dy * dy + dz * dz + Y.y;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, Y.y)));
         const double ir = rsqrt_hh(r2);
-        const double c = -ir * ir * ir;
-        v[i][0] = fma(c, dy * W.x - dz * Z.y, v[i][0]);
-        v[i][1] = fma(c, dz * Z.x - dx * W.x, v[i][1]);
-        v[i][2] = fma(c, dx * Z.y - dy * Z.x, v[i][2]);
+        const double c = ir * ir * ir;
+        A[i][0] = fma(c, Z.x, A[i][0]);
+        A[i][1] = fma(c, Z.y, A[i][1]);
+        A[i][2] = fma(c, P.x, A[i][2]);
+        W[i][0] = fma(c, P.y, W[i][0]);
+        W[i][1] = fma(c, Q.x, W[i][1]);
+        W[i][2] = fma(c, Q.y, W[i][2]);
       }
+    }
+    // velocity kernel coefficient is -1/rho^3
+#pragma unroll
+    for (int i = 0; i < UVD_PPT; ++i) {
+      v[i][0] -= pos[i][1] * A[i][2] - pos[i][2] * A[i][1] - W[i][0];
+      v[i][1] -= pos[i][2] * A[i][0] - pos[i][0] * A[i][2] - W[i][1];
+      v[i][2] -= pos[i][0] * A[i][1] - pos[i][1] * A[i][0] - W[i][2];
     }
   }
   const double k4pi = 1.0 / (4.0 * DUST_PI);

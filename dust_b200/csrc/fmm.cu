@@ -1042,7 +1042,7 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
 #define P2W_LQ 4  // levels whose near-field loads are issued together
 
 template <bool VS, bool DF, bool VD, bool TV, bool F32>
-__global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
+__global__ void __launch_bounds__(P2W_WARPS * 32, 5) k_p2p_w(FmmDev d) {
   using R = typename std::conditional<F32, float, double>::type;
   __shared__ R s_src[P2W_WARPS][P2W_NV][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
@@ -1120,7 +1120,8 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
   const double k4pi = 1.0 / (4.0 * DUST_PI);
   const double *bl = d.B + (size_t)ci * 3 * nm, *gl = d.Gx + (size_t)ci * 3 * nm1;
   // L2P of one target (FP64): velocity and the gradient of the local field
-  auto l2p = [&](uint32_t ti, double *lv, double *g) {
+  // (the monomials m0, m0 + ms, ... only: the caller splits the sum)
+  auto l2p = [&](uint32_t ti, int m0, int ms, double *lv, double *g) {
     const double x = d.P[ti] - cc[0], y = d.P[n + ti] - cc[1], z = d.P[2 * n + ti] - cc[2];
     double px[DUST_MAXP + 1], py[DUST_MAXP + 1], pz[DUST_MAXP + 1];
     px[0] = py[0] = pz[0] = 1.0;
@@ -1132,7 +1133,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
     }
     for (int e = 0; e < 3; ++e) lv[e] = 0.0;
     for (int e = 0; e < 9; ++e) g[e] = 0.0;
-    for (int m = 0; m < nm; ++m) {
+    for (int m = m0; m < nm; m += ms) {
       int mi, mj, mk;
       mono_exp(m, mi, mj, mk);
       const double pr = px[mi] * py[mj] * pz[mk];
@@ -1155,7 +1156,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
     double part = 0.0;
     for (int t = lane; t < nt; t += 32) {
       double lv[3], g[9];
-      l2p(lo + t, lv, g);
+      l2p(lo + t, 0, 1, lv, g);
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) {
           const double sy = 0.5 * (g[a + 3 * b] + g[b + 3 * a]);
@@ -1190,32 +1191,22 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
     if (F32)
       for (int e = 0; e < 12; ++e) acc[32 * e] = 0.0;
     int since = 0;
-    // the sources of the next tile are loaded into registers while the
-    // current tile is evaluated (the loads' latency hides behind the pairs)
-    double pv[7];
-    uint32_t psid = 0;
-    auto fetch = [&](uint32_t v) {
+    for (uint32_t s0 = 0; s0 < S; s0 += P2W_TILE) {
+      __syncwarp();
+      const uint32_t v = s0 + lane;
       if (v < S) {
         int a = 0, b = nr - 1;
         while (a < b) {  // last r with rcum[r] <= v
           const int mid = (a + b + 1) >> 1;
           if (rcum[mid] <= v) a = mid; else b = mid - 1;
         }
-        psid = rlo[a] + (v - rcum[a]);
-#pragma unroll
-        for (int q = 0; q < 7; ++q) pv[q] = d.P[(size_t)q * n + psid];
-      }
-    };
-    fetch((uint32_t)lane);
-    for (uint32_t s0 = 0; s0 < S; s0 += P2W_TILE) {
-      __syncwarp();
-      const uint32_t v = s0 + lane;
-      if (v < S) {
-        const uint32_t sidx = psid;
+        const uint32_t sidx = rlo[a] + (v - rcum[a]);
         s_sid[w][lane] = sidx;
-        for (int q = 0; q < 3; ++q) fs[q * P2W_TILE + lane] = F32 ? (R)(pv[q] - cc[q]) : (R)pv[q];
-        for (int q = 3; q < 6; ++q) fs[q * P2W_TILE + lane] = (R)pv[q];
-        const double rv = pv[6];
+        for (int q = 0; q < 3; ++q)
+          fs[q * P2W_TILE + lane] =
+              F32 ? (R)(d.P[(size_t)q * n + sidx] - cc[q]) : (R)d.P[(size_t)q * n + sidx];
+        for (int q = 3; q < 6; ++q) fs[q * P2W_TILE + lane] = (R)d.P[(size_t)q * n + sidx];
+        const double rv = d.P[(size_t)6 * n + sidx];
         if constexpr (F32) {
           const float s2 = (float)rv * (float)rv;
           fs[6 * P2W_TILE + lane] = s2;
@@ -1227,7 +1218,6 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
         }
       }
       __syncwarp();
-      fetch(s0 + P2W_TILE + lane);
       const int m = (int)min((uint32_t)P2W_TILE, S - s0);
       if (act)
         for (int u = grp; u < m; u += G) {
@@ -1272,10 +1262,22 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
         for (int g = 1; g < G; ++g) Q[e] += acc[32 * e + g * TPR];
     }
     __syncwarp();
+    // L2P (FP64) split over the groups: lane (tl, grp) sums the monomials
+    // grp, grp + G, ... of its target; group 0 adds the other groups' parts
+    double lv[3], g[9];
+    if (act) {
+      l2p(ti, grp, G, lv, g);
+      for (int e = 0; e < 3; ++e) acc[32 * e] = lv[e];
+      for (int e = 0; e < 9; ++e) acc[32 * (3 + e)] = g[e];
+    }
+    __syncwarp();
     if (act && grp == 0) {
+      for (int q = 1; q < G; ++q) {
+        for (int e = 0; e < 3; ++e) lv[e] += acc[32 * e + q * TPR];
+        for (int e = 0; e < 9; ++e) g[e] += acc[32 * (3 + e) + q * TPR];
+      }
       const double tad[3] = {d.P[3 * n + ti], d.P[4 * n + ti], d.P[5 * n + ti]};
-      double lv[3], g[9], ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
-      l2p(ti, lv, g);
+      double ls[3] = {0, 0, 0}, lr[3] = {0, 0, 0};
       if (VS) {
         for (int e = 0; e < 3; ++e) ls[e] = tad[0] * g[e] + tad[1] * g[e + 3] + tad[2] * g[e + 6];
         if (DF) {
@@ -1295,6 +1297,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
         d.out[(size_t)(6 + e) * n + ti] = lr[e] + Q[6 + e] * k4pi;
       }
     }
+    __syncwarp();  // acc is reused by the next 32 targets
   }
 }
 

@@ -55,80 +55,109 @@ __device__ __forceinline__ void np_note_lmax(unsigned *bits, float v) {
   atomicMax(bits, __float_as_uint(v));
 }
 
-// Diagonal block: shared a[i * NP_LD + c] (row-major, padded), then the two
-// inverse triangles; the block's LU and max |l| back to global memory.
+// Diagonal block.  Threads 0..63 hold one column each in registers (the
+// steps are unrolled, so every row index is a constant).  At step j the
+// owner of column j scales its rows below j by the reciprocal of the pivot
+// (as dgetf2 does) and publishes the multipliers in shared memory (two
+// buffers, so one barrier per step), and every later column subtracts its
+// row-j element times them.  The factored block then goes to shared memory
+// and the inverse triangles are solved one column per thread, Uinv by
+// threads 0..63 (back substitution) and Linv by threads 64..127 (forward
+// substitution), reading the factors as broadcasts; columns of the inverse
+// are zero above (Linv) or below (Uinv) the diagonal by the recurrences
+// themselves.  The block's LU, max |l| and the inverses go to global memory.
+#define NPD_T 128
 template <typename T>
-__global__ void __launch_bounds__(NP_T) k_np_diag(T *A, int lda, int k, int jb, T *Linv,
-                                                  T *Uinv, unsigned *lmax_bits) {
+__global__ void __launch_bounds__(NPD_T) k_np_diag(T *A, int lda, int k, int jb, T *Linv,
+                                                   T *Uinv, unsigned *lmax_bits) {
   extern __shared__ __align__(16) unsigned char np_sm[];
-  T *a = (T *)np_sm;                   // jb x jb, ld NP_LD
-  T *inv = a + NP_NB * NP_LD;          // Uinv | Linv, ld NP_LD (Uinv in columns 0..jb)
-  T *linv = inv + NP_NB * NP_LD;
-  __shared__ float s_lmax;
+  T *a = (T *)np_sm;                   // the block, [row][col], ld NP_LD
+  T *inv = a + NP_NB * NP_LD;          // Uinv, [row][col]
+  T *linv = inv + NP_NB * NP_LD;       // Linv, [row][col]
+  __shared__ T s_l[2][NP_NB];
+  __shared__ T s_rd[NP_NB];            // 1 / U(r, r)
   const int tid = threadIdx.x;
-  if (tid == 0) s_lmax = 0.f;
-  for (int e = tid; e < jb * jb; e += NP_T) {
-    const int i = e % jb, c = e / jb;
-    a[i * NP_LD + c] = A[(size_t)(k + i) + (size_t)(k + c) * lda];
+  for (int e = tid; e < NP_NB * NP_NB; e += NPD_T) {
+    const int i = e % NP_NB, c = e / NP_NB;
+    a[i * NP_LD + c] = (i < jb && c < jb) ? A[(size_t)(k + i) + (size_t)(k + c) * lda]
+                                          : (i == c ? (T)1 : (T)0);
   }
   __syncthreads();
   float lm = 0.f;
   bool zero = false;
-  // thread (row i, column phase cp) forms its row's multiplier itself and
-  // updates its columns; the multiplier is stored into column j only after
-  // the step's barrier (no later step reads column j), so one barrier per
-  // column suffices
-  const int i = tid & (NP_NB - 1), cp = tid / NP_NB;  // row, column phase (0..3)
-  T lprev = (T)0;
-  for (int j = 0; j < jb; ++j) {
-    if (j > 0 && cp == 0 && i > j - 1 && i < jb) a[i * NP_LD + j - 1] = lprev;
-    const T piv = a[j * NP_LD + j];
-    if (piv == (T)0) zero = true;
-    if (i > j && i < jb) {
-      const T l = a[i * NP_LD + j] / piv;
-      for (int c = j + 1 + cp; c < jb; c += NP_T / NP_NB) a[i * NP_LD + c] -= l * a[j * NP_LD + c];
-      lprev = l;
-      if (cp == 0) lm = fmaxf(lm, (float)fabs((double)l));
+  {
+    const int t = tid;  // column (threads >= 64 only pass the barriers)
+    T col[NP_NB];
+#pragma unroll
+    for (int r = 0; r < NP_NB; ++r) col[r] = t < NP_NB ? a[r * NP_LD + t] : (T)0;
+#pragma unroll
+    for (int j = 0; j < NP_NB; ++j) {
+      if (j < jb) {
+        if (t == j) {
+          const T piv = col[j];
+          if (piv == (T)0) zero = true;
+          const T rinv = (T)1 / piv;
+#pragma unroll
+          for (int r = j + 1; r < NP_NB; ++r) {
+            col[r] *= rinv;
+            s_l[j & 1][r] = col[r];
+            if (r < jb) lm = fmaxf(lm, (float)fabs((double)col[r]));
+          }
+        }
+        __syncthreads();
+        if (t > j && t < NP_NB) {
+          const T u = col[j];
+#pragma unroll
+          for (int r = j + 1; r < NP_NB; ++r) col[r] = fma(-s_l[j & 1][r], u, col[r]);
+        }
+      }
     }
     __syncthreads();
+    if (t < NP_NB)
+#pragma unroll
+      for (int r = 0; r < NP_NB; ++r) a[r * NP_LD + t] = col[r];
   }
   if (zero) lm = INFINITY;
-  // max |l| of the block (CTA reduction through one shared word)
   for (int o = 16; o > 0; o >>= 1) lm = fmaxf(lm, __shfl_xor_sync(0xffffffffu, lm, o));
-  if ((tid & 31) == 0) atomicMax((unsigned *)&s_lmax, __float_as_uint(lm));
-  // inverse triangles by substitution, one column per group of 4 lanes (the
-  // dot products split over the group, summed by shuffles): Uinv column c
-  // from row c up, then Linv column c from row c down
+  if ((tid & 31) == 0) np_note_lmax(lmax_bits, lm);
+  __syncthreads();
+  if (tid < NP_NB) s_rd[tid] = (T)1 / a[tid * NP_LD + tid];
+  __syncthreads();
   {
-    const int c = tid >> 2, q = tid & 3;
-    const bool on = c < jb;
-    for (int r = NP_NB - 1; r >= 0; --r) {
-      T part = (T)0;
-      if (on && r <= c)
-        for (int p = r + 1 + q; p <= c; p += 4) part += a[r * NP_LD + p] * inv[p * NP_LD + c];
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
-      if (on && r <= c && q == 0) inv[r * NP_LD + c] = ((r == c ? (T)1 : (T)0) - part) / a[r * NP_LD + r];
-      __syncwarp();
-    }
-    for (int r = 0; r < NP_NB; ++r) {
-      T part = (T)0;
-      if (on && r > c)
-        for (int p = c + q; p < r; p += 4) part += a[r * NP_LD + p] * linv[p * NP_LD + c];
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
-      if (on && r >= c && r < jb && q == 0) linv[r * NP_LD + c] = r == c ? (T)1 : -part;
-      __syncwarp();
+    T x[NP_NB];
+    if (tid < NP_NB) {
+      // Uinv column c: U x = e_c, rows from the bottom
+      const int c = tid;
+#pragma unroll
+      for (int r = NP_NB - 1; r >= 0; --r) {
+        T acc = (r == c) ? (T)1 : (T)0;
+#pragma unroll
+        for (int p = r + 1; p < NP_NB; ++p) acc = fma(-a[r * NP_LD + p], x[p], acc);
+        x[r] = acc * s_rd[r];
+      }
+#pragma unroll
+      for (int r = 0; r < NP_NB; ++r) inv[r * NP_LD + c] = x[r];
+    } else if (tid < 2 * NP_NB) {
+      // Linv column c: L x = e_c (unit diagonal), rows from the top
+      const int c = tid - NP_NB;
+#pragma unroll
+      for (int r = 0; r < NP_NB; ++r) {
+        T acc = (r == c) ? (T)1 : (T)0;
+#pragma unroll
+        for (int p = 0; p < r; ++p) acc = fma(-a[r * NP_LD + p], x[p], acc);
+        x[r] = acc;
+      }
+#pragma unroll
+      for (int r = 0; r < NP_NB; ++r) linv[r * NP_LD + c] = x[r];
     }
   }
   __syncthreads();
-  for (int e = tid; e < jb * jb; e += NP_T) {
+  for (int e = tid; e < jb * jb; e += NPD_T) {
     const int r = e % jb, c = e / jb;
     A[(size_t)(k + r) + (size_t)(k + c) * lda] = a[r * NP_LD + c];
     Uinv[r + (size_t)c * NP_NB] = r <= c ? inv[r * NP_LD + c] : (T)0;
     Linv[r + (size_t)c * NP_NB] = r > c ? linv[r * NP_LD + c] : (r == c ? (T)1 : (T)0);
   }
-  if (tid == 0) np_note_lmax(lmax_bits, s_lmax);
 }
 
 // 64 x 64 tiles of the panel: blocks [0, nrb) take 64 rows of A21 (rows
@@ -265,7 +294,7 @@ int lu_getrf_nopiv(cublasHandle_t cb, cudaStream_t st, LuWork &w, int n, T *A, i
     for (int k = K; k < Ke; k += NP_NB) {
       const int jb = std::min(NP_NB, n - k), m2 = n - k - jb, wc = Ke - k - jb;
       T *Linv = inv0 + 2 * tri * (size_t)(k / NP_NB), *Uinv = Linv + tri;
-      k_np_diag<T><<<1, NP_T, smd, st>>>(A, lda, k, jb, Linv, Uinv, bits);
+      k_np_diag<T><<<1, NPD_T, smd, st>>>(A, lda, k, jb, Linv, Uinv, bits);
       const int nrb = (m2 + NP_NB - 1) / NP_NB, ncb = (wc + NP_NB - 1) / NP_NB;
       if (nrb + ncb > 0)
         k_np_panel<T><<<nrb + ncb, NP_T, smp, st>>>(A, lda, n, k, jb, Linv, Uinv, nrb, k + jb,
@@ -364,22 +393,41 @@ __global__ void __launch_bounds__(NP_T) k_np_subst(const T *A, int lda, int n, i
   T *w = (T *)np_sm;               // Inv_i
   T *b = w + NP_NB * NP_LD;        // B_i (a chunk of right-hand sides)
   T *y = b + NP_NB * NP_LD;        // Y_i
-  T *l = y + NP_NB * NP_LD;        // A_(r,i)
+  T *l = y + NP_NB * NP_LD;        // A_(r,i) of the CTA's first tile
+  T *o = l + NP_NB * NP_LD;        // the update of a tile
   const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
   const unsigned G = gridDim.x;
   const int nb = (n + NP_NB - 1) / NP_NB;
-  for (int s = 0; s < nb; ++s) {
-    const int i = FWD ? s : nb - 1 - s;
-    const int k = i * NP_NB, jb = min(NP_NB, n - k);
+  // the inverse triangle and the first coupling tile of a step depend only
+  // on the factors, so they are loaded before the grid barrier that ends the
+  // previous step; only B's block i waits for it
+  auto step_of = [&](int s) { return FWD ? s : nb - 1 - s; };
+  auto load_inv_tile = [&](int s, T *lt) {
+    const int i = step_of(s), k = i * NP_NB, jb = min(NP_NB, n - k);
     const T *W = Inv + 2 * (size_t)NP_NB * NP_NB * i + (FWD ? 0 : (size_t)NP_NB * NP_NB);
     const int nrest = FWD ? n - k - jb : k;
     const int ntile = (nrest + NP_NB - 1) / NP_NB;
-    for (int c0 = 0; c0 < nrhs; c0 += NP_NB) {
+    const int tile = blockIdx.x;
+    const int r0 = FWD ? k + jb + NP_NB * tile : NP_NB * tile;
+    const int nr = tile < ntile ? min(NP_NB, (FWD ? n : k) - r0) : 0;
+    for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+      const int r = e % NP_NB, c = e / NP_NB;
+      w[r * NP_LD + c] = (r < jb && c < jb) ? W[r + (size_t)c * NP_NB] : (T)0;
+      lt[r * NP_LD + c] = (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
+    }
+  };
+  load_inv_tile(0, l);
+  for (int s = 0; s < nb; ++s) {
+    const int i = step_of(s);
+    const int k = i * NP_NB, jb = min(NP_NB, n - k);
+    const int nrest = FWD ? n - k - jb : k;
+    const int ntile = (nrest + NP_NB - 1) / NP_NB;
+    const bool busy = blockIdx.x == 0 || (int)blockIdx.x < ntile;
+    for (int c0 = 0; c0 < nrhs && busy; c0 += NP_NB) {
       const int nc = min(NP_NB, nrhs - c0);
       __syncthreads();
       for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
         const int r = e % NP_NB, c = e / NP_NB;
-        w[r * NP_LD + c] = (r < jb && c < jb) ? W[r + (size_t)c * NP_NB] : (T)0;
         // B changes between steps on other SMs: read it past L1
         b[r * NP_LD + c] =
             (r < jb && c < nc) ? __ldcg(B + (size_t)(k + r) + (size_t)(c0 + c) * ldb) : (T)0;
@@ -400,29 +448,37 @@ __global__ void __launch_bounds__(NP_T) k_np_subst(const T *A, int lda, int n, i
       for (int tile = blockIdx.x; tile < ntile; tile += G) {
         const int r0 = FWD ? k + jb + NP_NB * tile : NP_NB * tile;
         const int nr = min(NP_NB, (FWD ? n : k) - r0);
-        __syncthreads();
-        for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
-          const int r = e % NP_NB, c = e / NP_NB;
-          l[r * NP_LD + c] = (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
+        T *lt = l;
+        if (tile != (int)blockIdx.x) {
+          // a further tile of this CTA: its coupling block is loaded here
+          lt = o;
+          __syncthreads();
+          for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
+            const int r = e % NP_NB, c = e / NP_NB;
+            lt[r * NP_LD + c] =
+                (r < nr && c < jb) ? A[(size_t)(r0 + r) + (size_t)(k + c) * lda] : (T)0;
+          }
+          __syncthreads();
         }
-        __syncthreads();
-        np_mm64(l, y, ty, tx, acc);
+        np_mm64(lt, y, ty, tx, acc);
         // through shared memory, then coalesced along the columns
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-          for (int v = 0; v < 4; ++v) l[(4 * ty + u) * NP_LD + 4 * tx + v] = acc[u][v];
+          for (int v = 0; v < 4; ++v) o[(4 * ty + u) * NP_LD + 4 * tx + v] = acc[u][v];
         __syncthreads();
         for (int e = tid; e < NP_NB * NP_NB; e += NP_T) {
           const int r = e % NP_NB, c = e / NP_NB;
           if (r < nr && c < nc) {
             T *bp = B + (size_t)(r0 + r) + (size_t)(c0 + c) * ldb;
-            *bp = __ldcg(bp) - l[r * NP_LD + c];
+            *bp = __ldcg(bp) - o[r * NP_LD + c];
           }
         }
       }
     }
+    __syncthreads();
+    if (s + 1 < nb) load_inv_tile(s + 1, l);
     if (!np_grid_barrier(bar, G, err)) return;
   }
 }
@@ -437,7 +493,7 @@ int lu_getrs_nopiv(cudaStream_t st, LuWork &w, int n, int nrhs, const T *A, int 
   T *X = (T *)((char *)w.np_x.p + 256);
   unsigned *bar = (unsigned *)w.np_x.p;  // arrivals, generation, error word
   int *err = (int *)(bar + 2);
-  const int sm = 4 * NP_NB * NP_LD * (int)sizeof(T);
+  const int sm = 5 * NP_NB * NP_LD * (int)sizeof(T);
   static int G = 0;  // co-resident CTAs, per element type
   if (G == 0) {
     DUST_CUDA(cudaFuncSetAttribute(k_np_subst<T, true>,
