@@ -81,6 +81,54 @@ def update_params(dt, box_min, box_max, ndt_update_wake=1, vortstretch=True, dif
     return u
 
 
+class PaParams(C.Structure):
+    """dust_pa_params: penetration avoidance (avoid_collision)."""
+    _fields_ = [("check_radius", C.c_double), ("element_radius", C.c_double),
+                ("u_ref", C.c_double)]
+
+
+def pa_params(u_ref, check_radius=5.0, element_radius=1.5):
+    return PaParams(float(check_radius), float(element_radius), float(u_ref))
+
+
+class WakeParams(C.Structure):
+    """dust_wake_params: the panel wake and its shedding."""
+    _fields_ = [
+        ("n_stripes", C.c_int),
+        ("n_points", C.c_int),
+        ("n_wake_panels", C.c_int),
+        ("dt", C.c_double),
+        ("ndt_update_wake", C.c_int),
+        ("min_vel_at_te", C.c_double),
+        ("box_min", C.c_double * 3),
+        ("box_max", C.c_double * 3),
+        ("vortex_rad", C.c_double),
+        ("k_vortex_rad", C.c_double),
+        ("refine_wake", C.c_int),
+        ("k_refine", C.c_int),
+        ("u_inf", C.c_double * 3),
+    ]
+
+
+def wake_params(n_stripes, n_points, n_wake_panels, dt, box_min, box_max, u_inf,
+                vortex_rad=0.1, k_vortex_rad=1.0, min_vel_at_te=1e-8, ndt_update_wake=1,
+                refine_wake=False, k_refine=1):
+    w = WakeParams()
+    w.n_stripes, w.n_points, w.n_wake_panels = int(n_stripes), int(n_points), int(n_wake_panels)
+    w.dt, w.ndt_update_wake, w.min_vel_at_te = float(dt), int(ndt_update_wake), float(min_vel_at_te)
+    for d in range(3):
+        w.box_min[d], w.box_max[d], w.u_inf[d] = float(box_min[d]), float(box_max[d]), float(u_inf[d])
+    w.vortex_rad, w.k_vortex_rad = float(vortex_rad), float(k_vortex_rad)
+    w.refine_wake, w.k_refine = int(bool(refine_wake)), int(k_refine)
+    return w
+
+
+class Te(C.Structure):
+    """dust_te: trailing-edge topology (1-based, 2 ints per stripe)."""
+    _fields_ = [("ii", C.POINTER(C.c_int)), ("neigh", C.POINTER(C.c_int)),
+                ("neigh_o", C.POINTER(C.c_int)), ("gen_elems", C.POINTER(C.c_int))]
+
+
 class Panels(C.Structure):
     _fields_ = [
         ("n", C.c_int),

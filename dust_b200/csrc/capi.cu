@@ -54,7 +54,9 @@ extern "C" int dust_abi_sizes(int64_t *out, int n) {
   int64_t s[] = {(int64_t)sizeof(dust_fmm_params), (int64_t)sizeof(dust_panels),
                  (int64_t)sizeof(dust_lines),      (int64_t)sizeof(dust_elements),
                  (int64_t)sizeof(dust_fmm_stats),  (int64_t)sizeof(dust_solve_report),
-                 (int64_t)sizeof(dust_wake_rows),  (int64_t)sizeof(dust_update_params)};
+                 (int64_t)sizeof(dust_wake_rows),  (int64_t)sizeof(dust_update_params),
+                 (int64_t)sizeof(dust_pa_params),  (int64_t)sizeof(dust_wake_params),
+                 (int64_t)sizeof(dust_te)};
   int m = (int)(sizeof(s) / sizeof(s[0]));
   for (int i = 0; i < n && i < m; ++i) out[i] = s[i];
   return m;

@@ -173,6 +173,14 @@ __global__ void __launch_bounds__(EP_T) k_elements_vel(int n, const double *pts,
   vel[3 * (size_t)t + 2] = v[2] * k4pi + u2;
 }
 
+int elements_vel_points(const ElemDev &e, int n, const double *pts, const double *u_inf,
+                        double *vel, cudaStream_t st) {
+  if (n <= 0) return DUST_OK;
+  k_elements_vel<<<nblk(n, EP_T), EP_T, 0, st>>>(n, pts, e, u_inf[0], u_inf[1], u_inf[2], vel);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
 #define UV_T 128
 // All-pairs particle kernels (direct-sum truth).
 __global__ void __launch_bounds__(UV_T) k_direct(int n, int ntgt, const double *cen,

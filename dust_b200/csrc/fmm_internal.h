@@ -110,6 +110,13 @@ int elem_build_device(const dust_panels *body, const dust_panels *wake,
                       bool host_arrays, DevBuf &raw, DevBuf &geo, ElemDev &out,
                       cudaStream_t st);
 RegParams reg_params(const dust_fmm_params *prm);
+// velocity at n device points from the elements of e (x 1/4pi) plus u_inf
+int elements_vel_points(const ElemDev &e, int n, const double *pts, const double *u_inf,
+                        double *vel, cudaStream_t st);
+// the particles' uvort kernels with the end vortices of `lines`
+int points_uvort_device(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                        const double *cen, const double *dir, const double *mag,
+                        const double *rv, const ElemDev &lines, double *uv, cudaStream_t st);
 // Argument check shared by the uvort entry points: the points and the
 // output when there are points, the four particle arrays when there are
 // particles, the end vortices' vertices and strengths when there are any.

@@ -240,3 +240,158 @@ class DeviceStepper:
                 C.c_void_p(stream)), "dust_particles_update_device")
         self._mark()
         return self.res
+
+
+class WakeStepper:
+    """The reference's time loop for static bodies with panel wakes, device
+    resident (src/dust.f90:510-1160 with update_wake / complete_wake of
+    src/aeroel/mod_wake.f90).  Per step:
+
+      1. prepare_wake: the live particles in slot order (dust_particles_live_device)
+      2. uvort at the body centres from the particles and the end vortices
+      3. assemble_linsys with the wake's rows (implicit first row + explicit
+         rows), solve_linsys (static LU of initialize_linsys reused)
+      4. update_wake: first wake row from the solution; particle velocity,
+         stretching, diffusion by the FMM with body, wake panels and end
+         vortices (scattered to the slots); wake points moved
+      5. complete_wake: particles moved (penetration avoidance when ``pa``),
+         wake rows from the trailing edge, shedding, end vortices
+
+    ``case``: synth.WingWakeCase (body, trailing-edge topology, parameters);
+    ``fprm``: FmmParams of the FMM and of the direct sums."""
+
+    def __init__(self, case, fprm, mode=abi.DUST_SOLVE_LU64, pa=None, device="cuda"):
+        import torch
+        from . import wake as WK
+        self.torch, self.WK = torch, WK
+        self.case, self.fprm, self.mode, self.pa = case, fprm, mode, pa
+        dev = torch.device(device)
+        self.dev = dev
+        T = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt,
+                                                        device=dev)
+        c = case
+        self.wake = WK.PanelWake(c.wake_params(), c.ii, c.neigh, c.neigh_o, c.gen, c.te_pts,
+                                 c.te_dir, c.te_scaling)
+        self.te_pts, self.te_dir, self.te_sc = T(c.te_pts), T(c.te_dir), T(c.te_scaling)
+        self.ever, self.env = T(c.body.ver), T(c.body.n_ver, torch.int32)
+        self.ekind = T(c.body.kind, torch.int32)
+        self.n = c.rank
+        self.euv = torch.zeros((self.n, 3), dtype=torch.float64, device=dev)
+        self.ecen = torch.zeros((self.n, 3), dtype=torch.float64, device=dev)
+        self.res = torch.zeros(self.n, dtype=torch.float64, device=dev)
+        ns = c.n_slots
+        Z = lambda *s: torch.zeros(s, dtype=torch.float64, device=dev)
+        self.S = dict(cen=Z(ns, 3), dir=Z(ns, 3), mag=Z(ns), rv=Z(ns), vel=Z(ns, 3),
+                      str=Z(ns, 3), rot=Z(ns, 3))
+        self.free = torch.ones(ns, dtype=torch.int32, device=dev)
+        self.L = dict(cen=Z(ns, 3), dir=Z(ns, 3), mag=Z(ns), rv=Z(ns), vel=Z(ns, 3),
+                      str=Z(ns, 3), rot=Z(ns, 3))
+        self.idx = torch.zeros(ns, dtype=torch.int32, device=dev)
+        self.n_freed = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.upd = c.update_params()
+        self._ps = fprm.struct()
+        # initialize_linsys: static rows with the first (implicit) wake row
+        wp, ev, ni, ip = self.wake.elements()
+        self._init_wake = self._host_wake_rows()
+        self.ls = Linsys(fprm, c.rank, c.nstatic, c.body, self._init_wake[0], ni, c.gen)
+        self.oc = Octree(fprm)
+        # every library call of the step is queued on this stream (a NULL
+        # stream would send the FMM to the octree's own stream)
+        self.stream = torch.cuda.Stream()
+        self.n_live = 0
+        self.shed_total = 0
+        self.steps_done = 0
+
+    def _host_wake_rows(self):
+        L, pts, _, idou, _ = self.wake.get_state()
+        c = self.case
+        ver = np.zeros((L * len(c.ii), 4, 3))
+        for r in range(L):
+            for iw, (p1, p2) in enumerate(c.ii - 1):
+                ver[r * len(c.ii) + iw] = [pts[r, p1], pts[r, p2], pts[r + 1, p2], pts[r + 1, p1]]
+        return (abi.PanelSet(ver, kind=np.full(len(ver), abi.DUST_ELEM_VORTLATT),
+                             mag=idou.reshape(-1)),)
+
+    @staticmethod
+    def _p(t, ctype=C.c_double):
+        return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))
+
+    def body_struct(self, with_mag=True):
+        P = self._p
+        return abi.Panels(self.n, P(self.env, C.c_int), P(self.ekind, C.c_int), P(self.ever),
+                          P(self.res) if with_mag else abi._dp(), abi._dp(), P(self.euv))
+
+    def step(self):
+        torch = self.torch
+        torch.cuda.current_stream().synchronize()
+        with torch.cuda.stream(self.stream):
+            self._step()
+        self.stream.synchronize()
+        return self.res
+
+    def _step(self):
+        torch, WK, P = self.torch, self.WK, self._p
+        S, L = self.S, self.L
+        stream = self.stream.cuda_stream
+        # 1. prepare_wake
+        nl = WK.live_particles_device(self.free, S["cen"], S["dir"], S["mag"], S["rv"],
+                                      L["cen"], L["dir"], L["mag"], L["rv"], self.idx, stream)
+        self.n_live = nl
+        # 2. uvort at the body centres
+        body = self.body_struct()
+        check(lib().dust_panels_centres_device(C.byref(body), P(self.ecen), C.c_void_p(stream)),
+              "dust_panels_centres_device")
+        wp, ev, ni, ip = self.wake.elements()
+        check(lib().dust_points_uvort_device(C.byref(self._ps), self.n, P(self.ecen), nl,
+                                             P(L["cen"]), P(L["dir"]), P(L["mag"]), P(L["rv"]),
+                                             C.byref(ev), P(self.euv), C.c_void_p(stream)),
+              "dust_points_uvort_device")
+        self.stream.synchronize()
+        # 3. assemble + solve
+        wk = abi.WakeRows(wp, ni, ip)
+        check(lib().dust_linsys_assemble_device(self.ls._h, C.byref(body), C.byref(wk)),
+              "dust_linsys_assemble_device")
+        rep = abi.SolveReport()
+        check(lib().dust_linsys_solve_device(self.ls._h, int(self.mode), P(self.res),
+                                             C.byref(rep)), "dust_linsys_solve_device")
+        self.last_report = {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+        # 4. update_wake
+        self.wake.set_first_row(self.res, stream)
+        wp, ev, ni, ip = self.wake.elements()
+        if nl > 0:
+            els = abi.Elements(body, wp, ev)
+            check(lib().dust_fmm_apply_device(self.oc._h, nl, P(L["cen"]), P(L["dir"]),
+                                              P(L["mag"]), P(L["rv"]), C.byref(els),
+                                              P(L["vel"]), P(L["str"]), P(L["rot"]),
+                                              C.c_void_p(stream), 0), "dust_fmm_apply_device")
+            WK.scatter_particles_device(nl, self.idx, L["vel"], L["str"], L["rot"], S["vel"],
+                                        S["str"], S["rot"], stream)
+        self.wake.update(self._ps, body, L["cen"], L["dir"], L["mag"], L["rv"], n=nl,
+                         stream=stream)
+        # 5. complete_wake
+        if nl > 0:
+            if self.pa is not None:
+                WK.complete_wake_particles_pa_device(self.upd, self.pa, body, S["cen"], S["dir"],
+                                                     S["mag"], S["rv"], S["vel"], S["str"],
+                                                     S["rot"], self.free, self.n_freed, stream)
+            else:
+                check(lib().dust_particles_update_device(
+                    C.byref(self.upd), int(self.free.shape[0]), P(S["cen"]), P(S["dir"]),
+                    P(S["mag"]), P(S["vel"]), P(S["str"]), P(S["rot"]), P(self.free, C.c_int),
+                    P(self.n_freed, C.c_int), C.c_void_p(stream)), "dust_particles_update_device")
+        shed = self.wake.complete(self.te_pts, self.te_dir, self.te_sc, None, S["cen"],
+                                  S["dir"], S["mag"], S["rv"], S["vel"], self.free, stream)
+        self.shed_total += shed
+        self.steps_done += 1
+
+    def particles(self):
+        """Live particles in slot order (host): cen, alpha = dir mag, r_vortex."""
+        live = self.torch.nonzero(self.free == 0).flatten()
+        S = self.S
+        return (S["cen"][live].cpu().numpy(),
+                (S["dir"][live] * S["mag"][live][:, None]).cpu().numpy(),
+                S["rv"][live].cpu().numpy())
+
+    def close(self):
+        self.wake.close()
+        self.oc.close()

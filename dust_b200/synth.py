@@ -565,3 +565,72 @@ class RotorFuselageCase:
     def fmm_params(self):
         from .params import FmmParams
         return FmmParams(u_inf=(0.0, 0.0, 0.0), rankine_rad=0.1)
+
+
+class WingWakeCase:
+    """Flat rectangular vortex-lattice wing (span 10, chord 1, 40 x 10
+    panels: 400 unknowns, all static) at 5 degrees of incidence in a 1 m/s
+    stream, with the reference's panel wake (n_wake_panels rows behind the
+    trailing edge) shedding one particle per stripe per step once it is
+    full (classical complete_wake branch).  Trailing-edge topology as the
+    pre-processor builds it for a structured strip (build_te_parametric,
+    src/geo/mod_build_geo.f90:2244-2310): stripe i spans trailing-edge
+    points (i + 1, i), neighbours i +- 1 with orientation 1, generating
+    element = the strip's last chordwise panel; t_te the chordwise unit
+    vector of the trailing panels' side edges; first-row scaling 0.3
+    (implicit_panel_scale).  Particle core 0.1 chord for every particle
+    (vortex_rad = rankine_rad = 0.1, k_vortex_rad = 0)."""
+
+    def __init__(self, span=10.0, chord=1.0, n_span=40, n_chord=10, alpha_deg=5.0, dt=0.05,
+                 n_wake_panels=4, n_wake_particles=None, steps=200, u_inf=(1.0, 0.0, 0.0),
+                 box_min=(-1.0, -8.0, -8.0), box_max=(15.0, 8.0, 8.0)):
+        x = np.linspace(0.0, chord, n_chord + 1)
+        y = np.linspace(-span / 2, span / 2, n_span + 1)
+        X, Y = np.meshgrid(x, y, indexing="ij")
+        P = np.stack([X, Y, np.zeros_like(X)], axis=2)
+        a = np.deg2rad(alpha_deg)
+        R = np.array([[np.cos(a), 0, np.sin(a)], [0, 1, 0], [-np.sin(a), 0, np.cos(a)]])
+        P = P @ R.T
+        ver = _quad_grid(P)  # panel (i, j) at index i * n_span + j
+        self.body = abi.PanelSet(ver, kind=np.full(len(ver), abi.DUST_ELEM_VORTLATT))
+        self.rank = self.nstatic = len(ver)
+        ns = n_span
+        i = np.arange(1, ns + 1)
+        self.ii = np.stack([i + 1, i], axis=1).astype(np.int32)
+        self.neigh = np.stack([i + 1, i - 1], axis=1).astype(np.int32)
+        self.neigh[-1, 0] = 0
+        self.neigh[0, 1] = 0
+        self.neigh_o = np.ones((ns, 2), dtype=np.int32)
+        self.neigh_o[-1, 0] = 0
+        self.neigh_o[0, 1] = 0
+        self.gen = np.zeros((ns, 2), dtype=np.int32)
+        self.gen[:, 0] = (n_chord - 1) * n_span + np.arange(ns) + 1
+        self.te_pts = np.ascontiguousarray(P[n_chord])
+        t = P[n_chord] - P[n_chord - 1]
+        self.te_dir = np.ascontiguousarray(t / np.linalg.norm(t, axis=1)[:, None])
+        self.te_scaling = np.full(ns + 1, 0.3)
+        self.u_inf = np.asarray(u_inf, dtype=np.float64)
+        self.dt = float(dt)
+        self.steps = int(steps)
+        self.n_wake_panels = int(n_wake_panels)
+        self.box_min = np.asarray(box_min, dtype=np.float64)
+        self.box_max = np.asarray(box_max, dtype=np.float64)
+        self.n_slots = int(n_wake_particles or ns * (steps + 1))
+        self.vortex_rad = 0.1
+
+    def wake_params(self):
+        return abi.wake_params(len(self.ii), len(self.te_pts), self.n_wake_panels, self.dt,
+                               self.box_min, self.box_max, self.u_inf,
+                               vortex_rad=self.vortex_rad, k_vortex_rad=0.0)
+
+    def fmm_params(self, levels=6, degree=4, precision=abi.DUST_PREC_FP64):
+        from .params import FmmParams
+        side = float(np.max(self.box_max - self.box_min))
+        return FmmParams(box_length=side, n_box=(1, 1, 1), origin=tuple(self.box_min),
+                         n_octree_levels=levels, min_octree_part=5, multipole_degree=degree,
+                         rankine_rad=self.vortex_rad, cutoff_rad=0.001, vortstretch=True,
+                         diffusion=True, nu_inf=1.8e-5 / 1.225,
+                         u_inf=tuple(float(v) for v in self.u_inf), precision=precision)
+
+    def update_params(self):
+        return abi.update_params(self.dt, self.box_min, self.box_max, 1, True, True, False, 0.0)

@@ -56,9 +56,9 @@ extern "C" {
 #define DUST_PREC_FP32C  1     /* FP32 pair arithmetic on tile-relative
                                   coordinates, partial sums per tile in FP32
                                   and across tiles in FP64; M2L of levels >= 2
-                                  on the tensor cores (3xTF32, p <= 4); tables,
-                                  level-1 M2L, M2M, L2L and near element pairs
-                                  stay FP64                                   */
+                                  in FP32 (SIMT, FP64 accumulation across
+                                  offsets); tables, level-1 M2L, P2M, M2M,
+                                  L2L, L2P and near element pairs stay FP64   */
 
 /* Octree / FMM parameters.  One field per DUST input key
  * (src/general/mod_sim_param.f90:376-452, read at :772-804). */
@@ -480,13 +480,167 @@ DUST_API int dust_particles_update_device(const dust_update_params *u, int n, do
                                           double *stretch, const double *rotu,
                                           int *free_flag, int *n_freed, void *stream);
 
+/* ------------------------------------------------ penetration avoidance */
+/* sim_param%pa_rad_mult, %pa_elrad_mult and %u_ref
+ * (src/general/mod_sim_param.f90:697-702, 627-636). */
+typedef struct dust_pa_params {
+  double check_radius;    /* penetration_avoidance_check_radius (5.0)        */
+  double element_radius;  /* penetration_avoidance_element_radius (1.5)      */
+  double u_ref;           /* u_ref (default |u_inf|)                         */
+} dust_pa_params;
+
+/* complete_wake's particle loop with penetration avoidance (use_pa,
+ * src/aeroel/mod_wake.f90:1312-1317): before the move, every live
+ * particle's velocity goes through avoid_collision (:2350-2534) against the
+ * body elements `elems` (the reference's elems_tot, in its order; surface
+ * panels and vortex rings, device arrays, ub = body velocity at the centres
+ * or NULL), and the corrected velocity is written back to vel (part%vel).
+ * Then the step of dust_particles_update_device.  The reference's own
+ * expressions are kept, including the vortex-ring branch's componentwise
+ * normal distance norm2(dist * n) and its doubling of the layer thickness
+ * (initially the particle's r_vortex) at every ring that passes the
+ * approach test.  Device arrays, queued on `stream`; the element records
+ * are built into a work buffer kept between calls (grown on first use). */
+DUST_API int dust_particles_update_pa_device(const dust_update_params *u,
+                                             const dust_pa_params *pa,
+                                             const dust_panels *elems, int n, double *cen,
+                                             double *dir, const double *mag,
+                                             const double *r_vortex, double *vel,
+                                             double *stretch, const double *rotu,
+                                             int *free_flag, int *n_freed, void *stream);
+
+/* The live particles of a slot array in slot order (the part_p list that
+ * prepare_wake rebuilds, src/aeroel/mod_wake.f90:804-846): copies cen, dir
+ * (3, n_live), mag, r_vortex (n_live) of every slot with free_flag == 0
+ * into the l* arrays and its slot index into idx; *n_live (host) receives
+ * the count.  Device arrays; synchronises `stream`. */
+DUST_API int dust_particles_live_device(int n_slots, const int *free_flag, const double *cen,
+                                        const double *dir, const double *mag,
+                                        const double *r_vortex, double *lcen, double *ldir,
+                                        double *lmag, double *lrv, int *idx, int *n_live,
+                                        void *stream);
+/* Scatters per-live-particle outputs (3, n_live) back to their slots:
+ * out[idx[i]] = in[i] for each non-NULL pair.  Device arrays. */
+DUST_API int dust_particles_scatter_device(int n_live, const int *idx, const double *lvel,
+                                           const double *lstr, const double *lrot, double *vel,
+                                           double *str, double *rot, void *stream);
+
+/* ---------------------------------------------- panel wake and shedding */
+/* The panel wake behind the trailing edges and the particles it sheds,
+ * device resident: the panel part of t_wake (src/aeroel/mod_wake.f90:
+ * 160-296) with initialize_wake (:331-579), load_wake (:597-778, restart),
+ * update_wake (:860-1214) and complete_wake (:1222-2105).  The wake panels
+ * are vortex rings of rows 1..len (len grows by one per step up to
+ * n_wake_panels, then the wake is full); a full wake sheds one particle per
+ * stripe per step (k_refine x n subparticles with refine_wake) into the
+ * lowest free particle slots and carries an end vortex on its last row.
+ * Uniform wind u_inf (variable_wind without gusts).  Not built: ring wakes
+ * of actuator disks, join_te, interpolate_wake, HCAS, precice. */
+typedef struct dust_wake_params {
+  int    n_stripes;           /* wake%n_pan_stripes = size(te%e, 2)          */
+  int    n_points;            /* wake%n_pan_points = size(te%i, 2)           */
+  int    n_wake_panels;       /* n_wake_panels (wake%nmax_pan), >= 1         */
+  double dt;                  /* dt                                          */
+  int    ndt_update_wake;     /* ndt_update_wake                             */
+  double min_vel_at_te;       /* implicit_panel_min_vel                      */
+  double box_min[3], box_max[3]; /* particles_box_min / max                  */
+  double vortex_rad;          /* vortex_rad                                  */
+  double k_vortex_rad;        /* k_vortex_rad                                */
+  int    refine_wake;         /* refine_wake                                 */
+  int    k_refine;            /* k_refine                                    */
+  double u_inf[3];            /* u_inf                                       */
+} dust_wake_params;
+
+/* Trailing-edge topology (t_tedge: te%ii, te%neigh, te%o, te%e, written by
+ * the pre-processor, src/geo/mod_build_geo.f90:2135-2152, 2284-2289), host
+ * arrays of 2*n_stripes ints, 1-based as in the reference: the two
+ * trailing-edge points of each stripe, the neighbouring stripe on each side
+ * (0 = none) and its orientation (+1 / -1), the generating elements
+ * (0 = none). */
+typedef struct dust_te {
+  const int *ii;
+  const int *neigh;
+  const int *neigh_o;
+  const int *gen_elems;
+} dust_te;
+
+typedef struct dust_wake dust_wake;
+
+/* initialize_wake (:331-579) for the panel wake: first row of points =
+ * te_pts (3, n_points; the midpoints of te%i, wake%w_start_points), second
+ * row te_pts + te_dir scaling |u_inf - te_vel| dt ndt / |te_dir| (te_dir =
+ * R_g pan_gen_dir, te_scaling = pan_gen_scaling, te_vel = calc_node_vel or
+ * NULL for 0; below min_vel_at_te: te_dir scaling min_vel_at_te dt ndt, the
+ * reference's unnormalised form at this call), len = 1, intensities 0.
+ * Host arrays. */
+DUST_API int dust_wake_create(const dust_wake_params *prm, const dust_te *te,
+                              const double *te_pts, const double *te_dir,
+                              const double *te_scaling, const double *te_vel,
+                              dust_wake **out);
+DUST_API int dust_wake_destroy(dust_wake *w);
+
+/* Device views of the wake's elements for the other entry points (valid
+ * until the next call on w): the wake panels of rows 1..len in the
+ * reference's pan_p order (row by row, stripes in order; vortex rings, mag =
+ * pan_idou), the implicit first row's generating elements (n_impl =
+ * n_stripes, impl_ind 1-based, device) for dust_wake_rows, and the end
+ * vortices of a full wake (n = 0 before that; mag => last_pan_idou). */
+DUST_API int dust_wake_elements(dust_wake *w, dust_panels *wake_pan, dust_lines *end_vort,
+                                int *n_impl, const int **impl_ind);
+
+/* update_wake :884-892: the first row's intensities from the solution
+ * (device res, 1-based gen_elems): mag(gen 1) - mag(gen 2). */
+DUST_API int dust_wake_set_first_row_device(dust_wake *w, const double *res, void *stream);
+
+/* The rest of update_wake's panel part (:894-939, :1128-1176): velocity at
+ * the wake points by compute_vel_from_all (:2109-2150: the body elements
+ * `body` with their intensities, the wake panels, the end vortices, the n
+ * particles (device arrays) and u_inf), rows 3.. moved (the third with dt,
+ * the others with dt ndt, as the reference), the extra row of a full wake
+ * (points_end), then the length and the intensities shifted one row back
+ * (end_pan_idou = last row).  prm supplies rankine_rad, cutoff_rad and
+ * far_field_ratio_doublet.  Device arrays, queued on `stream`. */
+DUST_API int dust_wake_update_device(dust_wake *w, const dust_fmm_params *prm,
+                                     const dust_panels *body, int n, const double *cen,
+                                     const double *dir, const double *mag,
+                                     const double *r_vortex, void *stream);
+
+/* complete_wake's panel part and shedding (:1247-1292, :1358-2010 without
+ * interpolate_wake, :2091-2103): first two rows from the trailing edge (as
+ * dust_wake_create, with the normalised form below min_vel_at_te), then for
+ * a full wake one particle per stripe (or k_refine subparticles) at the
+ * centre of the last row's far panel with circulation vector from the
+ * side and end intensities, written into the lowest free slots of the
+ * particle arrays (n_slots each, free_flag cleared for them; vel may be
+ * NULL); *n_shed (host) receives the number shed; end vortices attached.
+ * A slot shortage returns DUST_ERR_CAPACITY ("Exceeding the maximum number
+ * of wake particles", :1985).  Device arrays; synchronises `stream`. */
+DUST_API int dust_wake_complete_device(dust_wake *w, const double *te_pts,
+                                       const double *te_dir, const double *te_scaling,
+                                       const double *te_vel, int n_slots, double *cen,
+                                       double *dir, double *mag, double *r_vortex,
+                                       double *vel, int *free_flag, int *n_shed,
+                                       void *stream);
+
+/* State as save_status writes it (src/io/mod_dust_io.f90:355-411) and
+ * load_wake reads it back (:597-778): points (len+1, n_points, 3), point
+ * velocities (same), pan_idou (len, n_stripes), last_pan_idou (n_stripes);
+ * host arrays, any may be NULL on get.  set_state takes len in 1..n_wake_panels
+ * and marks the wake full when len == n_wake_panels (load_wake :764). */
+DUST_API int dust_wake_get_state(const dust_wake *w, int *len, double *points,
+                                 double *point_vel, double *idou, double *last_idou);
+DUST_API int dust_wake_set_state(dust_wake *w, int len, const double *points,
+                                 const double *point_vel, const double *idou,
+                                 const double *last_idou);
+
 /* ---------------------------------------------------------------- misc */
 DUST_API const char *dust_status_string(int status);
 DUST_API const char *dust_last_error(void); /* text of the last CUDA error seen      */
 DUST_API int dust_device_ok(void);   /* DUST_OK if a usable sm_100 device is present */
 /* sizeof() of the ABI structs in declaration order (dust_fmm_params,
  * dust_panels, dust_lines, dust_elements, dust_fmm_stats, dust_solve_report,
- * dust_wake_rows, dust_update_params), for binding checks; returns the
+ * dust_wake_rows, dust_update_params, dust_pa_params, dust_wake_params,
+ * dust_te), for binding checks; returns the
  * number of sizes. */
 DUST_API int dust_abi_sizes(int64_t *out, int n);
 

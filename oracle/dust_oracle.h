@@ -16,18 +16,22 @@
  *   src/aeroel/mod_vortlatt.f90  vortex-lattice rows
  *   src/aeroel/mod_vortline.f90  vortex line velocity
  *   src/linsys/mod_linsys.f90    static/moving block LU sequence
- *   src/aeroel/mod_wake.f90      particle loop of complete_wake
+ *   src/aeroel/mod_wake.f90      particle loop of complete_wake, avoid_collision
  *
  * Parity pins: the reference is Fortran and cannot be compiled here (no
- * Fortran compiler, LAPACK or HDF5), and it has no unit-level golden vectors
- * for this path.  The LU sequence is pinned against LAPACK itself (the
- * reference's third-party solver) through scipy; the FMM and the influence
- * kernels are pinned only by analytic known answers and independent
- * formulas (solid-angle sums and the Van Oosterom-Strackee solid angle,
- * vortex-ring and straight-segment Biot-Savart laws, quadrature of the
- * source potential, the particle-pair kernel, FMM -> direct-sum
- * convergence).  Parity of those parts against the reference's own outputs
- * is "unpinned".
+ * Fortran compiler, LAPACK or HDF5).  Its regression fixtures hold its own
+ * results (tests/sym_test/static/{v,p,nl_v}/Output/ref_res_00{10,11}.h5):
+ * the step-11 re-solve (particle and end-vortex uvort, both influence
+ * kernels, both row builders, the wake coupling, the LU) and the step
+ * 10 -> 11 wake advance (element and particle velocities, stretching,
+ * diffusion, penetration avoidance, the Euler update and the shedding) are
+ * checked against them (tests/test_reference_fixture.py).  The LU sequence
+ * is also pinned against LAPACK (the reference's third-party solver)
+ * through scipy; the FMM's multipole parts and the rest of the influence
+ * kernels by analytic known answers and independent formulas (solid-angle
+ * sums and the Van Oosterom-Strackee solid angle, vortex-ring and
+ * straight-segment Biot-Savart laws, quadrature of the source potential,
+ * the particle-pair kernel, FMM -> direct-sum convergence).
  */
 #ifndef DUST_ORACLE_H
 #define DUST_ORACLE_H
@@ -140,6 +144,15 @@ void or_dgemm_nn_minus(int m, int n, int k, const double *A, int lda,
 int or_particles_update(const dust_update_params *u, int n, double *cen, double *dir,
                         const double *mag, const double *vel, double *stretch,
                         const double *rotu, int *free_flag, int *n_freed);
+
+/* The same loop with penetration avoidance (avoid_collision,
+ * mod_wake.f90:2350-2534) against the body elements `elems` (host arrays);
+ * vel is overwritten with the corrected velocities. */
+int or_particles_update_pa(const dust_update_params *u, const dust_pa_params *pa,
+                           const dust_panels *elems, int n, double *cen, double *dir,
+                           const double *mag, const double *r_vortex, double *vel,
+                           double *stretch, const double *rotu, int *free_flag,
+                           int *n_freed);
 
 #ifdef __cplusplus
 }

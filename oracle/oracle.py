@@ -41,6 +41,7 @@ def lib():
         L.or_linsys_rows.restype = C.c_int
         L.or_last_tree_flags.restype = C.c_int
         L.or_particles_update.restype = C.c_int
+        L.or_particles_update_pa.restype = C.c_int
     return _lib
 
 
@@ -275,3 +276,23 @@ def particles_update(u, cen, dir_, mag, vel, stretch, rotu, free):
         raise RuntimeError(f"oracle particles_update status {rc}")
     return cen, dir_, stretch, free, nf.value
 
+
+
+def particles_update_pa(u, pa, body, cen, dir_, mag, rvort, vel, stretch, rotu, free):
+    """complete_wake's particle loop with penetration avoidance against the
+    panel set ``body`` (abi.PanelSet) on copies; returns (cen, dir, vel,
+    stretch, free, n_freed)."""
+    cen, dir_, vel, stretch = (np.array(abi.f64(a), dtype=np.float64, order="C")
+                               for a in (cen, dir_, vel, stretch))
+    mag, rvort, rotu = abi.f64(mag), abi.f64(rvort), abi.f64(rotu)
+    free = np.array(free, dtype=np.int32, order="C")
+    nf = C.c_int(0)
+    bs = body.struct()
+    rc = lib().or_particles_update_pa(C.byref(u), C.byref(pa), C.byref(bs), mag.shape[0],
+                                      abi.dptr(cen), abi.dptr(dir_), abi.dptr(mag),
+                                      abi.dptr(rvort), abi.dptr(vel), abi.dptr(stretch),
+                                      abi.dptr(rotu), free.ctypes.data_as(C.POINTER(C.c_int)),
+                                      C.byref(nf))
+    if rc != 0:
+        raise RuntimeError(f"oracle particles_update_pa status {rc}")
+    return cen, dir_, vel, stretch, free, nf.value

@@ -333,8 +333,88 @@ def extract(case_dir, name):
     return out
 
 
+def extract_step_pair(case_dir, name):
+    """Two consecutive result files (output steps 10 and 11, dt_out = dt) of a
+    fmm = F vortex-lattice case: the state that step 10's update_wake and
+    complete_wake start from (saved after solve_linsys, before update_wake)
+    and the particles, panel wake and last intensities they produce, as
+    saved at step 11 (src/dust.f90:648, 1017, 1071, 1108)."""
+    eltype, ver, nch, nsp = build_case(case_dir)
+    assert eltype == "v", "vortex-lattice trailing edge only"
+    f10 = h5v0.File(os.path.join(case_dir, "Output", "ref_res_0010.h5"))
+    f11 = h5v0.File(os.path.join(case_dir, "Output", "ref_res_0011.h5"))
+    at = f10.attrs()
+
+    def comp_vort(f):
+        comps = f["Components"]
+        return np.concatenate([comps[k]["Solution/Vort"].read()
+                               for k in sorted(comps.keys()) if k.startswith("Comp")])
+
+    sp = f10["PanelWake/StartPoints"].read()  # (stripes, 2), 1-based
+    i_strip = np.arange(1, nsp + 1)
+    assert np.array_equal(sp[:, 0], i_strip + 1) and np.array_equal(sp[:, 1], i_strip)
+    # build_te_parametric (src/geo/mod_build_geo.f90:2244-2310), vortex
+    # lattice: e_te(1, i) = i nch; neighbours i +- 1 with orientation 1, none
+    # at the ends; t_te from the trailing element's side edges, normalised
+    gen = np.zeros((nsp, 2), dtype=np.int32)
+    gen[:, 0] = i_strip * nch
+    neigh = np.stack([i_strip + 1, i_strip - 1], axis=1).astype(np.int32)
+    neigh[-1, 0] = 0
+    neigh[0, 1] = 0
+    neigh_o = np.ones((nsp, 2), dtype=np.int32)
+    neigh_o[-1, 0] = 0
+    neigh_o[0, 1] = 0
+    t_te = np.zeros((nsp + 1, 3))
+    e1 = ver[gen[0, 0] - 1]
+    t_te[0] = 0.5 * (e1[2] - e1[1])
+    for i1 in range(1, nsp + 1):
+        e = ver[gen[i1 - 1, 0] - 1]
+        t_te[i1] = 0.5 * (e[3] - e[0])
+    t_te = t_te / np.sqrt((t_te ** 2).sum(axis=1))[:, None]
+    wp10 = f10["PanelWake/WakePoints"].read()
+    te_pts = np.concatenate([ver[nch - 1, 2][None], ver[i_strip * nch - 1, 3]])
+    worst = float(np.abs(te_pts - wp10[0]).max())
+    assert worst < 1e-12, "rebuilt trailing edge differs from the wake start points by %g" % worst
+    out = dict(
+        eltype=eltype, ver=ver, nver=np.full(len(ver), 4, dtype=np.int32),
+        ii=sp.astype(np.int32), neigh=neigh, neigh_o=neigh_o, gen=gen,
+        te_pts=te_pts, te_dir=t_te, te_scaling=float(at["first_panel_scaling"]),
+        vort10=comp_vort(f10),
+        wake_pts10=wp10, wake_vel10=f10["PanelWake/WakeVels"].read(),
+        wake_vort10=f10["PanelWake/WakeVort"].read(),
+        last10=f10["ParticleWake/LastPanIdou"].read(),
+        part_cen10=f10["ParticleWake/WakePoints"].read(),
+        part_alpha10=f10["ParticleWake/WakeVort"].read(),
+        part_rv10=f10["ParticleWake/VortexRad"].read(),
+        part_vel10=f10["ParticleWake/WakeVels"].read(),
+        wake_pts11=f11["PanelWake/WakePoints"].read(),
+        wake_vort11=f11["PanelWake/WakeVort"].read(),
+        last11=f11["ParticleWake/LastPanIdou"].read(),
+        part_cen11=f11["ParticleWake/WakePoints"].read(),
+        part_alpha11=f11["ParticleWake/WakeVort"].read(),
+        part_rv11=f11["ParticleWake/VortexRad"].read(),
+        u_inf=np.asarray(at["u_inf"], dtype=np.float64), u_ref=float(at["u_ref"]),
+        dt=float(at["dt"]), box_min=np.asarray(at["particles_box_min"], dtype=np.float64),
+        box_max=np.asarray(at["particles_box_max"], dtype=np.float64),
+        n_wake_panels=int(at["n_wake_panels"]), n_wake_particles=int(at["n_wake_particles"]),
+        min_vel_at_te=float(at["min_vel_at_te"]),
+        rankine_rad=float(at["RankineRad"]), vortex_rad=float(at["VortexRad"]),
+        k_vortex_rad=float(at["KVortexRad"]), cutoff_rad=float(at["CutoffRad"]),
+        far_field_ratio_doublet=float(at["FarFieldRatioDoublet"]),
+        nu_inf=float(at["mu_inf"]) / float(at["rho_inf"]),
+        vortstretch=int(at["Vortstretch"] in (True, "T", 1)),
+        diffusion=int(at["vortdiff"] in (True, "T", 1)),
+        penetration_avoidance=int(at["PenetrationAvoidance"] in (True, "T", 1)),
+        pa_check_radius=float(at["PenetrationAvoidanceCheckRadius"]),
+        pa_element_radius=float(at["PenetrationAvoidanceElementRadius"]),
+        te_match=worst, time10=float(f10["time"].read()), time11=float(f11["time"].read()),
+        source=name)
+    return out
+
+
 CASES = {"sym_static_v": "tests/sym_test/static/v",
          "sym_static_p": "tests/sym_test/static/p"}
+STEP_PAIRS = {"sym_static_nl_v_steps_10_11": "tests/sym_test/static/nl_v"}
 
 
 DEFAULT_ROOT = os.environ.get("DUST_REFERENCE_ROOT", "/root/reference")
@@ -348,6 +428,13 @@ def main(ref_root, out_dir=HERE):
         print("%s: %d elements, %d wake panels, %d particles, TE match %.1e -> %s"
               % (name, len(d["ver"]), len(d["wake_ver"]), len(d["part_cen"]), d["te_match"],
                  os.path.relpath(path)))
+    for name, rel in STEP_PAIRS.items():
+        d = extract_step_pair(os.path.join(ref_root, rel), name)
+        path = os.path.join(out_dir, "ref_%s.npz" % name)
+        np.savez_compressed(path, **d)
+        print("%s: %d elements, %d -> %d particles, TE match %.1e -> %s"
+              % (name, len(d["ver"]), len(d["part_cen10"]), len(d["part_cen11"]),
+                 d["te_match"], os.path.relpath(path)))
 
 
 if __name__ == "__main__":

@@ -26,7 +26,7 @@ def test_struct_sizes_match_header():
     n = L.dust_abi_sizes(sizes, 16)
     mine = [C.sizeof(t) for t in (abi.FmmParams, abi.Panels, abi.Lines, abi.Elements,
                                    abi.FmmStats, abi.SolveReport, abi.WakeRows,
-                                   abi.UpdateParams)]
+                                   abi.UpdateParams, abi.PaParams, abi.WakeParams, abi.Te)]
     assert n == len(mine)
     assert list(sizes)[:n] == mine
 
