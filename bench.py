@@ -839,8 +839,9 @@ def run_wing_workload(n_steps=200, n_wake_panels=1, levels=6, cpu=True):
     case = synth.WingWakeCase(steps=n_steps, n_wake_panels=n_wake_panels)
     fp = case.fmm_params(levels=levels)
     gpu = WakeStepper(case, fp)
-    ms, res = [], []
+    ms, res, phases = [], [], []
     for s in range(n_steps):
+        gpu.phase_events = s >= n_steps - 20
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
@@ -849,6 +850,8 @@ def run_wing_workload(n_steps=200, n_wake_panels=1, levels=6, cpu=True):
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
         res.append(gpu.res.cpu().numpy())
+        if gpu.phase_events:
+            phases.append(gpu.phase_ms())
     gc, ga, gr = gpu.particles()
     gpu.close()
     out = {"workload": "VLM wing 40 x 10 (400 unknowns), panel wake of %d row(s), %d steps of "
@@ -859,7 +862,9 @@ def run_wing_workload(n_steps=200, n_wake_panels=1, levels=6, cpu=True):
            "steps": n_steps, "particles_final": int(len(gc)),
            "ms_per_step_mean": round(float(np.mean(ms)), 4),
            "ms_per_step_last20": round(float(np.mean(ms[-20:])), 4),
-           "ms_total": round(float(np.sum(ms)), 2)}
+           "ms_total": round(float(np.sum(ms)), 2),
+           "phases_ms_last20": {k: round(float(np.mean([p[k] for p in phases])), 4)
+                                for k in phases[0]} if phases else None}
     if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import cpu_step

@@ -298,6 +298,8 @@ class WakeStepper:
         # every library call of the step is queued on this stream (a NULL
         # stream would send the FMM to the octree's own stream)
         self.stream = torch.cuda.Stream()
+        self.phase_events = False  # CUDA events between the phases of a step
+        self.events = []
         self.n_live = 0
         self.shed_total = 0
         self.steps_done = 0
@@ -329,14 +331,32 @@ class WakeStepper:
         self.stream.synchronize()
         return self.res
 
+    PHASES = ("live", "uvort", "assemble_solve", "fmm", "wake_update", "particles",
+              "wake_complete")
+
+    def _mark(self):
+        if self.phase_events:
+            e = self.torch.cuda.Event(enable_timing=True)
+            e.record(self.stream)
+            self.events.append(e)
+
+    def phase_ms(self):
+        """Milliseconds of each phase of the last step (phase_events on)."""
+        ev = self.events
+        return {k: ev[i].elapsed_time(ev[i + 1]) for i, k in enumerate(self.PHASES)
+                if i + 1 < len(ev)}
+
     def _step(self):
         torch, WK, P = self.torch, self.WK, self._p
         S, L = self.S, self.L
         stream = self.stream.cuda_stream
+        self.events = []
+        self._mark()
         # 1. prepare_wake
         nl = WK.live_particles_device(self.free, S["cen"], S["dir"], S["mag"], S["rv"],
                                       L["cen"], L["dir"], L["mag"], L["rv"], self.idx, stream)
         self.n_live = nl
+        self._mark()
         # 2. uvort at the body centres
         body = self.body_struct()
         check(lib().dust_panels_centres_device(C.byref(body), P(self.ecen), C.c_void_p(stream)),
@@ -347,6 +367,7 @@ class WakeStepper:
                                              C.byref(ev), P(self.euv), C.c_void_p(stream)),
               "dust_points_uvort_device")
         self.stream.synchronize()
+        self._mark()
         # 3. assemble + solve
         wk = abi.WakeRows(wp, ni, ip)
         check(lib().dust_linsys_assemble_device(self.ls._h, C.byref(body), C.byref(wk)),
@@ -355,6 +376,7 @@ class WakeStepper:
         check(lib().dust_linsys_solve_device(self.ls._h, int(self.mode), P(self.res),
                                              C.byref(rep)), "dust_linsys_solve_device")
         self.last_report = {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+        self._mark()
         # 4. update_wake
         self.wake.set_first_row(self.res, stream)
         wp, ev, ni, ip = self.wake.elements()
@@ -366,8 +388,10 @@ class WakeStepper:
                                               C.c_void_p(stream), 0), "dust_fmm_apply_device")
             WK.scatter_particles_device(nl, self.idx, L["vel"], L["str"], L["rot"], S["vel"],
                                         S["str"], S["rot"], stream)
+        self._mark()
         self.wake.update(self._ps, body, L["cen"], L["dir"], L["mag"], L["rv"], n=nl,
                          stream=stream)
+        self._mark()
         # 5. complete_wake
         if nl > 0:
             if self.pa is not None:
@@ -379,8 +403,10 @@ class WakeStepper:
                     C.byref(self.upd), int(self.free.shape[0]), P(S["cen"]), P(S["dir"]),
                     P(S["mag"]), P(S["vel"]), P(S["str"]), P(S["rot"]), P(self.free, C.c_int),
                     P(self.n_freed, C.c_int), C.c_void_p(stream)), "dust_particles_update_device")
+        self._mark()
         shed = self.wake.complete(self.te_pts, self.te_dir, self.te_sc, None, S["cen"],
                                   S["dir"], S["mag"], S["rv"], S["vel"], self.free, stream)
+        self._mark()
         self.shed_total += shed
         self.steps_done += 1
 
