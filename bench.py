@@ -266,6 +266,25 @@ def cpu_baseline(case, params, m2l_pairs, fmm_stride=32, uvort_stride=64):
     cpu_step.solve_linsys_lapack(A, P, nst, np.ones(rank))
     parts["solve"] = time.perf_counter() - t
     del A
+    # (3b) the pressure equation of the surface panels: the particles'
+    # rotational term at every uvort_stride-th surface panel (scaled by the
+    # panel count) and the LAPACK dgetrs on a system of the full size
+    sp = np.nonzero(case.elems.kind == abi.DUST_ELEM_SURFPAN)[0]
+    if len(sp):
+        pts = np.ascontiguousarray(cen_el[sp][::uvort_stride])
+        vel0 = np.zeros_like(case.cen)
+        vel0[:, 0] = 1.0
+        t = time.perf_counter()
+        O.pressure_particles(pts, case.cen, case.dir, case.mag, case.r_vortex, vel0)
+        parts["pressure"] = (time.perf_counter() - t) * len(sp) / len(pts)
+        from scipy.linalg import lapack
+        Ap = np.asfortranarray(rng.standard_normal((len(sp), len(sp))) * (1.0 / len(sp)))
+        Ap[np.arange(len(sp)), np.arange(len(sp))] += 1.0
+        Pp = np.arange(1, len(sp) + 1, dtype=np.int32)
+        t = time.perf_counter()
+        lapack.dgetrs(Ap, Pp - 1, np.ones(len(sp)))
+        parts["pressure"] += time.perf_counter() - t
+        del Ap
     # (4) FMM with the element sums
     els = abi.elements_struct(case.elems, case.wake, case.end_vort)
     O.set_sample_stride(fmm_stride)
@@ -278,7 +297,9 @@ def cpu_baseline(case, params, m2l_pairs, fmm_stride=32, uvort_stride=64):
                     + t_app * n / max(npart_s, 1))
     total_ms = 1e3 * sum(parts.values())
     sample = ("bounded sample scaled to one step per phase by the exact work ratio: uvort at "
-              "1/%d of the collocation points; assembly from 8 moving rows (per entry); "
+              "1/%d of the collocation points (the pressure equation's particle term at the "
+              "same share of the surface panels, plus its dgetrs in full); assembly from 8 "
+              "moving rows (per entry); "
               "LAPACK solve in full; FMM tree/P2M/M2M/L2L in full, M2L at 1/%d of the target "
               "cells (by pair count), L2P+P2P+elements at 1/%d of the leaves (by particle "
               "count); phase s: %s" % (uvort_stride, fmm_stride, fmm_stride,
@@ -428,7 +449,8 @@ def main():
                          "loads": case.loads(res, st.euv.cpu().numpy()),
                          "report": st.last_report, "clocks": clk.summary(), "res": res,
                          "fmm": [t.cpu().numpy() for t in (st.vel, st.str, st.rot)],
-                         "cen": st.cen.cpu().numpy(), "n_freed": int(st.free.sum())}
+                         "cen": st.cen.cpu().numpy(), "n_freed": int(st.free.sum()),
+                         "res_pres": st.res_pres.cpu().numpy() if st.pr is not None else None}
         # further untimed steps up to the accuracy horizon (phase breakdown and
         # launch counts below run one more step each)
         while not args.no_advect and len(by_step[name]) < n_acc:
@@ -453,6 +475,12 @@ def main():
         return {"vel_induced": rel(a[0] - uinf, b[0] - uinf), "stretch": rel(a[1], b[1]),
                 "rot": rel(a[2], b[2])}
     fmm_errs = {k: fmm_err(k) for k in results}
+    # the pressure equation's solution (surface panels) against the FP64 step
+    for k in results:
+        a, b = results[k]["res_pres"], results["plain"]["res_pres"]
+        fmm_errs[k]["pressure_solution"] = (
+            float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            if a is not None and b is not None else None)
     # the particles after all advected steps against the FP64 run's
     cp = results["plain"]["cen"]
     for k in results:
@@ -970,8 +998,9 @@ def phase_breakdown(st, case, params):
     st.phase_events = False
     t = lambda a, b: round(ev[a].elapsed_time(ev[b]), 3)
     first = "fmm_prepare_and_uvort" if st.fmm_uvort else "uvort"
-    return {"total": t(0, 5), first: t(0, 1), "assemble": t(1, 2), "solve": t(2, 3),
-            "fmm_total": t(3, 4), "particles_update": t(4, 5), "fmm_tree": round(s["ms_tree"], 3),
+    return {"total": t(0, 6), first: t(0, 1), "assemble": t(1, 2), "pressure": t(2, 3),
+            "solve": t(3, 4), "fmm_total": t(4, 5), "particles_update": t(5, 6),
+            "fmm_tree": round(s["ms_tree"], 3),
             "fmm_upward": round(s["ms_upward"], 3), "fmm_m2l": round(s["ms_m2l"], 3),
             "fmm_p2p": round(s["ms_p2p"], 3), "fmm_elements": round(s["ms_elems"], 3),
             "n_leaves": s["n_leaves"], "n_active_cells": s["n_active_cells"],
@@ -1102,7 +1131,8 @@ def e2e_bytes(case, n, advect, fmm_uvort=False):
     strengths), dust_fmm_apply (particles, panels, wake panels, end vortices
     -> vel, stretch, rotu) and, when advecting, dust_particles_update
     (cen, dir, mag, vel, stretch, rotu, free flags -> cen, dir, stretch, free
-    flags, count)."""
+    flags, count); with surface panels, dust_pressure_assemble (particles and
+    their velocities) and dust_pressure_solve (-> solution)."""
     d, i = 8, 4
     nr, nw, nl = case.rank, case.wake.n, case.end_vort.n
     panels = nr * (12 * d + 2 * i + 7 * d)        # ver, n_ver, kind, mag, ub, uvort
@@ -1120,6 +1150,13 @@ def e2e_bytes(case, n, advect, fmm_uvort=False):
         h2d += panels + wakep + nw * 2 * i        # assemble (+ implicit indices)
         h2d += parts + panels + wakep + lines     # FMM
     d2h = nr * 3 * d + nr * d + n * 9 * d         # uvort, strengths, vel/stretch/rotu
+    from dust_b200 import abi
+    nsp = int(np.sum(case.elems.kind == abi.DUST_ELEM_SURFPAN))
+    if nsp:
+        # dust_pressure_assemble (particles with their velocities), and from
+        # the second step dust_pressure_solve (-> the surface panels' solution)
+        h2d += parts + n * 3 * d
+        d2h += nsp * d
     if advect:
         h2d += n * (16 * d + i)
         d2h += n * (9 * d + i) + i

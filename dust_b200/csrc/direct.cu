@@ -913,6 +913,40 @@ void points_lines_add(int npts, const double *pts, const ElemDev &lines, double 
     k_uvort_lines<<<nblk(npts, 128), 128, 0, st>>>(npts, pts, lines, uv);
 }
 
+// Morton order of n particles over the octree box of prm (keys of 10 bits
+// per axis): *perm (in scratch, from offset 0) receives the particle index
+// of every sorted position; *used the scratch bytes taken.
+size_t morton_perm_bytes(int n, cudaStream_t st) {
+  const size_t N = (size_t)std::max(n, 1);
+  size_t tb = 0;
+  uint32_t *dummy = nullptr;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, dummy, dummy, dummy, dummy, n, 0, 30, st);
+  return (16 * N + 255) / 256 * 256 + (tb + 255) / 256 * 256;
+}
+
+int morton_perm(const dust_fmm_params *prm, int n, const double *cen, DevBuf &scratch,
+                uint32_t **perm, size_t *used, cudaStream_t st) {
+  const size_t N = (size_t)std::max(n, 1);
+  size_t tb = 0;
+  uint32_t *dummy = nullptr;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, dummy, dummy, dummy, dummy, n, 0, 30, st);
+  const size_t off_t = (16 * N + 255) / 256 * 256;
+  DUST_TRY(devbuf_grow(scratch, off_t + tb + 256));
+  char *b = (char *)scratch.p;
+  uint32_t *k_in = (uint32_t *)b, *v_in = k_in + N, *k_out = v_in + N, *v_out = k_out + N;
+  const double hbox =
+      prm->box_length * std::max(prm->n_box[0], std::max(prm->n_box[1], prm->n_box[2]));
+  if (n > 0) {
+    k_uv_keys<<<nblk(n, 256), 256, 0, st>>>(n, cen, prm->origin[0], prm->origin[1],
+                                             prm->origin[2], 1024.0 / hbox, k_in, v_in);
+    DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
+                                              st));
+  }
+  *perm = v_out;
+  *used = off_t + (tb + 255) / 256 * 256;
+  return DUST_OK;
+}
+
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st) {

@@ -135,6 +135,11 @@ int m2l_scale_sources(dust_octree *o, FmmDev &d, cudaStream_t st);
 int elem_output_device(FmmDev &d, const ElemDev &e, DevBuf &ffbuf, DevBuf &work,
                        size_t &near_cap, int precision, double *vel, double *str, double *rot,
                        cudaStream_t st, cudaEvent_t *kev = nullptr, bool *kev_done = nullptr);
+// Morton order of n particles over the octree box (10 bits per axis): the
+// permutation in scratch (grown to morton_perm_bytes(n) if needed)
+size_t morton_perm_bytes(int n, cudaStream_t st);
+int morton_perm(const dust_fmm_params *prm, int n, const double *cen, DevBuf &scratch,
+                uint32_t **perm, size_t *used, cudaStream_t st);
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st);

@@ -769,6 +769,45 @@ extern "C" int dust_wake_complete_device(dust_wake *w, const double *te_pts,
   return DUST_OK;
 }
 
+// velocities of the wake panels' vertices (pan_w_vel at (row, point) of
+// each vertex, in the panels' vertex order) and of the end vortices'
+// vertices (row len), for the pressure equation's rotational terms
+__global__ void k_wake_vv(int ns, int npt, int len, int attached, const int *ii,
+                          const double *pvel, double *wvv, double *evv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (len + 1) * ns) return;
+  int r = t / ns, iw = t % ns;
+  int p1 = ii[2 * iw] - 1, p2 = ii[2 * iw + 1] - 1;
+  const double *a = pvel + 3 * ((size_t)r * npt + p1), *b = pvel + 3 * ((size_t)r * npt + p2);
+  if (r < len) {
+    const double *c = pvel + 3 * ((size_t)(r + 1) * npt + p2);
+    const double *d = pvel + 3 * ((size_t)(r + 1) * npt + p1);
+    double *v = wvv + 12 * (size_t)t;
+    for (int k = 0; k < 3; ++k) {
+      v[k] = a[k];
+      v[3 + k] = b[k];
+      v[6 + k] = c[k];
+      v[9 + k] = d[k];
+    }
+  } else if (attached && evv) {
+    double *e = evv + 6 * (size_t)iw;
+    for (int k = 0; k < 3; ++k) {
+      e[k] = a[k];
+      e[3 + k] = b[k];
+    }
+  }
+}
+
+extern "C" int dust_wake_vertex_velocities_device(dust_wake *w, double *wake_vv, double *end_vv,
+                                                  void *stream) {
+  if (!w || !wake_vv) return DUST_ERR_BAD_ARG;
+  const int ns = w->p.n_stripes;
+  k_wake_vv<<<nblk((size_t)(w->len_geo + 1) * ns, 128), 128, 0, (cudaStream_t)stream>>>(
+      ns, w->p.n_points, w->len_geo, w->attached ? 1 : 0, w->ii, w->pvel, wake_vv, end_vv);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
 extern "C" int dust_wake_get_state(const dust_wake *w, int *len, double *points,
                                    double *point_vel, double *idou, double *last_idou) {
   if (!w) return DUST_ERR_BAD_ARG;

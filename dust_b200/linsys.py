@@ -106,3 +106,77 @@ def dense_solve_device(A, B, X, mode=abi.DUST_SOLVE_LU64, tol=1e-12, stream=None
                                         C.c_double(tol), C.byref(rep),
                                         C.c_void_p(stream or 0)), "dust_dense_solve_device")
     return {k: getattr(rep, k) for k, _ in abi.SolveReport._fields_}
+
+
+class Pressure:
+    """The pressure integral equation of a linear system
+    (dust_pressure_*: initialize_pressure_sys, assemble_pressure_sys,
+    solve_pressure_sys of src/linsys/mod_pressure_equation.f90).  Create it
+    right after the Linsys; per step, after the Linsys assembly, call
+    assemble_device and solve_device (torch CUDA tensors)."""
+
+    def __init__(self, ls):
+        self.ls = ls
+        h = C.c_void_p()
+        check(lib().dust_pressure_create(ls._h, C.byref(h)), "dust_pressure_create")
+        self._h = h
+        nsp, nss = C.c_int(0), C.c_int(0)
+        check(lib().dust_pressure_size(h, C.byref(nsp), C.byref(nss)), "dust_pressure_size")
+        self.n_sp, self.nstatic_sp = nsp.value, nss.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dust_pressure_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _p(t):
+        return (C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double)) if t is not None
+                else C.POINTER(C.c_double)())
+
+    def assemble_device(self, bern=None, parts=None, vel=None, wake=None, wake_vv=None,
+                        end_vort=None, end_vv=None, stream=0):
+        """parts = (cen, dir, mag, r_vortex) device tensors of the live
+        particles, vel their velocities; wake / end_vort abi.Panels / abi.Lines
+        structs of device pointers with wake_vv / end_vv device tensors."""
+        P = self._p
+        cen, dir_, mag, rv = parts if parts is not None else (None,) * 4
+        n = int(mag.shape[0]) if mag is not None else 0
+        check(lib().dust_pressure_assemble_device(
+            self._h, self.ls._h, P(bern), n, P(cen), P(dir_), P(mag), P(rv), P(vel),
+            C.byref(wake) if wake is not None else None, P(wake_vv),
+            C.byref(end_vort) if end_vort is not None else None, P(end_vv),
+            C.c_void_p(stream)), "dust_pressure_assemble_device")
+
+    def solve_device(self, res, stream=0):
+        check(lib().dust_pressure_solve_device(self._h, self._p(res), C.c_void_p(stream)),
+              "dust_pressure_solve_device")
+
+    def assemble(self, bern=None, parts=None, vel=None):
+        """Host-array variant of assemble_device (particles only)."""
+        cen, dir_, mag, rv = (abi.f64(a) for a in parts) if parts is not None else (None,) * 4
+        n = int(mag.shape[0]) if mag is not None else 0
+        check(lib().dust_pressure_assemble(self._h, self.ls._h, abi.dptr(abi.f64(bern)), n,
+                                           abi.dptr(cen), abi.dptr(dir_), abi.dptr(mag),
+                                           abi.dptr(rv), abi.dptr(abi.f64(vel)), None, None,
+                                           None, None), "dust_pressure_assemble")
+
+    def solve(self):
+        res = np.zeros(self.n_sp)
+        check(lib().dust_pressure_solve(self._h, abi.dptr(res)), "dust_pressure_solve")
+        return res
+
+    def get_system(self):
+        """dump_linsys_pres: (A_pres, b_pres) as assembled (host)."""
+        n = self.n_sp
+        A = np.empty(n * n)
+        b = np.empty(n)
+        check(lib().dust_pressure_get_system(self._h, abi.dptr(A), abi.dptr(b)),
+              "dust_pressure_get_system")
+        return A.reshape(n, n).T.copy(), b

@@ -9,6 +9,9 @@ the same sequence on the GPU through the C ABI:
 
   1. uvort at every implicit element centre  (dust_points_uvort[_device])
   2. dust_linsys_assemble[_device]
+  2b. the pressure integral equation of the surface panels, when there are
+     any (dust_pressure_assemble[_device] every step, _solve from the second
+     step: dust.f90:621, 641-643)
   3. dust_linsys_solve[_device]              (doublet intensities)
   4. wake bookkeeping: implicit wake panel mag = mag(ind1) - mag(ind2)
      (update_wake, mod_wake.f90:881-889)
@@ -30,7 +33,7 @@ import numpy as np
 
 from . import abi
 from ._lib import check, lib
-from .linsys import Linsys
+from .linsys import Linsys, Pressure
 from .octree import Octree
 
 
@@ -47,7 +50,7 @@ def update_params_for(case, params):
 
 class HostStepper:
     def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, out=None, advect=False,
-                 fmm_uvort=False, uvort_params=None):
+                 fmm_uvort=False, uvort_params=None, pressure=True):
         """``out``: optional (vel, stretch, rotu) host arrays the particle
         outputs are written to every step (e.g. page-locked buffers);
         ``advect``: move the particles at the end of each step;
@@ -66,6 +69,10 @@ class HostStepper:
         c = case
         self.free = np.zeros(c.mag.shape[0], dtype=np.int32)
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
+        self.pr = (Pressure(self.ls) if pressure and np.any(c.elems.kind == abi.DUST_ELEM_SURFPAN)
+                   else None)
+        self.vel_prev = np.zeros((c.mag.shape[0], 3))
+        self.steps_done = 0
         self.oc = Octree(params)
         self.ind = c.impl_ind.astype(np.int64) - 1
 
@@ -91,6 +98,14 @@ class HostStepper:
                                           abi.dptr(uv)), "dust_points_uvort")
         c.elems.uvort = uv
         self.ls.assemble_linsys(c.elems, c.wake, c.n_impl, c.impl_ind)
+        if self.pr is not None:
+            # assemble_pressure_sys every step, solve_pressure_sys from the
+            # second (dust.f90:621, 641-643); the body is at rest in the
+            # frame of its Bernoulli sources, the particles' velocities are
+            # those of the previous update
+            self.pr.assemble(None, (c.cen, c.dir, c.mag, c.r_vortex), self.vel_prev)
+            if self.steps_done > 0:
+                self.res_pres = self.pr.solve()
         res, rep = self.ls.solve_linsys(self.mode)
         self.last_report = rep
         c.elems.mag = res
@@ -102,6 +117,8 @@ class HostStepper:
         else:
             vel, st, ro = self.oc.apply_multipole(c.cen, c.dir, c.mag, c.r_vortex, els,
                                                   out=self.out)
+        self.vel_prev = vel
+        self.steps_done += 1
         if self.advect:
             nf = C.c_int(0)
             check(lib().dust_particles_update(C.byref(self.upd), c.mag.shape[0], abi.dptr(c.cen),
@@ -116,7 +133,7 @@ class DeviceStepper:
     """All per-step inputs resident in HBM; library calls on device pointers."""
 
     def __init__(self, case, params, mode=abi.DUST_SOLVE_LU64, device="cuda", advect=False,
-                 fmm_uvort=False, uvort_params=None):
+                 fmm_uvort=False, uvort_params=None, pressure=True):
         import torch
         self.torch = torch
         self.case = case
@@ -153,13 +170,21 @@ class DeviceStepper:
         self.has2 = T((ind[:, 1] >= 0).astype(np.float64))
         self.lver = T(c.end_vort.ver)
         self.lmag = T(c.end_vort.mag)
-        self.vel = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
+        self.vel = torch.zeros((self.n, 3), dtype=torch.float64, device=dev)
         self.str = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
         self.rot = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
         self.res = torch.empty(c.rank, dtype=torch.float64, device=dev)
         self.free = torch.zeros(self.n, dtype=torch.int32, device=dev)
         self.n_freed = torch.zeros(1, dtype=torch.int32, device=dev)
         self.ls = Linsys(params, c.rank, c.nstatic, c.elems, c.wake, c.n_impl, c.impl_ind)
+        # the pressure integral equation of the surface panels
+        # (mod_pressure_equation.f90), assembled every step, solved from the
+        # second (dust.f90:621, 641-643)
+        self.pr = (Pressure(self.ls) if pressure and np.any(c.elems.kind == abi.DUST_ELEM_SURFPAN)
+                   else None)
+        if self.pr is not None:
+            self.res_pres = torch.zeros(self.pr.n_sp, dtype=torch.float64, device=dev)
+        self.steps_done = 0
         self.oc = Octree(params)
         self._ps = params.struct()
         self.phase_events = False
@@ -210,6 +235,14 @@ class DeviceStepper:
         if self.phase_events:
             self.ls.sync()
         self._mark()
+        if self.pr is not None:
+            # the particles' velocities of the previous update (the body is at
+            # rest in the frame of its Bernoulli sources)
+            self.pr.assemble_device(None, (self.cen, self.dir, self.mag, self.rv), self.vel,
+                                    stream=stream)
+            if self.steps_done > 0:
+                self.pr.solve_device(self.res_pres, stream)
+        self._mark()
         rep = abi.SolveReport()
         check(lib().dust_linsys_solve_device(self.ls._h, int(self.mode), P(self.res),
                                              C.byref(rep)), "dust_linsys_solve_device")
@@ -233,6 +266,7 @@ class DeviceStepper:
                                               P(self.str), P(self.rot), C.c_void_p(stream), 0),
                   "dust_fmm_apply_device")
         self._mark()
+        self.steps_done += 1
         if self.advect:
             check(lib().dust_particles_update_device(
                 C.byref(self.upd), self.n, P(self.cen), P(self.dir), P(self.mag), P(self.vel),

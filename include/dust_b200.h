@@ -622,6 +622,15 @@ DUST_API int dust_wake_complete_device(dust_wake *w, const double *te_pts,
                                        double *vel, int *free_flag, int *n_shed,
                                        void *stream);
 
+/* Velocities of the wake panels' vertices, wake_vv[12 * len * n_stripes]
+ * (pan_w_vel at each vertex's row and point, in the panels' vertex order),
+ * and of the end vortices' vertices, end_vv[6 * n_stripes] (row len; may be
+ * NULL; written only once the end vortices are attached): the vertex
+ * velocities of assemble_pressure_sys (src/linsys/mod_pressure_equation.f90:
+ * 194-223).  Device arrays. */
+DUST_API int dust_wake_vertex_velocities_device(dust_wake *w, double *wake_vv, double *end_vv,
+                                                void *stream);
+
 /* State as save_status writes it (src/io/mod_dust_io.f90:355-411) and
  * load_wake reads it back (:597-778): points (len+1, n_points, 3), point
  * velocities (same), pan_idou (len, n_stripes), last_pan_idou (n_stripes);
@@ -632,6 +641,63 @@ DUST_API int dust_wake_get_state(const dust_wake *w, int *len, double *points,
 DUST_API int dust_wake_set_state(dust_wake *w, int len, const double *points,
                                  const double *point_vel, const double *idou,
                                  const double *last_idou);
+
+/* ---------------------------------------------------- pressure equation */
+/* The pressure integral equation of the linear-system module
+ * (src/linsys/mod_pressure_equation.f90; A_pres and its static LU in
+ * src/linsys/mod_linsys.f90:184-187, 250-257, 318-323).  Its unknowns are
+ * the surface panels (DUST_ELEM_SURFPAN) among the system's elements, in
+ * element order (static first); A_pres is their block of the influence
+ * matrix before the wake correction. */
+typedef struct dust_pressure dust_pressure;
+
+/* initialize_pressure_sys (:44-79) with the static part of initialize_linsys:
+ * the static block of A_pres and b_static_pres from the geometry `ls` was
+ * created with, and the LU of the static block.  Call right after
+ * dust_linsys_create. */
+DUST_API int dust_pressure_create(dust_linsys *ls, dust_pressure **out);
+DUST_API int dust_pressure_destroy(dust_pressure *p);
+/* Number of surface panels and of static ones. */
+DUST_API int dust_pressure_size(const dust_pressure *p, int *n_sp, int *nstatic_sp);
+
+/* assemble_pressure_sys (:139-235) after dust_linsys_assemble of the same
+ * step (its element geometry): the moving parts of A_pres, b_pres from the
+ * Bernoulli sources `bern` (n_sp, device; the output of press_normvel_der,
+ * :395-455; NULL = 0, as for bodies at rest) through the source-potential
+ * influence (build_row_surfpan, mod_surfpan.f90:396-437), plus the
+ * rotational terms of the n live particles (cen, dir, mag, r_vortex and their
+ * velocities vel(3, n)), of the end vortices and of the wake panels with
+ * their vertex velocities (end_vv[6 * n_end], wake_vv[12 * n_wake], e.g. from
+ * dust_wake_vertex_velocities_device).  Device arrays; the kernels run on
+ * `stream`, which is synchronised. */
+DUST_API int dust_pressure_assemble_device(dust_pressure *p, const dust_linsys *ls,
+                                           const double *bern, int n, const double *cen,
+                                           const double *dir, const double *mag,
+                                           const double *r_vortex, const double *vel,
+                                           const dust_panels *wake, const double *wake_vv,
+                                           const dust_lines *end_vort, const double *end_vv,
+                                           void *stream);
+
+/* solve_pressure_sys (:243-387): the block LU sequence of solve_linsys on
+ * A_pres (static LU reused, Schur update and LU of the moving block, getrs);
+ * res[n_sp] (device) receives the solution (the elements' pres_sol). */
+DUST_API int dust_pressure_solve_device(dust_pressure *p, double *res, void *stream);
+
+/* The same two calls on host arrays (copied to a device buffer kept by the
+ * handle; the solution copied back): for host codes that keep the particles
+ * in host memory. */
+DUST_API int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, const double *bern,
+                                    int n, const double *cen, const double *dir,
+                                    const double *mag, const double *r_vortex,
+                                    const double *vel, const dust_panels *wake,
+                                    const double *wake_vv, const dust_lines *end_vort,
+                                    const double *end_vv);
+DUST_API int dust_pressure_solve(dust_pressure *p, double *res);
+
+/* Host copies of A_pres (n_sp x n_sp column-major; its static block holds
+ * that block's LU) and b_pres after assembly and before the solve, as
+ * dump_linsys_pres writes them (:462-489).  Either may be NULL. */
+DUST_API int dust_pressure_get_system(dust_pressure *p, double *A, double *b);
 
 /* ---------------------------------------------------------------- misc */
 DUST_API const char *dust_status_string(int status);

@@ -16,6 +16,7 @@
  *   src/aeroel/mod_vortlatt.f90  vortex-lattice rows
  *   src/aeroel/mod_vortline.f90  vortex line velocity
  *   src/linsys/mod_linsys.f90    static/moving block LU sequence
+ *   src/linsys/mod_pressure_equation.f90  pressure integral equation
  *   src/aeroel/mod_wake.f90      particle loop of complete_wake, avoid_collision
  *
  * Parity pins: the reference is Fortran and cannot be compiled here (no
@@ -138,6 +139,25 @@ void or_dtrsm_llnu(int m, int n, const double *A, int lda, double *B, int ldb);
 void or_dtrsm_runn(int m, int n, const double *A, int lda, double *B, int ldb);
 void or_dgemm_nn_minus(int m, int n, int k, const double *A, int lda,
                        const double *B, int ldb, double *C, int ldc);
+
+/* The pressure integral equation of one step (mod_pressure_equation.f90,
+ * the pressure parts of mod_linsys.f90 and build_row_surfpan): A_pres
+ * (n_sp x n_sp column-major, n_sp = surface panels among the rank elements,
+ * static first), b_pres and res_pres.  bern: Bernoulli source per surface
+ * panel or NULL; particles with their velocities vel(3, n); wake panels with
+ * the velocities of their four vertices wake_vv[12 * n_wake]; end vortices
+ * with those of their two vertices end_vv[6 * n_end]. */
+int or_pressure_run(const dust_fmm_params *prm, int rank, int nstatic,
+                    const dust_panels *elems_init, const dust_panels *elems_step,
+                    const double *bern, int n, const double *cen, const double *dir,
+                    const double *mag, const double *r_vortex, const double *vel,
+                    const dust_panels *wake, const double *wake_vv, const dust_lines *end_vort,
+                    const double *end_vv, double *A_out, double *b_out, double *res);
+
+/* The particles' term of assemble_pressure_sys alone at n_pts points. */
+int or_pressure_particles(int n_pts, const double *pts, int n, const double *cen,
+                          const double *dir, const double *mag, const double *r_vortex,
+                          const double *vel, double *out);
 
 /* Particle loop of complete_wake (mod_wake.f90:1309-1355), arguments as
  * dust_particles_update. */

@@ -42,6 +42,8 @@ def lib():
         L.or_last_tree_flags.restype = C.c_int
         L.or_particles_update.restype = C.c_int
         L.or_particles_update_pa.restype = C.c_int
+        L.or_pressure_run.restype = C.c_int
+        L.or_pressure_particles.restype = C.c_int
     return _lib
 
 
@@ -296,3 +298,42 @@ def particles_update_pa(u, pa, body, cen, dir_, mag, rvort, vel, stretch, rotu, 
     if rc != 0:
         raise RuntimeError(f"oracle particles_update_pa status {rc}")
     return cen, dir_, vel, stretch, free, nf.value
+
+
+def pressure_run(prm, rank, nstatic, elems_init, elems_step, bern, parts, vel, wake=None,
+                 wake_vv=None, end_vort=None, end_vv=None):
+    """The pressure integral equation of one step; returns (A_pres (n_sp,
+    n_sp), b_pres, res_pres).  parts = (cen, dir, mag, r_vortex)."""
+    cen, dir_, mag, rv = (abi.f64(a) for a in parts)
+    vel = abi.f64(vel)
+    wk = wake if wake is not None else abi.empty_panels()
+    ev = end_vort if end_vort is not None else abi.empty_lines()
+    ws, es = wk.struct(), ev.struct()
+    ei, est = elems_init.struct(), elems_step.struct()
+    nsp = int(np.sum(np.asarray(elems_step.kind) == abi.DUST_ELEM_SURFPAN))
+    A = np.zeros(max(nsp, 1) ** 2)
+    b = np.zeros(max(nsp, 1))
+    res = np.zeros(max(nsp, 1))
+    p = prm.struct()
+    rc = lib().or_pressure_run(C.byref(p), int(rank), int(nstatic), C.byref(ei), C.byref(est),
+                               abi.dptr(abi.f64(bern)), mag.shape[0], abi.dptr(cen),
+                               abi.dptr(dir_), abi.dptr(mag), abi.dptr(rv), abi.dptr(vel),
+                               C.byref(ws), abi.dptr(abi.f64(wake_vv)), C.byref(es),
+                               abi.dptr(abi.f64(end_vv)), abi.dptr(A), abi.dptr(b),
+                               abi.dptr(res))
+    if rc != 0:
+        raise RuntimeError(f"oracle pressure status {rc}")
+    return A[:nsp * nsp].reshape(nsp, nsp).T.copy(), b[:nsp], res[:nsp]
+
+
+def pressure_particles(pts, cen, dir_, mag, rvort, vel):
+    """The particles' rotational term of the pressure equation at points."""
+    pts = abi.f64(pts).reshape(-1, 3)
+    cen, dir_, mag, rvort, vel = (abi.f64(a) for a in (cen, dir_, mag, rvort, vel))
+    out = np.zeros(pts.shape[0])
+    rc = lib().or_pressure_particles(pts.shape[0], abi.dptr(pts), mag.shape[0], abi.dptr(cen),
+                                     abi.dptr(dir_), abi.dptr(mag), abi.dptr(rvort),
+                                     abi.dptr(vel), abi.dptr(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle pressure particles status {rc}")
+    return out
