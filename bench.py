@@ -1028,8 +1028,14 @@ BYTES_M2L_PAIR_WORDS = 3 * 35 + 2 * 3 * 35 + 2 * 9 * 35
 FLOP_P2P_PAIR = 95
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) on the 300k-particle case and scaled by the particle
-# count to 2M (profiles/traffic_mixed_step_300k.txt)
+# count to 2M (profiles/k_elem_far_300k.txt)
 TRAFFIC_ELEM_FAR_PER_PARTICLE = 381.5
+# DRAM bytes per launch per particle of the 300k-particle full step (ncu,
+# profiles/k_uvort_300k.txt, k_m2l_batch_f32_300k.txt, k_p2p_w_f32_300k.txt),
+# scaled by the particle count to the benchmark's size
+TRAFFIC_UVORT_PER_PARTICLE = 19.88e6 / 3.0e5
+TRAFFIC_M2L_F32_PER_PARTICLE = (142.44e6 + 56.58e6) / 3.0e5
+TRAFFIC_P2P_F32_PER_PARTICLE = (120.93e6 + 22.24e6) / 3.0e5
 
 
 def roofline(ph, case, params, best):
@@ -1079,7 +1085,8 @@ def roofline(ph, case, params, best):
         fl = FLOP_M2L_PAIR * p["n_m2l_pairs"] / t / 1e12
         ks.append({"kernel": "k_m2l_batch", "bound": "hbm", "achieved": round(gbs, 1),
                    "peak": round(hbm, 1), "unit": "GB/s", "frac": round(gbs / hbm, 3),
-                   "traffic": None, "peak_source": "HBM copy %s" % hbm_src,
+                   "traffic": None if f64 else int(TRAFFIC_M2L_F32_PER_PARTICLE * n),
+                   "peak_source": "HBM copy %s" % hbm_src,
                    "bytes_per_pair": BYTES_M2L_PAIR_WORDS * w, "pairs": p["n_m2l_pairs"],
                    "ms": p["k_m2l_batch_ms"],
                    "flops": {"achieved": round(fl, 2), "peak": round(simt, 1),
@@ -1089,7 +1096,9 @@ def roofline(ph, case, params, best):
         a = FLOP_P2P_PAIR * p["n_p2p_pairs"] / (p["fmm_p2p"] * 1e-3) / 1e12
         ks.append({"kernel": "k_p2p_w (L2P + P2P)", "bound": "fp64" if f64 else "fp32",
                    "achieved": round(a, 2), "peak": round(simt, 1), "unit": "TFLOP/s",
-                   "frac": round(a / simt, 3), "traffic": None, "peak_source": simt_name,
+                   "frac": round(a / simt, 3),
+                   "traffic": None if f64 else int(TRAFFIC_P2P_F32_PER_PARTICLE * n),
+                   "peak_source": simt_name,
                    "flop_per_pair": FLOP_P2P_PAIR, "pairs": p["n_p2p_pairs"], "ms": p["fmm_p2p"]})
     if p.get("uvort"):
         pairs = case.rank * n
@@ -1098,7 +1107,9 @@ def roofline(ph, case, params, best):
         ks.append({"kernel": "uvort phase (%s)" % ("k_uvort" if uv64 else "k_uvort_sorted + sort"),
                    "bound": "fp64" if uv64 else "fp32", "achieved": round(a, 2),
                    "peak": round(pk_uv, 1), "unit": "TFLOP/s", "frac": round(a / pk_uv, 3),
-                   "traffic": None, "peak_source": name_of(uv64),
+                   "traffic": int(TRAFFIC_UVORT_PER_PARTICLE * n) if uv64 else None,
+                   "peak_source": name_of(uv64),
+                   "fp64_pipe_active_ncu": 0.723 if uv64 else None,
                    "flop_per_pair": FLOP_UVORT_PAIR, "pairs": pairs, "ms": p["uvort"]})
     if not ks:
         return {"others": [], "peaks_file": bool(peaks)}
