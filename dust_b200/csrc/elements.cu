@@ -173,10 +173,61 @@ __global__ void __launch_bounds__(EP_T) k_elements_vel(int n, const double *pts,
   vel[3 * (size_t)t + 2] = v[2] * k4pi + u2;
 }
 
+// The same sum for a few points (the wake's points): the panels are split
+// into chunks over blockIdx.y so that more than a handful of CTAs share the
+// work; each chunk adds its part atomically into vel (zeroed first), the
+// first chunk also the lines and u_inf.
+#define EPC_PANELS 32
+__global__ void __launch_bounds__(EP_T) k_elements_vel_chunk(int n, const double *pts,
+                                                             ElemDev e, double u0, double u1,
+                                                             double u2, double *vel) {
+  __shared__ PanelGeo s_p[EP_TILE];
+  const int t = blockIdx.x * EP_T + threadIdx.x;
+  const bool act = t < n;
+  double pos[3] = {0, 0, 0};
+  if (act)
+    for (int c = 0; c < 3; ++c) pos[c] = pts[3 * (size_t)t + c];
+  double v[3] = {0, 0, 0};
+  const int ntot = e.nbody + e.nwake;
+  const int q_lo = blockIdx.y * EPC_PANELS, q_hi = min(ntot, q_lo + EPC_PANELS);
+  for (int p0 = q_lo; p0 < q_hi; p0 += EP_TILE) {
+    __syncthreads();
+    const int m = min(EP_TILE, q_hi - p0);
+    const int words = sizeof(PanelGeo) / 8;
+    for (int w = threadIdx.x; w < m * words; w += EP_T) {
+      const int pp = w / words, ww = w % words, g = p0 + pp;
+      const PanelGeo *src = g < e.nbody ? e.body + g : e.wake + (g - e.nbody);
+      ((double *)&s_p[pp])[ww] = ((const double *)src)[ww];
+    }
+    __syncthreads();
+    if (act)
+      for (int q = 0; q < m; ++q) {
+        double u[3];
+        vel_pan(e.rp, s_p[q], pos, u);
+        for (int c = 0; c < 3; ++c) v[c] += u[c];
+      }
+  }
+  if (!act) return;
+  if (blockIdx.y == 0)
+    for (int q = 0; q < e.nline; ++q) {
+      double u[3];
+      vel_line(e.rp, e.lines[q], pos, u);
+      for (int c = 0; c < 3; ++c) v[c] += u[c];
+    }
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+  const double w[3] = {u0, u1, u2};
+  for (int c = 0; c < 3; ++c)
+    atomicAdd(vel + 3 * (size_t)t + c, v[c] * k4pi + (blockIdx.y == 0 ? w[c] : 0.0));
+}
+
 int elements_vel_points(const ElemDev &e, int n, const double *pts, const double *u_inf,
                         double *vel, cudaStream_t st) {
   if (n <= 0) return DUST_OK;
-  k_elements_vel<<<nblk(n, EP_T), EP_T, 0, st>>>(n, pts, e, u_inf[0], u_inf[1], u_inf[2], vel);
+  const int ntot = e.nbody + e.nwake;
+  const int ny = std::max(1, (ntot + EPC_PANELS - 1) / EPC_PANELS);
+  DUST_CUDA(cudaMemsetAsync(vel, 0, (size_t)n * 24, st));
+  k_elements_vel_chunk<<<dim3(nblk(n, EP_T), ny), EP_T, 0, st>>>(n, pts, e, u_inf[0], u_inf[1],
+                                                                  u_inf[2], vel);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }
