@@ -766,6 +766,99 @@ __global__ void __launch_bounds__(UV2_T) k_uvort(int npts, const double *pts, in
   }
 }
 
+// FP64 uvort fused with the particles' term of the pressure equation
+// (assemble_pressure_sys, src/linsys/mod_pressure_equation.f90:170-186):
+// both sums run over the same (point, particle) pairs and share the
+// difference, rho^2 and rho^-3, so the pressure term adds four FMAs per pair
+// to k_uvort's nineteen FP64 operations instead of a second pass over the
+// particles.  pt[i] = sum_q (x_q - p_i) . (dir_q x vel_q) mag_q rho^-3.
+__global__ void __launch_bounds__(UV2_T) k_uvort_pres(int npts, const double *pts, int n,
+                                                      const double *cen, const double *dir,
+                                                      const double *mag, const double *rv,
+                                                      const double *vel, int chunk, double *uv,
+                                                      double *pt) {
+  __shared__ __align__(16) double s_q[UV2_TILE][14];
+  const int t0 = blockIdx.x * UV2_T * UVD_PPT + threadIdx.x;
+  const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
+  double pos[UVD_PPT][3], v[UVD_PPT][3], pr[UVD_PPT];
+#pragma unroll
+  for (int i = 0; i < UVD_PPT; ++i) {
+    const int t = t0 + i * UV2_T;
+    for (int c = 0; c < 3; ++c) {
+      pos[i][c] = t < npts ? pts[3 * (size_t)t + c] : 0.0;
+      v[i][c] = 0.0;
+    }
+    pr[i] = 0.0;
+  }
+  for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
+    __syncthreads();
+    const int q = q0 + threadIdx.x;
+    const int m = min(UV2_TILE, q_hi - q0);
+    if (threadIdx.x < m) {
+      const double mg = mag[q], r = rv[q];
+      double *w = s_q[threadIdx.x];
+      const double x = cen[3 * (size_t)q], y = cen[3 * (size_t)q + 1], z = cen[3 * (size_t)q + 2];
+      const double dx_ = dir[3 * (size_t)q], dy_ = dir[3 * (size_t)q + 1],
+                   dz_ = dir[3 * (size_t)q + 2];
+      const double ax = mg * dx_, ay = mg * dy_, az = mg * dz_;
+      const double vx = vel[3 * (size_t)q], vy = vel[3 * (size_t)q + 1],
+                   vz = vel[3 * (size_t)q + 2];
+      w[0] = x, w[1] = y, w[2] = z, w[3] = r * r;
+      w[4] = ax, w[5] = ay, w[6] = az;
+      w[7] = y * az - z * ay, w[8] = z * ax - x * az, w[9] = x * ay - y * ax;
+      // -(mag dir x vel): the pair term is (p - x_q) . (-w)
+      w[10] = -mg * (dy_ * vz - dz_ * vy);
+      w[11] = -mg * (dz_ * vx - dx_ * vz);
+      w[12] = -mg * (dx_ * vy - dy_ * vx);
+      w[13] = 0.0;
+    }
+    __syncthreads();
+    double A[UVD_PPT][3], W[UVD_PPT][3], Pq[UVD_PPT];
+#pragma unroll
+    for (int i = 0; i < UVD_PPT; ++i) {
+      for (int c = 0; c < 3; ++c) A[i][c] = W[i][c] = 0.0;
+      Pq[i] = 0.0;
+    }
+#pragma unroll 2
+    for (int u = 0; u < m; ++u) {
+      const double2 *w = (const double2 *)s_q[u];
+      const double2 X = w[0], Y = w[1], Z = w[2], P = w[3], Q = w[4], R = w[5], S = w[6];
+      // X = (x, y), Y = (z, r_v^2), Z = (ax, ay), P = (az, wx), Q = (wy, wz),
+      // R = (-ux, -uy), S = (-uz, 0), u = mag dir x vel
+#pragma unroll
+      for (int i = 0; i < UVD_PPT; ++i) {
+        const double dx = pos[i][0] - X.x, dy = pos[i][1] - X.y, dz = pos[i][2] - Y.x;
+        const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, Y.y)));
+        const double ir = rsqrt_hh(r2);
+        const double c = ir * ir * ir;
+        A[i][0] = fma(c, Z.x, A[i][0]);
+        A[i][1] = fma(c, Z.y, A[i][1]);
+        A[i][2] = fma(c, P.x, A[i][2]);
+        W[i][0] = fma(c, P.y, W[i][0]);
+        W[i][1] = fma(c, Q.x, W[i][1]);
+        W[i][2] = fma(c, Q.y, W[i][2]);
+        Pq[i] = fma(c, fma(dx, R.x, fma(dy, R.y, dz * S.x)), Pq[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < UVD_PPT; ++i) {
+      v[i][0] -= pos[i][1] * A[i][2] - pos[i][2] * A[i][1] - W[i][0];
+      v[i][1] -= pos[i][2] * A[i][0] - pos[i][0] * A[i][2] - W[i][1];
+      v[i][2] -= pos[i][0] * A[i][1] - pos[i][1] * A[i][0] - W[i][2];
+      pr[i] += Pq[i];
+    }
+  }
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+#pragma unroll
+  for (int i = 0; i < UVD_PPT; ++i) {
+    const int t = t0 + i * UV2_T;
+    if (t < npts) {
+      for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t + c, v[i][c] * k4pi);
+      atomicAdd(pt + t, pr[i]);
+    }
+  }
+}
+
 // FP32C uvort on particles sorted along a Morton curve: a tile of 128
 // consecutive particles is spatially compact, so coordinates relative to the
 // tile's first particle are small and are rounded to FP32 once per tile.
@@ -1082,6 +1175,43 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
     }
   }
   if (nl > 0) k_uvort_lines<<<nblk(n_pts, 128), 128, 0, st>>>(n_pts, pts, e, uvort);
+  DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+// ------------------------------------- uvort with the pressure particle term
+// dust_points_uvort_pressure_device: the FP64 uvort sum of
+// dust_points_uvort_device and the pressure equation's particle term in one
+// pass (k_uvort_pres); the end vortices go to uvort as before.
+static DevBuf g_uvp_raw, g_uvp_geo;  // end-vortex records (one host thread)
+
+extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n_pts,
+                                                 const double *pts, int n, const double *cen,
+                                                 const double *dir, const double *mag,
+                                                 const double *r_vortex, const double *vel,
+                                                 const dust_lines *end_vort, double *uvort,
+                                                 double *pterm, void *stream) {
+  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
+    return DUST_ERR_BAD_ARG;
+  if (n_pts > 0 && !pterm) return DUST_ERR_BAD_ARG;
+  if (n > 0 && !vel) return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), false,
+                             g_uvp_raw, g_uvp_geo, e, st));
+  DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
+  DUST_CUDA(cudaMemsetAsync(pterm, 0, (size_t)n_pts * 8, st));
+  if (n > 0) {
+    const int pb = (int)nblk(n_pts, UV2_T * UVD_PPT);
+    const int want = std::max(1, (148 * 8 + pb - 1) / pb);
+    int chunk = (n + want - 1) / want;
+    chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);
+    const int nch = (n + chunk - 1) / chunk;
+    k_uvort_pres<<<dim3(pb, nch), UV2_T, 0, st>>>(n_pts, pts, n, cen, dir, mag, r_vortex, vel,
+                                                  chunk, uvort, pterm);
+  }
+  points_lines_add(n_pts, pts, e, uvort, st);
   DUST_CUDA(cudaGetLastError());
   return DUST_OK;
 }

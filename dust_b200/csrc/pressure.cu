@@ -446,6 +446,18 @@ extern "C" int dust_pressure_size(const dust_pressure *p, int *n_sp, int *nstati
   return DUST_OK;
 }
 
+// b[i] += term[id[i]]: the particle term evaluated at the element centres
+__global__ void k_pres_add_term(int nsp, const int *id, const double *term, double *b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nsp) b[i] += term[id[i]];
+}
+
+static int pres_assemble(dust_pressure *p, const dust_linsys *ls, const double *bern, int n,
+                         const double *cen, const double *dir, const double *mag,
+                         const double *r_vortex, const double *vel, const double *pterm,
+                         const dust_panels *wake, const double *wake_vv,
+                         const dust_lines *end_vort, const double *end_vv, void *stream);
+
 extern "C" int dust_pressure_assemble_device(dust_pressure *p, const dust_linsys *ls,
                                              const double *bern, int n, const double *cen,
                                              const double *dir, const double *mag,
@@ -453,6 +465,26 @@ extern "C" int dust_pressure_assemble_device(dust_pressure *p, const dust_linsys
                                              const dust_panels *wake, const double *wake_vv,
                                              const dust_lines *end_vort, const double *end_vv,
                                              void *stream) {
+  return pres_assemble(p, ls, bern, n, cen, dir, mag, r_vortex, vel, nullptr, wake, wake_vv,
+                       end_vort, end_vv, stream);
+}
+
+extern "C" int dust_pressure_assemble_terms_device(dust_pressure *p, const dust_linsys *ls,
+                                                   const double *bern, const double *pterm,
+                                                   const dust_panels *wake,
+                                                   const double *wake_vv,
+                                                   const dust_lines *end_vort,
+                                                   const double *end_vv, void *stream) {
+  if (!pterm) return DUST_ERR_BAD_ARG;
+  return pres_assemble(p, ls, bern, 0, nullptr, nullptr, nullptr, nullptr, nullptr, pterm, wake,
+                       wake_vv, end_vort, end_vv, stream);
+}
+
+static int pres_assemble(dust_pressure *p, const dust_linsys *ls, const double *bern, int n,
+                         const double *cen, const double *dir, const double *mag,
+                         const double *r_vortex, const double *vel, const double *pterm,
+                         const dust_panels *wake, const double *wake_vv,
+                         const dust_lines *end_vort, const double *end_vv, void *stream) {
   if (!p || !ls || !ls->el || ls->n != p->n || n < 0) return DUST_ERR_BAD_ARG;
   if (n > 0 && (!cen || !dir || !mag || !r_vortex || !vel)) return DUST_ERR_BAD_ARG;
   const int nw = wake ? wake->n : 0, ne = end_vort ? end_vort->n : 0;
@@ -509,6 +541,7 @@ extern "C" int dust_pressure_assemble_device(dust_pressure *p, const dust_linsys
     k_pres_particles<<<dim3(nbx, ny), PR_T, 0, st>>>(ls->el, id, nsp, n, cen, dir, mag,
                                                      r_vortex, vel, chunk, b);
   }
+  if (pterm) k_pres_add_term<<<nblk(nsp, 128), 128, 0, st>>>(nsp, id, pterm, b);
   if (nw + ne > 0)
     k_pres_wake<<<nblk(nsp, 128), 128, 0, st>>>(ls->el, id, nsp, nw, wake ? wake->n_ver : nullptr,
                                                 wake ? wake->ver : nullptr,

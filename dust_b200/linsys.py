@@ -154,6 +154,17 @@ class Pressure:
             C.byref(end_vort) if end_vort is not None else None, P(end_vv),
             C.c_void_p(stream)), "dust_pressure_assemble_device")
 
+    def assemble_terms_device(self, bern=None, pterm=None, wake=None, wake_vv=None,
+                              end_vort=None, end_vv=None, stream=0):
+        """assemble_device with the particle term already evaluated at every
+        element centre (pterm, device tensor of the system's rank)."""
+        P = self._p
+        check(lib().dust_pressure_assemble_terms_device(
+            self._h, self.ls._h, P(bern), P(pterm),
+            C.byref(wake) if wake is not None else None, P(wake_vv),
+            C.byref(end_vort) if end_vort is not None else None, P(end_vv),
+            C.c_void_p(stream)), "dust_pressure_assemble_terms_device")
+
     def solve_device(self, res, stream=0):
         check(lib().dust_pressure_solve_device(self._h, self._p(res), C.c_void_p(stream)),
               "dust_pressure_solve_device")

@@ -184,6 +184,11 @@ class DeviceStepper:
                    else None)
         if self.pr is not None:
             self.res_pres = torch.zeros(self.pr.n_sp, dtype=torch.float64, device=dev)
+            self.pterm = torch.zeros(c.rank, dtype=torch.float64, device=dev)
+        # with an FP64 direct uvort the pressure equation's particle term is
+        # evaluated in the same pass (dust_points_uvort_pressure_device)
+        self.fused_pterm = (self.pr is not None and not fmm_uvort and
+                            self._ups.precision == abi.DUST_PREC_FP64)
         self.steps_done = 0
         self.oc = Octree(params)
         self._ps = params.struct()
@@ -220,6 +225,13 @@ class DeviceStepper:
             check(lib().dust_fmm_points_uvort_device(self.oc._h, C.byref(lines), P(self.euv),
                                                      C.c_void_p(stream)),
                   "dust_fmm_points_uvort_device")
+        elif self.fused_pterm:
+            # the particles' velocities of the previous update go into the
+            # pressure term
+            check(lib().dust_points_uvort_pressure_device(
+                C.byref(self._ups), c.rank, P(self.ecen), self.n, P(self.cen), P(self.dir),
+                P(self.mag), P(self.rv), P(self.vel), C.byref(lines), P(self.euv),
+                P(self.pterm), C.c_void_p(stream)), "dust_points_uvort_pressure_device")
         else:
             check(lib().dust_points_uvort_device(C.byref(self._ups), c.rank, P(self.ecen),
                                                  self.n, P(self.cen), P(self.dir), P(self.mag),
@@ -238,8 +250,11 @@ class DeviceStepper:
         if self.pr is not None:
             # the particles' velocities of the previous update (the body is at
             # rest in the frame of its Bernoulli sources)
-            self.pr.assemble_device(None, (self.cen, self.dir, self.mag, self.rv), self.vel,
-                                    stream=stream)
+            if self.fused_pterm:
+                self.pr.assemble_terms_device(None, self.pterm, stream=stream)
+            else:
+                self.pr.assemble_device(None, (self.cen, self.dir, self.mag, self.rv), self.vel,
+                                        stream=stream)
             if self.steps_done > 0:
                 self.pr.solve_device(self.res_pres, stream)
         self._mark()

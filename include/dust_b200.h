@@ -242,6 +242,21 @@ DUST_API int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts,
                                       const dust_lines *end_vort, double *uvort,
                                       void *stream);
 
+/* dust_points_uvort_device (FP64 whatever prm->precision) together with the
+ * particles' rotational term of the pressure equation at the same points
+ * (assemble_pressure_sys, src/linsys/mod_pressure_equation.f90:170-186):
+ *   pterm[i] = sum_q (x_q - pts_i) . (dir_q x vel_q) mag_q /
+ *              (|x_q - pts_i|^2 + r_q^2)^(3/2),
+ * vel(3, n) the particles' velocities, pterm[n_pts] device output.  Both
+ * sums run in one pass over the (point, particle) pairs and share the
+ * distance and the kernel coefficient.  Device arrays, queued on `stream`. */
+DUST_API int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n_pts,
+                                               const double *pts, int n, const double *cen,
+                                               const double *dir, const double *mag,
+                                               const double *r_vortex, const double *vel,
+                                               const dust_lines *end_vort, double *uvort,
+                                               double *pterm, void *stream);
+
 /* No counterpart in the reference.  Same result as dust_points_uvort_device
  * (same kernels and summation order) for callers that must not allocate
  * device memory during a step: a host code that hands the whole device to
@@ -677,6 +692,16 @@ DUST_API int dust_pressure_assemble_device(dust_pressure *p, const dust_linsys *
                                            const dust_panels *wake, const double *wake_vv,
                                            const dust_lines *end_vort, const double *end_vv,
                                            void *stream);
+
+/* dust_pressure_assemble_device with the particles' term already evaluated
+ * at every element centre (pterm[rank], device; e.g. by
+ * dust_points_uvort_pressure_device in the same pass as uvort): the term of
+ * each surface panel is taken from its element's entry. */
+DUST_API int dust_pressure_assemble_terms_device(dust_pressure *p, const dust_linsys *ls,
+                                                 const double *bern, const double *pterm,
+                                                 const dust_panels *wake, const double *wake_vv,
+                                                 const dust_lines *end_vort, const double *end_vv,
+                                                 void *stream);
 
 /* solve_pressure_sys (:243-387): the block LU sequence of solve_linsys on
  * A_pres (static LU reused, Schur update and LU of the moving block, getrs);

@@ -144,3 +144,30 @@ def test_gpu_pressure_matches_oracle():
     assert rel(b32, b) < 1e-6 and rel(res32.cpu().numpy(), ref) < 1e-6
     pr32.close()
     ls32.close()
+    # the particle term evaluated in the uvort pass at every element centre
+    from dust_b200._lib import check, lib
+    cen_el, _, _ = O.panel_geometry(c["step"])
+    pts = T(cen_el)
+    uv, uv2, pt = (torch.zeros((n, 3), dtype=torch.float64, device=dev),
+                   torch.zeros((n, 3), dtype=torch.float64, device=dev),
+                   torch.zeros(n, dtype=torch.float64, device=dev))
+    ps = c["prm"].struct()
+    check(lib().dust_points_uvort_pressure_device(C.byref(ps), n, dp(pts), parts[2].shape[0],
+                                                  dp(parts[0]), dp(parts[1]), dp(parts[2]),
+                                                  dp(parts[3]), dp(T(c["vel"])), C.byref(lp),
+                                                  dp(uv), dp(pt), None), "uvort+pressure")
+    check(lib().dust_points_uvort_device(C.byref(ps), n, dp(pts), parts[2].shape[0],
+                                         dp(parts[0]), dp(parts[1]), dp(parts[2]), dp(parts[3]),
+                                         C.byref(lp), dp(uv2), None), "uvort")
+    torch.cuda.synchronize()
+    assert rel(uv.cpu().numpy(), uv2.cpu().numpy()) < 1e-13
+    ref_pt = O.pressure_particles(cen_el, *c["parts"], c["vel"])
+    assert rel(pt.cpu().numpy(), ref_pt) < 1e-12
+    ls2 = linsys.Linsys(c["prm"], n, nst, c["init"], *w)
+    pr2 = linsys.Pressure(ls2)
+    ls2.assemble_linsys(c["step"], *w)
+    pr2.assemble_terms_device(bern, pt, wp, wvv, lp, evv)
+    _, bt = pr2.get_system()
+    assert rel(bt, b) < 1e-12
+    pr2.close()
+    ls2.close()
