@@ -143,3 +143,11 @@ int morton_perm(const dust_fmm_params *prm, int n, const double *cen, DevBuf &sc
 int points_uvort_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
                      const double *cen, const double *dir, const double *mag, const double *rv,
                      const ElemDev &lines, DevBuf &scratch, double *uv, cudaStream_t st);
+
+// gemv.cu: y = alpha A x + beta y and y = alpha A^T x + beta y (A column-major
+// m x k, device arrays), and out[0] = max |v_i|, out[1] = ||v||_2 (device)
+template <typename T>
+int gemv_n(cudaStream_t st, int m, int k, T alpha, const T *A, int lda, const T *x, T beta, T *y);
+template <typename T>
+int gemv_t(cudaStream_t st, int m, int k, T alpha, const T *A, int lda, const T *x, T beta, T *y);
+int vec_absmax_nrm2(cudaStream_t st, int n, const double *v, double *out_dev);

@@ -55,8 +55,7 @@ int linsys_matmat(const dust_linsys *L, int nc, const double *X, int ldx, double
     // one vector: matrix-vector products (bandwidth bound)
     auto gemv = [&](int m, int k, const double *Ap, int lda, const double *Xp, double *Yp,
                     const double *beta) {
-      return cublasDgemv(cb, CUBLAS_OP_N, m, k, &one, Ap, lda, Xp, 1, beta, Yp, 1) ==
-             CUBLAS_STATUS_SUCCESS;
+      return gemv_n<double>(st, m, k, 1.0, Ap, lda, Xp, *beta, Yp) == DUST_OK;
     };
     if (nst == 0) {
       ok = gemv(n, n, A, n, X, Y, &zero);
@@ -123,19 +122,13 @@ static int gm_precond(dust_linsys *L, dust_precond *P, const double *v, double *
   }
   double *t = (double *)tmp, *y = t + n;
   float *v32 = (float *)(y + n), *z32 = v32 + nst;
-  const float onef = 1.0f, zerof = 0.0f;
-  const double one = 1.0, mone = -1.0;
   k_to_f32<<<nblk(nst, 256), 256, 0, st>>>(nst, v, v32);
-  if (cublasSgemv(cb, CUBLAS_OP_N, nst, nst, &onef, (const float *)L->ainv32.p, nst, v32, 1,
-                  &zerof, z32, 1) != CUBLAS_STATUS_SUCCESS)
-    return DUST_ERR_CUDA;
+  DUST_TRY(gemv_n<float>(st, nst, nst, 1.0f, (const float *)L->ainv32.p, nst, v32, 0.0f, z32));
   k_to_f64<<<nblk(nst, 256), 256, 0, st>>>(nst, z32, z);
   if (nmv == 0) return DUST_OK;
   DUST_CUDA(cudaMemsetAsync(t, 0, (size_t)nst * 8, st));
   DUST_CUDA(cudaMemcpyAsync(t + nst, v + nst, (size_t)nmv * 8, cudaMemcpyDeviceToDevice, st));
-  if (cublasDgemv(cb, CUBLAS_OP_N, nmv, nst, &mone, (const double *)L->A.p + nst, n, z, 1, &one,
-                  t + nst, 1) != CUBLAS_STATUS_SUCCESS)
-    return DUST_ERR_CUDA;
+  DUST_TRY(gemv_n<double>(st, nmv, nst, -1.0, (const double *)L->A.p + nst, n, z, 1.0, t + nst));
   pc_apply(P, t, y, st);
   DUST_CUDA(cudaMemcpyAsync(z + nst, y + nst, (size_t)nmv * 8, cudaMemcpyDeviceToDevice, st));
   return DUST_OK;
@@ -181,10 +174,12 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
   char *ptmp = (char *)(hd + nhd);  // gm_precond scratch
   auto precond = [&](const double *v, double *out) { return gm_precond(L, P, v, out, ptmp, st, cb); };
   const double *b = (const double *)L->b.p;
-  const double one = 1.0, mone = -1.0, zero = 0.0;
   cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST);
   auto nrm2 = [&](const double *v, double *out) {  // synchronises the stream
-    return cublasDnrm2(cb, n, v, 1, out) == CUBLAS_STATUS_SUCCESS;
+    double h2[2];
+    return vec_absmax_nrm2(st, n, v, hd + 2 * (m + 1)) == DUST_OK &&
+           cudaMemcpyAsync(h2, hd + 2 * (m + 1), 16, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+           cudaStreamSynchronize(st) == cudaSuccess && ((*out = h2[1]), true);
   };
   auto resid = [&]() -> int {  // r = b - A x
     DUST_TRY(linsys_matmat(L, 1, x, n, w, n, st, cb));
@@ -219,20 +214,14 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
       // result stay on the device until one copy to the host
       for (int pass = 0; pass < 2; ++pass) {
         double *hp = hd + (size_t)pass * (m + 1);
-        if (cublasDgemv(cb, CUBLAS_OP_T, n, k + 1, &one, V, n, w, 1, &zero, hp, 1) !=
-                CUBLAS_STATUS_SUCCESS ||
-            cublasDgemv(cb, CUBLAS_OP_N, n, k + 1, &mone, V, n, hp, 1, &one, w, 1) !=
-                CUBLAS_STATUS_SUCCESS)
-          return DUST_ERR_CUDA;
+        DUST_TRY(gemv_t<double>(st, n, k + 1, 1.0, V, n, w, 0.0, hp));
+        DUST_TRY(gemv_n<double>(st, n, k + 1, -1.0, V, n, hp, 1.0, w));
       }
-      cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_DEVICE);
-      const bool nok = cublasDnrm2(cb, n, w, 1, hd + 2 * (m + 1)) == CUBLAS_STATUS_SUCCESS;
-      cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST);
-      if (!nok) return DUST_ERR_CUDA;
+      DUST_TRY(vec_absmax_nrm2(st, n, w, hd + 2 * (m + 1)));
       DUST_CUDA(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * nhd, cudaMemcpyDeviceToHost, st));
       DUST_CUDA(cudaStreamSynchronize(st));
       for (int q = 0; q <= k; ++q) hc[q] = hh[q] + hh[(size_t)(m + 1) + q];
-      const double hn = hh[2 * (size_t)(m + 1)];
+      const double hn = hh[2 * (size_t)(m + 1) + 1];
       hc[k + 1] = hn;
       if (hn > 0.0) k_scale<<<nblk(n, 256), 256, 0, st>>>(n, 1.0 / hn, w, V + (size_t)(k + 1) * n);
       // Givens rotations on the new column
@@ -260,8 +249,7 @@ int linsys_gmres_nn(dust_linsys *L, double *x, dust_solve_report *rep) {
       y[q] = d != 0.0 ? sum / d : 0.0;
     }
     DUST_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
-    if (cublasDgemv(cb, CUBLAS_OP_N, n, k, &one, V, n, hd, 1, &zero, u, 1) != CUBLAS_STATUS_SUCCESS)
-      return DUST_ERR_CUDA;
+    DUST_TRY(gemv_n<double>(st, n, k, 1.0, V, n, hd, 0.0, u));
     DUST_TRY(precond(u, z));
     k_add<<<nblk(n, 256), 256, 0, st>>>(n, z, x);
     DUST_TRY(resid());

@@ -100,7 +100,7 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   // work: Y (nst x nmv), S (nmv x nmv), Ads32 (nmv x nst), Asd32 (nst x nmv),
   // vectors
   size_t need = 4 * ((size_t)nst * nmv * 3 + (size_t)nmv * nmv + (size_t)n * 4) + 8 * (size_t)n * 4 +
-                (size_t)nmv * 8 + 2048;
+                (size_t)nmv * 8 + 8192;
   DUST_TRY(devbuf_grow(L->mx, need));
   char *b = (char *)L->mx.p;
   auto take = [&](size_t bytes) {
@@ -120,6 +120,7 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   int *piv = (int *)take((size_t)nmv * 4 + 64);
   int *info = piv + nmv;
   int *perm = (int *)take((size_t)nmv * 4);
+  double *nrm = (double *)take(64);  // max |.| and 2-norms of the residual and x
   const bool use_perm = (size_t)nmv * 4 <= 200 * 1024;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -151,12 +152,9 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
   cudaEventRecord(e1, st);
   DUST_CUDA(cudaMemsetAsync(rs, 0, (size_t)n * 8, st));
   k_rowabs_blocks<<<dim3(nblk(n, 128), nblk(n, RA_COLS)), 128, 0, st>>>(n, nst, As, A, rs);
-  int imax = 0;
-  if (cublasIdamax(L->cb, n, rs, 1, &imax) != CUBLAS_STATUS_SUCCESS) return DUST_ERR_CUDA;
+  DUST_TRY(vec_absmax_nrm2(st, n, rs, nrm));
   double anorm = 0.0;
-  DUST_CUDA(cudaMemcpyAsync(&anorm, rs + imax - 1, 8, cudaMemcpyDeviceToHost, st));
-  const double one = 1.0, mone = -1.0, zero = 0.0;
-  const float onef = 1.0f, monef = -1.0f, zerof = 0.0f;
+  DUST_CUDA(cudaMemcpyAsync(&anorm, nrm, 8, cudaMemcpyDeviceToHost, st));
   DUST_CUDA(cudaMemsetAsync(x, 0, (size_t)n * 8, st));
   DUST_CUDA(cudaMemcpyAsync(r, L->b.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
   double worst = 1e300;
@@ -165,27 +163,18 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
     if (it > 0) {
       // r = b - A x, blockwise with the unfactored static block
       DUST_CUDA(cudaMemcpyAsync(r, L->b.p, (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
-      if (nst > 0 &&
-          cublasDgemv(L->cb, CUBLAS_OP_N, nst, nst, &mone, As, nst, x, 1, &one, r, 1) !=
-              CUBLAS_STATUS_SUCCESS)
-        return DUST_ERR_CUDA;
+      if (nst > 0) DUST_TRY(gemv_n<double>(st, nst, nst, -1.0, As, nst, x, 1.0, r));
       if (nmv > 0) {
         // columns nst.. of all rows, and the static columns of the moving rows
-        if (cublasDgemv(L->cb, CUBLAS_OP_N, n, nmv, &mone, A + (size_t)nst * n, n, x + nst, 1,
-                        &one, r, 1) != CUBLAS_STATUS_SUCCESS)
-          return DUST_ERR_CUDA;
-        if (nst > 0 && cublasDgemv(L->cb, CUBLAS_OP_N, nmv, nst, &mone, A + nst, n, x, 1, &one,
-                                   r + nst, 1) != CUBLAS_STATUS_SUCCESS)
-          return DUST_ERR_CUDA;
+        DUST_TRY(gemv_n<double>(st, n, nmv, -1.0, A + (size_t)nst * n, n, x + nst, 1.0, r));
+        if (nst > 0) DUST_TRY(gemv_n<double>(st, nmv, nst, -1.0, A + nst, n, x, 1.0, r + nst));
       }
-      int ir = 0, ix = 0;
-      if (cublasIdamax(L->cb, n, r, 1, &ir) != CUBLAS_STATUS_SUCCESS ||
-          cublasIdamax(L->cb, n, x, 1, &ix) != CUBLAS_STATUS_SUCCESS)
-        return DUST_ERR_CUDA;
-      double hr = 0, hx = 0;
-      DUST_CUDA(cudaMemcpyAsync(&hr, r + ir - 1, 8, cudaMemcpyDeviceToHost, st));
-      DUST_CUDA(cudaMemcpyAsync(&hx, x + ix - 1, 8, cudaMemcpyDeviceToHost, st));
+      DUST_TRY(vec_absmax_nrm2(st, n, r, nrm));
+      DUST_TRY(vec_absmax_nrm2(st, n, x, nrm + 2));
+      double hh[4];
+      DUST_CUDA(cudaMemcpyAsync(hh, nrm, 32, cudaMemcpyDeviceToHost, st));
       DUST_CUDA(cudaStreamSynchronize(st));
+      const double hr = hh[0], hx = hh[2];
       double den = anorm * fabs(hx);
       worst = den > 0 ? fabs(hr) / den : fabs(hr);
       if (worst <= tol || it == max_iter) break;
@@ -194,25 +183,18 @@ int linsys_solve_schur_mixed(dust_linsys *L, double *x, double tol, int max_iter
     k_vec_f32<<<nblk(n, 256), 256, 0, st>>>(n, r, r32);
     if (nst > 0) {
       // y_s = Ainv r_s  (in d32[0:nst])
-      if (cublasSgemv(L->cb, CUBLAS_OP_N, nst, nst, &onef, Ainv, nst, r32, 1, &zerof, d32, 1) !=
-          CUBLAS_STATUS_SUCCESS)
-        return DUST_ERR_CUDA;
+      DUST_TRY(gemv_n<float>(st, nst, nst, 1.0f, Ainv, nst, r32, 0.0f, d32));
     }
     if (nmv > 0) {
       DUST_CUDA(cudaMemcpyAsync(t32, r32 + nst, (size_t)nmv * 4, cudaMemcpyDeviceToDevice, st));
-      if (nst > 0 && cublasSgemv(L->cb, CUBLAS_OP_N, nmv, nst, &monef, Ads, nmv, d32, 1, &onef,
-                                 t32, 1) != CUBLAS_STATUS_SUCCESS)
-        return DUST_ERR_CUDA;
+      if (nst > 0) DUST_TRY(gemv_n<float>(st, nmv, nst, -1.0f, Ads, nmv, d32, 1.0f, t32));
       DUST_TRY(lu_getrs<float>(L->cb, st, nmv, 1, S, nmv, piv, t32, nmv,
                                use_perm ? perm : nullptr));
       DUST_CUDA(cudaMemcpyAsync(d32 + nst, t32, (size_t)nmv * 4, cudaMemcpyDeviceToDevice, st));
-      if (nst > 0 && cublasSgemv(L->cb, CUBLAS_OP_N, nst, nmv, &monef, Y, nst, t32, 1, &onef, d32,
-                                 1) != CUBLAS_STATUS_SUCCESS)
-        return DUST_ERR_CUDA;
+      if (nst > 0) DUST_TRY(gemv_n<float>(st, nst, nmv, -1.0f, Y, nst, t32, 1.0f, d32));
     }
     k_vec_add<<<nblk(n, 256), 256, 0, st>>>(n, d32, x);
   }
-  (void)zero;
   DUST_CUDA(cudaGetLastError());
   if (rep) {
     rep->mode_used = DUST_SOLVE_MIXED;
