@@ -541,6 +541,7 @@ def main():
             "steps_advected": 0 if args.no_advect else n_acc,
             "load_error_by_step": load_err_by_step,
             "load_error_max_over_steps": load_err_max,
+            "loads_plain_by_step": [[float(x) for x in l] for l in by_step.get("plain", [])],
             "fp64_sensitivity_floor": floor,
             "headline_rule": "fastest mode whose loads are within max(1e-6, 2 x the FP64 "
                              "sensitivity floor at that step) of the plain FP64 run after "
