@@ -986,6 +986,130 @@ __global__ void __launch_bounds__(UV2_T) k_uvort_sorted(int npts, const double *
       for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t[i] + c, v[i][c] * k4pi);
 }
 
+// sorted block of the fused pass: x y z (double); ax ay az s2 -wx -wy -wz
+// (float) with w = mag (dir x vel) formed in FP64 and rounded once
+__global__ void k_uvp_gather(int n, const uint32_t *perm, const double *cen, const double *dir,
+                             const double *mag, const double *rv, const double *vel, double *X,
+                             float *F) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t q = perm[t];
+  const double m = mag[q];
+  const double dx = dir[3 * (size_t)q], dy = dir[3 * (size_t)q + 1], dz = dir[3 * (size_t)q + 2];
+  const double vx = vel[3 * (size_t)q], vy = vel[3 * (size_t)q + 1], vz = vel[3 * (size_t)q + 2];
+  for (int d = 0; d < 3; ++d) X[(size_t)d * n + t] = cen[3 * (size_t)q + d];
+  F[t] = (float)(m * dx);
+  F[(size_t)n + t] = (float)(m * dy);
+  F[2 * (size_t)n + t] = (float)(m * dz);
+  F[3 * (size_t)n + t] = (float)(rv[q] * rv[q]);
+  F[4 * (size_t)n + t] = (float)(-m * (dy * vz - dz * vy));
+  F[5 * (size_t)n + t] = (float)(-m * (dz * vx - dx * vz));
+  F[6 * (size_t)n + t] = (float)(-m * (dx * vy - dy * vx));
+}
+
+// k_uvort_sorted with the pressure equation's particle term at the same
+// points in the same pass (the FP32C counterpart of k_uvort_pres): per pair
+// the difference, rho^-3 and the cross product of uvort, and d . (-w) rho^-3
+// for the pressure term; 13 values per particle, interleaved in pairs
+// as in k_uvort_sorted (value k of particle q at [q / 2][2 k + q % 2]).
+__global__ void __launch_bounds__(UV2_T) k_uvort_pres_sorted(int npts, const double *pts, int n,
+                                                             const double *X, const float *F,
+                                                             int chunk, double *uv, double *pt) {
+  __shared__ __align__(16) float s_pk[UV2_TILE / 2][28];
+  __shared__ double s_ref[3];
+  int t[UV2_PPT];
+  double pos[UV2_PPT][3], v[UV2_PPT][3], pr[UV2_PPT];
+#pragma unroll
+  for (int i = 0; i < UV2_PPT; ++i) {
+    t[i] = (blockIdx.x * UV2_PPT + i) * UV2_T + threadIdx.x;
+    for (int c = 0; c < 3; ++c) {
+      pos[i][c] = t[i] < npts ? pts[3 * (size_t)t[i] + c] : 0.0;
+      v[i][c] = 0.0;
+    }
+    pr[i] = 0.0;
+  }
+  const int q_lo = blockIdx.y * chunk, q_hi = min(n, q_lo + chunk);
+  for (int q0 = q_lo; q0 < q_hi; q0 += UV2_TILE) {
+    __syncthreads();
+    const int q = q0 + threadIdx.x;
+    const int m = min(UV2_TILE, q_hi - q0);
+    if (threadIdx.x < 3) s_ref[threadIdx.x] = X[(size_t)threadIdx.x * n + q0];
+    __syncthreads();
+    if (threadIdx.x < UV2_TILE) {
+      // particles beyond the chunk: far away (1e6), no strength
+      float val[14] = {-1.0e6f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (threadIdx.x < m) {
+        const float ax = F[q], ay = F[(size_t)n + q], az = F[2 * (size_t)n + q];
+        val[0] = (float)(s_ref[0] - X[q]);
+        val[1] = (float)(s_ref[1] - X[(size_t)n + q]);
+        val[2] = (float)(s_ref[2] - X[2 * (size_t)n + q]);
+        val[3] = F[(size_t)3 * n + q];
+        val[4] = ax, val[5] = ay, val[6] = az;
+        val[7] = -ax, val[8] = -ay, val[9] = -az;
+        val[10] = F[(size_t)4 * n + q];
+        val[11] = F[(size_t)5 * n + q];
+        val[12] = F[(size_t)6 * n + q];
+      }
+      for (int k = 0; k < 14; ++k) s_pk[threadIdx.x >> 1][2 * k + (threadIdx.x & 1)] = val[k];
+    }
+    __syncthreads();
+    float px[UV2_PPT], py[UV2_PPT], pz[UV2_PPT];
+    float2 V[UV2_PPT][3], W[UV2_PPT];
+#pragma unroll
+    for (int i = 0; i < UV2_PPT; ++i) {
+      px[i] = (float)(pos[i][0] - s_ref[0]);
+      py[i] = (float)(pos[i][1] - s_ref[1]);
+      pz[i] = (float)(pos[i][2] - s_ref[2]);
+      for (int c = 0; c < 3; ++c) V[i][c] = make_float2(0.f, 0.f);
+      W[i] = make_float2(0.f, 0.f);
+    }
+    const int mp = (m + 1) >> 1;
+#pragma unroll 2
+    for (int u = 0; u < mp; ++u) {
+      const float4 P0 = *(const float4 *)&s_pk[u][0], P1 = *(const float4 *)&s_pk[u][4],
+                   P2 = *(const float4 *)&s_pk[u][8], P3 = *(const float4 *)&s_pk[u][12],
+                   P4 = *(const float4 *)&s_pk[u][16], P5 = *(const float4 *)&s_pk[u][20],
+                   P6 = *(const float4 *)&s_pk[u][24];
+      const float2 nx = make_float2(P0.x, P0.y), ny = make_float2(P0.z, P0.w),
+                   nz = make_float2(P1.x, P1.y), s2 = make_float2(P1.z, P1.w),
+                   ax = make_float2(P2.x, P2.y), ay = make_float2(P2.z, P2.w),
+                   az = make_float2(P3.x, P3.y), mx = make_float2(P3.z, P3.w),
+                   my = make_float2(P4.x, P4.y), mz = make_float2(P4.z, P4.w),
+                   wx = make_float2(P5.x, P5.y), wy = make_float2(P5.z, P5.w),
+                   wz = make_float2(P6.x, P6.y);
+#pragma unroll
+      for (int i = 0; i < UV2_PPT; ++i) {
+        const float2 dx = __fadd2_rn(make_float2(px[i], px[i]), nx),
+                     dy = __fadd2_rn(make_float2(py[i], py[i]), ny),
+                     dz = __fadd2_rn(make_float2(pz[i], pz[i]), nz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
+        const float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+        const float2 c = __fmul2_rn(__fmul2_rn(ir, ir), ir);
+        const float2 cx = __fmul2_rn(c, dx), cy = __fmul2_rn(c, dy), cz = __fmul2_rn(c, dz);
+        // c (d x alpha)
+        V[i][0] = __ffma2_rn(cy, az, __ffma2_rn(cz, my, V[i][0]));
+        V[i][1] = __ffma2_rn(cz, ax, __ffma2_rn(cx, mz, V[i][1]));
+        V[i][2] = __ffma2_rn(cx, ay, __ffma2_rn(cy, mx, V[i][2]));
+        // c d . (-w): the pair term (x_q - p) . w rho^-3
+        W[i] = __ffma2_rn(cx, wx, __ffma2_rn(cy, wy, __ffma2_rn(cz, wz, W[i])));
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < UV2_PPT; ++i) {
+      // velocity kernel coefficient is -1/rho^3
+      for (int c = 0; c < 3; ++c) v[i][c] -= (double)(V[i][c].x + V[i][c].y);
+      pr[i] += (double)(W[i].x + W[i].y);
+    }
+  }
+  const double k4pi = 1.0 / (4.0 * DUST_PI);
+#pragma unroll
+  for (int i = 0; i < UV2_PPT; ++i)
+    if (t[i] < npts) {
+      for (int c = 0; c < 3; ++c) atomicAdd(uv + 3 * (size_t)t[i] + c, v[i][c] * k4pi);
+      atomicAdd(pt + t[i], pr[i]);
+    }
+}
+
 __global__ void k_uvort_lines(int npts, const double *pts, ElemDev e, double *uv) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts) return;
@@ -1180,10 +1304,12 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
 }
 
 // ------------------------------------- uvort with the pressure particle term
-// dust_points_uvort_pressure_device: the FP64 uvort sum of
+// dust_points_uvort_pressure_device: the uvort sum of
 // dust_points_uvort_device and the pressure equation's particle term in one
-// pass (k_uvort_pres); the end vortices go to uvort as before.
-static DevBuf g_uvp_raw, g_uvp_geo;  // end-vortex records (one host thread)
+// pass, FP64 (k_uvort_pres) or FP32C on Morton-sorted particles
+// (k_uvort_pres_sorted); the end vortices go to uvort as before.
+// end-vortex records and the FP32C pass's sorted particles (one host thread)
+static DevBuf g_uvp_raw, g_uvp_geo, g_uvp_sort;
 
 extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n_pts,
                                                  const double *pts, int n, const double *cen,
@@ -1202,7 +1328,35 @@ extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int
                              g_uvp_raw, g_uvp_geo, e, st));
   DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
   DUST_CUDA(cudaMemsetAsync(pterm, 0, (size_t)n_pts * 8, st));
-  if (n > 0) {
+  if (n > 0 && prm->precision == DUST_PREC_FP32C) {
+    // particles along a Morton curve, then the packed FP32 fused pass
+    const size_t N = (size_t)n;
+    size_t tb = 0;
+    uint32_t *dummy = nullptr;
+    DUST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, dummy, dummy, dummy, dummy, n, 0, 30,
+                                              st));
+    const size_t off_f = round256(16 * N), off_x = off_f + round256(28 * N),
+                 off_t = off_x + round256(24 * N);
+    DUST_TRY(devbuf_grow(g_uvp_sort, off_t + round256(tb)));
+    char *b = (char *)g_uvp_sort.p;
+    uint32_t *k_in = (uint32_t *)b, *v_in = k_in + N, *k_out = v_in + N, *v_out = k_out + N;
+    float *F = (float *)(b + off_f);
+    double *X = (double *)(b + off_x);
+    const double hbox =
+        prm->box_length * std::max(prm->n_box[0], std::max(prm->n_box[1], prm->n_box[2]));
+    k_uv_keys<<<nblk(n, 256), 256, 0, st>>>(n, cen, prm->origin[0], prm->origin[1],
+                                             prm->origin[2], 1024.0 / hbox, k_in, v_in);
+    DUST_CUDA(cub::DeviceRadixSort::SortPairs(b + off_t, tb, k_in, k_out, v_in, v_out, n, 0, 30,
+                                              st));
+    k_uvp_gather<<<nblk(n, 256), 256, 0, st>>>(n, v_out, cen, dir, mag, r_vortex, vel, X, F);
+    const int pb = (int)nblk(n_pts, UV2_T * UV2_PPT);
+    const int want = std::max(1, (148 * 8 + pb - 1) / pb);
+    int chunk = (n + want - 1) / want;
+    chunk = std::max(UV2_TILE, (chunk + UV2_TILE - 1) / UV2_TILE * UV2_TILE);
+    const int nch = (n + chunk - 1) / chunk;
+    k_uvort_pres_sorted<<<dim3(pb, nch), UV2_T, 0, st>>>(n_pts, pts, n, X, F, chunk, uvort,
+                                                         pterm);
+  } else if (n > 0) {
     const int pb = (int)nblk(n_pts, UV2_T * UVD_PPT);
     const int want = std::max(1, (148 * 8 + pb - 1) / pb);
     int chunk = (n + want - 1) / want;

@@ -185,10 +185,10 @@ class DeviceStepper:
         if self.pr is not None:
             self.res_pres = torch.zeros(self.pr.n_sp, dtype=torch.float64, device=dev)
             self.pterm = torch.zeros(c.rank, dtype=torch.float64, device=dev)
-        # with an FP64 direct uvort the pressure equation's particle term is
-        # evaluated in the same pass (dust_points_uvort_pressure_device)
-        self.fused_pterm = (self.pr is not None and not fmm_uvort and
-                            self._ups.precision == abi.DUST_PREC_FP64)
+        # with a direct uvort the pressure equation's particle term is
+        # evaluated in the same pass (dust_points_uvort_pressure_device, in
+        # the uvort's precision)
+        self.fused_pterm = self.pr is not None and not fmm_uvort
         self.steps_done = 0
         self.oc = Octree(params)
         self._ps = params.struct()

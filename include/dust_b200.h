@@ -242,8 +242,10 @@ DUST_API int dust_points_uvort_device(const dust_fmm_params *prm, int n_pts,
                                       const dust_lines *end_vort, double *uvort,
                                       void *stream);
 
-/* dust_points_uvort_device (FP64 whatever prm->precision) together with the
- * particles' rotational term of the pressure equation at the same points
+/* dust_points_uvort_device (FP64, or with prm->precision DUST_PREC_FP32C
+ * packed FP32 pairs on Morton-sorted particles with FP64 sums per tile of
+ * 128) together with the particles' rotational term of the pressure
+ * equation at the same points
  * (assemble_pressure_sys, src/linsys/mod_pressure_equation.f90:170-186):
  *   pterm[i] = sum_q (x_q - pts_i) . (dir_q x vel_q) mag_q /
  *              (|x_q - pts_i|^2 + r_q^2)^(3/2),

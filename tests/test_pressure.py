@@ -163,6 +163,24 @@ def test_gpu_pressure_matches_oracle():
     assert rel(uv.cpu().numpy(), uv2.cpu().numpy()) < 1e-13
     ref_pt = O.pressure_particles(cen_el, *c["parts"], c["vel"])
     assert rel(pt.cpu().numpy(), ref_pt) < 1e-12
+    # the same fused pass in DUST_PREC_FP32C (Morton-sorted packed FP32
+    # pairs): uvort against the FP32C uvort-only pass and the FP64 sum, the
+    # particle term against the oracle
+    ps32 = p32.struct()
+    uv32, uv32b, pt32 = (torch.zeros((n, 3), dtype=torch.float64, device=dev),
+                         torch.zeros((n, 3), dtype=torch.float64, device=dev),
+                         torch.zeros(n, dtype=torch.float64, device=dev))
+    check(lib().dust_points_uvort_pressure_device(C.byref(ps32), n, dp(pts), parts[2].shape[0],
+                                                  dp(parts[0]), dp(parts[1]), dp(parts[2]),
+                                                  dp(parts[3]), dp(T(c["vel"])), C.byref(lp),
+                                                  dp(uv32), dp(pt32), None), "uvort+pressure f32")
+    check(lib().dust_points_uvort_device(C.byref(ps32), n, dp(pts), parts[2].shape[0],
+                                         dp(parts[0]), dp(parts[1]), dp(parts[2]), dp(parts[3]),
+                                         C.byref(lp), dp(uv32b), None), "uvort f32")
+    torch.cuda.synchronize()
+    assert rel(uv32.cpu().numpy(), uv32b.cpu().numpy()) < 1e-13
+    assert rel(uv32.cpu().numpy(), uv2.cpu().numpy()) < 1e-6
+    assert rel(pt32.cpu().numpy(), ref_pt) < 1e-6
     ls2 = linsys.Linsys(c["prm"], n, nst, c["init"], *w)
     pr2 = linsys.Pressure(ls2)
     ls2.assemble_linsys(c["step"], *w)
