@@ -1037,6 +1037,10 @@ FLOP_ELEM_PAIR = 31
 #  uvort pair (k_uvort / k_uvort_sorted): d (3) + rho^2 (6) + rsqrt (1) + rho^-3 (2)
 #  + c d (3) + c d x alpha accumulated (6 fma, 12)
 FLOP_UVORT_PAIR = 27
+#  with the pressure equation's particle term in the same pass (k_uvort_pres /
+#  k_uvort_pres_sorted; difference and rho^-3 shared): d . (-w) (5) + times
+#  rho^-3 (1) + accumulation (1)
+FLOP_UVORT_PRES_PAIR = FLOP_UVORT_PAIR + 7
 #  M2L pair at p = 4 with stretching: 56 outputs x 35 inputs x 3 components x
 #  2 cross-product terms, one FMA each
 FLOP_M2L_PAIR = 56 * 35 * 6 * 2
@@ -1122,15 +1126,21 @@ def roofline(ph, case, params, best):
                    "flop_per_pair": FLOP_P2P_PAIR, "pairs": p["n_p2p_pairs"], "ms": p["fmm_p2p"]})
     if p.get("uvort"):
         pairs = case.rank * n
-        a = FLOP_UVORT_PAIR * pairs / (p["uvort"] * 1e-3) / 1e12
+        # with the pressure equation the step's uvort pass carries its
+        # particle term (dust_points_uvort_pressure_device)
+        fused = bool(p.get("pressure"))
+        fpp = FLOP_UVORT_PRES_PAIR if fused else FLOP_UVORT_PAIR
+        a = fpp * pairs / (p["uvort"] * 1e-3) / 1e12
         pk_uv = fp64_peak if uv64 else fp32_peak
-        ks.append({"kernel": "uvort phase (%s)" % ("k_uvort" if uv64 else "k_uvort_sorted + sort"),
+        kname = ("k_uvort_pres" if fused else "k_uvort") if uv64 else \
+            ("k_uvort_pres_sorted + sort" if fused else "k_uvort_sorted + sort")
+        ks.append({"kernel": "uvort phase (%s)" % kname,
                    "bound": "fp64" if uv64 else "fp32", "achieved": round(a, 2),
                    "peak": round(pk_uv, 1), "unit": "TFLOP/s", "frac": round(a / pk_uv, 3),
                    "traffic": int(TRAFFIC_UVORT_PER_PARTICLE * n) if uv64 else None,
                    "peak_source": name_of(uv64),
                    "fp64_pipe_active_ncu": 0.723 if uv64 else None,
-                   "flop_per_pair": FLOP_UVORT_PAIR, "pairs": pairs, "ms": p["uvort"]})
+                   "flop_per_pair": fpp, "pairs": pairs, "ms": p["uvort"]})
     if not ks:
         return {"others": [], "peaks_file": bool(peaks)}
     ks.sort(key=lambda k: -k["ms"])

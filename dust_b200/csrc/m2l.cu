@@ -86,7 +86,7 @@ __device__ __forceinline__ void m2l_copy4(double *dst, const double *src, int co
 template <typename T, int TCc>
 __device__ __forceinline__ void m2l_tile(const T *__restrict__ sD, const T *__restrict__ sA,
                                          const uint16_t *__restrict__ isum, int nm, int nm1,
-                                         int nout, int lane, const int *tl,
+                                         int nout, int lane, const int *tl, int kreal,
                                          double *__restrict__ s_acc) {
   for (int mb = 0; mb < nout; mb += 64) {
     const int m0 = mb + lane, m1 = m0 + 32;
@@ -113,11 +113,12 @@ __device__ __forceinline__ void m2l_tile(const T *__restrict__ sD, const T *__re
     }
 #pragma unroll
     for (int c = 0; c < TCc; ++c) {
+      if (c >= kreal) break;  // zero-padded slots of the tile
       double *acc = s_acc + (size_t)tl[c] * nout * 3;
       if (m0 < nout)
-        for (int e = 0; e < 3; ++e) atomicAdd(acc + 3 * m0 + e, (double)pa[c][0][e]);
+        for (int e = 0; e < 3; ++e) atomicAdd(acc + e * nout + m0, (double)pa[c][0][e]);
       if (m1 < nout)
-        for (int e = 0; e < 3; ++e) atomicAdd(acc + 3 * m1 + e, (double)pa[c][1][e]);
+        for (int e = 0; e < 3; ++e) atomicAdd(acc + e * nout + m1, (double)pa[c][1][e]);
     }
   }
 }
@@ -212,28 +213,30 @@ __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches
     const T *Dg = dtab + (size_t)tab * nD * 4;
     __syncwarp();
     m2l_copy4(sD, Dg, nD, lane);
-    for (int h = 0; h < 2; ++h) {
-      unsigned m = msk[h];
-      while (m) {
-        // next chunk of present targets: the largest tile <= what is left
-        const int left = min(__popc(m), TCX);
-        const int kc = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
-        int tl[M2L_TC];
-        for (int c = 0; c < kc; ++c) {
-          const int t = __ffs(m) - 1;
-          m &= m - 1;
-          tl[c] = t + 32 * h;
-          const int sc_ = __shfl_sync(0xffffffffu, src[h], t);
-          m2l_copy4(sA + (size_t)c * nm * 4, ahat + (size_t)(sc_ - ahat_cell0) * 4 * nm, nm,
-                    lane);
-        }
-        __syncwarp();
-        if (kc == 8) m2l_tile<T, 8>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
-        else if (kc == 4) m2l_tile<T, 4>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
-        else if (kc == 2) m2l_tile<T, 2>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
-        else m2l_tile<T, 1>(sD, sA, isum, nm, nm1, nout, lane, tl, s_acc);
-        __syncwarp();
+    // the present targets of both halves in chunks of up to TCX; a chunk of
+    // 3-4 (5-8) runs the 4- (8-) target tile with zero sources in the spare
+    // slots, which costs less than splitting it (every tile re-reads the
+    // offset's table entries for its outputs)
+    unsigned long long m = (unsigned long long)msk[0] | ((unsigned long long)msk[1] << 32);
+    while (m) {
+      const int kc = min(__popcll(m), TCX);
+      const int tile = kc <= 2 ? kc : kc <= 4 ? 4 : 8;
+      int tl[M2L_TC];
+      for (int c = 0; c < kc; ++c) {
+        const int t = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        tl[c] = t;
+        const int sc_ = __shfl_sync(0xffffffffu, t >= 32 ? src[1] : src[0], t & 31);
+        m2l_copy4(sA + (size_t)c * nm * 4, ahat + (size_t)(sc_ - ahat_cell0) * 4 * nm, nm, lane);
       }
+      for (int c = kc; c < tile; ++c)
+        for (int e = lane; e < 4 * nm; e += 32) sA[(size_t)c * nm * 4 + e] = (T)0;
+      __syncwarp();
+      if (tile == 8) m2l_tile<T, 8>(sD, sA, isum, nm, nm1, nout, lane, tl, kc, s_acc);
+      else if (tile == 4) m2l_tile<T, 4>(sD, sA, isum, nm, nm1, nout, lane, tl, kc, s_acc);
+      else if (tile == 2) m2l_tile<T, 2>(sD, sA, isum, nm, nm1, nout, lane, tl, kc, s_acc);
+      else m2l_tile<T, 1>(sD, sA, isum, nm, nm1, nout, lane, tl, kc, s_acc);
+      __syncwarp();
     }
     }
   }
@@ -249,11 +252,11 @@ __global__ void __launch_bounds__(256) k_m2l_batch(FmmDev d, const int4 *batches
     const double *acc = s_acc + (size_t)t * nout * 3;
     if (d.use_vs) {
       double *g = d.Gx + (size_t)ci * 3 * nm1;
-      for (int c = 0; c < 3; ++c) g[3 * mo + c] += sc * acc[3 * mo + c];
+      for (int c = 0; c < 3; ++c) g[3 * mo + c] += sc * acc[c * nout + mo];
     }
     if (mo < nm) {
       double *bb = d.B + (size_t)ci * 3 * nm;
-      for (int c = 0; c < 3; ++c) bb[3 * mo + c] += sc * acc[3 * mo + c];
+      for (int c = 0; c < 3; ++c) bb[3 * mo + c] += sc * acc[c * nout + mo];
     }
   }
 }
