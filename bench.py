@@ -414,6 +414,7 @@ def main():
     results = {}
     steppers = {}
     by_step = {}
+    first_out = {}
     n_acc = max(args.accuracy_steps, max(args.warmup, 3) + args.steps)
     for name, mode in modes:
         prm = params if name.startswith("plain") else params.replace(precision=abi.DUST_PREC_FP32C)
@@ -433,9 +434,14 @@ def main():
         record = (lambda: by_step[name].append(
             case.loads(st.res.cpu().numpy(), st.euv.cpu().numpy()))) \
             if not args.profile_step else (lambda: None)
-        for _ in range(max(args.warmup, 1 if args.profile_step else 3)):
+        for w in range(max(args.warmup, 1 if args.profile_step else 3)):
             st.step()
             record()
+            if w == 0 and not args.profile_step:
+                # the first step's particle outputs: every mode evaluates the
+                # same initial wake, so their difference is the method's own
+                # (no trajectory divergence yet)
+                first_out[name] = [t.cpu().numpy() for t in (st.vel, st.str, st.rot)]
         torch.cuda.synchronize()
         if args.profile_step:
             continue
@@ -487,6 +493,12 @@ def main():
         return {"vel_induced": rel(a[0] - uinf, b[0] - uinf), "stretch": rel(a[1], b[1]),
                 "rot": rel(a[2], b[2])}
     fmm_errs = {k: fmm_err(k) for k in results}
+    for k in results:
+        if k in first_out and "plain" in first_out:
+            a, b = first_out[k], first_out["plain"]
+            rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+            fmm_errs[k]["first_step"] = {"vel_induced": rel(a[0] - uinf, b[0] - uinf),
+                                         "stretch": rel(a[1], b[1]), "rot": rel(a[2], b[2])}
     # the pressure equation's solution (surface panels) against the FP64 step
     for k in results:
         a, b = results[k]["res_pres"], results["plain"]["res_pres"]

@@ -213,8 +213,7 @@ extern "C" int dust_octree_destroy(dust_octree *o) {
   devbuf_free(o->m2l_buf);
   devbuf_free(o->ahat);
   devbuf_free(o->m2l_bat);
-  devbuf_free(o->m2l_img);
-  devbuf_free(o->m2l_src);
+  devbuf_free(o->jsum);
   devbuf_free(o->shift);
   devbuf_free(o->ffbuf);
   devbuf_free(o->elem_work);

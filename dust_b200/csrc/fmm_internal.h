@@ -68,14 +68,14 @@ struct dust_octree {
   DevBuf ffbuf;                        // far-field panel records
   DevBuf elem_work;                    // FP32C element sums: far sums, near-pair list
   size_t near_cap = 0;                 // capacity of the near-pair list
-  DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless M2L tables (FP64)
-  DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless M2L tables (FP32)
+  DevBuf dtabs[DUST_MAXLEV + 1];       // dimensionless scalar M2L tables (FP64)
+  DevBuf dtab32[DUST_MAXLEV + 1];      // dimensionless scalar M2L tables (FP32)
+  DevBuf jsum;                         // scalar M2L index table [n][slot][lane]
+  int m2l_nJ = 0, m2l_SL = 0, m2l_P = 0;  // L indices, 32-lane slots, table stride
   DevBuf m2l_buf;                      // class-sorted M2L target lists
   DevBuf m2l_bat;                      // M2L batch descriptors
   uint32_t *m2l_list = nullptr;
   DevBuf ahat;                         // pre-scaled M2L source coefficients
-  DevBuf m2l_img;                      // tensor-core M2L table images (FP32C)
-  DevBuf m2l_src;                      // tensor-core M2L interaction lists + masks
   DevBuf shift;                        // M2M / L2L term tables of every level
   const void *shift_t[DUST_MAXLEV + 1][3], *shift_o[DUST_MAXLEV + 1][3];
   int shift_n[DUST_MAXLEV + 1][3];
