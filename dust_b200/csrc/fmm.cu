@@ -1028,7 +1028,7 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
 // each 32-source tile staged in the warp's own shared memory, and group 0
 // adds the other groups' sums from shared memory.  A source is found from
 // its position in the concatenated ranges by a binary search over the
-// range prefix sums.
+// range prefix sums (walked forward tile by tile).
 //   FP64: pairs by p2p_pair on absolute coordinates, summed in FP64.
 //   FP32C (F32): pairs by p2p_pair_f on coordinates relative to the leaf
 //   centre (differences formed in FP64, rounded once), FP32 partial sums of
@@ -1041,7 +1041,7 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
 #define P2W_LQ 4  // levels whose near-field loads are issued together
 
 template <bool VS, bool DF, bool VD, bool TV, bool F32>
-__global__ void __launch_bounds__(P2W_WARPS * 32, 5) k_p2p_w(FmmDev d) {
+__global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
   using R = typename std::conditional<F32, float, double>::type;
   __shared__ R s_src[P2W_WARPS][P2W_NV][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
@@ -1190,22 +1190,31 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 5) k_p2p_w(FmmDev d) {
     if (F32)
       for (int e = 0; e < 12; ++e) acc[32 * e] = 0.0;
     int since = 0;
+    // the sources of the next tile are loaded into registers while the
+    // current tile is evaluated; each lane's range index only moves forward
+    // (source v = s0 + lane grows by the tile size)
+    int ra = 0;
+    double pf[7];
+    uint32_t psid = 0;
+    bool pv = false;
+    auto fetch = [&](uint32_t v) {
+      pv = v < S;
+      if (pv) {
+        while (ra + 1 < nr && rcum[ra + 1] <= v) ++ra;  // last r with rcum[r] <= v
+        psid = rlo[ra] + (v - rcum[ra]);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) pf[q] = d.P[(size_t)q * n + psid];
+      }
+    };
+    fetch(lane);
     for (uint32_t s0 = 0; s0 < S; s0 += P2W_TILE) {
       __syncwarp();
-      const uint32_t v = s0 + lane;
-      if (v < S) {
-        int a = 0, b = nr - 1;
-        while (a < b) {  // last r with rcum[r] <= v
-          const int mid = (a + b + 1) >> 1;
-          if (rcum[mid] <= v) a = mid; else b = mid - 1;
-        }
-        const uint32_t sidx = rlo[a] + (v - rcum[a]);
-        s_sid[w][lane] = sidx;
+      if (pv) {
+        s_sid[w][lane] = psid;
         for (int q = 0; q < 3; ++q)
-          fs[q * P2W_TILE + lane] =
-              F32 ? (R)(d.P[(size_t)q * n + sidx] - cc[q]) : (R)d.P[(size_t)q * n + sidx];
-        for (int q = 3; q < 6; ++q) fs[q * P2W_TILE + lane] = (R)d.P[(size_t)q * n + sidx];
-        const double rv = d.P[(size_t)6 * n + sidx];
+          fs[q * P2W_TILE + lane] = F32 ? (R)(pf[q] - cc[q]) : (R)pf[q];
+        for (int q = 3; q < 6; ++q) fs[q * P2W_TILE + lane] = (R)pf[q];
+        const double rv = pf[6];
         if constexpr (F32) {
           const float s2 = (float)rv * (float)rv;
           fs[6 * P2W_TILE + lane] = s2;
@@ -1217,6 +1226,7 @@ __global__ void __launch_bounds__(P2W_WARPS * 32, 5) k_p2p_w(FmmDev d) {
         }
       }
       __syncwarp();
+      fetch(s0 + P2W_TILE + lane);
       const int m = (int)min((uint32_t)P2W_TILE, S - s0);
       if (act)
         for (int u = grp; u < m; u += G) {
