@@ -1053,9 +1053,11 @@ FLOP_UVORT_PAIR = 27
 #  k_uvort_pres_sorted; difference and rho^-3 shared): d . (-w) (5) + times
 #  rho^-3 (1) + accumulation (1)
 FLOP_UVORT_PRES_PAIR = FLOP_UVORT_PAIR + 7
-#  M2L pair at p = 4 with stretching: 56 outputs x 35 inputs x 3 components x
-#  2 cross-product terms, one FMA each
-FLOP_M2L_PAIR = 56 * 35 * 6 * 2
+#  M2L pair at p = 4 with stretching, in the scalar form the kernel evaluates:
+#  L_c(j) = sum_n Shat(j+n) a_c(n) for the 83 indices 1 <= |j| <= 6, the 35
+#  source monomials and 3 components, one FMA each (the cross-product form
+#  it replaces takes 56 x 35 x 6 FMAs)
+FLOP_M2L_PAIR = 83 * 35 * 3 * 2
 #  M2L pair, algorithmic bytes at p = 4 (35 monomials, w bytes a word): source
 #  a (3 x 35 w) + target b read and write (2 x 3 x 35 w) + stretching c read
 #  and write (2 x 9 x 35 w)
@@ -1070,8 +1072,12 @@ TRAFFIC_ELEM_FAR_PER_PARTICLE = 381.5
 # profiles/k_uvort_300k.txt, k_m2l_batch_f32_300k.txt, k_p2p_w_f32_300k.txt),
 # scaled by the particle count to the benchmark's size
 TRAFFIC_UVORT_PER_PARTICLE = 19.88e6 / 3.0e5
-TRAFFIC_M2L_F32_PER_PARTICLE = (142.44e6 + 56.58e6) / 3.0e5
-TRAFFIC_P2P_F32_PER_PARTICLE = (120.93e6 + 22.24e6) / 3.0e5
+TRAFFIC_M2L_F32_PER_PARTICLE = (138.53e6 + 53.36e6) / 3.0e5
+TRAFFIC_P2P_F32_PER_PARTICLE = (119.14e6 + 18.42e6) / 3.0e5
+# FMA-pipe activity of the FP32C kernels in the same captures
+# (sm__pipe_fma_cycles_active, profiles/*_300k.txt)
+FMA_PIPE_NCU = {"k_m2l_batch": 0.376, "k_p2p_w": 0.270, "k_uvort_pres_sorted": 0.807,
+                "k_elem_far": 0.67}
 
 
 def roofline(ph, case, params, best):
@@ -1107,6 +1113,7 @@ def roofline(ph, case, params, best):
         ks.append({"kernel": "k_elem_far", "bound": "fp32", "achieved": round(a, 2),
                    "peak": round(fp32_peak, 1), "unit": "TFLOP/s", "frac": round(a / fp32_peak, 3),
                    "traffic": tr, "peak_source": simt_name, "flop_per_pair": FLOP_ELEM_PAIR,
+                   "fma_pipe_active_ncu": FMA_PIPE_NCU["k_elem_far"],
                    "pairs": p["n_elem_pairs"], "ms": p["k_elem_far_ms"]})
     elif p.get("fmm_elements"):
         a = FLOP_ELEM_PAIR * p["n_elem_pairs"] / (p["fmm_elements"] * 1e-3) / 1e12
@@ -1127,7 +1134,9 @@ def roofline(ph, case, params, best):
                    "ms": p["k_m2l_batch_ms"],
                    "flops": {"achieved": round(fl, 2), "peak": round(simt, 1),
                              "unit": "TFLOP/s", "frac": round(fl / simt, 3),
-                             "flop_per_pair": FLOP_M2L_PAIR, "peak_source": simt_name}})
+                             "flop_per_pair": FLOP_M2L_PAIR, "peak_source": simt_name,
+                             "fma_pipe_active_ncu": None if f64 else
+                             FMA_PIPE_NCU["k_m2l_batch"]}})
     if p.get("fmm_p2p"):
         a = FLOP_P2P_PAIR * p["n_p2p_pairs"] / (p["fmm_p2p"] * 1e-3) / 1e12
         ks.append({"kernel": "k_p2p_w (L2P + P2P)", "bound": "fp64" if f64 else "fp32",
@@ -1135,6 +1144,7 @@ def roofline(ph, case, params, best):
                    "frac": round(a / simt, 3),
                    "traffic": None if f64 else int(TRAFFIC_P2P_F32_PER_PARTICLE * n),
                    "peak_source": simt_name,
+                   "fma_pipe_active_ncu": None if f64 else FMA_PIPE_NCU["k_p2p_w"],
                    "flop_per_pair": FLOP_P2P_PAIR, "pairs": p["n_p2p_pairs"], "ms": p["fmm_p2p"]})
     if p.get("uvort"):
         pairs = case.rank * n
@@ -1152,6 +1162,8 @@ def roofline(ph, case, params, best):
                    "traffic": int(TRAFFIC_UVORT_PER_PARTICLE * n) if uv64 else None,
                    "peak_source": name_of(uv64),
                    "fp64_pipe_active_ncu": 0.723 if uv64 else None,
+                   "fma_pipe_active_ncu": None if uv64 or not fused else
+                   FMA_PIPE_NCU["k_uvort_pres_sorted"],
                    "flop_per_pair": fpp, "pairs": pairs, "ms": p["uvort"]})
     if not ks:
         return {"others": [], "peaks_file": bool(peaks)}
