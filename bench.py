@@ -1196,8 +1196,11 @@ def e2e_bytes(case, n, advect, fmm_uvort=False):
     strengths), dust_fmm_apply (particles, panels, wake panels, end vortices
     -> vel, stretch, rotu) and, when advecting, dust_particles_update
     (cen, dir, mag, vel, stretch, rotu, free flags -> cen, dir, stretch, free
-    flags, count); with surface panels, dust_pressure_assemble (particles and
-    their velocities) and dust_pressure_solve (-> solution)."""
+    flags, count); with surface panels, uvort through
+    dust_points_uvort_pressure (also the particles' velocities -> the
+    pressure equation's particle term), dust_pressure_assemble_terms (that
+    term) and dust_pressure_solve (-> solution); with the FMM uvort,
+    dust_pressure_assemble (particles and their velocities) instead."""
     d, i = 8, 4
     nr, nw, nl = case.rank, case.wake.n, case.end_vort.n
     panels = nr * (12 * d + 2 * i + 7 * d)        # ver, n_ver, kind, mag, ub, uvort
@@ -1217,11 +1220,17 @@ def e2e_bytes(case, n, advect, fmm_uvort=False):
     d2h = nr * 3 * d + nr * d + n * 9 * d         # uvort, strengths, vel/stretch/rotu
     from dust_b200 import abi
     nsp = int(np.sum(case.elems.kind == abi.DUST_ELEM_SURFPAN))
-    if nsp:
+    if nsp and fmm_uvort:
         # dust_pressure_assemble (particles with their velocities), and from
         # the second step dust_pressure_solve (-> the surface panels' solution)
         h2d += parts + n * 3 * d
         d2h += nsp * d
+    elif nsp:
+        # the particles' velocities into dust_points_uvort_pressure (-> its
+        # term at every element), that term into dust_pressure_assemble_terms,
+        # dust_pressure_solve (-> the surface panels' solution)
+        h2d += n * 3 * d + nr * d
+        d2h += nr * d + nsp * d
     if advect:
         h2d += n * (16 * d + i)
         d2h += n * (9 * d + i) + i

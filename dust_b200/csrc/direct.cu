@@ -1311,21 +1311,11 @@ extern "C" int dust_points_uvort_device_noalloc(const dust_fmm_params *prm, int 
 // end-vortex records and the FP32C pass's sorted particles (one host thread)
 static DevBuf g_uvp_raw, g_uvp_geo, g_uvp_sort;
 
-extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n_pts,
-                                                 const double *pts, int n, const double *cen,
-                                                 const double *dir, const double *mag,
-                                                 const double *r_vortex, const double *vel,
-                                                 const dust_lines *end_vort, double *uvort,
-                                                 double *pterm, void *stream) {
-  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
-    return DUST_ERR_BAD_ARG;
-  if (n_pts > 0 && !pterm) return DUST_ERR_BAD_ARG;
-  if (n > 0 && !vel) return DUST_ERR_BAD_ARG;
-  if (n_pts == 0) return DUST_OK;
-  cudaStream_t st = (cudaStream_t)stream;
-  ElemDev e;
-  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), false,
-                             g_uvp_raw, g_uvp_geo, e, st));
+// the fused pass on device arrays, end vortices already built into e
+static int uvort_pressure_run(const dust_fmm_params *prm, int n_pts, const double *pts, int n,
+                              const double *cen, const double *dir, const double *mag,
+                              const double *r_vortex, const double *vel, const ElemDev &e,
+                              double *uvort, double *pterm, cudaStream_t st) {
   DUST_CUDA(cudaMemsetAsync(uvort, 0, (size_t)n_pts * 24, st));
   DUST_CUDA(cudaMemsetAsync(pterm, 0, (size_t)n_pts * 8, st));
   if (n > 0 && prm->precision == DUST_PREC_FP32C) {
@@ -1367,5 +1357,77 @@ extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int
   }
   points_lines_add(n_pts, pts, e, uvort, st);
   DUST_CUDA(cudaGetLastError());
+  return DUST_OK;
+}
+
+static bool uvort_pressure_args_ok(const dust_fmm_params *prm, int n_pts, const double *pts,
+                                   int n, const double *cen, const double *dir,
+                                   const double *mag, const double *r_vortex, const double *vel,
+                                   const dust_lines *end_vort, const double *uvort,
+                                   const double *pterm) {
+  if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort)) return false;
+  if (n_pts > 0 && !pterm) return false;
+  if (n > 0 && !vel) return false;
+  return true;
+}
+
+extern "C" int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n_pts,
+                                                 const double *pts, int n, const double *cen,
+                                                 const double *dir, const double *mag,
+                                                 const double *r_vortex, const double *vel,
+                                                 const dust_lines *end_vort, double *uvort,
+                                                 double *pterm, void *stream) {
+  if (!uvort_pressure_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, vel, end_vort, uvort,
+                              pterm))
+    return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), false,
+                             g_uvp_raw, g_uvp_geo, e, st));
+  return uvort_pressure_run(prm, n_pts, pts, n, cen, dir, mag, r_vortex, vel, e, uvort, pterm,
+                            st);
+}
+
+// Host arrays: inputs copied to a staging buffer kept across calls (one host
+// thread), outputs copied back.
+static DevBuf g_uvp_stage;
+
+extern "C" int dust_points_uvort_pressure(const dust_fmm_params *prm, int n_pts,
+                                          const double *pts, int n, const double *cen,
+                                          const double *dir, const double *mag,
+                                          const double *r_vortex, const double *vel,
+                                          const dust_lines *end_vort, double *uvort,
+                                          double *pterm) {
+  if (!uvort_pressure_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, vel, end_vort, uvort,
+                              pterm))
+    return DUST_ERR_BAD_ARG;
+  if (n_pts == 0) return DUST_OK;
+  cudaStream_t st = 0;
+  ElemDev e;
+  DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), true,
+                             g_uvp_raw, g_uvp_geo, e, st));
+  const size_t P = (size_t)n_pts, N = (size_t)n;
+  const size_t o_u = round256(24 * P), o_t = o_u + round256(24 * P), o_c = o_t + round256(8 * P);
+  const size_t o_d = o_c + round256(24 * N), o_m = o_d + round256(24 * N),
+               o_r = o_m + round256(8 * N), o_v = o_r + round256(8 * N),
+               end = o_v + round256(24 * N);
+  DUST_TRY(devbuf_grow(g_uvp_stage, end));
+  char *b = (char *)g_uvp_stage.p;
+  double *dp = (double *)b, *du = (double *)(b + o_u), *dt = (double *)(b + o_t);
+  double *dc = (double *)(b + o_c), *dd = (double *)(b + o_d), *dm = (double *)(b + o_m),
+         *dr = (double *)(b + o_r), *dv = (double *)(b + o_v);
+  DUST_CUDA(cudaMemcpyAsync(dp, pts, 24 * P, cudaMemcpyHostToDevice, st));
+  if (n > 0) {
+    DUST_CUDA(cudaMemcpyAsync(dc, cen, 24 * N, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dd, dir, 24 * N, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dm, mag, 8 * N, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dr, r_vortex, 8 * N, cudaMemcpyHostToDevice, st));
+    DUST_CUDA(cudaMemcpyAsync(dv, vel, 24 * N, cudaMemcpyHostToDevice, st));
+  }
+  DUST_TRY(uvort_pressure_run(prm, n_pts, dp, n, dc, dd, dm, dr, dv, e, du, dt, st));
+  DUST_CUDA(cudaMemcpyAsync(uvort, du, 24 * P, cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaMemcpyAsync(pterm, dt, 8 * P, cudaMemcpyDeviceToHost, st));
+  DUST_CUDA(cudaStreamSynchronize(st));
   return DUST_OK;
 }

@@ -324,7 +324,7 @@ extern "C" int dust_elements_vel(const dust_fmm_params *prm, int n_pts, const do
                                  const dust_elements *elems, double *vel) {
   if (!prm || n_pts < 0 || (n_pts > 0 && (!pts || !vel))) return DUST_ERR_BAD_ARG;
   if (n_pts == 0) return DUST_OK;
-  Scratch s;
+  static Scratch s;  // kept across calls (one host thread)
   cudaStream_t st = 0;
   ElemDev e;
   RegParams rp = reg_params(prm);
@@ -369,7 +369,7 @@ extern "C" int dust_points_uvort(const dust_fmm_params *prm, int n_pts, const do
   if (!uvort_args_ok(prm, n_pts, pts, n, cen, dir, mag, r_vortex, end_vort, uvort))
     return DUST_ERR_BAD_ARG;
   if (n_pts == 0) return DUST_OK;
-  Scratch s;
+  static Scratch s;  // kept across calls (one host thread)
   cudaStream_t st = 0;
   ElemDev e;
   DUST_TRY(elem_build_device(nullptr, nullptr, end_vort, prm->u_inf, reg_params(prm), true,
@@ -398,7 +398,7 @@ extern "C" int dust_direct_particles(const dust_fmm_params *prm, int n, const do
                                      double *stretch, double *rotu) {
   if (!prm || n < 0 || n_tgt < 0 || n_tgt > n || (n_tgt > 0 && !vel)) return DUST_ERR_BAD_ARG;
   if (n_tgt == 0) return DUST_OK;
-  Scratch s;
+  static Scratch s;  // kept across calls (one host thread)
   cudaStream_t st = 0;
   size_t N = (size_t)n;
   DUST_TRY(devbuf_grow(s.a, N * 8 * 8));
@@ -435,7 +435,7 @@ extern "C" int dust_panels_geometry(const dust_panels *pan, double *cen, double 
                                     double *area) {
   if (!pan || pan->n < 0) return DUST_ERR_BAD_ARG;
   if (pan->n == 0) return DUST_OK;
-  Scratch s;
+  static Scratch s;  // kept across calls (one host thread)
   cudaStream_t st = 0;
   ElemDev e;
   RegParams rp{10.0, 0.1, 0.001};

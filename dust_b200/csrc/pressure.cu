@@ -578,13 +578,14 @@ extern "C" int dust_pressure_get_system(dust_pressure *p, double *A, double *b) 
 }
 
 // Host-array variants: the inputs are copied to the device (one staging
-// buffer kept by the handle), the solution back to the host.
-extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, const double *bern,
-                                      int n, const double *cen, const double *dir,
-                                      const double *mag, const double *r_vortex,
-                                      const double *vel, const dust_panels *wake,
-                                      const double *wake_vv, const dust_lines *end_vort,
-                                      const double *end_vv) {
+// buffer kept by the handle), the solution back to the host.  pterm (host,
+// rank values) replaces the particle arrays when the particles' term was
+// evaluated with uvort (dust_points_uvort_pressure).
+static int pres_assemble_host(dust_pressure *p, const dust_linsys *ls, const double *bern, int n,
+                              const double *cen, const double *dir, const double *mag,
+                              const double *r_vortex, const double *vel, const double *pterm,
+                              const dust_panels *wake, const double *wake_vv,
+                              const dust_lines *end_vort, const double *end_vv) {
   if (!p || !ls || n < 0) return DUST_ERR_BAD_ARG;
   if (n > 0 && (!cen || !dir || !mag || !r_vortex || !vel)) return DUST_ERR_BAD_ARG;
   const int nw = wake ? wake->n : 0, ne = end_vort ? end_vort->n : 0;
@@ -592,7 +593,7 @@ extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, c
       (ne > 0 && (!end_vort->ver || !end_vort->mag || !end_vv)))
     return DUST_ERR_BAD_ARG;
   if (p->nsp == 0) return DUST_OK;
-  const size_t N = (size_t)n;
+  const size_t N = (size_t)n, R = pterm ? (size_t)ls->n : 0;
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   size_t off = 0;
   const size_t o_b = off; off += al((bern ? p->nsp : 0) * 8);
@@ -601,6 +602,7 @@ extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, c
   const size_t o_m = off; off += al(8 * N);
   const size_t o_r = off; off += al(8 * N);
   const size_t o_v = off; off += al(24 * N);
+  const size_t o_pt = off; off += al(8 * R);
   const size_t o_wv = off; off += al(96 * (size_t)nw);
   const size_t o_wn = off; off += al(4 * (size_t)nw);
   const size_t o_wm = off; off += al(8 * (size_t)nw);
@@ -622,6 +624,7 @@ extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, c
   DUST_TRY(put(o_m, mag, 8 * N));
   DUST_TRY(put(o_r, r_vortex, 8 * N));
   DUST_TRY(put(o_v, vel, 24 * N));
+  DUST_TRY(put(o_pt, pterm, 8 * R));
   dust_panels dw;
   dust_lines de;
   memset(&dw, 0, sizeof(dw));
@@ -645,11 +648,29 @@ extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, c
     de.mag = (const double *)(s + o_em);
   }
   auto D = [&](size_t o, const void *h) { return h ? (const double *)(s + o) : nullptr; };
-  return dust_pressure_assemble_device(p, ls, D(o_b, bern), n, D(o_c, cen), D(o_d, dir),
-                                       D(o_m, mag), D(o_r, r_vortex), D(o_v, vel),
-                                       nw > 0 ? &dw : nullptr, D(o_wvv, nw > 0 ? wake_vv : nullptr),
-                                       ne > 0 ? &de : nullptr, D(o_evv, ne > 0 ? end_vv : nullptr),
-                                       st);
+  return pres_assemble(p, ls, D(o_b, bern), n, D(o_c, cen), D(o_d, dir), D(o_m, mag),
+                       D(o_r, r_vortex), D(o_v, vel), D(o_pt, pterm), nw > 0 ? &dw : nullptr,
+                       D(o_wvv, nw > 0 ? wake_vv : nullptr), ne > 0 ? &de : nullptr,
+                       D(o_evv, ne > 0 ? end_vv : nullptr), st);
+}
+
+extern "C" int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, const double *bern,
+                                      int n, const double *cen, const double *dir,
+                                      const double *mag, const double *r_vortex,
+                                      const double *vel, const dust_panels *wake,
+                                      const double *wake_vv, const dust_lines *end_vort,
+                                      const double *end_vv) {
+  return pres_assemble_host(p, ls, bern, n, cen, dir, mag, r_vortex, vel, nullptr, wake, wake_vv,
+                            end_vort, end_vv);
+}
+
+extern "C" int dust_pressure_assemble_terms(dust_pressure *p, const dust_linsys *ls,
+                                            const double *bern, const double *pterm,
+                                            const dust_panels *wake, const double *wake_vv,
+                                            const dust_lines *end_vort, const double *end_vv) {
+  if (!pterm) return DUST_ERR_BAD_ARG;
+  return pres_assemble_host(p, ls, bern, 0, nullptr, nullptr, nullptr, nullptr, nullptr, pterm,
+                            wake, wake_vv, end_vort, end_vv);
 }
 
 extern "C" int dust_pressure_solve(dust_pressure *p, double *res) {

@@ -299,8 +299,10 @@ extern "C" int dust_particles_update(const dust_update_params *u, int n, double 
   // one device block: cen, dir, vel, stretch, rotu (3 n each), mag (n),
   // free flags (n ints), the counter
   const size_t bytes = 5 * v3 + v1 + (size_t)n * sizeof(int) + 256;
-  char *b = nullptr;
-  DUST_CUDA(cudaMalloc((void **)&b, bytes));
+  // kept across calls (one host thread), so a step loop allocates nothing
+  static DevBuf stage;
+  DUST_TRY(devbuf_grow(stage, bytes));
+  char *b = (char *)stage.p;
   double *dc = (double *)b, *dd = (double *)(b + v3), *dv = (double *)(b + 2 * v3),
          *ds = (double *)(b + 3 * v3), *dr = (double *)(b + 4 * v3), *dm = (double *)(b + 5 * v3);
   int *df = (int *)(b + 5 * v3 + v1);
@@ -329,6 +331,5 @@ extern "C" int dust_particles_update(const dust_update_params *u, int n, double 
        cudaStreamSynchronize(st) != cudaSuccess))
     s = DUST_ERR_CUDA;
   if (s == DUST_ERR_CUDA) dust_set_last_error("particle update copies", __FILE__, __LINE__);
-  cudaFree(b);
   return s;
 }

@@ -178,6 +178,13 @@ class Pressure:
                                            abi.dptr(rv), abi.dptr(abi.f64(vel)), None, None,
                                            None, None), "dust_pressure_assemble")
 
+    def assemble_terms(self, bern=None, pterm=None):
+        """Host-array variant of assemble_terms_device (pterm of the system's
+        rank from points_uvort_pressure)."""
+        check(lib().dust_pressure_assemble_terms(self._h, self.ls._h, abi.dptr(abi.f64(bern)),
+                                                 abi.dptr(abi.f64(pterm)), None, None, None,
+                                                 None), "dust_pressure_assemble_terms")
+
     def solve(self):
         res = np.zeros(self.n_sp)
         check(lib().dust_pressure_solve(self._h, abi.dptr(res)), "dust_pressure_solve")

@@ -88,9 +88,18 @@ class HostStepper:
         evs = c.end_vort.struct()
         uv = np.empty((c.rank, 3))
         cen_el = np.ascontiguousarray(cen_el)
+        pterm = None
         if self.fmm_uvort:
             self.oc.prepare(c.cen, c.dir, c.mag, c.r_vortex, cen_el)
             uv = self.oc.points_uvort(c.end_vort)
+        elif self.pr is not None:
+            # the pressure equation's particle term in the same pass as uvort,
+            # with the particles' velocities of the previous update
+            pterm = np.empty(c.rank)
+            check(lib().dust_points_uvort_pressure(
+                C.byref(ps), c.rank, abi.dptr(cen_el), c.mag.shape[0], abi.dptr(c.cen),
+                abi.dptr(c.dir), abi.dptr(c.mag), abi.dptr(c.r_vortex), abi.dptr(self.vel_prev),
+                C.byref(evs), abi.dptr(uv), abi.dptr(pterm)), "dust_points_uvort_pressure")
         else:
             check(lib().dust_points_uvort(C.byref(ps), c.rank, abi.dptr(cen_el),
                                           c.mag.shape[0], abi.dptr(c.cen), abi.dptr(c.dir),
@@ -103,7 +112,10 @@ class HostStepper:
             # second (dust.f90:621, 641-643); the body is at rest in the
             # frame of its Bernoulli sources, the particles' velocities are
             # those of the previous update
-            self.pr.assemble(None, (c.cen, c.dir, c.mag, c.r_vortex), self.vel_prev)
+            if pterm is not None:
+                self.pr.assemble_terms(None, pterm)
+            else:
+                self.pr.assemble(None, (c.cen, c.dir, c.mag, c.r_vortex), self.vel_prev)
             if self.steps_done > 0:
                 self.res_pres = self.pr.solve()
         res, rep = self.ls.solve_linsys(self.mode)

@@ -14,7 +14,10 @@
  * All calls return an int status (DUST_OK == 0).  A non-zero status maps to
  * the reference's `call error(...)` (src/general/mod_handling.f90:181).
  * Handles are not re-entrant: one handle is driven by one host thread and
- * owns one CUDA stream.
+ * owns one CUDA stream.  The handle-less host-array calls (dust_points_uvort,
+ * dust_points_uvort_pressure, dust_particles_update, ...) keep their device
+ * staging buffers across calls, so they too are called from one host thread
+ * at a time.
  */
 #ifndef DUST_B200_H
 #define DUST_B200_H
@@ -258,6 +261,18 @@ DUST_API int dust_points_uvort_pressure_device(const dust_fmm_params *prm, int n
                                                const double *r_vortex, const double *vel,
                                                const dust_lines *end_vort, double *uvort,
                                                double *pterm, void *stream);
+
+/* dust_points_uvort_pressure_device on host arrays (inputs copied to a
+ * device staging buffer kept across calls -- one host thread --, uvort and
+ * pterm copied back): for a host code that calls get_vort_vel and
+ * assemble_pressure_sys in the same step; pterm then goes to
+ * dust_pressure_assemble_terms. */
+DUST_API int dust_points_uvort_pressure(const dust_fmm_params *prm, int n_pts,
+                                        const double *pts, int n, const double *cen,
+                                        const double *dir, const double *mag,
+                                        const double *r_vortex, const double *vel,
+                                        const dust_lines *end_vort, double *uvort,
+                                        double *pterm);
 
 /* No counterpart in the reference.  Same result as dust_points_uvort_device
  * (same kernels and summation order) for callers that must not allocate
@@ -720,6 +735,13 @@ DUST_API int dust_pressure_assemble(dust_pressure *p, const dust_linsys *ls, con
                                     const double *wake_vv, const dust_lines *end_vort,
                                     const double *end_vv);
 DUST_API int dust_pressure_solve(dust_pressure *p, double *res);
+/* dust_pressure_assemble_terms_device on host arrays (pterm[rank] from
+ * dust_points_uvort_pressure; bern, wake, end vortices as in
+ * dust_pressure_assemble). */
+DUST_API int dust_pressure_assemble_terms(dust_pressure *p, const dust_linsys *ls,
+                                          const double *bern, const double *pterm,
+                                          const dust_panels *wake, const double *wake_vv,
+                                          const dust_lines *end_vort, const double *end_vv);
 
 /* Host copies of A_pres (n_sp x n_sp column-major; its static block holds
  * that block's LU) and b_pres after assembly and before the solve, as
