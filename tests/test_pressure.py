@@ -187,5 +187,23 @@ def test_gpu_pressure_matches_oracle():
     pr2.assemble_terms_device(bern, pt, wp, wvv, lp, evv)
     _, bt = pr2.get_system()
     assert rel(bt, b) < 1e-12
+    # the host-array form of the fused pass: the same kernels (the chunks'
+    # partial sums meet in atomic FP64 adds, so equal up to their order);
+    # its term through the host-array assembly (no wake rows, end vortices or
+    # Bernoulli sources there) against the device assembly of the same inputs
+    hp = [np.ascontiguousarray(a) for a in c["parts"]]
+    uvh, pth = np.empty((n, 3)), np.empty(n)
+    evs = c["lines"].struct()
+    check(lib().dust_points_uvort_pressure(C.byref(ps), n, abi.dptr(np.ascontiguousarray(cen_el)),
+                                           hp[2].shape[0], *(abi.dptr(a) for a in hp),
+                                           abi.dptr(np.ascontiguousarray(c["vel"])),
+                                           C.byref(evs), abi.dptr(uvh), abi.dptr(pth)),
+          "uvort+pressure host")
+    assert rel(uvh, uv.cpu().numpy()) < 1e-13 and rel(pth, pt.cpu().numpy()) < 1e-13
+    pr2.assemble_terms_device(None, T(pth))
+    _, bd = pr2.get_system()
+    pr2.assemble_terms(None, pth)
+    _, bh = pr2.get_system()
+    assert np.array_equal(bh, bd)
     pr2.close()
     ls2.close()
