@@ -23,6 +23,8 @@ struct dust_linsys {
   DevBuf mvb;     // unfactored moving block (LU64 step), restored if the
                   // unpivoted LU is not certified
   int static_pivoted = 0, last_pivoted = 0;  // which LU ran (lu_getrf_auto)
+  DevBuf permv;          // net row permutation of the pivots (lu_getrs)
+  bool perm_ok = false;  // permv holds the static-only system's permutation
   bool ainv_ready = false;
   struct dust_precond *pc = nullptr;  // learned preconditioner (GMRES_NN)
   DevBuf kr;                          // GMRES Krylov basis and vectors
