@@ -1034,14 +1034,14 @@ __device__ __forceinline__ void p2p_pair_f(const float *tp, const float *ta, flo
 //   centre (differences formed in FP64, rounded once), FP32 partial sums of
 //   up to 128 sources folded into FP64.
 // L2P (mod_octree.f90:1171-1212) is FP64 in both.
-#define P2W_WARPS 4
+#define P2W_WARPS 1  // one warp per CTA: leaves finish independently
 #define P2W_TILE 32
 #define P2W_MAXR (26 * DUST_MAXLEV + 4)
 #define P2W_NV 8  // staged per source: x y z, alpha x y z, r_v^2, 1 / r_v^2
 #define P2W_LQ 4  // levels whose near-field loads are issued together
 
 template <bool VS, bool DF, bool VD, bool TV, bool F32>
-__global__ void __launch_bounds__(P2W_WARPS * 32, 4) k_p2p_w(FmmDev d) {
+__global__ void __launch_bounds__(P2W_WARPS * 32, 16) k_p2p_w(FmmDev d) {
   using R = typename std::conditional<F32, float, double>::type;
   __shared__ R s_src[P2W_WARPS][P2W_NV][P2W_TILE];
   __shared__ uint32_t s_sid[P2W_WARPS][P2W_TILE];
