@@ -1073,10 +1073,10 @@ TRAFFIC_ELEM_FAR_PER_PARTICLE = 381.5
 # scaled by the particle count to the benchmark's size
 TRAFFIC_UVORT_PER_PARTICLE = 19.88e6 / 3.0e5
 TRAFFIC_M2L_F32_PER_PARTICLE = (138.53e6 + 53.36e6) / 3.0e5
-TRAFFIC_P2P_F32_PER_PARTICLE = (119.14e6 + 18.42e6) / 3.0e5
+TRAFFIC_P2P_F32_PER_PARTICLE = (119.11e6 + 21.72e6) / 3.0e5
 # FMA-pipe activity of the FP32C kernels in the same captures
 # (sm__pipe_fma_cycles_active, profiles/*_300k.txt)
-FMA_PIPE_NCU = {"k_m2l_batch": 0.376, "k_p2p_w": 0.270, "k_uvort_pres_sorted": 0.807,
+FMA_PIPE_NCU = {"k_m2l_batch": 0.376, "k_p2p_w": 0.305, "k_uvort_pres_sorted": 0.807,
                 "k_elem_far": 0.67}
 
 
