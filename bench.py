@@ -342,10 +342,12 @@ def run_reference(args, rank, ws):
             "phases_ms": phases, "init_s": round(t_init, 1),
             "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": cores,
                              "kind": "port",
-                             "sample": "%d whole step(s), timed in full, after "
-                                       "initialize_linsys (%.1f s, untimed); oracle C loops "
-                                       "(OpenMP, %d threads) + OpenBLAS LAPACK/BLAS"
-                                       % (nsteps, t_init, cores)},
+                             "sample": "%d whole step(s) (uvort, assembly, solve, the "
+                                       "pressure equation, FMM with the element sums, the "
+                                       "particle update), timed in full, after "
+                                       "initialize_linsys and the static LUs (%.1f s, "
+                                       "untimed); oracle C loops (OpenMP, %d threads) + "
+                                       "OpenBLAS LAPACK/BLAS" % (nsteps, t_init, cores)},
             "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -13,11 +13,18 @@ third-party LAPACK, in the reference's call sequence:
   dtrsm('R','U','N','N'), dgemm, dgetrf of the moving block, dlaswp, pivot
   shift, dgetrs -- scipy.linalg.lapack / blas (OpenBLAS);
 * the implicit wake panels' intensities (update_wake, mod_wake.f90:881-889);
+* the pressure integral equation of the surface panels
+  (mod_pressure_equation.f90:139-387): the particles' rotational term at the
+  surface panels with the previous update's velocities (or_pressure_particles;
+  the Bernoulli sources are zero for bodies at rest) and dgetrs with the
+  static LU of A_pres (dust.f90:621, 641-643);
 * sort_particles + calculate_multipole + apply_multipole with the element
-  sums (mod_octree.f90:703-1429) -- or_fmm_apply.
+  sums (mod_octree.f90:703-1429) -- or_fmm_apply;
+* complete_wake's particle loop (mod_wake.f90:1309-1355) --
+  or_particles_update.
 
-initialize_linsys's static rows and the static LU (dgetrf) run once, in
-``CpuStep.__init__``, outside the step.
+initialize_linsys's static rows, the static LU (dgetrf) and A_pres's static
+LU run once, in ``CpuStep.__init__``, outside the step.
 """
 import ctypes as C
 import time
@@ -106,6 +113,20 @@ class CpuStep:
             self.P[:c.nstatic] = piv
         else:
             self.P = np.zeros(c.rank, dtype=np.int32)
+        # A_pres: the surface panels' block of the influence matrix without
+        # the wake correction (every surface panel is static here)
+        self.sp = np.nonzero(c.elems.kind == abi.DUST_ELEM_SURFPAN)[0]
+        if len(self.sp):
+            Aw, _, _ = O.linsys_init(params, c.rank, c.nstatic, c.elems,
+                                     (abi.empty_panels(), 0, None))
+            self.lu_p, self.piv_p, info = lapack.dgetrf(Aw[np.ix_(self.sp, self.sp)])
+            if info != 0:
+                raise RuntimeError("A_pres dgetrf info %d" % info)
+            del Aw
+        self.vel = np.zeros((c.mag.shape[0], 3))
+        from dust_b200.step import update_params_for
+        self.upd = update_params_for(c, params)
+        self.free = np.zeros(c.mag.shape[0], dtype=np.int32)
         self.t_init = time.perf_counter() - t0
         self.ind = c.impl_ind.astype(np.int64) - 1
 
@@ -127,6 +148,12 @@ class CpuStep:
         # block are rebuilt by the next assembly
         res, _ = solve_linsys_lapack(self.A, self.P, c.nstatic, b)
         t["solve"] = time.perf_counter() - t0
+        if len(self.sp):
+            t0 = time.perf_counter()
+            bp = O.pressure_particles(np.ascontiguousarray(cen_el[self.sp]), c.cen, c.dir, c.mag,
+                                      c.r_vortex, self.vel)
+            self.res_pres, info = lapack.dgetrs(self.lu_p, self.piv_p, bp)
+            t["pressure"] = time.perf_counter() - t0
         t0 = time.perf_counter()
         c.elems.mag = res
         m2 = np.where(self.ind[:, 1] >= 0, res[np.maximum(self.ind[:, 1], 0)], 0.0)
@@ -134,5 +161,10 @@ class CpuStep:
         els = abi.elements_struct(c.elems, c.wake, c.end_vort)
         vel, st, ro, cnt = O.fmm_apply(prm, c.cen, c.dir, c.mag, c.r_vortex, els)
         t["fmm"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        cen, dir_, _, self.free, _ = O.particles_update(self.upd, c.cen, c.dir, c.mag, vel, st,
+                                                        ro, self.free)
+        c.cen[:], c.dir[:] = cen, dir_
+        t["particles_update"] = time.perf_counter() - t0
         self.res, self.vel = res, vel
         return t
